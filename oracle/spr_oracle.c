@@ -1,0 +1,353 @@
+/*
+ * CPU restatement of SPR's numeric phase -- the oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY: loaded by tests/, by the smoke check and by the
+ * CPU-baseline leg of bench.py; never linked into the product.
+ *
+ * Restates, in plain C of its own, the algorithm of
+ *   SPRSOL  src/SPR/sprsol.f:5-52      (IOP dispatch)
+ *   SPRFC1  src/SPR/sprfc1.f:5-283     (checks, error mapping, MSPAR(1/26/27))
+ *   SPRF11  src/SPR/sprfc1.f:286-713   (multifrontal loop, TOL(2)/TOL(3))
+ *   SPRF12/13/14 sprfc1.f:716-982      (relative indices, extend-add)
+ *   SPRF15/17 sprfc1.f:985-1299        (LDL' of the S fully-summed columns)
+ *   LMVY18  src/SPR/lmvy18.f:5-173     (column update inside SPRF17)
+ *   LMMY18  src/SPR/lmmy18.f:5-192     (Schur update of the update matrix)
+ *   SPRFS1/3/5/6, SPRFB1/2 src/SPR/sprfs1.f  (forward + diagonal solve)
+ *   SPRBS1/4/6 src/SPR/sprbs1.f        (back solve)
+ * for the plain configuration the GPU path handles (MSPAR(57)<=0,
+ * MSPAR(58)=0, no panels: numerically identical, panels only re-block).
+ *
+ * Every floating-point update is accumulated in the same order as the
+ * reference (the 8-way unrolled groups of LMMY18/LMVY18/SPRFS6 add their
+ * terms left to right, i.e. sequentially in k), and the scaling uses the
+ * reciprocal of the pivot as SPRF17 does, so with -ffp-contract=off the
+ * results are bitwise equal to the reference's.  Fronts are held as dense
+ * column-major F x F arrays instead of SPR's packed stack: storage differs,
+ * arithmetic does not.
+ *
+ * Integers are int64_t (the SPR_I8 build).  All arrays are 1-based in the
+ * Fortran sense; this file indexes them 0-based.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef int64_t I;
+
+typedef struct {
+    I neq, nsuper, nofsub, nzerol, mfront;
+    const I *xsuper, *xsibl, *sibl, *xlindx, *lindx, *xlnz;
+} sym_t;
+
+/* Pointers into MTREES/MSIFA exactly as SPRFC1 derives them (sprfc1.f:165-196). */
+static void sym_from_mspar(sym_t *s, const I *mspar, const I *mtrees, const I *msifa)
+{
+    s->neq = mspar[7];
+    s->nsuper = mspar[10];
+    s->mfront = mspar[13];
+    s->nofsub = mspar[14];
+    s->nzerol = mspar[15];
+    const I *xs = mtrees + (mspar[44] - 1);
+    s->xsuper = xs;
+    s->xsibl = xs + (s->nsuper + 1);
+    s->sibl = xs + 2 * (s->nsuper + 1);
+    s->xlindx = mtrees + (mspar[45] - 1);
+    s->lindx = msifa + (mspar[46] - 1);
+    s->xlnz = msifa + (mspar[47] - 1);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Factorisation: SPRFC1 / SPRF11                                          */
+/* ---------------------------------------------------------------------- */
+
+typedef struct {
+    double *upd;     /* dense (F-S) x (F-S) update matrix, column-major    */
+    I n;             /* its order                                          */
+} update_t;
+
+/* Returns the SPRF11 ERROR code (0, -30 or -35) and fills numneg/supeqt. */
+static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
+                       I *numneg_out, I *supeqt_out)
+{
+    const I ns = s->nsuper;
+    I numneg = 0, supeqt = 0, error = 0;
+    tol[1] = 0.0;
+    tol[2] = 0.0;
+    /* pre-pass: original diagonal, zero check, trace (sprfc1.f:465-488) */
+    for (I js = 0; js < ns; js++) {
+        I len = s->xlindx[js + 1] - s->xlindx[js];
+        I p = s->xlnz[js] - 1;
+        for (I j = s->xsuper[js]; j < s->xsuper[js + 1]; j++) {
+            diag[j - 1] = lnz[p];
+            if (diag[j - 1] == 0.0) {
+                numneg++;
+                if (numneg == 1) {
+                    supeqt = j;
+                    error = -35;
+                }
+            }
+            tol[2] = tol[2] + diag[j - 1];
+            p += len;
+            len -= 1;
+        }
+    }
+    if (error < 0) {
+        *numneg_out = numneg;
+        *supeqt_out = supeqt;
+        return error;
+    }
+    update_t *pend = (update_t *)calloc((size_t)ns, sizeof(update_t));
+    I *rel = (I *)malloc(sizeof(I) * (size_t)(s->mfront + 1));
+    for (I js = 0; js < ns && error == 0; js++) {
+        const I fst = s->xsuper[js];
+        const I S = s->xsuper[js + 1] - fst;
+        const I F = s->xlindx[js + 1] - s->xlindx[js];
+        const I *rows = s->lindx + (s->xlindx[js] - 1);
+        double *X = (double *)calloc((size_t)(F * F), sizeof(double));
+        /* fully-summed columns from LNZ; packed column j has F-j entries */
+        I p = s->xlnz[js] - 1;
+        for (I j = 0; j < S; j++)
+            for (I i = j; i < F; i++)
+                X[i + j * F] = lnz[p++];
+        /* extend-add of the children, last sibling first (sprfc1.f:534) */
+        for (I k = s->xsibl[js + 1] - 1; k >= s->xsibl[js]; k--) {
+            const I c = s->sibl[k - 1] - 1;
+            const I cS = s->xsuper[c + 1] - s->xsuper[c];
+            const I *crow = s->lindx + (s->xlindx[c] - 1) + cS;
+            const I n = pend[c].n;
+            double *U = pend[c].upd;
+            /* SPRF12: monotone merge of the child's rows into the parent's */
+            I sup = 0;
+            for (I t = 0; t < n; t++) {
+                while (rows[sup] < crow[t]) sup++;
+                rel[t] = sup;
+                sup++;
+            }
+            for (I b = 0; b < n; b++)
+                for (I a = b; a < n; a++)
+                    X[rel[a] + rel[b] * F] += U[a + b * n];
+            free(U);
+            pend[c].upd = NULL;
+        }
+        /* SPRF17: left-looking LDL' of columns 0..S-1 over all F rows */
+        for (I j = 0; j < S && error == 0; j++) {
+            for (I k = 0; k < j; k++) {
+                const double a = -(X[j + k * F] * diag[fst - 1 + k]);
+                for (I i = j; i < F; i++)
+                    X[i + j * F] = X[i + j * F] + a * X[i + k * F];
+            }
+            const double adiag = diag[fst - 1 + j];
+            double d = X[j + j * F];
+            if (fabs(d) <= tol[0] * fabs(adiag)) {
+                error = -(j + 1);
+                tol[1] = d;
+                tol[2] = adiag;
+                break;
+            }
+            if (d < 0.0) numneg++;
+            diag[fst - 1 + j] = d;
+            const double r = adiag / d;
+            tol[1] = (tol[1] > r) ? tol[1] : r;
+            d = 1.0 / d;
+            for (I i = j + 1; i < F; i++) X[i + j * F] = X[i + j * F] * d;
+        }
+        if (error != 0) {
+            supeqt = fst - error - 1;
+            error = -30;
+            free(X);
+            break;
+        }
+        /* LMMY18: Y <- Y - X D X' on the lower part of the update matrix */
+        const I q = F - S;
+        if (q > 0) {
+            double *U = (double *)malloc(sizeof(double) * (size_t)(q * q));
+            for (I b = 0; b < q; b++) {
+                for (I a = b; a < q; a++) U[a + b * q] = X[(S + a) + (S + b) * F];
+                for (I k = 0; k < S; k++) {
+                    const double a1 = -(X[(S + b) + k * F] * diag[fst - 1 + k]);
+                    for (I a = b; a < q; a++)
+                        U[a + b * q] = U[a + b * q] + a1 * X[(S + a) + k * F];
+                }
+            }
+            pend[js].upd = U;
+            pend[js].n = q;
+        }
+        /* store the S-column trapezoid back into LNZ (sprfc1.f:630-637) */
+        p = s->xlnz[js] - 1;
+        for (I j = 0; j < S; j++)
+            for (I i = j; i < F; i++)
+                lnz[p++] = X[i + j * F];
+        free(X);
+    }
+    for (I js = 0; js < ns; js++) free(pend[js].upd);
+    free(pend);
+    free(rel);
+    if (error == 0) {
+        double mdiag = 0.0;
+        for (I i = 0; i < s->neq; i++)
+            if (diag[i] > 0.0 && (mdiag == 0.0 || mdiag > diag[i])) mdiag = diag[i];
+        tol[1] = (tol[1] != 0.0) ? 1.0 / tol[1] : 0.0;
+        tol[2] = (mdiag != 0.0) ? tol[2] / mdiag : 0.0;
+    }
+    *numneg_out = numneg;
+    *supeqt_out = supeqt;
+    return error;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Solves: SPRFS3/SPRFS5/SPRFS6 and SPRBS4/SPRBS6                          */
+/* ---------------------------------------------------------------------- */
+
+static void oracle_forward(const sym_t *s, const double *lnz, double *b, double *loc)
+{
+    I p0 = 0;
+    for (I js = 0; js < s->nsuper; js++) {
+        const I S = s->xsuper[js + 1] - s->xsuper[js];
+        const I F = s->xlindx[js + 1] - s->xlindx[js];
+        const I *rows = s->lindx + (s->xlindx[js] - 1);
+        const double *L = lnz + p0;
+        for (I i = 0; i < F; i++) loc[i] = rows[i] <= s->neq ? b[rows[i] - 1] : 0.0;
+        /* column j of the packed trapezoid starts at j*F - j(j-1)/2 */
+        for (I j = 0; j < S; j++) {
+            const I cj = j * F - (j * (j - 1)) / 2;
+            const double x = loc[j];
+            for (I i = j + 1; i < S; i++) loc[i] = loc[i] - x * L[cj + (i - j)];
+        }
+        /* SPRFS6 (sprfs1.f:929-1141): the S mod 8 leading columns in
+         * ascending order, then groups of 8 taken from the group's last
+         * column down to its first. */
+        const I lft = S % 8;
+        for (I i = S; i < F; i++) {
+            double y = loc[i];
+            for (I j = 0; j < lft; j++) {
+                const I cj = j * F - (j * (j - 1)) / 2;
+                y = y - loc[j] * L[cj + (i - j)];
+            }
+            for (I jg = lft + 7; jg < S; jg += 8) {
+                for (I j = jg; j > jg - 8; j--) {
+                    const I cj = j * F - (j * (j - 1)) / 2;
+                    y = y - loc[j] * L[cj + (i - j)];
+                }
+            }
+            loc[i] = y;
+        }
+        for (I j = 0; j < S; j++) loc[j] = loc[j] / L[j * F - (j * (j - 1)) / 2];
+        for (I i = 0; i < F; i++)
+            if (rows[i] <= s->neq) b[rows[i] - 1] = loc[i];
+        p0 += F * S - (S * (S - 1)) / 2;
+    }
+}
+
+static void oracle_backward(const sym_t *s, const double *lnz, double *b, double *loc)
+{
+    I p0 = s->nzerol;
+    for (I js = s->nsuper - 1; js >= 0; js--) {
+        const I S = s->xsuper[js + 1] - s->xsuper[js];
+        const I F = s->xlindx[js + 1] - s->xlindx[js];
+        const I *rows = s->lindx + (s->xlindx[js] - 1);
+        p0 -= F * S - (S * (S - 1)) / 2;
+        const double *L = lnz + p0;
+        for (I i = 0; i < F; i++) loc[i] = rows[i] <= s->neq ? b[rows[i] - 1] : 0.0;
+        for (I j = S - 1; j >= 0; j--) {
+            const I cj = j * F - (j * (j - 1)) / 2;
+            double r = 0.0;
+            for (I i = j + 1; i < F; i++) r = r + loc[i] * L[cj + (i - j)];
+            loc[j] = loc[j] - r;
+        }
+        for (I i = 0; i < F; i++)
+            if (rows[i] <= s->neq) b[rows[i] - 1] = loc[i];
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Fortran-ABI entry points (same arguments as the reference routines)     */
+/* ---------------------------------------------------------------------- */
+
+void orc_sprfc1_(I *mspar, I *mtrees, I *msifa, double *sm, double *tol,
+                 I *iwork, double *rwork, const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {                  /* sprfc1.f:140-148 */
+        mspar[0] = -5;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 5;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    I numneg = 0, supeqt = 0;
+    I lierr = oracle_factor(&s, sm, sm + s.neq, tol, &numneg, &supeqt);
+    if (lierr != 0) {                    /* sprfc1.f:251-265 */
+        *ierr = (lierr / 10 == -3) ? -3 : -4;
+        mspar[26] = supeqt;
+    } else if (numneg > 0) {
+        *ierr = 3;
+    }
+    mspar[25] = numneg;
+}
+
+void orc_sprfs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                 const I *ldb, const I *nrhs, I *iwork, double *rwork,
+                 const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {
+        mspar[0] = -7;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 7;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    if (*ldb < s.neq) {
+        mspar[0] = -2;
+        *ierr = -2;
+        return;
+    }
+    double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
+    for (I r = 0; r < *nrhs; r++) oracle_forward(&s, sm + s.neq, b + r * (*ldb), loc);
+    free(loc);
+}
+
+void orc_sprbs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                 const I *ldb, const I *nrhs, double *rwork, const I *lpu, I *ierr)
+{
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {                  /* sprbs1.f:131-139 */
+        mspar[0] = -7;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 7;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    if (*ldb < s.neq) {
+        mspar[0] = -2;
+        *ierr = -2;
+        return;
+    }
+    double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
+    for (I r = 0; r < *nrhs; r++) oracle_backward(&s, sm + s.neq, b + r * (*ldb), loc);
+    free(loc);
+}
+
+void orc_sprsol_(const I *iop, I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                 const I *ldb, const I *nrhs, double *tol, I *iwork, double *rwork,
+                 const I *lpu, I *ierr)
+{
+    *ierr = 0;                           /* sprsol.f:32-49 */
+    if (*iop <= 3) orc_sprfc1_(mspar, mtrees, msifa, sm, tol, iwork, rwork, lpu, ierr);
+    if (*iop >= 2 && *iop <= 5 && *ierr >= 0)
+        orc_sprfs1_(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork, rwork, lpu, ierr);
+    if (*iop >= 3 && *iop != 5 && *ierr >= 0)
+        orc_sprbs1_(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork, lpu, ierr);
+}
