@@ -1,0 +1,183 @@
+"""B200 implementation of the numeric phase of SAM's SPR sparse solver.
+
+The product is the C-ABI library ``libspr_b200.so`` (built in-tree by
+``sam_lib_b200.build``): it exports the reference's Fortran entry points
+``sprsol_``, ``sprfc1_``, ``sprfs1_`` and ``sprbs1_`` (INTEGER*8 ABI;
+``libspr_b200_i4.so`` has the INTEGER*4 ABI) plus a device-level API.  This
+module is the Python mirror of that interface: the same routine names,
+argument meaning and IERR conventions as src/SPR/sprsol.f, sprfc1.f,
+sprfs1.f and sprbs1.f, with numpy arrays standing in for the Fortran arrays.
+
+There is no CPU fallback: if the library is missing, importing the
+interface raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_I8 = os.path.join(HERE, 'libspr_b200.so')
+LIB_I4 = os.path.join(HERE, 'libspr_b200_i4.so')
+
+_libs = {}
+
+
+def load(int_kind=8):
+    """Loads the in-tree GPU library (raises if it has not been built)."""
+    path = LIB_I8 if int_kind == 8 else LIB_I4
+    lib = _libs.get(path)
+    if lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError('spr_b200: %s is missing; run `python -m sam_lib_b200.build`' % path)
+        lib = C.CDLL(path)
+        vp = C.c_void_p
+        lib.spr_b200_open.argtypes = [vp, vp, vp, C.POINTER(vp)]
+        lib.spr_b200_open.restype = C.c_int
+        lib.spr_b200_close.argtypes = [vp]
+        lib.spr_b200_close.restype = None
+        lib.spr_b200_set_stream.argtypes = [vp, vp]
+        lib.spr_b200_factor_dev.argtypes = [vp, vp, C.c_double, vp]
+        lib.spr_b200_factor_dev.restype = C.c_int
+        lib.spr_b200_solve_dev.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, C.c_int]
+        lib.spr_b200_solve_dev.restype = C.c_int
+        lib.spr_b200_info.argtypes = [vp, vp]
+        lib.spr_b200_info.restype = C.c_int
+        lib.spr_b200_release_all.argtypes = []
+        lib.spr_b200_release_all.restype = None
+        _libs[path] = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ref(v, dtype):
+    return C.byref(dtype(int(v)))
+
+
+def _ints(int_kind):
+    return (np.int64, C.c_int64) if int_kind == 8 else (np.int32, C.c_int32)
+
+
+def _check_int(a, np_t, name):
+    if a.dtype != np_t or not a.flags['C_CONTIGUOUS']:
+        raise TypeError('%s must be a contiguous %s array' % (name, np.dtype(np_t).name))
+
+
+def sprsol(iop, mspar, mtrees, msifa, sm, b, ldb, nrhs, tol, iwork=None, rwork=None, lpu=-1,
+           int_kind=8):
+    """SPRSOL (src/SPR/sprsol.f:5): returns IERR; SM, B, TOL, MSPAR updated in place."""
+    np_t, c_t = _ints(int_kind)
+    for a, n in ((mspar, 'MSPAR'), (mtrees, 'MTREES'), (msifa, 'MSIFA')):
+        _check_int(a, np_t, n)
+    if sm.dtype != np.float64 or b.dtype != np.float64 or tol.dtype != np.float64:
+        raise TypeError('SM, B and TOL must be float64')
+    if not b.flags['F_CONTIGUOUS']:
+        raise TypeError('B must be Fortran-ordered (LDB, NRHS)')
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprsol_(_ref(iop, c_t), _ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm),
+                           _ptr(b), _ref(ldb, c_t), _ref(nrhs, c_t), _ptr(tol), _ptr(iwork),
+                           _ptr(rwork), _ref(lpu, c_t), C.byref(ierr))
+    return ierr.value
+
+
+def sprfc1(mspar, mtrees, msifa, sm, tol, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFC1 (src/SPR/sprfc1.f:5): LDL' factorisation of SM; returns IERR."""
+    np_t, c_t = _ints(int_kind)
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfc1_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
+                           _ptr(iwork), _ptr(rwork), _ref(lpu, c_t), C.byref(ierr), None, None)
+    return ierr.value
+
+
+def sprfs1(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFS1 (src/SPR/sprfs1.f:5): forward reduction + diagonal scaling; returns IERR."""
+    np_t, c_t = _ints(int_kind)
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfs1_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(b),
+                           _ref(ldb, c_t), _ref(nrhs, c_t), _ptr(iwork), _ptr(rwork),
+                           _ref(lpu, c_t), C.byref(ierr))
+    return ierr.value
+
+
+def sprbs1(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork=None, lpu=-1, int_kind=8):
+    """SPRBS1 (src/SPR/sprbs1.f:5): back substitution; returns IERR."""
+    _, c_t = _ints(int_kind)
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprbs1_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(b),
+                           _ref(ldb, c_t), _ref(nrhs, c_t), _ptr(rwork), _ref(lpu, c_t),
+                           C.byref(ierr))
+    return ierr.value
+
+
+def release_all():
+    """Frees the device contexts cached by the Fortran entry points."""
+    load(8).spr_b200_release_all()
+
+
+class DeviceSolver:
+    """Device-resident factor/solve on one SPR structure (INTEGER*8 arrays).
+
+    ``factor(d_sm)`` and ``solve(d_sm, d_b)`` take device pointers (ints) or
+    torch CUDA tensors: SM = [D(NEQ) | LNZ(NZEROL)] and B (NEQ x NRHS,
+    column-major, i.e. a torch tensor of shape (NRHS, NEQ)).
+    """
+
+    def __init__(self, mspar, mtrees, msifa):
+        self.lib = load(8)
+        self.h = C.c_void_p()
+        rc = self.lib.spr_b200_open(_ptr(mspar), _ptr(mtrees), _ptr(msifa), C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError('spr_b200_open failed with %d' % rc)
+        self.neq = int(mspar[7])
+        self.nzerol = int(mspar[15])
+
+    @staticmethod
+    def _dev(x):
+        return x if isinstance(x, int) else x.data_ptr()
+
+    def set_stream(self, stream_ptr):
+        self.lib.spr_b200_set_stream(self.h, C.c_void_p(stream_ptr))
+
+    def factor(self, d_sm, tol1=1.0e-12):
+        """Returns dict(tol2, tol3, numneg, supeqt, lierr) like SPRF11."""
+        out = np.zeros(5)
+        rc = self.lib.spr_b200_factor_dev(self.h, C.c_void_p(self._dev(d_sm)), tol1, _ptr(out))
+        if rc != 0:
+            raise RuntimeError('spr_b200_factor_dev failed with %d' % rc)
+        return dict(tol2=out[0], tol3=out[1], numneg=int(out[2]), supeqt=int(out[3]),
+                    lierr=int(out[4]))
+
+    def solve(self, d_sm, d_b, nrhs, ldb=None, which=3):
+        ldb = self.neq if ldb is None else ldb
+        rc = self.lib.spr_b200_solve_dev(self.h, C.c_void_p(self._dev(d_sm)),
+                                         C.c_void_p(self._dev(d_b)), ldb, nrhs, which)
+        if rc != 0:
+            raise RuntimeError('spr_b200_solve_dev failed with %d' % rc)
+
+    def info(self):
+        out = np.zeros(8)
+        self.lib.spr_b200_info(self.h, _ptr(out))
+        keys = ('factor_flops', 'solve_flops', 'arena_bytes', 'levels', 'factor_ms', 'solve_ms',
+                'launches', 'gemm_launches')
+        return dict(zip(keys, out.tolist()))
+
+    def close(self):
+        if self.h:
+            self.lib.spr_b200_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,504 @@
+// C ABI of the GPU numeric phase: the SPR entry points a Fortran-77 host
+// calls (SPRSOL/SPRFC1/SPRFS1/SPRBS1 with gfortran naming: lower case plus a
+// trailing underscore, every argument by reference) and a device-level API.
+//
+// Integer width: SPR_INT is int64_t for the default INTEGER*8 build
+// (-fdefault-integer-8, src/SPR/CMakeLists.txt:12-29) and int32_t for the
+// I4 build; the same source is compiled once per width.
+//
+// Ownership follows SPR: the caller owns every array; the library keeps one
+// device context per (MSPAR, MTREES, MSIFA) triple (plan + device buffers),
+// and remembers which host SM its device factor came from, so a factorisation
+// followed by solves on the same, unmodified SM reuses the device-resident
+// factor.  The factor is always written back into SM, so host-only consumers
+// of the factor keep working.
+#include <cuda_runtime.h>
+
+#include <cinttypes>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "engine.h"
+
+#ifndef SPR_INT
+#define SPR_INT int64_t
+#endif
+typedef SPR_INT I;
+
+#ifndef SPR_SUFFIX
+#define SPR_SUFFIX
+#endif
+#define SPR_CAT2(a, b) a##b
+#define SPR_CAT(a, b) SPR_CAT2(a, b)
+#define SPR_API(name) SPR_CAT(name, SPR_SUFFIX)
+
+namespace {
+
+using sprb::Engine;
+using sprb::FactorResult;
+
+struct Ctx {
+    Engine eng;
+    std::vector<int64_t> mspar_snap;   // structure fingerprint (MSPAR without state slots)
+    uint64_t tree_hash = 0;
+    double* d_sm = nullptr;
+    double* d_b = nullptr;
+    int64_t b_cap = 0;
+    cudaStream_t stream = nullptr;
+    // device factor residency
+    const double* sm_host = nullptr;
+    uint64_t sm_fp = 0;
+    bool resident = false;
+    ~Ctx() {
+        if (d_sm) cudaFree(d_sm);
+        if (d_b) cudaFree(d_b);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+std::mutex g_mu;
+std::map<std::tuple<const void*, const void*, const void*>, std::unique_ptr<Ctx>> g_ctx;
+
+uint64_t mix(uint64_t h, uint64_t v) {
+    h ^= v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    return h;
+}
+
+// Sampled fingerprint of SM: detects a re-assembled or different matrix
+// between a factorisation and later solves without reading all of SM.
+uint64_t sm_fingerprint(const double* sm, int64_t n) {
+    uint64_t h = mix(0, (uint64_t)n);
+    const int64_t samples = 4096;
+    const int64_t step = n > samples ? n / samples : 1;
+    for (int64_t i = 0; i < n; i += step) {
+        uint64_t v;
+        std::memcpy(&v, sm + i, 8);
+        h = mix(h, v);
+    }
+    for (int64_t i = n > 64 ? n - 64 : 0; i < n; ++i) {
+        uint64_t v;
+        std::memcpy(&v, sm + i, 8);
+        h = mix(h, v);
+    }
+    return h;
+}
+
+std::vector<int64_t> widen(const I* a, int64_t n) {
+    std::vector<int64_t> v(n);
+    for (int64_t i = 0; i < n; ++i) v[i] = (int64_t)a[i];
+    return v;
+}
+
+void msg(I lpu, const char* routine, const char* text) {
+    if (lpu < 0) return;
+    fprintf(stderr, " *** ERROR return from SPR routine %s (GPU)\n     %s\n", routine, text);
+}
+
+// Structure fingerprint: MSPAR slots that describe the symbolic structure
+// plus a sample of the tree arrays.
+void structure_key(const I* mspar, const I* mtrees, const I* msifa, std::vector<int64_t>& snap,
+                   uint64_t& h) {
+    snap.clear();
+    for (int i = 2; i < 25; ++i) snap.push_back((int64_t)mspar[i]);
+    for (int i = 40; i < 50; ++i) snap.push_back((int64_t)mspar[i]);
+    h = 0;
+    const int64_t nsuper = mspar[10];
+    const I* xs = mtrees + (mspar[44] - 1);
+    for (int64_t i = 0; i < 3 * (nsuper + 1) - 1; i += 1 + nsuper / 64) h = mix(h, (uint64_t)xs[i]);
+    const I* xl = msifa + (mspar[47] - 1);
+    for (int64_t i = 0; i <= nsuper; i += 1 + nsuper / 64) h = mix(h, (uint64_t)xl[i]);
+}
+
+// Returns the context for this structure (building it when needed) or null.
+Ctx* get_ctx(I* mspar, I* mtrees, I* msifa, int& err) {
+    err = 0;
+    std::vector<int64_t> snap;
+    uint64_t h;
+    structure_key(mspar, mtrees, msifa, snap, h);
+    auto key = std::make_tuple((const void*)mspar, (const void*)mtrees, (const void*)msifa);
+    auto it = g_ctx.find(key);
+    if (it != g_ctx.end() && it->second->mspar_snap == snap && it->second->tree_hash == h) return it->second.get();
+    if (it != g_ctx.end()) g_ctx.erase(it);
+    std::unique_ptr<Ctx> c(new Ctx());
+    const int64_t nspar = 60;
+    std::vector<int64_t> ms(nspar, 0);
+    for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
+    const int64_t ntrees = mspar[3], nmsifa = mspar[2];
+    std::vector<int64_t> mt = widen(mtrees, ntrees), mf = widen(msifa, nmsifa);
+    int rc = c->eng.open(ms.data(), mt.data(), mf.data());
+    if (rc != 0) {
+        err = rc;
+        return nullptr;
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        err = -4;
+        return nullptr;
+    }
+    c->eng.set_stream(c->stream);
+    const int64_t nsm = mspar[7] + mspar[15];
+    if (cudaMalloc((void**)&c->d_sm, nsm * sizeof(double)) != cudaSuccess) {
+        err = -4;
+        return nullptr;
+    }
+    c->mspar_snap = snap;
+    c->tree_hash = h;
+    Ctx* raw = c.get();
+    g_ctx[key] = std::move(c);
+    return raw;
+}
+
+// Reference length checks of SPRFC1 (src/SPR/sprfc1.f:150-236).
+bool fc1_lengths_ok(const I* mspar) {
+    const int64_t neq = mspar[7], nsuper = mspar[10], nb = mspar[11], mfront = mspar[13];
+    const int64_t nofsub = mspar[14], nzerol = mspar[15], wstack = mspar[16], nelact = mspar[18];
+    const int64_t nblock = mspar[21], nmsifa = mspar[2], ntrees = mspar[3];
+    const int64_t niwork = mfront + 1, nrwork = wstack, nsm = neq + nzerol;
+    const int64_t iwused = mfront + 1;
+    const int64_t xsuper = mspar[44], xlindx = mspar[45];
+    const int64_t supsup = xlindx + nsuper + 1, elseq = supsup + nsuper, xelseq = elseq + nelact;
+    const int64_t xblock = xelseq + nb + 1, mtused = xblock + nb;
+    (void)xsuper;
+    const int64_t lindx = mspar[46], xlnz = mspar[47];
+    (void)lindx;
+    const int64_t xsplit = xlnz + nsuper + 1, split = xsplit + nsuper, mlused = split + nblock;
+    const int64_t smused = neq + nzerol, rwused = wstack;
+    (void)nofsub;
+    return !(iwused > niwork || mtused > ntrees || mlused > nmsifa || smused > nsm || rwused > nrwork);
+}
+
+bool solve_lengths_ok(const I* mspar, I ldb) {
+    int64_t neq = mspar[7];
+    if (mspar[56] == 1 && ldb < neq) neq = ldb;   // sprfs1.f:201
+    return ldb >= neq;
+}
+
+int ensure_b(Ctx* c, int64_t n) {
+    if (c->b_cap >= n) return 0;
+    if (c->d_b) cudaFree(c->d_b);
+    c->d_b = nullptr;
+    c->b_cap = 0;
+    if (cudaMalloc((void**)&c->d_b, n * sizeof(double)) != cudaSuccess) return -4;
+    c->b_cap = n;
+    return 0;
+}
+
+// H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR.
+I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu) {
+    const int64_t neq = mspar[7], nzerol = mspar[15];
+    const int64_t nsm = neq + nzerol;
+    cudaStream_t s = c->stream;
+    if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return -4;
+    FactorResult r;
+    if (c->eng.factor(c->d_sm, tol[0], r) != 0) {
+        msg(lpu, "SPRFC1", "CUDA failure in the factorisation");
+        return -4;
+    }
+    if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -4;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
+    I ierr = 0;
+    tol[1] = r.tol2;
+    tol[2] = r.tol3;
+    if (r.lierr != 0) {                               // sprfc1.f:251-265
+        ierr = (r.lierr / 10 == -3) ? -3 : -4;
+        mspar[26] = (I)r.supeqt;
+        if (lpu >= 0) {
+            char buf[256];
+            if (r.lierr == -35)
+                snprintf(buf, sizeof buf, "SINGULAR EQUATION SYSTEM: %" PRId64 " ZERO PIVOT(S), FIRST IN EQUATION %" PRId64,
+                         r.numneg, r.supeqt);
+            else
+                snprintf(buf, sizeof buf, "PIVOT BELOW THE TOL(1) THRESHOLD IN EQUATION %" PRId64
+                         " (%" PRId64 " NEGATIVE PIVOTS BEFORE IT)", r.supeqt, r.numneg);
+            msg(lpu, "SPRFC1", buf);
+        }
+        c->resident = false;
+    } else {
+        if (r.numneg > 0) {
+            ierr = 3;
+            if (lpu >= 0)
+                fprintf(stderr, " *** WARNING from SPR routine SPRFC1 (GPU)\n     THE STIFFNESS MATRIX IS NOT POSITIVE "
+                        "DEFINITE: %" PRId64 " NEGATIVE PIVOT(S)\n", r.numneg);
+        }
+        c->sm_host = sm;
+        c->sm_fp = sm_fingerprint(sm, nsm);
+        c->resident = true;
+    }
+    mspar[25] = (I)r.numneg;
+    return ierr;
+}
+
+// Makes the device SM hold this host SM's factor (re-uploading if needed).
+int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm) {
+    const int64_t nsm = mspar[7] + mspar[15];
+    if (c->resident && c->sm_host == sm && c->sm_fp == sm_fingerprint(sm, nsm)) return 0;
+    if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return -4;
+    c->sm_host = sm;
+    c->sm_fp = sm_fingerprint(sm, nsm);
+    c->resident = true;
+    return 0;
+}
+
+// Forward (which=1), back (2) or both (3) for B(LDB,NRHS) on the host.
+int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I nrhs, int which) {
+    const int64_t neq = (mspar[56] == 1 && ldb < mspar[7]) ? (int64_t)ldb : (int64_t)mspar[7];
+    if (nrhs <= 0) return 0;
+    if (ensure_factor_on_device(c, mspar, sm) != 0) return -4;
+    if (ensure_b(c, (int64_t)mspar[7] * nrhs) != 0) return -4;
+    cudaStream_t s = c->stream;
+    const bool peri2e = mspar[57] >= 1;                 // sprfs1.f:240-250, SPRFB3/SPRFB4
+    std::vector<double> tmp;
+    const int64_t nfull = mspar[7];
+    if (peri2e || neq != nfull) {
+        tmp.assign(nfull * nrhs, 0.0);
+        const I* p2e = msifa;                           // PERI2E = MSIFA(1..NEQ)
+        for (int64_t r = 0; r < nrhs; ++r)
+            for (int64_t k = 0; k < nfull; ++k) {
+                const int64_t src = peri2e ? (int64_t)p2e[k] - 1 : k;
+                tmp[r * nfull + k] = (src < neq) ? b[r * ldb + src] : 0.0;
+            }
+        if (cudaMemcpyAsync(c->d_b, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return -4;
+    } else if (ldb == nfull) {
+        if (cudaMemcpyAsync(c->d_b, b, nfull * nrhs * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return -4;
+    } else {
+        if (cudaMemcpy2DAsync(c->d_b, nfull * sizeof(double), b, ldb * sizeof(double), nfull * sizeof(double), nrhs,
+                              cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return -4;
+    }
+    if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, which) != 0) return -4;
+    if (peri2e || neq != nfull) {
+        if (cudaMemcpyAsync(tmp.data(), c->d_b, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return -4;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
+        const I* p2e = msifa;
+        for (int64_t r = 0; r < nrhs; ++r)
+            for (int64_t k = 0; k < nfull; ++k) {
+                const int64_t dst = peri2e ? (int64_t)p2e[k] - 1 : k;
+                if (dst < neq) b[r * ldb + dst] = tmp[r * nfull + k];
+            }
+    } else if (ldb == nfull) {
+        if (cudaMemcpyAsync(b, c->d_b, nfull * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return -4;
+    } else {
+        if (cudaMemcpy2DAsync(b, ldb * sizeof(double), c->d_b, nfull * sizeof(double), nfull * sizeof(double), nrhs,
+                              cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return -4;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
+    return 0;
+}
+
+bool unsupported_mode(const I* mspar) {
+    // partial factorisation with retained (superelement) DOFs stays on the
+    // reference's code path: the GPU path reports it instead of guessing.
+    return mspar[56] > 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// SPRFC1 (src/SPR/sprfc1.f:5): LDL' factorisation of SM in place.
+void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I* iwork, double* rwork, const I* lpu,
+                      I* ierr, void (*mvmult)(), void (*mmmult)()) {
+    (void)iwork;
+    (void)rwork;
+    (void)mvmult;   // the GPU path always applies the LDL' kernels (LMVY18/LMMY18)
+    (void)mmmult;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfc1.f:140-148
+        mspar[0] = -5;
+        *ierr = -1;
+        msg(*lpu, "SPRFC1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 5;
+    *ierr = 0;
+    if (!fc1_lengths_ok(mspar)) {
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFC1", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (unsupported_mode(mspar)) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRFC1", "PARTIAL FACTORISATION (MSPAR(57)>0) IS NOT HANDLED BY THE GPU PATH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c) {
+        mspar[0] = -5;
+        *ierr = (err == -2) ? -2 : -4;
+        msg(*lpu, "SPRFC1", "COULD NOT SET UP THE GPU CONTEXT");
+        return;
+    }
+    *ierr = do_factor(c, mspar, sm, tol, *lpu);
+    if (*ierr < 0 && *ierr != -3) mspar[0] = -5;
+}
+
+// SPRFS1 (src/SPR/sprfs1.f:5): forward reduction and diagonal scaling of B.
+void SPR_API(sprfs1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb, const I* nrhs, I* iwork,
+                      double* rwork, const I* lpu, I* ierr) {
+    (void)iwork;
+    (void)rwork;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfs1.f:136-144
+        mspar[0] = -7;
+        *ierr = -1;
+        msg(*lpu, "SPRFS1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 7;
+    *ierr = 0;
+    if (!solve_lengths_ok(mspar, *ldb)) {
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFS1", "MTREES/MSIFA/SM/B, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 1) != 0) {
+        mspar[0] = -7;
+        *ierr = -4;
+        msg(*lpu, "SPRFS1", "GPU FORWARD SOLVE FAILED");
+    }
+}
+
+// SPRBS1 (src/SPR/sprbs1.f:5): back substitution of B.
+void SPR_API(sprbs1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb, const I* nrhs,
+                      double* rwork, const I* lpu, I* ierr) {
+    (void)rwork;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprbs1.f:131-139
+        mspar[0] = -7;
+        *ierr = -1;
+        msg(*lpu, "SPRBS1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 7;
+    *ierr = 0;
+    if (!solve_lengths_ok(mspar, *ldb)) {
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRBS1", "MTREES/MSIFA/SM/B, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 2) != 0) {
+        mspar[0] = -7;
+        *ierr = -4;
+        msg(*lpu, "SPRBS1", "GPU BACK SUBSTITUTION FAILED");
+    }
+}
+
+// SPRSOL (src/SPR/sprsol.f:5): factor (IOP<=3), forward (2<=IOP<=5) and back
+// (IOP>=3, IOP/=5) in one call.  When both sweeps run, B crosses the bus once.
+void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb,
+                      const I* nrhs, double* tol, I* iwork, double* rwork, const I* lpu, I* ierr) {
+    *ierr = 0;
+    const I op = *iop;
+    if (op <= 3) SPR_API(sprfc1_)(mspar, mtrees, msifa, sm, tol, iwork, rwork, lpu, ierr, nullptr, nullptr);
+    const bool fwd = op >= 2 && op <= 5 && *ierr >= 0;
+    const bool bwd = op >= 3 && op != 5;
+    if (fwd && bwd) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (mspar[0] < 0) {
+            mspar[0] = -7;
+            *ierr = -1;
+            msg(*lpu, "SPRFS1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+            return;
+        }
+        mspar[0] = 7;
+        *ierr = 0;                                       // the solves reset IERR (sprfs1.f:143-144)
+        if (!solve_lengths_ok(mspar, *ldb)) {
+            mspar[0] = -2;
+            *ierr = -2;
+            msg(*lpu, "SPRFS1", "MTREES/MSIFA/SM/B, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+            return;
+        }
+        int err = 0;
+        Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+        if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3) != 0) {
+            mspar[0] = -7;
+            *ierr = -4;
+            msg(*lpu, "SPRSOL", "GPU SOLVE FAILED");
+        }
+        return;
+    }
+    if (fwd) SPR_API(sprfs1_)(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork, rwork, lpu, ierr);
+    if (bwd && !fwd && *ierr >= 0) SPR_API(sprbs1_)(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork, lpu, ierr);
+}
+
+// ---------------------------------------------------------------------------
+// Device-level API: factor/solve on device-resident SM and B.
+// ---------------------------------------------------------------------------
+int SPR_API(spr_b200_open)(const I* mspar, const I* mtrees, const I* msifa, void** handle) {
+    std::unique_ptr<Engine> e(new Engine());
+    std::vector<int64_t> ms(60, 0);
+    for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
+    std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
+    int rc = e->open(ms.data(), mt.data(), mf.data());
+    if (rc != 0) return rc;
+    *handle = e.release();
+    return 0;
+}
+
+void SPR_API(spr_b200_close)(void* handle) { delete static_cast<Engine*>(handle); }
+
+int SPR_API(spr_b200_set_stream)(void* handle, void* stream) {
+    static_cast<Engine*>(handle)->set_stream((cudaStream_t)stream);
+    return 0;
+}
+
+// out[0]=TOL(2) out[1]=TOL(3) out[2]=NUMNEG out[3]=SUPEQT out[4]=LIERR
+int SPR_API(spr_b200_factor_dev)(void* handle, double* d_sm, double tol1, double* out) {
+    FactorResult r;
+    int rc = static_cast<Engine*>(handle)->factor(d_sm, tol1, r);
+    if (rc != 0) return rc;
+    out[0] = r.tol2;
+    out[1] = r.tol3;
+    out[2] = (double)r.numneg;
+    out[3] = (double)r.supeqt;
+    out[4] = (double)r.lierr;
+    return 0;
+}
+
+int SPR_API(spr_b200_solve_dev)(void* handle, const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which) {
+    return static_cast<Engine*>(handle)->solve(d_sm, d_b, ldb, nrhs, which);
+}
+
+// info[0]=RINFO(3) factor flops, [1]=RINFO(4)-style solve flops per RHS,
+// [2]=front arena bytes, [3]=levels, [4]=last factor ms, [5]=last solve ms,
+// [6]=kernel launches of the last factorisation, [7]=Schur-update launches.
+int SPR_API(spr_b200_info)(void* handle, double* info) {
+    Engine* e = static_cast<Engine*>(handle);
+    const sprb::Plan& p = e->plan();
+    info[0] = p.factor_flops;
+    info[1] = p.solve_flops;
+    info[2] = (double)p.arena_doubles * 8.0;
+    info[3] = (double)p.levels.size();
+    info[4] = e->timing.factor_ms;
+    info[5] = e->timing.solve_ms;
+    info[6] = (double)e->timing.launches;
+    info[7] = (double)e->timing.gemm_launches;
+    return 0;
+}
+
+// Releases every cached context (device memory of the Fortran entry points).
+void SPR_API(spr_b200_release_all)(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_ctx.clear();
+}
+
+}  // extern "C"

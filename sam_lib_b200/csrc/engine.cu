@@ -1,0 +1,946 @@
+// GPU numeric phase of SPR for sm_100a: supernodal multifrontal LDL'
+// factorisation and the forward/diagonal/back solves.
+//
+// Semantics follow the reference routines (file:line in src/SPR):
+//   SPRF11 multifrontal loop ............ sprfc1.f:286-713
+//   SPRF12/13/14 extend-add ............. sprfc1.f:716-982
+//   SPRF15/SPRF17 (+LMVY18) pivots ...... sprfc1.f:985-1299, lmvy18.f
+//   LMMY18 Schur update ................. lmmy18.f:5-192
+//   SPRFS3/5/6 forward + diagonal ....... sprfs1.f:266-1141
+//   SPRBS4/6 back substitution .......... sprbs1.f:251-574
+// The arithmetic is FP64 throughout; the order of the floating-point updates
+// differs from the reference (blocked, FMA), so results agree to rounding.
+//
+// Execution: one pass per elimination-tree level (leaves first).  Fronts of
+// order <= kSmallMaxF are assembled, factored and written back by one CTA in
+// shared memory (fused extend-add + LDL' + Schur update).  Larger fronts are
+// assembled into dense column-major buffers in HBM and factored with a
+// blocked right-looking LDL' (diagonal block, panel TRSM, FP64 DMMA Schur
+// update), all fronts of the level batched into each launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+
+namespace sprb {
+
+#define CK(x)                                                                    \
+    do {                                                                         \
+        cudaError_t e_ = (x);                                                    \
+        if (e_ != cudaSuccess) {                                                 \
+            fprintf(stderr, "spr_b200: CUDA error %s at %s:%d\n",                \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+            return -4;                                                           \
+        }                                                                        \
+    } while (0)
+
+constexpr int kMaxRHS = 16;          // right-hand sides per solve pass
+
+// ---------------------------------------------------------------------------
+// Device views
+// ---------------------------------------------------------------------------
+struct Stats {
+    int zero_count;
+    int first_zero;          // smallest 0-based column with an exact zero diagonal
+    int any_fail;            // exact zero diagonal found: nothing is factored (sprfc1.f:488)
+    int pivot_fail;          // some pivot failed the TOL(1) test
+    unsigned long long numneg;
+    double tol2;             // max(a_jj / d_j), sprfc1.f:1284
+    double trace;            // sum a_jj, sprfc1.f:483
+    double mindpos;          // smallest positive pivot, sprfc1.f:690-697
+};
+
+struct PV {
+    const int32_t *fst, *S, *F, *child_ptr, *child, *rows, *rel, *cchild, *ct, *buf_ld;
+    const int64_t *lnz_off, *rel_off, *rbase, *cptr, *buf_off, *upd_off;
+    double* arena;
+    double* lnz;
+    double* dvec;
+    double* adiag;
+    int32_t* sn_neg;
+    int32_t* sn_fail;
+    int32_t* sn_bad;         // front failed, or depends on a failed front
+    double* sn_faild;
+    double* sn_faila;
+    Stats* st;
+    double tol1;
+};
+
+struct Engine::Dev {
+    // plan arrays
+    int32_t *fst = nullptr, *S = nullptr, *F = nullptr, *child_ptr = nullptr, *child = nullptr,
+            *rows = nullptr, *rel = nullptr, *cchild = nullptr, *ct = nullptr, *buf_ld = nullptr;
+    int64_t *lnz_off = nullptr, *rel_off = nullptr, *rbase = nullptr, *cptr = nullptr,
+            *buf_off = nullptr, *upd_off = nullptr;
+    Job* jobs = nullptr;
+    int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
+    std::vector<int64_t> small_begin;            // per level offset into level_nodes
+    int32_t* all_nodes = nullptr;                // all nodes of every level (solves)
+    std::vector<int64_t> all_begin, all_count;
+    // work
+    double* arena = nullptr;
+    double* adiag = nullptr;
+    int32_t* sn_neg = nullptr;
+    int32_t* sn_fail = nullptr;
+    int32_t* sn_bad = nullptr;
+    double* sn_faild = nullptr;
+    double* sn_faila = nullptr;
+    Stats* st = nullptr;
+    double* vbuf = nullptr;                      // solve front vectors
+    int64_t vbuf_rhs = 0;
+    double* bbuf = nullptr;                      // contiguous copy of B (ldb = NEQ)
+    int64_t bbuf_rhs = 0;
+    std::vector<void*> owned;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+template <typename T>
+static int dev_upload(std::vector<void*>& owned, T** dst, const std::vector<T>& src) {
+    size_t n = std::max<size_t>(src.size(), 1);
+    CK(cudaMalloc((void**)dst, n * sizeof(T)));
+    owned.push_back(*dst);
+    if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_max_double(double* addr, double v) {
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+    unsigned long long old = *a;
+    while (__longlong_as_double((long long)old) < v) {
+        unsigned long long assumed = old;
+        old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
+        if (old == assumed) break;
+    }
+}
+
+__device__ __forceinline__ int64_t find_job(const Job* jobs, int64_t n, int64_t t) {
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].task0 <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// packed lower, column-major, order F: column j holds rows j..F-1
+__device__ __forceinline__ int pk(int i, int j, int F) { return j * F - ((j * (j - 1)) >> 1) + (i - j); }
+
+__device__ __forceinline__ int64_t lnz_col(int64_t j, int64_t F) { return j * F - (j * (j - 1)) / 2; }
+
+// record a failed pivot (sprfc1.f:1274-1279): first failure per supernode wins
+// A failed front poisons its ancestors only: fronts earlier in postorder than
+// the first failure are still factored, so NUMNEG matches the reference's count
+// of negative pivots met before it stops (sprfc1.f:610-616).
+__device__ void record_fail(const PV& P, int js, int col, double d, double ad) {
+    P.sn_fail[js] = col;
+    P.sn_faild[js] = d;
+    P.sn_faila[js] = ad;
+    P.sn_bad[js] = 1;
+    atomicExch(&P.st->pivot_fail, 1);
+}
+
+__device__ __forceinline__ bool children_bad(const PV& P, int js) {
+    for (int k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k)
+        if (P.sn_bad[P.child[k]]) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Pre-pass: original diagonal, zero test, trace (sprfc1.f:465-488)
+// ---------------------------------------------------------------------------
+__global__ void k_prepass(PV P, int64_t nsuper) {
+    for (int64_t js = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; js < nsuper;
+         js += (int64_t)gridDim.x * blockDim.x) {
+        const int s = P.S[js], f = P.F[js], fst = P.fst[js];
+        const double* col = P.lnz + P.lnz_off[js];
+        for (int j = 0; j < s; ++j) {
+            const double a = col[lnz_col(j, f)];
+            P.adiag[fst + j] = a;
+            if (a == 0.0) {
+                atomicAdd(&P.st->zero_count, 1);
+                atomicMin(&P.st->first_zero, fst + j);
+                atomicExch(&P.st->any_fail, 1);
+            }
+        }
+    }
+}
+
+// Deterministic single-CTA reductions over a vector: sum, or min over positives.
+template <bool kMinPos>
+__global__ void k_reduce(const double* v, int64_t n, double* out) {
+    __shared__ double red[1024];
+    double acc = kMinPos ? 0.0 : 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = v[i];
+        if (kMinPos) {
+            if (x > 0.0 && (acc == 0.0 || x < acc)) acc = x;
+        } else {
+            acc += x;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            const double a = red[threadIdx.x], b = red[threadIdx.x + s];
+            if (kMinPos) {
+                red[threadIdx.x] = (a == 0.0) ? b : ((b == 0.0) ? a : (a < b ? a : b));
+            } else {
+                red[threadIdx.x] = a + b;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// ---------------------------------------------------------------------------
+// Small fronts: fused extend-add + LDL' + Schur update, one CTA per front.
+// Shared memory holds the packed lower front F(F+1)/2 plus one column.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P) {
+    extern __shared__ double sh[];
+    if (P.st->any_fail) return;
+    const int js = nodes[blockIdx.x];
+    if (children_bad(P, js)) {
+        if (threadIdx.x == 0) P.sn_bad[js] = 1;
+        return;
+    }
+    const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    const int npk = F * (F + 1) / 2;
+    double* A = sh;
+    double* wcol = sh + npk;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    // fully-summed columns: the packed trapezoid of LNZ is the front's first SUPSZE entries
+    const int supsze = F * S - (S * (S - 1)) / 2;
+    const double* lnz = P.lnz + P.lnz_off[js];
+    for (int i = tid; i < npk; i += blockDim.x) A[i] = (i < supsze) ? lnz[i] : 0.0;
+    __syncthreads();
+    // extend-add, children last sibling first (sprfc1.f:534-584)
+    for (int k = P.child_ptr[js + 1] - 1; k >= P.child_ptr[js]; --k) {
+        const int c = P.child[k];
+        const int q = P.F[c] - P.S[c];
+        if (q <= 0) continue;
+        const int32_t* rel = P.rel + P.rel_off[c];
+        const double* U = P.arena + P.upd_off[c];
+        const int ld = P.buf_ld[c];
+        for (int t = warp; t < q; t += nwarp) {
+            const int pj = rel[t];
+            for (int r = t + lane; r < q; r += 32) A[pk(rel[r], pj, F)] += U[r + (int64_t)t * ld];
+        }
+        __syncthreads();
+    }
+    // LDL' of the S fully-summed columns with the trailing (Schur) update
+    int neg = 0;
+    double tmax = 0.0;
+    bool failed = false;
+    for (int k = 0; k < S; ++k) {
+        const double d = A[pk(k, k, F)];
+        const double ad = P.adiag[fst + k];
+        if (fabs(d) <= P.tol1 * fabs(ad)) {            // sprfc1.f:1274
+            if (tid == 0) record_fail(P, js, k, d, ad);
+            failed = true;
+            break;
+        }
+        if (d < 0.0) ++neg;
+        tmax = fmax(tmax, ad / d);
+        const double rd = 1.0 / d;
+        for (int i = k + 1 + tid; i < F; i += blockDim.x) {
+            const double a = A[pk(i, k, F)];
+            wcol[i] = a;
+            A[pk(i, k, F)] = a * rd;
+        }
+        __syncthreads();
+        for (int j = k + 1 + warp; j < F; j += nwarp) {
+            const double ljk = A[pk(j, k, F)];
+            const int cj = pk(j, j, F) - j;
+            for (int i = j + lane; i < F; i += 32) A[cj + i] -= wcol[i] * ljk;
+        }
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) {
+            P.sn_neg[js] = neg;
+            atomicAdd(&P.st->numneg, (unsigned long long)neg);
+        }
+        return;
+    }
+    // write back the S columns (LNZ layout == packed layout) and the pivots
+    double* lnzw = P.lnz + P.lnz_off[js];
+    for (int i = tid; i < supsze; i += blockDim.x) lnzw[i] = A[i];
+    for (int j = tid; j < S; j += blockDim.x) P.dvec[fst + j] = A[pk(j, j, F)];
+    const int q = F - S;
+    if (q > 0) {
+        double* U = P.arena + P.upd_off[js];
+        const int ld = P.buf_ld[js];
+        for (int t = warp; t < q; t += nwarp)
+            for (int r = t + lane; r < q; r += 32) U[r + (int64_t)t * ld] = A[pk(S + r, S + t, F)];
+    }
+    if (tid == 0) {
+        P.sn_neg[js] = neg;
+        atomicAdd(&P.st->numneg, (unsigned long long)neg);
+        atomic_max_double(&P.st->tol2, tmax);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Large fronts
+// ---------------------------------------------------------------------------
+
+// A large front whose child failed (or depends on a failure) is skipped.
+__global__ void k_poison(const Job* jobs, int64_t njobs, PV P) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const int js = jobs[j].node;
+    if (children_bad(P, js)) P.sn_bad[js] = 1;
+}
+
+// Extend-add into a dense column-major front: one warp per front column.
+__global__ void k_assemble(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {
+    if (P.st->any_fail) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int j = jb.c0 + (int)(task - jb.task0);
+    const int F = P.F[js], S = P.S[js];
+    const int ld = P.buf_ld[js];
+    double* col = P.arena + P.buf_off[js] + (int64_t)j * ld;
+    if (j < S) {
+        const double* src = P.lnz + P.lnz_off[js] + lnz_col(j, F) - j;
+        for (int i = j + lane; i < F; i += 32) col[i] = src[i];
+    } else {
+        for (int i = j + lane; i < F; i += 32) col[i] = 0.0;
+    }
+    __syncwarp();
+    const int64_t e0 = P.cptr[P.rbase[js] + j], e1 = P.cptr[P.rbase[js] + j + 1];
+    for (int64_t e = e0; e < e1; ++e) {
+        const int c = P.cchild[e], t = P.ct[e];
+        const int q = P.F[c] - P.S[c];
+        const int32_t* rel = P.rel + P.rel_off[c];
+        const double* U = P.arena + P.upd_off[c] + (int64_t)t * P.buf_ld[c];
+        for (int r = t + lane; r < q; r += 32) col[rel[r]] += U[r];
+        __syncwarp();
+    }
+}
+
+// LDL' of one nb x nb diagonal block (right-looking, in shared memory),
+// pivot test / inertia / TOL(2) as SPRF17 (sprfc1.f:1272-1294).
+__global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
+    __shared__ double A[kNB][kNB + 1];
+    __shared__ double w[kNB];
+    if (P.st->any_fail) return;
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    if (P.sn_bad[js]) return;
+    const int ld = P.buf_ld[js], fst = P.fst[js];
+    double* front = P.arena + P.buf_off[js];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+        const int i = e % nb, j = e / nb;
+        if (i >= j) A[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
+    }
+    __syncthreads();
+    int neg = 0;
+    double tmax = 0.0;
+    int failed = -1;
+    for (int k = 0; k < nb; ++k) {
+        const double d = A[k][k];
+        const double ad = P.adiag[fst + k0 + k];
+        if (fabs(d) <= P.tol1 * fabs(ad)) {
+            failed = k;
+            if (tid == 0) record_fail(P, js, k0 + k, d, ad);
+            break;
+        }
+        if (d < 0.0) ++neg;
+        tmax = fmax(tmax, ad / d);
+        const double rd = 1.0 / d;
+        for (int i = k + 1 + tid; i < nb; i += blockDim.x) {
+            w[i] = A[i][k];
+            A[i][k] = A[i][k] * rd;
+        }
+        __syncthreads();
+        const int m = nb - k - 1;
+        for (int e = tid; e < m * m; e += blockDim.x) {
+            const int ii = e % m, jj = e / m;
+            if (ii >= jj) A[k + 1 + ii][k + 1 + jj] -= w[k + 1 + ii] * A[k + 1 + jj][k];
+        }
+        __syncthreads();
+    }
+    if (failed < 0) {
+        for (int e = tid; e < nb * nb; e += blockDim.x) {
+            const int i = e % nb, j = e / nb;
+            if (i >= j) front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld] = A[i][j];
+        }
+        for (int k = tid; k < nb; k += blockDim.x) P.dvec[fst + k0 + k] = A[k][k];
+    }
+    if (tid == 0) {
+        P.sn_neg[js] += neg;
+        atomicAdd(&P.st->numneg, (unsigned long long)neg);
+        if (failed < 0) atomic_max_double(&P.st->tol2, tmax);
+    }
+}
+
+// Panel TRSM: rows below the diagonal block, L21 = A21 L11^-T D^-1.
+// One CTA of kTRSMRows threads per row block, one thread per row.
+constexpr size_t kTrsmSmem = sizeof(double) * ((size_t)kNB * (kNB + 1) + (size_t)kNB * kTRSMRows + kNB);
+
+__global__ void __launch_bounds__(kTRSMRows) k_trsm(const Job* jobs, int64_t njobs, PV P) {
+    extern __shared__ double tsh[];
+    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(tsh);
+    double(*W)[kTRSMRows] = reinterpret_cast<double(*)[kTRSMRows]>(tsh + kNB * (kNB + 1));
+    double* rd = tsh + kNB * (kNB + 1) + kNB * kTRSMRows;
+    if (P.st->any_fail) return;
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    if (P.sn_bad[js]) return;
+    const int F = P.F[js], ld = P.buf_ld[js];
+    const int r0 = jb.c0 + (int)(task - jb.task0) * kTRSMRows;
+    double* front = P.arena + P.buf_off[js];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+        const int i = e % nb, j = e / nb;
+        if (i > j) L[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
+    }
+    for (int k = tid; k < nb; k += blockDim.x)
+        rd[k] = 1.0 / front[(int64_t)(k0 + k) * (ld + 1)];
+    const int i = r0 + tid;
+    const bool live = i < F;
+    if (live)
+        for (int c = 0; c < nb; ++c) W[c][tid] = front[(int64_t)i + (int64_t)(k0 + c) * ld];
+    __syncthreads();
+    if (!live) return;
+    for (int c = 0; c < nb; ++c) {
+        double acc = W[c][tid];
+        for (int m = 0; m < c; ++m) acc -= W[m][tid] * L[c][m];
+        W[c][tid] = acc;
+        front[(int64_t)i + (int64_t)(k0 + c) * ld] = acc * rd[c];
+    }
+}
+
+// Schur update C -= L D L' on 64x64 lower-triangle tiles with FP64 DMMA
+// (mma.sync m8n8k4).  A = rows i of L scaled by D, B = rows j of L.
+// 128 threads = 2x2 warps of 32x32; K staged through shared memory in
+// double-buffered 16-wide slices with cp.async.
+namespace gemm {
+constexpr int BM = kTile, BN = kTile, BK = 16, LDS = BM + 4;
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    const int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+}  // namespace gemm
+
+__global__ void __launch_bounds__(128) k_gemm(const Job* jobs, int64_t njobs, PV P) {
+    using namespace gemm;
+    __shared__ __align__(16) double As[2][BK][LDS];
+    __shared__ __align__(16) double Bs[2][BK][LDS];
+    __shared__ double Ds[2][BK];
+    if (P.st->any_fail) return;
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int F = P.F[js], ld = P.buf_ld[js];
+    // decode the lower-triangle tile (column tile jt, row tile it >= jt)
+    const int64_t u = task - jb.task0;
+    const int nct = (jb.c_end - jb.c0 + BN - 1) / BN;
+    const int nr = (jb.r_end - jb.c0 + BM - 1) / BM;
+    int lo = 0, hi = nct - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t pre = (int64_t)mid * nr - ((int64_t)mid * (mid - 1)) / 2;
+        if (pre <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const int jt = lo;
+    const int it = jt + (int)(u - ((int64_t)jt * nr - ((int64_t)jt * (jt - 1)) / 2));
+    const int i0 = jb.c0 + it * BM, j0 = jb.c0 + jt * BN;
+    const int r_end = jb.r_end, c_end = jb.c_end;
+    double* front = P.arena + P.buf_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    (void)F;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+    const int k_lo = jb.k_lo, k_hi = jb.k_hi;
+    const int nk = (k_hi - k_lo + BK - 1) / BK;
+    auto load_stage = [&](int stage, int kt) {
+        const int kb = k_lo + kt * BK;
+#pragma unroll
+        for (int e = 0; e < (BM * BK) / 128; ++e) {
+            const int idx = tid + e * 128;
+            const int r = idx % BM, k = idx / BM;
+            const int kk = kb + k;
+            const bool kv = kk < k_hi;
+            const int ra = i0 + r, rb = j0 + r;
+            const double* ga = front + (int64_t)(kv ? kk : k_lo) * ld + (ra < r_end ? ra : i0);
+            const double* gb = front + (int64_t)(kv ? kk : k_lo) * ld + (rb < r_end ? rb : j0);
+            cp_async8(&As[stage][k][r], ga, kv && ra < r_end);
+            cp_async8(&Bs[stage][k][r], gb, kv && rb < r_end);
+        }
+        if (tid < BK) {
+            const int kk = kb + tid;
+            Ds[stage][tid] = kk < k_hi ? front[(int64_t)kk * (ld + 1)] : 0.0;
+        }
+        cp_async_commit();
+    };
+
+    load_stage(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int cur = kt & 1;
+        if (kt + 1 < nk) {
+            load_stage(cur ^ 1, kt + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < BK; k4 += 4) {
+            const int kk = k4 + (lane & 3);
+            const double dk = Ds[cur][kk];
+            double a[4], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) a[mi] = As[cur][kk][wm + mi * 8 + (lane >> 2)] * dk;
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[cur][kk][wn + ni * 8 + (lane >> 2)];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+        __syncthreads();
+    }
+    // epilogue: C -= acc on the lower part, inside [.., r_end) x [.., c_end)
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+        const int r = i0 + wm + mi * 8 + (lane >> 2);
+        if (r >= r_end) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = j0 + wn + ni * 8 + 2 * (lane & 3) + h;
+                if (c < c_end && r >= c) front[(int64_t)r + (int64_t)c * ld] -= acc[mi][ni][h];
+            }
+        }
+    }
+}
+
+// Store the S factored columns of a dense front into LNZ (sprfc1.f:630-637).
+__global__ void k_writeback(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {
+    if (P.st->any_fail) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int j = jb.c0 + (int)(task - jb.task0);
+    const int F = P.F[js], ld = P.buf_ld[js];
+    const double* col = P.arena + P.buf_off[js] + (int64_t)j * ld;
+    double* dst = P.lnz + P.lnz_off[js] + lnz_col(j, F) - j;
+    for (int i = j + lane; i < F; i += 32) dst[i] = col[i];
+}
+
+// ---------------------------------------------------------------------------
+// Solves (multi-RHS), one CTA per front, level by level.
+// Front vectors live in vbuf: front p uses F_p x nrhs doubles at rbase[p]*nrhs
+// (column r at offset r*F_p).  After the forward sweep, rows S..F of a front
+// vector are its update vector for the parent.
+// ---------------------------------------------------------------------------
+constexpr int kSolveThreads = 256;
+constexpr int kSolveBlk = 32;
+
+__global__ void __launch_bounds__(kSolveThreads)
+k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
+    const int js = nodes[blockIdx.x];
+    const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const double* Lb = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31;
+    // gather: own rows from b, plus the children's update vectors (SPRFB1 + extend-add)
+    for (int i = tid; i < F; i += blockDim.x) {
+        const int64_t e0 = P.cptr[P.rbase[js] + i], e1 = P.cptr[P.rbase[js] + i + 1];
+        for (int r = 0; r < nrhs; ++r) {
+            double v = (i < S) ? b[(int64_t)(fst + i) + r * ldb] : 0.0;
+            for (int64_t e = e0; e < e1; ++e) {
+                const int c = P.cchild[e], t = P.ct[e];
+                const int fc = P.F[c];
+                v += vbuf[P.rbase[c] * nrhs + (int64_t)r * fc + P.S[c] + t];
+            }
+            w[(int64_t)r * F + i] = v;
+        }
+    }
+    __syncthreads();
+    for (int jb = 0; jb < S; jb += kSolveBlk) {
+        const int je = min(jb + kSolveBlk, S);
+        // triangle of the block (SPRFS5 :600-608), one warp
+        if (tid < 32) {
+            for (int j = jb; j < je; ++j) {
+                const double* cj = Lb + lnz_col(j, F) - j;
+                const int i = j + 1 + lane;
+                if (i < je)
+                    for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= w[(int64_t)r * F + j] * cj[i];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // rectangle below the block (SPRFS6)
+        for (int i = je + tid; i < F; i += blockDim.x) {
+            double acc[kMaxRHS];
+            for (int r = 0; r < nrhs; ++r) acc[r] = w[(int64_t)r * F + i];
+            for (int j = jb; j < je; ++j) {
+                const double l = Lb[lnz_col(j, F) - j + i];
+                for (int r = 0; r < nrhs; ++r) acc[r] -= w[(int64_t)r * F + j] * l;
+            }
+            for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = acc[r];
+        }
+        __syncthreads();
+    }
+    // diagonal (SPRFS5 :622-625) and scatter of the own rows (SPRFB2)
+    for (int j = tid; j < S; j += blockDim.x) {
+        const double d = Lb[lnz_col(j, F)];
+        for (int r = 0; r < nrhs; ++r) {
+            const double y = w[(int64_t)r * F + j] / d;
+            w[(int64_t)r * F + j] = y;
+            b[(int64_t)(fst + j) + r * ldb] = y;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSolveThreads)
+k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
+    __shared__ double part[kSolveBlk][kMaxRHS];
+    const int js = nodes[blockIdx.x];
+    const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const double* Lb = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    // gather: own rows (forward result) and the ancestors' solved rows.  The
+    // row list of front js starts at rbase[js] (LINDX is the concatenation of
+    // the fronts' row lists, XLINDX(js) - 1 == sum of the previous F).
+    for (int i = tid; i < F; i += blockDim.x) {
+        const int row = (i < S) ? (fst + i) : P.rows[P.rbase[js] + i];
+        for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = b[(int64_t)row + r * ldb];
+    }
+    __syncthreads();
+    const int nblk = (S + kSolveBlk - 1) / kSolveBlk;
+    for (int bi = nblk - 1; bi >= 0; --bi) {
+        const int jb = bi * kSolveBlk, je = min(jb + kSolveBlk, S);
+        // contributions of the rows below the block (SPRBS6 dot products)
+        for (int c = jb + warp; c < je; c += nwarp) {
+            const double* cc = Lb + lnz_col(c, F) - c;
+            double acc[kMaxRHS];
+            for (int r = 0; r < nrhs; ++r) acc[r] = 0.0;
+            for (int i = je + lane; i < F; i += 32) {
+                const double l = cc[i];
+                for (int r = 0; r < nrhs; ++r) acc[r] += l * w[(int64_t)r * F + i];
+            }
+            for (int r = 0; r < nrhs; ++r) {
+                double v = acc[r];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) part[c - jb][r] = v;
+            }
+        }
+        __syncthreads();
+        // triangle of the block, bottom-up, one warp
+        if (tid < 32) {
+            for (int c = je - 1; c >= jb; --c) {
+                const double* cc = Lb + lnz_col(c, F) - c;
+                for (int r = 0; r < nrhs; ++r) {
+                    double v = 0.0;
+                    const int i = c + 1 + lane;
+                    if (i < je) v = cc[i] * w[(int64_t)r * F + i];
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0) w[(int64_t)r * F + c] -= part[c - jb][r] + v;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+    }
+    for (int j = tid; j < S; j += blockDim.x)
+        for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = w[(int64_t)r * F + j];
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine() : d_(new Dev()) {}
+
+Engine::~Engine() {
+    if (!d_) return;
+    for (void* p : d_->owned) cudaFree(p);
+    if (d_->arena) cudaFree(d_->arena);
+    if (d_->vbuf) cudaFree(d_->vbuf);
+    if (d_->bbuf) cudaFree(d_->bbuf);
+    if (d_->ev0) cudaEventDestroy(d_->ev0);
+    if (d_->ev1) cudaEventDestroy(d_->ev1);
+}
+
+int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa) {
+    int rc = build_plan(mspar, mtrees, msifa, P_);
+    if (rc != 0) return rc;
+    Dev& D = *d_;
+    auto& o = D.owned;
+    if (dev_upload(o, &D.fst, P_.fst) || dev_upload(o, &D.S, P_.S) || dev_upload(o, &D.F, P_.F) ||
+        dev_upload(o, &D.child_ptr, P_.child_ptr) || dev_upload(o, &D.child, P_.child) ||
+        dev_upload(o, &D.rows, P_.rows) || dev_upload(o, &D.rel, P_.rel) ||
+        dev_upload(o, &D.cchild, P_.cchild) || dev_upload(o, &D.ct, P_.ct) ||
+        dev_upload(o, &D.buf_ld, P_.buf_ld) || dev_upload(o, &D.lnz_off, P_.lnz_off) ||
+        dev_upload(o, &D.rel_off, P_.rel_off) || dev_upload(o, &D.rbase, P_.rbase) ||
+        dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
+        dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs))
+        return -4;
+    std::vector<int32_t> small, all;
+    D.small_begin.clear();
+    D.all_begin.clear();
+    D.all_count.clear();
+    for (const LevelPlan& lp : P_.levels) {
+        D.small_begin.push_back((int64_t)small.size());
+        small.insert(small.end(), lp.small_nodes.begin(), lp.small_nodes.end());
+        D.all_begin.push_back((int64_t)all.size());
+        all.insert(all.end(), lp.small_nodes.begin(), lp.small_nodes.end());
+        all.insert(all.end(), lp.large_nodes.begin(), lp.large_nodes.end());
+        D.all_count.push_back((int64_t)(lp.small_nodes.size() + lp.large_nodes.size()));
+    }
+    if (dev_upload(o, &D.level_nodes, small) || dev_upload(o, &D.all_nodes, all)) return -4;
+    CK(cudaMalloc((void**)&D.arena, std::max<int64_t>(P_.arena_doubles, 32) * sizeof(double)));
+    CK(cudaMalloc((void**)&D.adiag, P_.neq * sizeof(double)));
+    o.push_back(D.adiag);
+    CK(cudaMalloc((void**)&D.sn_neg, P_.nsuper * sizeof(int32_t)));
+    o.push_back(D.sn_neg);
+    CK(cudaMalloc((void**)&D.sn_fail, P_.nsuper * sizeof(int32_t)));
+    o.push_back(D.sn_fail);
+    CK(cudaMalloc((void**)&D.sn_bad, P_.nsuper * sizeof(int32_t)));
+    o.push_back(D.sn_bad);
+    CK(cudaMalloc((void**)&D.sn_faild, P_.nsuper * sizeof(double)));
+    o.push_back(D.sn_faild);
+    CK(cudaMalloc((void**)&D.sn_faila, P_.nsuper * sizeof(double)));
+    o.push_back(D.sn_faila);
+    CK(cudaMalloc((void**)&D.st, sizeof(Stats)));
+    o.push_back(D.st);
+    CK(cudaEventCreate(&D.ev0));
+    CK(cudaEventCreate(&D.ev1));
+    int smem_max = 0;
+    CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
+    const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + kSmallMaxF) * sizeof(double);
+    if ((size_t)smem_max < need) return -4;
+    CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    return 0;
+}
+
+static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
+    PV v;
+    v.fst = D.fst;
+    v.S = D.S;
+    v.F = D.F;
+    v.child_ptr = D.child_ptr;
+    v.child = D.child;
+    v.rows = D.rows;
+    v.rel = D.rel;
+    v.cchild = D.cchild;
+    v.ct = D.ct;
+    v.buf_ld = D.buf_ld;
+    v.lnz_off = D.lnz_off;
+    v.rel_off = D.rel_off;
+    v.rbase = D.rbase;
+    v.cptr = D.cptr;
+    v.buf_off = D.buf_off;
+    v.upd_off = D.upd_off;
+    v.arena = D.arena;
+    v.dvec = d_sm;
+    v.lnz = d_sm + P.neq;
+    v.adiag = D.adiag;
+    v.sn_neg = D.sn_neg;
+    v.sn_fail = D.sn_fail;
+    v.sn_bad = D.sn_bad;
+    v.sn_faild = D.sn_faild;
+    v.sn_faila = D.sn_faila;
+    v.st = D.st;
+    v.tol1 = tol1;
+    return v;
+}
+
+int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    PV pv = make_view(D, P_, d_sm, tol1);
+    Stats init{};
+    init.first_zero = 0x7fffffff;
+    CK(cudaMemcpyAsync(D.st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(D.sn_neg, 0, P_.nsuper * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(D.sn_fail, 0xff, P_.nsuper * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(D.sn_bad, 0, P_.nsuper * sizeof(int32_t), s));
+    timing.gemm_ms = 0.f;
+    timing.gemm_launches = 0;
+    timing.launches = 0;
+    CK(cudaEventRecord(D.ev0, s));
+    k_prepass<<<(int)std::min<int64_t>((P_.nsuper + 255) / 256, 1184), 256, 0, s>>>(pv, P_.nsuper);
+    k_reduce<false><<<1, 1024, 0, s>>>(D.adiag, P_.neq, &D.st->trace);
+    timing.launches += 2;
+    std::vector<cudaEvent_t> gev;
+    for (size_t L = 0; L < P_.levels.size(); ++L) {
+        const LevelPlan& lp = P_.levels[L];
+        if (!lp.small_nodes.empty()) {
+            const int F = lp.small_maxF;
+            const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
+            k_small_front<<<(int)lp.small_nodes.size(), 256, smem, s>>>(D.level_nodes + D.small_begin[L], pv);
+            ++timing.launches;
+        }
+        if (lp.large_nodes.empty()) continue;
+        const Job* jobs = D.jobs;
+        {
+            const Launch& l = lp.assemble;
+            k_poison<<<(int)((l.job_count + 127) / 128), 128, 0, s>>>(jobs + l.job_begin, l.job_count, pv);
+            const int64_t threads = l.ntasks * 32;
+            k_assemble<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, l.ntasks, pv);
+            ++timing.launches;
+        }
+        for (size_t st = 0; st < lp.panel.size(); ++st) {
+            const Launch& pl = lp.panel[st];
+            k_diag<<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+            ++timing.launches;
+            if (pl.ntasks > 0) {
+                k_trsm<<<(int)pl.ntasks, kTRSMRows, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, pv);
+                ++timing.launches;
+            }
+            const Launch& il = lp.inner[st];
+            if (il.ntasks > 0) {
+                k_gemm<<<(int)il.ntasks, 128, 0, s>>>(jobs + il.job_begin, il.job_count, pv);
+                ++timing.launches;
+                ++timing.gemm_launches;
+            }
+        }
+        if (lp.outer.ntasks > 0) {
+            k_gemm<<<(int)lp.outer.ntasks, 128, 0, s>>>(jobs + lp.outer.job_begin, lp.outer.job_count, pv);
+            ++timing.launches;
+            ++timing.gemm_launches;
+        }
+        {
+            const Launch& l = lp.writeback;
+            const int64_t threads = l.ntasks * 32;
+            k_writeback<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, l.ntasks, pv);
+            ++timing.launches;
+        }
+    }
+    k_reduce<true><<<1, 1024, 0, s>>>(pv.dvec, P_.neq, &D.st->mindpos);
+    ++timing.launches;
+    CK(cudaEventRecord(D.ev1, s));
+    CK(cudaGetLastError());
+    Stats hs;
+    CK(cudaMemcpyAsync(&hs, D.st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaEventElapsedTime(&timing.factor_ms, D.ev0, D.ev1));
+    res = FactorResult();
+    if (hs.zero_count > 0) {                       // sprfc1.f:474-488
+        // the reference's pre-pass has already replaced D by the original diagonal
+        CK(cudaMemcpy(pv.dvec, D.adiag, P_.neq * sizeof(double), cudaMemcpyDeviceToDevice));
+        res.lierr = -35;
+        res.numneg = hs.zero_count;
+        res.supeqt = (int64_t)hs.first_zero + 1;
+        res.tol2 = 0.0;
+        res.tol3 = hs.trace;
+        return 0;
+    }
+    if (hs.pivot_fail) {                           // sprfc1.f:610-616
+        std::vector<int32_t> fail(P_.nsuper), neg(P_.nsuper);
+        CK(cudaMemcpy(fail.data(), D.sn_fail, P_.nsuper * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(neg.data(), D.sn_neg, P_.nsuper * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        int64_t jf = -1;
+        for (int64_t js = 0; js < P_.nsuper; ++js)
+            if (fail[js] >= 0) {
+                jf = js;
+                break;
+            }
+        int64_t nn = 0;
+        for (int64_t js = 0; js <= jf; ++js) nn += neg[js];
+        double fd = 0.0, fa = 0.0;
+        CK(cudaMemcpy(&fd, D.sn_faild + jf, sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&fa, D.sn_faila + jf, sizeof(double), cudaMemcpyDeviceToHost));
+        res.lierr = -30;
+        res.numneg = nn;
+        res.supeqt = (int64_t)P_.fst[jf] + fail[jf] + 1;
+        res.tol2 = fd;
+        res.tol3 = fa;
+        return 0;
+    }
+    res.numneg = hs.numneg;
+    res.tol2 = (hs.tol2 != 0.0) ? 1.0 / hs.tol2 : 0.0;          // sprfc1.f:699-703
+    res.tol3 = (hs.mindpos != 0.0) ? hs.trace / hs.mindpos : 0.0;  // sprfc1.f:704-708
+    return 0;
+}
+
+void Engine::ensure_vectors(int64_t nrhs) {
+    Dev& D = *d_;
+    if (D.vbuf_rhs < nrhs) {
+        if (D.vbuf) cudaFree(D.vbuf);
+        D.vbuf = nullptr;
+        cudaMalloc((void**)&D.vbuf, std::max<int64_t>(P_.rbase.back(), 1) * nrhs * sizeof(double));
+        D.vbuf_rhs = nrhs;
+    }
+}
+
+int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    PV pv = make_view(D, P_, const_cast<double*>(d_sm), 0.0);
+    const int64_t chunk = std::min<int64_t>(nrhs, kMaxRHS);
+    ensure_vectors(chunk);
+    if (!D.vbuf) return -4;
+    CK(cudaEventRecord(D.ev0, s));
+    for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
+        const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
+        double* b = d_b + r0 * ldb;
+        if (which & 1) {
+            for (size_t L = 0; L < P_.levels.size(); ++L) {
+                if (D.all_count[L] == 0) continue;
+                k_forward<<<(int)D.all_count[L], kSolveThreads, 0, s>>>(D.all_nodes + D.all_begin[L], pv, D.vbuf, b,
+                                                                        ldb, nr);
+            }
+        }
+        if (which & 2) {
+            for (size_t L = P_.levels.size(); L-- > 0;) {
+                if (D.all_count[L] == 0) continue;
+                k_backward<<<(int)D.all_count[L], kSolveThreads, 0, s>>>(D.all_nodes + D.all_begin[L], pv, D.vbuf, b,
+                                                                         ldb, nr);
+            }
+        }
+    }
+    CK(cudaEventRecord(D.ev1, s));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    CK(cudaEventElapsedTime(&timing.solve_ms, D.ev0, D.ev1));
+    return 0;
+}
+
+}  // namespace sprb

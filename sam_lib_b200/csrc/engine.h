@@ -1,0 +1,56 @@
+// GPU numeric phase of SPR: device state and entry points used by the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "plan.h"
+
+namespace sprb {
+
+// Outcome of a factorisation, in the reference's terms (SPRF11/SPRFC1,
+// src/SPR/sprfc1.f:240-283 and :690-708).
+struct FactorResult {
+    int64_t lierr = 0;       // 0, -30 (pivot below threshold) or -35 (zero diagonal)
+    int64_t numneg = 0;      // MSPAR(26)
+    int64_t supeqt = 0;      // MSPAR(27) on error
+    double tol2 = 0.0;       // TOL(2)
+    double tol3 = 0.0;       // TOL(3)
+};
+
+struct Timing {              // CUDA-event times of the last calls (ms)
+    float factor_ms = 0.f, solve_ms = 0.f;
+    float gemm_ms = 0.f;     // Schur-update kernels only (sum over launches)
+    int64_t gemm_launches = 0, launches = 0;
+};
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+    // Builds the plan and uploads the symbolic structure.  Returns 0 or IERR-style code.
+    int open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa);
+    const Plan& plan() const { return P_; }
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    cudaStream_t stream() const { return stream_; }
+    // Device-resident factorisation of sm = [D(NEQ) | LNZ(NZEROL)] (device pointer).
+    int factor(double* d_sm, double tol1, FactorResult& res);
+    // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
+    int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
+    // Timing of the Schur-update kernels can be switched on (events around each launch).
+    void set_profile(bool on) { profile_ = on; }
+    Timing timing;
+    struct Dev;              // device copies of the plan and work buffers
+
+private:
+    void upload_plan();
+    void ensure_vectors(int64_t nrhs);
+    Plan P_;
+    cudaStream_t stream_ = nullptr;
+    bool profile_ = false;
+    std::unique_ptr<Dev> d_;
+};
+
+}  // namespace sprb

@@ -1,0 +1,284 @@
+// Execution plan of the GPU numeric phase (see plan.h).
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+namespace sprb {
+
+namespace {
+
+// First-fit allocator over a linear arena, in units of doubles.  Blocks are
+// aligned to 32 doubles (256 bytes) so every front starts on a TMA/vector
+// friendly boundary.
+class Arena {
+public:
+    int64_t alloc(int64_t n) {
+        n = (n + 31) / 32 * 32;
+        if (n == 0) n = 32;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                int64_t off = it->first;
+                int64_t rest = it->second - n;
+                free_.erase(it);
+                if (rest > 0) free_[off + n] = rest;
+                return off;
+            }
+        }
+        int64_t off = top_;
+        top_ += n;
+        return off;
+    }
+    void release(int64_t off, int64_t n) {
+        n = (n + 31) / 32 * 32;
+        if (n == 0) n = 32;
+        auto it = free_.emplace(off, n).first;
+        // coalesce with the next block
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        // coalesce with the previous block
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+                it = pv;
+            }
+        }
+        // shrink the top
+        if (it->first + it->second == top_) {
+            top_ = it->first;
+            free_.erase(it);
+        }
+    }
+    int64_t top() const { return top_; }
+
+private:
+    std::map<int64_t, int64_t> free_;
+    int64_t top_ = 0;
+};
+
+inline int32_t round_up4(int32_t x) { return (x + 3) / 4 * 4; }
+
+}  // namespace
+
+int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa, Plan& P) {
+    // Pointer conventions of SPRFC1 (src/SPR/sprfc1.f:165-196).
+    P.neq = mspar[7];
+    P.nsuper = mspar[10];
+    P.maxsup = mspar[12];
+    P.mfront = mspar[13];
+    P.nofsub = mspar[14];
+    P.nzerol = mspar[15];
+    const int64_t ns = P.nsuper;
+    if (ns <= 0 || P.neq <= 0 || mspar[44] < 1 || mspar[45] < 1 || mspar[46] < 1 || mspar[47] < 1)
+        return -2;
+    const int64_t* xsuper = mtrees + (mspar[44] - 1);
+    const int64_t* xsibl = xsuper + (ns + 1);
+    const int64_t* sibl = xsuper + 2 * (ns + 1);
+    const int64_t* xlindx = mtrees + (mspar[45] - 1);
+    const int64_t* lindx = msifa + (mspar[46] - 1);
+    const int64_t* xlnz = msifa + (mspar[47] - 1);
+
+    P.fst.resize(ns);
+    P.S.resize(ns);
+    P.F.resize(ns);
+    P.parent.assign(ns, -1);
+    P.level.assign(ns, 0);
+    P.lnz_off.resize(ns);
+    P.lindx_off.resize(ns);
+    P.child_ptr.assign(ns + 1, 0);
+    P.factor_flops = 0.0;
+    P.solve_flops = 0.0;
+    for (int64_t js = 0; js < ns; ++js) {
+        P.fst[js] = (int32_t)(xsuper[js] - 1);
+        P.S[js] = (int32_t)(xsuper[js + 1] - xsuper[js]);
+        P.F[js] = (int32_t)(xlindx[js + 1] - xlindx[js]);
+        P.lnz_off[js] = xlnz[js] - 1;
+        P.lindx_off[js] = xlindx[js] - 1;
+        if (P.S[js] <= 0 || P.F[js] < P.S[js]) return -2;
+        const double s = P.S[js], f = P.F[js];
+        // RINFO(3) and RINFO(4) per supernode, src/SPR/sprtrs.f:1961-1980
+        P.factor_flops += ((f * f) + 2.0 * f) * s - 2.0 * (1.0 + f) * (s * (s + 1.0) / 2.0) +
+                          s * (s + 1.0) * (2.0 * s + 1.0) / 6.0;
+        P.solve_flops += f * s - s * (s - 1.0) / 2.0 - s;
+    }
+    P.solve_flops = 2.0 * P.solve_flops + (double)P.neq;
+    // children (SIBL order) and parents
+    P.child.clear();
+    for (int64_t js = 0; js < ns; ++js) {
+        P.child_ptr[js] = (int32_t)P.child.size();
+        for (int64_t k = xsibl[js]; k < xsibl[js + 1]; ++k) {
+            int64_t c = sibl[k - 1] - 1;
+            if (c < 0 || c >= js) return -2;   // postorder: children precede parents
+            P.child.push_back((int32_t)c);
+            P.parent[c] = (int32_t)js;
+        }
+    }
+    P.child_ptr[ns] = (int32_t)P.child.size();
+    // rows (0-based)
+    P.rows.resize(xlindx[ns] - 1);
+    for (size_t i = 0; i < P.rows.size(); ++i) P.rows[i] = (int32_t)(lindx[i] - 1);
+    // levels: leaves 0, parent = 1 + max(children)
+    int32_t nlev = 0;
+    for (int64_t js = 0; js < ns; ++js) {
+        int32_t lv = 0;
+        for (int32_t k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k)
+            lv = std::max(lv, P.level[P.child[k]] + 1);
+        P.level[js] = lv;
+        nlev = std::max(nlev, lv + 1);
+    }
+    // relative maps (SPRF12 merge) and the contribution lists
+    P.rel_off.assign(ns, -1);
+    P.rel.clear();
+    P.rbase.assign(ns + 1, 0);
+    for (int64_t js = 0; js < ns; ++js) P.rbase[js + 1] = P.rbase[js] + P.F[js];
+    std::vector<int64_t> ccount(P.rbase[ns] + 1, 0);
+    for (int64_t c = 0; c < ns; ++c) {
+        const int32_t q = P.F[c] - P.S[c];
+        const int32_t p = P.parent[c];
+        if (q <= 0) continue;
+        if (p < 0) return -2;                  // update rows without a parent
+        P.rel_off[c] = (int64_t)P.rel.size();
+        const int32_t* prow = &P.rows[P.lindx_off[p]];
+        const int32_t* crow = &P.rows[P.lindx_off[c] + P.S[c]];
+        int32_t sup = 0;
+        for (int32_t t = 0; t < q; ++t) {
+            while (sup < P.F[p] && prow[sup] < crow[t]) ++sup;
+            if (sup >= P.F[p] || prow[sup] != crow[t]) return -4;   // not a subset
+            P.rel.push_back(sup);
+            ccount[P.rbase[p] + sup + 1]++;
+            ++sup;
+        }
+    }
+    P.cptr.assign(P.rbase[ns] + 1, 0);
+    for (int64_t i = 0; i < P.rbase[ns]; ++i) P.cptr[i + 1] = P.cptr[i] + ccount[i + 1];
+    P.cchild.assign(P.cptr[P.rbase[ns]], 0);
+    P.ct.assign(P.cptr[P.rbase[ns]], 0);
+    {
+        std::vector<int64_t> fill(P.cptr.begin(), P.cptr.end() - 1);
+        // children in the reference's assembly order: last sibling first (sprfc1.f:534)
+        for (int64_t p = 0; p < ns; ++p) {
+            for (int32_t k = P.child_ptr[p + 1] - 1; k >= P.child_ptr[p]; --k) {
+                const int32_t c = P.child[k];
+                const int32_t q = P.F[c] - P.S[c];
+                for (int32_t t = 0; t < q; ++t) {
+                    const int32_t j = P.rel[P.rel_off[c] + t];
+                    const int64_t pos = fill[P.rbase[p] + j]++;
+                    P.cchild[pos] = c;
+                    P.ct[pos] = t;
+                }
+            }
+        }
+    }
+    // arena layout, level by level
+    P.buf_off.assign(ns, 0);
+    P.buf_ld.assign(ns, 0);
+    P.upd_off.assign(ns, 0);
+    P.levels.assign(nlev, LevelPlan());
+    std::vector<std::vector<int32_t>> bylev(nlev);
+    for (int64_t js = 0; js < ns; ++js) bylev[P.level[js]].push_back((int32_t)js);
+    std::vector<int64_t> buf_size(ns, 0);
+    Arena arena;
+    P.any_large = false;
+    for (int32_t L = 0; L < nlev; ++L) {
+        LevelPlan& lp = P.levels[L];
+        std::vector<int32_t> nodes = bylev[L];
+        // big buffers first: less fragmentation
+        std::stable_sort(nodes.begin(), nodes.end(),
+                         [&](int32_t a, int32_t b) { return P.F[a] > P.F[b]; });
+        for (int32_t js : nodes) {
+            const int32_t f = P.F[js], s = P.S[js], q = f - s;
+            if (f <= kSmallMaxF) {
+                lp.small_nodes.push_back(js);
+                lp.small_maxF = std::max(lp.small_maxF, f);
+                P.buf_ld[js] = std::max(q, 1);
+                buf_size[js] = (int64_t)q * q;
+                P.buf_off[js] = arena.alloc(buf_size[js]);
+                P.upd_off[js] = P.buf_off[js];
+            } else {
+                lp.large_nodes.push_back(js);
+                P.any_large = true;
+                const int32_t ld = round_up4(f);
+                P.buf_ld[js] = ld;
+                buf_size[js] = (int64_t)ld * f;
+                P.buf_off[js] = arena.alloc(buf_size[js]);
+                P.upd_off[js] = P.buf_off[js] + (int64_t)s * ld + s;
+            }
+        }
+        // after this level is assembled, its children are no longer needed
+        for (int32_t js : nodes)
+            for (int32_t k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k) {
+                const int32_t c = P.child[k];
+                arena.release(P.buf_off[c], buf_size[c]);
+            }
+    }
+    P.arena_doubles = arena.top();
+    // ---- batched launches of the large path
+    P.jobs.clear();
+    auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };
+    auto add_job = [&](Launch& l, Job j, int64_t ntask) {
+        if (ntask <= 0) return;
+        j.task0 = l.ntasks;
+        P.jobs.push_back(j);
+        l.ntasks += ntask;
+    };
+    auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
+    auto tiles = [](int32_t c0, int32_t c_end, int32_t r_end) -> int64_t {
+        const int64_t nct = (c_end - c0 + kTile - 1) / kTile;
+        const int64_t nr = (r_end - c0 + kTile - 1) / kTile;
+        return nct * nr - nct * (nct - 1) / 2;
+    };
+    for (int32_t L = 0; L < nlev; ++L) {
+        LevelPlan& lp = P.levels[L];
+        if (lp.large_nodes.empty()) continue;
+        open_launch(lp.assemble);
+        for (int32_t js : lp.large_nodes)
+            add_job(lp.assemble, Job{js, 0, P.F[js], P.F[js], 0, 0, 0}, P.F[js]);
+        close_launch(lp.assemble);
+        int32_t smax = 0;
+        for (int32_t js : lp.large_nodes) smax = std::max(smax, P.S[js]);
+        const int32_t nsteps = (smax + kNB - 1) / kNB;
+        lp.panel.assign(nsteps, Launch());
+        lp.inner.assign(nsteps, Launch());
+        for (int32_t st = 0; st < nsteps; ++st) {
+            const int32_t k0 = st * kNB;
+            open_launch(lp.panel[st]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t nb = std::min(kNB, s - k0);
+                const int64_t nrb = (f - (k0 + nb) + kTRSMRows - 1) / kTRSMRows;
+                add_job(lp.panel[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, 1 + nrb);
+            }
+            close_launch(lp.panel[st]);
+            open_launch(lp.inner[st]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t nb = std::min(kNB, s - k0);
+                const int32_t c0 = k0 + nb;
+                if (c0 >= s) continue;
+                add_job(lp.inner[st], Job{js, c0, s, f, k0, k0 + nb, 0}, tiles(c0, s, f));
+            }
+            close_launch(lp.inner[st]);
+        }
+        open_launch(lp.outer);
+        for (int32_t js : lp.large_nodes) {
+            const int32_t s = P.S[js], f = P.F[js];
+            if (f > s) add_job(lp.outer, Job{js, s, f, f, 0, s, 0}, tiles(s, f, f));
+        }
+        close_launch(lp.outer);
+        open_launch(lp.writeback);
+        for (int32_t js : lp.large_nodes)
+            add_job(lp.writeback, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, P.S[js]);
+        close_launch(lp.writeback);
+    }
+    return 0;
+}
+
+}  // namespace sprb

@@ -1,0 +1,88 @@
+// Host-side execution plan for the GPU numeric phase of SPR.
+//
+// Built once per symbolic structure (MSPAR/MTREES/MSIFA as produced by the
+// SPR host pipeline, src/SPR/sprtrs.f + sprsmb.f + sprpmp.f) and cached by the
+// C-ABI layer.  It turns SPR's postordered supernode list into
+//   * elimination-tree levels (all fronts of a level are independent),
+//   * relative-index maps child -> parent (the integer merge of SPRF12,
+//     src/SPR/sprfc1.f:716-790, done once instead of per factorisation),
+//   * per-parent contribution lists (which child update column lands on which
+//     parent column), so extend-add is a deterministic, atomic-free gather,
+//   * a device arena layout for fronts / update matrices (first-fit reuse:
+//     a child's buffer is released once its parent level is assembled),
+//   * the batched task lists of the panel steps of the large fronts.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace sprb {
+
+constexpr int kSmallMaxF = 176;     // fronts up to this order: one CTA, shared memory
+constexpr int kNB = 64;             // panel width of the blocked LDL' for large fronts
+constexpr int kTRSMRows = 128;      // rows per CTA in the panel (TRSM) kernel
+constexpr int kTile = 64;           // Schur-update tile (rows x cols)
+constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
+
+// A job is one front's share of one batched launch.  Tasks inside a job are
+// decoded on the device (binary search over `task0`, then closed-form
+// arithmetic), so the plan stays O(fronts x steps) instead of O(tiles).
+//   assembly / write-back : one task per column in [c0, c_end)
+//   panel (TRSM)          : task 0 = diagonal-block CTA, then row blocks of
+//                           kTRSMRows rows starting at c0 (= k_hi)
+//   Schur update          : lower-triangle 64x64 tiles of rows [c0, r_end) x
+//                           columns [c0, c_end), contraction over [k_lo, k_hi)
+struct Job {
+    int32_t node;
+    int32_t c0, c_end, r_end;
+    int32_t k_lo, k_hi;
+    int64_t task0;                   // first task of this job within its launch
+};
+
+struct Launch {                      // a contiguous range of Plan::jobs
+    int64_t job_begin = 0, job_count = 0, ntasks = 0;
+};
+
+struct LevelPlan {
+    std::vector<int32_t> small_nodes;        // fronts done by the fused one-CTA kernel
+    std::vector<int32_t> large_nodes;        // fronts done by the blocked path
+    int32_t small_maxF = 0;
+    Launch assemble;                          // large fronts: extend-add into dense fronts
+    std::vector<Launch> panel, inner;         // per panel step
+    Launch outer;                             // update block, K = S
+    Launch writeback;                         // S columns -> LNZ
+};
+
+struct Plan {
+    // sizes
+    int64_t neq = 0, nsuper = 0, nzerol = 0, nofsub = 0, maxsup = 0, mfront = 0;
+    // per supernode (postorder index js = 0..nsuper-1)
+    std::vector<int32_t> fst, S, F, parent, level;
+    std::vector<int64_t> lnz_off, lindx_off;
+    std::vector<int32_t> child_ptr, child;   // children in SIBL order
+    std::vector<int32_t> rows;               // LINDX (0-based rows), concatenated like LINDX
+    // update-row -> parent-row maps, one per non-root supernode with F > S
+    std::vector<int64_t> rel_off;            // per node, offset into rel
+    std::vector<int32_t> rel;
+    // contribution CSR: for parent p, column j: entries [cptr[rbase[p]+j], cptr[rbase[p]+j+1])
+    std::vector<int64_t> rbase;              // per node, prefix of F
+    std::vector<int64_t> cptr;
+    std::vector<int32_t> cchild, ct;         // (child, child update column)
+    // device arena (units of doubles)
+    std::vector<int64_t> buf_off;            // per node: start of its buffer
+    std::vector<int32_t> buf_ld;             // leading dimension of the front / update buffer
+    std::vector<int64_t> upd_off;            // per node: where its update matrix (F-S)^2 starts
+    int64_t arena_doubles = 0;
+    bool any_large = false;
+    // levels and tasks
+    std::vector<LevelPlan> levels;
+    std::vector<Job> jobs;
+    // statistics (the reference's own counters are recomputed for reporting)
+    double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
+    double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
+};
+
+// Builds the plan from the SPR control arrays.  Returns 0 on success or a
+// negative code when the structure is inconsistent (mirrors IERR=-2 checks).
+int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa, Plan& plan);
+
+}  // namespace sprb

@@ -1,0 +1,118 @@
+"""Oracle pinning (CPU): the C restatement against the translated reference.
+
+The oracle (oracle/spr_oracle.c) must reproduce the reference SPR numeric
+phase bit for bit: same factor in SM, same solution, same TOL/MSPAR/IERR.
+The reference itself is the machine translation of the Fortran sources
+(oracle/f77c.py -> oracle/_ref/libsprref.so).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import ref_system, shifted_sm, dense_from_sm
+
+
+_L = None
+
+
+def _lib():
+    global _L
+    if _L is None:
+        import os
+        here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        _L = C.CDLL(os.path.join(here, 'oracle', '_ref', 'liboracle.so'))
+    return _L
+
+
+def run_sprsol(which, rs, sm, b, iop=3, tol1=1e-12, mspar=None):
+    from oracle.refpipe import lib as reflib, _p, _i
+    sm = sm.copy()
+    b = np.asfortranarray(b.copy())
+    nrhs = 1 if b.ndim == 1 else b.shape[1]
+    msp = rs.mspar.copy() if mspar is None else mspar.copy()
+    tol = np.array([tol1, 0.0, 0.0])
+    iw = np.zeros(int(rs.mspar[13]) + int(rs.mspar[12]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + int(rs.mspar[13]) + 8)
+    ierr = C.c_int64(0)
+    f = reflib().sprsol_ if which == 'ref' else _lib().orc_sprsol_
+    f(_i(iop), _p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(b), _i(rs.neq), _i(nrhs),
+      _p(tol), _p(iw), _p(rw), _i(-1), C.byref(ierr))
+    return dict(sm=sm, b=b, tol=tol, ierr=ierr.value, mspar=msp)
+
+
+def rhs(neq, nrhs, seed):
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, size=(neq, nrhs))
+
+
+@pytest.mark.parametrize('n,emod', [(3, 'uniform'), (6, 'uniform'), (6, 'loguniform'), (9, 'loguniform')])
+def test_oracle_bitwise_equals_reference(n, emod):
+    rs, sm = ref_system(n, emod)
+    b = rhs(rs.neq, 3, n)
+    r = run_sprsol('ref', rs, sm, b)
+    o = run_sprsol('orc', rs, sm, b)
+    assert r['ierr'] == o['ierr'] == 0
+    assert np.array_equal(r['sm'], o['sm'])
+    assert np.array_equal(r['b'], o['b'])
+    assert np.array_equal(r['tol'], o['tol'])
+    assert np.array_equal(r['mspar'], o['mspar'])
+
+
+def test_reference_solution_is_accurate():
+    rs, sm = ref_system(6)
+    K = dense_from_sm(rs, sm)
+    b = rhs(rs.neq, 2, 0)
+    r = run_sprsol('ref', rs, sm, b)
+    res = np.linalg.norm(K @ r['b'] - b) / np.linalg.norm(b)
+    assert res < 1e-12
+
+
+def test_inertia_matches_eigenvalues_and_reference():
+    rs, sm = ref_system(3)
+    from scipy.linalg import eigh
+    K = dense_from_sm(rs, sm)
+    M = np.diag(K.diagonal() - dense_from_sm(rs, shifted_sm(rs, sm, 1.0)).diagonal())
+    w = eigh(K, M, eigvals_only=True)
+    sigma = 0.5 * (w[3] + w[4])           # between the 4th and 5th eigenvalue
+    ssm = shifted_sm(rs, sm, sigma)
+    b = rhs(rs.neq, 1, 1)
+    r = run_sprsol('ref', rs, ssm, b, iop=1)
+    o = run_sprsol('orc', rs, ssm, b, iop=1)
+    assert r['ierr'] == 3 and o['ierr'] == 3          # not positive definite warning
+    assert r['mspar'][25] == o['mspar'][25] == 4      # NUMNEG = eigenvalues below sigma
+    assert np.array_equal(r['sm'], o['sm'])
+    # SPRSOL IOP=3: the solves reset IERR to 0 (sprfs1.f:143-144), NUMNEG stays
+    r = run_sprsol('ref', rs, ssm, b, iop=3)
+    o = run_sprsol('orc', rs, ssm, b, iop=3)
+    assert r['ierr'] == o['ierr'] == 0
+    assert r['mspar'][25] == o['mspar'][25] == 4
+    assert np.array_equal(r['b'], o['b'])
+
+
+def test_error_codes_match_reference():
+    rs, sm = ref_system(3)
+    b = rhs(rs.neq, 1, 2)
+    # preceding error not cleared (sprfc1.f:140-148)
+    bad = rs.mspar.copy()
+    bad[0] = -3
+    r = run_sprsol('ref', rs, sm, b, mspar=bad)
+    o = run_sprsol('orc', rs, sm, b, mspar=bad)
+    assert r['ierr'] == o['ierr'] == -1 and r['mspar'][0] == o['mspar'][0] == -5
+    # exact zero diagonal (sprfc1.f:474-488): IERR=-3, MSPAR(27)=first equation
+    z = sm.copy()
+    neq = rs.neq
+    sp = rs.mspar
+    xlnz1 = int(rs.msifa[sp[47] - 1 + 5])       # first LNZ entry of supernode 6
+    z[neq + xlnz1 - 1] = 0.0
+    r = run_sprsol('ref', rs, z, b, iop=1)
+    o = run_sprsol('orc', rs, z, b, iop=1)
+    assert r['ierr'] == o['ierr'] == -3
+    assert r['mspar'][26] == o['mspar'][26] and r['mspar'][25] == o['mspar'][25] == 1
+    assert np.array_equal(r['tol'], o['tol'])
+    # pivot below threshold (sprfc1.f:1274-1279): huge TOL(1)
+    r = run_sprsol('ref', rs, sm, b, iop=1, tol1=0.9)
+    o = run_sprsol('orc', rs, sm, b, iop=1, tol1=0.9)
+    assert r['ierr'] == o['ierr'] == -3
+    assert r['mspar'][26] == o['mspar'][26]
+    assert r['mspar'][25] == o['mspar'][25]
+    assert np.array_equal(r['tol'], o['tol'])
