@@ -1,0 +1,81 @@
+/*
+ * spr_b200.h -- C ABI of the B200 numeric phase of SAM's SPR sparse solver.
+ *
+ * Drop-in entry points (gfortran/ifort-Linux naming: lower case + trailing
+ * underscore, every argument by reference, no hidden CHARACTER lengths).
+ * SPR_INT is int64_t for libspr_b200.so (the default SPR_I8 build,
+ * -fdefault-integer-8, src/SPR/CMakeLists.txt:12-29) and int32_t for
+ * libspr_b200_i4.so (BUILD_SPR_INTEGER8=OFF).  The caller owns every array;
+ * SM is overwritten by the factor ([D(NEQ) | L(NZEROL)], d on each column's
+ * diagonal as in the reference), B by the solution.  IERR, MSPAR(1),
+ * MSPAR(26) (NUMNEG) and MSPAR(27) (SUPEQT) and TOL(2:3) follow the
+ * reference routines cited below.
+ */
+#ifndef SPR_B200_H
+#define SPR_B200_H
+
+#include <stdint.h>
+
+#ifndef SPR_INT
+#define SPR_INT int64_t
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces SPRSOL, src/SPR/sprsol.f:5-52.  IOP<=3 factor, 2<=IOP<=5 forward,
+ * IOP>=3 and IOP/=5 back substitution. */
+void sprsol_(const SPR_INT* iop, SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm,
+             double* b, const SPR_INT* ldb, const SPR_INT* nrhs, double* tol, SPR_INT* iwork,
+             double* rwork, const SPR_INT* lpu, SPR_INT* ierr);
+
+/* Replaces SPRFC1, src/SPR/sprfc1.f:5-283 (LDL' factorisation).  MVMULT and
+ * MMMULT are the reference's LMVY18/LMMY18 (lmvy18.f:5, lmmy18.f:5); the GPU
+ * path always applies the LDL' update they define, so they are not called. */
+void sprfc1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* tol,
+             SPR_INT* iwork, double* rwork, const SPR_INT* lpu, SPR_INT* ierr,
+             void (*mvmult)(), void (*mmmult)());
+
+/* Replaces SPRFS1, src/SPR/sprfs1.f:5-263 (forward reduction + D^-1). */
+void sprfs1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
+             const SPR_INT* ldb, const SPR_INT* nrhs, SPR_INT* iwork, double* rwork,
+             const SPR_INT* lpu, SPR_INT* ierr);
+
+/* Replaces SPRBS1, src/SPR/sprbs1.f:5-248 (back substitution). */
+void sprbs1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
+             const SPR_INT* ldb, const SPR_INT* nrhs, double* rwork, const SPR_INT* lpu,
+             SPR_INT* ierr);
+
+/* ---- device-level API (no reference counterpart: the reference has no
+ * device memory; these let a caller keep SM and B resident in HBM) ---- */
+
+/* Builds the execution plan for one SPR structure (arrays as produced by
+ * SPRTRS/SPRSMB/SPRPMP, sprtrs.f:5, sprsmb.f:5, sprpmp.f:5).  0 on success. */
+int spr_b200_open(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                  void** handle);
+void spr_b200_close(void* handle);
+/* Runs subsequent work on the given cudaStream_t. */
+int spr_b200_set_stream(void* handle, void* stream);
+/* Factorises device SM in place (semantics of SPRF11, sprfc1.f:286-713).
+ * out[0]=TOL(2) out[1]=TOL(3) out[2]=NUMNEG out[3]=SUPEQT out[4]=LIERR
+ * (0, -30 pivot below TOL(1), -35 exact zero diagonal). */
+int spr_b200_factor_dev(void* handle, double* d_sm, double tol1, double* out);
+/* Forward (which=1, SPRFS3 sprfs1.f:266), back (which=2, SPRBS4 sprbs1.f:251)
+ * or both (3) on device B (ldb x nrhs, column-major) with device SM. */
+int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ldb,
+                       int64_t nrhs, int which);
+/* info[0]=RINFO(3) factor flops [1]=solve flops per RHS [2]=front arena bytes
+ * [3]=tree levels [4]=last factor ms [5]=last solve ms [6]=launches of the
+ * last factorisation [7]=Schur-update launches. */
+int spr_b200_info(void* handle, double* info);
+/* Host-only plan build + self-check (no GPU needed); see abi.cpp. */
+int spr_b200_plan_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                        double* out);
+/* Frees every device context cached by the Fortran entry points. */
+void spr_b200_release_all(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPR_B200_H */

@@ -495,6 +495,39 @@ int SPR_API(spr_b200_info)(void* handle, double* info) {
     return 0;
 }
 
+// Host-only: builds the plan and self-checks it (no GPU needed).
+// out[0]=rc [1]=NSUPER [2]=levels [3]=arena doubles [4]=buffers out of bounds
+// [5]=overlapping live buffers [6]=factor flops (RINFO(3)) [7]=solve flops
+// [8]=small fronts [9]=large fronts [10]=jobs
+int SPR_API(spr_b200_plan_check)(const I* mspar, const I* mtrees, const I* msifa, double* out) {
+    std::vector<int64_t> ms(60, 0);
+    for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
+    std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
+    sprb::Plan p;
+    const int rc = sprb::build_plan(ms.data(), mt.data(), mf.data(), p);
+    for (int i = 0; i < 11; ++i) out[i] = 0.0;
+    out[0] = rc;
+    if (rc != 0) return rc;
+    int64_t oob = 0, ov = 0;
+    sprb::check_plan(p, oob, ov);
+    int64_t nsmall = 0, nlarge = 0;
+    for (const auto& lp : p.levels) {
+        nsmall += (int64_t)lp.small_nodes.size();
+        nlarge += (int64_t)lp.large_nodes.size();
+    }
+    out[1] = (double)p.nsuper;
+    out[2] = (double)p.levels.size();
+    out[3] = (double)p.arena_doubles;
+    out[4] = (double)oob;
+    out[5] = (double)ov;
+    out[6] = p.factor_flops;
+    out[7] = p.solve_flops;
+    out[8] = (double)nsmall;
+    out[9] = (double)nlarge;
+    out[10] = (double)p.jobs.size();
+    return 0;
+}
+
 // Releases every cached context (device memory of the Fortran entry points).
 void SPR_API(spr_b200_release_all)(void) {
     std::lock_guard<std::mutex> lk(g_mu);

@@ -28,6 +28,7 @@ public:
         }
         int64_t off = top_;
         top_ += n;
+        peak_ = std::max(peak_, top_);
         return off;
     }
     void release(int64_t off, int64_t n) {
@@ -55,11 +56,12 @@ public:
             free_.erase(it);
         }
     }
-    int64_t top() const { return top_; }
+    int64_t peak() const { return peak_; }
 
 private:
     std::map<int64_t, int64_t> free_;
     int64_t top_ = 0;
+    int64_t peak_ = 0;
 };
 
 inline int32_t round_up4(int32_t x) { return (x + 3) / 4 * 4; }
@@ -217,7 +219,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 arena.release(P.buf_off[c], buf_size[c]);
             }
     }
-    P.arena_doubles = arena.top();
+    P.arena_doubles = arena.peak();
     // ---- batched launches of the large path
     P.jobs.clear();
     auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };
@@ -279,6 +281,38 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         close_launch(lp.writeback);
     }
     return 0;
+}
+
+int64_t buffer_doubles(const Plan& P, int64_t js) {
+    const int64_t f = P.F[js], s = P.S[js];
+    return (f <= kSmallMaxF) ? (f - s) * (f - s) : (int64_t)P.buf_ld[js] * f;
+}
+
+// Every buffer inside the arena, and no two buffers that are live at the same
+// level (from the node's own level to its parent's) overlap.
+void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps) {
+    oob = 0;
+    overlaps = 0;
+    const int64_t ns = P.nsuper;
+    for (int64_t js = 0; js < ns; ++js)
+        if (P.buf_off[js] < 0 || P.buf_off[js] + buffer_doubles(P, js) > P.arena_doubles) ++oob;
+    const int32_t nlev = (int32_t)P.levels.size();
+    std::vector<std::vector<int32_t>> live(nlev);
+    for (int64_t js = 0; js < ns; ++js) {
+        const int32_t l0 = P.level[js];
+        const int32_t l1 = P.parent[js] >= 0 ? P.level[P.parent[js]] : l0;
+        for (int32_t L = l0; L <= l1; ++L) live[L].push_back((int32_t)js);
+    }
+    for (int32_t L = 0; L < nlev; ++L) {
+        std::vector<std::pair<int64_t, int64_t>> iv;
+        for (int32_t js : live[L]) {
+            const int64_t n = buffer_doubles(P, js);
+            if (n > 0) iv.emplace_back(P.buf_off[js], P.buf_off[js] + n);
+        }
+        std::sort(iv.begin(), iv.end());
+        for (size_t k = 1; k < iv.size(); ++k)
+            if (iv[k].first < iv[k - 1].second) ++overlaps;
+    }
 }
 
 }  // namespace sprb

@@ -85,4 +85,10 @@ struct Plan {
 // negative code when the structure is inconsistent (mirrors IERR=-2 checks).
 int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa, Plan& plan);
 
+// Size in doubles of a node's device buffer (update matrix or dense front).
+int64_t buffer_doubles(const Plan& P, int64_t js);
+// Self-check of the arena layout: counts buffers outside the arena and
+// overlaps between buffers that are live at the same level.
+void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps);
+
 }  // namespace sprb

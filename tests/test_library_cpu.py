@@ -1,0 +1,53 @@
+"""CPU checks of the product library: it loads, exports the declared ABI,
+and its host-side plan is self-consistent (no GPU is touched)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import sam_lib_b200 as spr
+from conftest import ref_system
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, 'include', 'spr_b200.h')).read()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'\b(spr\w+_|spr_b200_\w+)\s*\(', text)))
+
+
+@pytest.mark.parametrize('kind', [8, 4])
+def test_library_exports_declared_abi(kind):
+    lib = spr.load(kind)
+    syms = declared_symbols()
+    assert {'sprsol_', 'sprfc1_', 'sprfs1_', 'sprbs1_'} <= set(syms)
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+@pytest.mark.parametrize('n', [3, 6, 12])
+def test_plan_self_check(n):
+    rs, _ = ref_system(n)
+    out = np.zeros(11)
+    rc = spr.load(8).spr_b200_plan_check(rs.mspar.ctypes.data_as(C.c_void_p),
+                                         rs.mtrees.ctypes.data_as(C.c_void_p),
+                                         rs.msifa.ctypes.data_as(C.c_void_p),
+                                         out.ctypes.data_as(C.c_void_p))
+    assert rc == 0 and out[0] == 0
+    assert out[1] == rs.mspar[10]                 # NSUPER
+    assert out[4] == 0, 'buffers outside the arena'
+    assert out[5] == 0, 'live buffers overlap'
+    assert abs(out[6] - rs.rinfo[2]) <= 1e-12 * rs.rinfo[2]   # RINFO(3)
+
+
+def test_plan_check_i4_abi():
+    rs, _ = ref_system(6)
+    out = np.zeros(11)
+    m4 = [a.astype(np.int32) for a in (rs.mspar, rs.mtrees, rs.msifa)]
+    rc = spr.load(4).spr_b200_plan_check(*[a.ctypes.data_as(C.c_void_p) for a in m4],
+                                         out.ctypes.data_as(C.c_void_p))
+    assert rc == 0 and out[4] == 0 and out[5] == 0
+    assert abs(out[6] - rs.rinfo[2]) <= 1e-12 * rs.rinfo[2]
