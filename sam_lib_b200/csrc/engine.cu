@@ -692,6 +692,183 @@ k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int
 }
 
 // ---------------------------------------------------------------------------
+// Solves of the large fronts: batched like the factorisation, one launch per
+// panel step for all large fronts of a level.  L is read from LNZ (packed).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ const double* lcol(const PV& P, int js, int F, int j) {
+    return P.lnz + P.lnz_off[js] + lnz_col(j, F) - j;      // index with the row
+}
+
+// gather of the forward sweep: own rows of B plus the children's update vectors
+__global__ void k_fwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+                             const double* b, int64_t ldb, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int i = (int)(task - jb.task0);
+    const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const int64_t e0 = P.cptr[P.rbase[js] + i], e1 = P.cptr[P.rbase[js] + i + 1];
+    for (int r = 0; r < nrhs; ++r) {
+        double v = (i < S) ? b[(int64_t)(fst + i) + r * ldb] : 0.0;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int c = P.cchild[e], t = P.ct[e];
+            v += vbuf[P.rbase[c] * nrhs + (int64_t)r * P.F[c] + P.S[c] + t];
+        }
+        w[(int64_t)r * F + i] = v;
+    }
+}
+
+// unit-lower triangle of one diagonal block: one warp per front
+__global__ void k_fwd_diag(const Job* jobs, PV P, double* vbuf, int nrhs) {
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const int lane = threadIdx.x;
+    for (int j = k0; j < k1; ++j) {
+        const double* cj = lcol(P, js, F, j);
+        for (int i = j + 1 + lane; i < k1; i += 32) {
+            const double l = cj[i];
+            for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= w[(int64_t)r * F + j] * l;
+        }
+        __syncwarp();
+    }
+}
+
+// rows below the block: w[i] -= L[i, block] y_block, one thread per row
+__global__ void __launch_bounds__(kTRSMRows) k_fwd_update(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                          int nrhs) {
+    __shared__ double y[kNB][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    const int F = P.F[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    for (int e = threadIdx.x; e < nb * nrhs; e += blockDim.x) {
+        const int c = e % nb, r = e / nb;
+        y[c][r] = w[(int64_t)r * F + k0 + c];
+    }
+    __syncthreads();
+    const int i = jb.c0 + (int)(task - jb.task0) * kTRSMRows + threadIdx.x;
+    if (i >= F) return;
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
+    const double* base = P.lnz + P.lnz_off[js];
+    for (int c = 0; c < nb; ++c) {
+        const double l = base[lnz_col(k0 + c, F) - (k0 + c) + i];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) acc[r] -= l * y[c][r];
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) w[(int64_t)r * F + i] = acc[r];
+}
+
+// y_j /= d_j and scatter of the own rows (thread per column)
+__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, double* b,
+                             int64_t ldb, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int j = (int)(task - jb.task0);
+    const int F = P.F[js], fst = P.fst[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const double d = lcol(P, js, F, j)[j];
+    for (int r = 0; r < nrhs; ++r) {
+        const double y = w[(int64_t)r * F + j] / d;
+        w[(int64_t)r * F + j] = y;
+        b[(int64_t)(fst + j) + r * ldb] = y;
+    }
+}
+
+// gather of the back sweep: own rows (forward result) and ancestors' solution
+__global__ void k_bwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+                             const double* b, int64_t ldb, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int i = (int)(task - jb.task0);
+    const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const int row = (i < S) ? (fst + i) : P.rows[P.rbase[js] + i];
+    for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = b[(int64_t)row + r * ldb];
+}
+
+// w[c] -= sum over rows [lo, hi) of L[i,c] w[i]; one warp per column c
+__device__ __forceinline__ void warp_col_dot(const PV& P, int js, int F, int c, int lo, int hi, double* w,
+                                             int nrhs) {
+    const int lane = threadIdx.x & 31;
+    const double* cc = lcol(P, js, F, c);
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    for (int i = lo + lane; i < hi; i += 32) {
+        const double l = cc[i];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) acc[r] += l * w[(int64_t)r * F + i];
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) {
+        if (r >= nrhs) break;
+        double v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) w[(int64_t)r * F + c] -= v;
+    }
+}
+
+// rectangle: contributions of the update rows [S, F) to every column c < S
+__global__ void k_bwd_rect(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, int nrhs) {
+    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int c = (int)(task - jb.task0);
+    const int F = P.F[js], S = P.S[js];
+    warp_col_dot(P, js, F, c, S, F, vbuf + P.rbase[js] * nrhs, nrhs);
+}
+
+// diagonal block of the back sweep, bottom-up: one warp per front
+__global__ void k_bwd_diag(const Job* jobs, PV P, double* vbuf, int nrhs) {
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js];
+    double* w = vbuf + P.rbase[js] * nrhs;
+    for (int c = k1 - 1; c >= k0; --c) {
+        warp_col_dot(P, js, F, c, c + 1, k1, w, nrhs);
+        __syncwarp();
+    }
+}
+
+// columns m < k0 receive the solved block: warp per column
+__global__ void k_bwd_update(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, int nrhs) {
+    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int m = (int)(task - jb.task0);
+    const int F = P.F[js];
+    warp_col_dot(P, js, F, m, jb.k_lo, jb.k_hi, vbuf + P.rbase[js] * nrhs, nrhs);
+}
+
+__global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* vbuf, double* b,
+                             int64_t ldb, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int j = (int)(task - jb.task0);
+    const int F = P.F[js], fst = P.fst[js];
+    const double* w = vbuf + P.rbase[js] * nrhs;
+    for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = w[(int64_t)r * F + j];
+}
+
+// ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
 Engine::Engine() : d_(new Dev()) {}
@@ -921,18 +1098,53 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
         const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
         double* b = d_b + r0 * ldb;
+        const Job* jobs = D.jobs;
+        auto blocks = [](int64_t threads) { return (int)((threads + 255) / 256); };
         if (which & 1) {
             for (size_t L = 0; L < P_.levels.size(); ++L) {
-                if (D.all_count[L] == 0) continue;
-                k_forward<<<(int)D.all_count[L], kSolveThreads, 0, s>>>(D.all_nodes + D.all_begin[L], pv, D.vbuf, b,
-                                                                        ldb, nr);
+                const LevelPlan& lp = P_.levels[L];
+                if (!lp.small_nodes.empty())
+                    k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(D.level_nodes + D.small_begin[L],
+                                                                                pv, D.vbuf, b, ldb, nr);
+                if (lp.large_nodes.empty()) continue;
+                const Launch& ga = lp.assemble;
+                k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
+                                                               D.vbuf, b, ldb, nr);
+                for (size_t st = 0; st < lp.panel.size(); ++st) {
+                    const Launch& pl = lp.panel[st];
+                    k_fwd_diag<<<(int)pl.job_count, 32, 0, s>>>(jobs + pl.job_begin, pv, D.vbuf, nr);
+                    if (pl.ntasks > 0)
+                        k_fwd_update<<<(int)pl.ntasks, kTRSMRows, 0, s>>>(jobs + pl.job_begin, pl.job_count, pv,
+                                                                          D.vbuf, nr);
+                }
+                const Launch& wb = lp.writeback;
+                k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                                                               D.vbuf, b, ldb, nr);
             }
         }
         if (which & 2) {
             for (size_t L = P_.levels.size(); L-- > 0;) {
-                if (D.all_count[L] == 0) continue;
-                k_backward<<<(int)D.all_count[L], kSolveThreads, 0, s>>>(D.all_nodes + D.all_begin[L], pv, D.vbuf, b,
-                                                                         ldb, nr);
+                const LevelPlan& lp = P_.levels[L];
+                if (!lp.small_nodes.empty())
+                    k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(
+                        D.level_nodes + D.small_begin[L], pv, D.vbuf, b, ldb, nr);
+                if (lp.large_nodes.empty()) continue;
+                const Launch& ga = lp.assemble;
+                k_bwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
+                                                               D.vbuf, b, ldb, nr);
+                const Launch& wb = lp.writeback;
+                k_bwd_rect<<<blocks(wb.ntasks * 32), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                                                                  D.vbuf, nr);
+                for (size_t st = lp.panel.size(); st-- > 0;) {
+                    const Launch& pl = lp.panel[st];
+                    k_bwd_diag<<<(int)pl.job_count, 32, 0, s>>>(jobs + pl.job_begin, pv, D.vbuf, nr);
+                    const Launch& bu = lp.bwd_update[st];
+                    if (bu.ntasks > 0)
+                        k_bwd_update<<<blocks(bu.ntasks * 32), 256, 0, s>>>(jobs + bu.job_begin, bu.job_count,
+                                                                            bu.ntasks, pv, D.vbuf, nr);
+                }
+                k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                                                               D.vbuf, b, ldb, nr);
             }
         }
     }

@@ -50,6 +50,7 @@ struct LevelPlan {
     std::vector<Launch> panel, inner;         // per panel step
     Launch outer;                             // update block, K = S
     Launch writeback;                         // S columns -> LNZ
+    std::vector<Launch> bwd_update;           // back solve: columns [0, k0) of each step
 };
 
 struct Plan {
