@@ -91,6 +91,7 @@ struct Engine::Dev {
     double* sn_faila = nullptr;
     Stats* st = nullptr;
     double* vbuf = nullptr;                      // solve front vectors
+    double* vbuf2 = nullptr;                     // solved diagonal blocks (same layout)
     int64_t vbuf_rhs = 0;
     double* bbuf = nullptr;                      // contiguous copy of B (ldb = NEQ)
     int64_t bbuf_rhs = 0;
@@ -720,47 +721,53 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     }
 }
 
-// unit-lower triangle of one diagonal block: one warp per front
-__global__ void k_fwd_diag(const Job* jobs, PV P, double* vbuf, int nrhs) {
-    const Job& jb = jobs[blockIdx.x];
-    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
-    const int F = P.F[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
-    const int lane = threadIdx.x;
-    for (int j = k0; j < k1; ++j) {
-        const double* cj = lcol(P, js, F, j);
-        for (int i = j + 1 + lane; i < k1; i += 32) {
-            const double l = cj[i];
-            for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= w[(int64_t)r * F + j] * l;
-        }
-        __syncwarp();
-    }
-}
-
-// rows below the block: w[i] -= L[i, block] y_block, one thread per row
-__global__ void __launch_bounds__(kTRSMRows) k_fwd_update(const Job* jobs, int64_t njobs, PV P, double* vbuf,
-                                                          int nrhs) {
-    __shared__ double y[kNB][kMaxRHS];
+// One forward step of a large front: every CTA loads the unit-lower
+// diagonal block L11 and the block of w into shared memory and solves it
+// (redundantly; 64x64 is cheap), CTA 0 of the job stores the solved block in
+// ysol, the others update kTRSMRows rows below it (SPRFS5 + SPRFS6).
+__global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                        double* ysol, int nrhs) {
+    __shared__ double Ls[kNB][kNB + 1];
+    __shared__ double yb[kNB][kMaxRHS];
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
-    for (int e = threadIdx.x; e < nb * nrhs; e += blockDim.x) {
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+        const int i = e % nb, j = e / nb;
+        if (i > j) Ls[i][j] = base[lnz_col(k0 + j, F) - (k0 + j) + (k0 + i)];
+    }
+    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int c = e % nb, r = e / nb;
-        y[c][r] = w[(int64_t)r * F + k0 + c];
+        yb[c][r] = w[(int64_t)r * F + k0 + c];
     }
     __syncthreads();
-    const int i = jb.c0 + (int)(task - jb.task0) * kTRSMRows + threadIdx.x;
+    for (int j = 0; j < nb - 1; ++j) {
+        if (tid > j && tid < nb)
+            for (int r = 0; r < nrhs; ++r) yb[tid][r] -= yb[j][r] * Ls[tid][j];
+        __syncthreads();
+    }
+    const int64_t u = task - jb.task0;
+    if (u == 0) {
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            ysol[vb + (int64_t)r * F + k0 + c] = yb[c][r];
+        }
+        return;
+    }
+    const int i = jb.c0 + (int)(u - 1) * kTRSMRows + tid;
     if (i >= F) return;
     double acc[kMaxRHS];
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
-    const double* base = P.lnz + P.lnz_off[js];
     for (int c = 0; c < nb; ++c) {
         const double l = base[lnz_col(k0 + c, F) - (k0 + c) + i];
 #pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) acc[r] -= l * y[c][r];
+        for (int r = 0; r < kMaxRHS; ++r) acc[r] -= l * yb[c][r];
     }
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r)
@@ -768,7 +775,7 @@ __global__ void __launch_bounds__(kTRSMRows) k_fwd_update(const Job* jobs, int64
 }
 
 // y_j /= d_j and scatter of the own rows (thread per column)
-__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, double* b,
+__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* ysol, double* b,
                              int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
@@ -776,13 +783,9 @@ __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     const int js = jb.node;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
+    const double* y = ysol + P.rbase[js] * nrhs;
     const double d = lcol(P, js, F, j)[j];
-    for (int r = 0; r < nrhs; ++r) {
-        const double y = w[(int64_t)r * F + j] / d;
-        w[(int64_t)r * F + j] = y;
-        b[(int64_t)(fst + j) + r * ldb] = y;
-    }
+    for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = y[(int64_t)r * F + j] / d;
 }
 
 // gather of the back sweep: own rows (forward result) and ancestors' solution
@@ -833,30 +836,65 @@ __global__ void k_bwd_rect(const Job* jobs, int64_t njobs, int64_t ntasks, PV P,
     warp_col_dot(P, js, F, c, S, F, vbuf + P.rbase[js] * nrhs, nrhs);
 }
 
-// diagonal block of the back sweep, bottom-up: one warp per front
-__global__ void k_bwd_diag(const Job* jobs, PV P, double* vbuf, int nrhs) {
-    const Job& jb = jobs[blockIdx.x];
-    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+// One back step of a large front: every CTA loads L11 and the block of w,
+// solves L11' x = w (redundantly, column-oriented in shared memory); CTA 0
+// stores x in xsol, the others apply x to kBwdCols columns m < k0 each
+// (one warp per column: w[m] -= L[k0:k1, m]' x), SPRBS6 in blocked form.
+__global__ void __launch_bounds__(256) k_bwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                  double* xsol, int nrhs) {
+    __shared__ double Ls[kNB][kNB + 1];
+    __shared__ double xb[kNB][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
-    for (int c = k1 - 1; c >= k0; --c) {
-        warp_col_dot(P, js, F, c, c + 1, k1, w, nrhs);
-        __syncwarp();
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+        const int i = e % nb, j = e / nb;
+        if (i > j) Ls[i][j] = base[lnz_col(k0 + j, F) - (k0 + j) + (k0 + i)];
+    }
+    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+        const int c = e % nb, r = e / nb;
+        xb[c][r] = w[(int64_t)r * F + k0 + c];
+    }
+    __syncthreads();
+    for (int c = nb - 1; c > 0; --c) {
+        if (tid < c)
+            for (int r = 0; r < nrhs; ++r) xb[tid][r] -= Ls[c][tid] * xb[c][r];
+        __syncthreads();
+    }
+    const int64_t u = task - jb.task0;
+    if (u == 0) {
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            xsol[vb + (int64_t)r * F + k0 + c] = xb[c][r];
+        }
+        return;
+    }
+    const int m = (int)(u - 1) * kBwdCols + warp;
+    if (m >= k0) return;
+    const double* cm = base + lnz_col(m, F) - m;       // column m, indexed by row
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    for (int c = lane; c < nb; c += 32) {
+        const double l = cm[k0 + c];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) acc[r] += l * xb[c][r];
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) {
+        if (r >= nrhs) break;
+        double v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) w[(int64_t)r * F + m] -= v;
     }
 }
 
-// columns m < k0 receive the solved block: warp per column
-__global__ void k_bwd_update(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, int nrhs) {
-    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
-    const int js = jb.node;
-    const int m = (int)(task - jb.task0);
-    const int F = P.F[js];
-    warp_col_dot(P, js, F, m, jb.k_lo, jb.k_hi, vbuf + P.rbase[js] * nrhs, nrhs);
-}
-
-__global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* vbuf, double* b,
+__global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* xsol, double* b,
                              int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
@@ -864,7 +902,7 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     const int js = jb.node;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
-    const double* w = vbuf + P.rbase[js] * nrhs;
+    const double* w = xsol + P.rbase[js] * nrhs;
     for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = w[(int64_t)r * F + j];
 }
 
@@ -878,6 +916,7 @@ Engine::~Engine() {
     for (void* p : d_->owned) cudaFree(p);
     if (d_->arena) cudaFree(d_->arena);
     if (d_->vbuf) cudaFree(d_->vbuf);
+    if (d_->vbuf2) cudaFree(d_->vbuf2);
     if (d_->bbuf) cudaFree(d_->bbuf);
     if (d_->ev0) cudaEventDestroy(d_->ev0);
     if (d_->ev1) cudaEventDestroy(d_->ev1);
@@ -1081,8 +1120,11 @@ void Engine::ensure_vectors(int64_t nrhs) {
     Dev& D = *d_;
     if (D.vbuf_rhs < nrhs) {
         if (D.vbuf) cudaFree(D.vbuf);
-        D.vbuf = nullptr;
-        cudaMalloc((void**)&D.vbuf, std::max<int64_t>(P_.rbase.back(), 1) * nrhs * sizeof(double));
+        if (D.vbuf2) cudaFree(D.vbuf2);
+        D.vbuf = D.vbuf2 = nullptr;
+        const size_t bytes = std::max<int64_t>(P_.rbase.back(), 1) * nrhs * sizeof(double);
+        if (cudaMalloc((void**)&D.vbuf, bytes) != cudaSuccess || cudaMalloc((void**)&D.vbuf2, bytes) != cudaSuccess)
+            return;
         D.vbuf_rhs = nrhs;
     }
 }
@@ -1093,7 +1135,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     PV pv = make_view(D, P_, const_cast<double*>(d_sm), 0.0);
     const int64_t chunk = std::min<int64_t>(nrhs, kMaxRHS);
     ensure_vectors(chunk);
-    if (!D.vbuf) return -4;
+    if (!D.vbuf || !D.vbuf2) return -4;
     CK(cudaEventRecord(D.ev0, s));
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
         const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
@@ -1110,16 +1152,14 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 const Launch& ga = lp.assemble;
                 k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
-                for (size_t st = 0; st < lp.panel.size(); ++st) {
-                    const Launch& pl = lp.panel[st];
-                    k_fwd_diag<<<(int)pl.job_count, 32, 0, s>>>(jobs + pl.job_begin, pv, D.vbuf, nr);
-                    if (pl.ntasks > 0)
-                        k_fwd_update<<<(int)pl.ntasks, kTRSMRows, 0, s>>>(jobs + pl.job_begin, pl.job_count, pv,
-                                                                          D.vbuf, nr);
+                for (size_t st = 0; st < lp.fsolve.size(); ++st) {
+                    const Launch& fl = lp.fsolve[st];
+                    k_fwd_step<<<(int)fl.ntasks, kTRSMRows, 0, s>>>(jobs + fl.job_begin, fl.job_count, pv, D.vbuf,
+                                                                    D.vbuf2, nr);
                 }
                 const Launch& wb = lp.writeback;
                 k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
-                                                               D.vbuf, b, ldb, nr);
+                                                               D.vbuf2, b, ldb, nr);
             }
         }
         if (which & 2) {
@@ -1135,16 +1175,13 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 const Launch& wb = lp.writeback;
                 k_bwd_rect<<<blocks(wb.ntasks * 32), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                   D.vbuf, nr);
-                for (size_t st = lp.panel.size(); st-- > 0;) {
-                    const Launch& pl = lp.panel[st];
-                    k_bwd_diag<<<(int)pl.job_count, 32, 0, s>>>(jobs + pl.job_begin, pv, D.vbuf, nr);
-                    const Launch& bu = lp.bwd_update[st];
-                    if (bu.ntasks > 0)
-                        k_bwd_update<<<blocks(bu.ntasks * 32), 256, 0, s>>>(jobs + bu.job_begin, bu.job_count,
-                                                                            bu.ntasks, pv, D.vbuf, nr);
+                for (size_t st = lp.bsolve.size(); st-- > 0;) {
+                    const Launch& bl = lp.bsolve[st];
+                    k_bwd_step<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf, D.vbuf2,
+                                                              nr);
                 }
                 k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
-                                                               D.vbuf, b, ldb, nr);
+                                                               D.vbuf2, b, ldb, nr);
             }
         }
     }

@@ -247,7 +247,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         const int32_t nsteps = (smax + kNB - 1) / kNB;
         lp.panel.assign(nsteps, Launch());
         lp.inner.assign(nsteps, Launch());
-        lp.bwd_update.assign(nsteps, Launch());
+        lp.fsolve.assign(nsteps, Launch());
+        lp.bsolve.assign(nsteps, Launch());
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
@@ -269,14 +270,23 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 add_job(lp.inner[st], Job{js, c0, s, f, k0, k0 + nb, 0}, tiles(c0, s, f));
             }
             close_launch(lp.inner[st]);
-            open_launch(lp.bwd_update[st]);
+            open_launch(lp.fsolve[st]);
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
-                if (k0 >= s || k0 == 0) continue;
+                if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
-                add_job(lp.bwd_update[st], Job{js, 0, k0, f, k0, k0 + nb, 0}, k0);
+                const int64_t nrb = (f - (k0 + nb) + kTRSMRows - 1) / kTRSMRows;
+                add_job(lp.fsolve[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, 1 + nrb);
             }
-            close_launch(lp.bwd_update[st]);
+            close_launch(lp.fsolve[st]);
+            open_launch(lp.bsolve[st]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t nb = std::min(kNB, s - k0);
+                add_job(lp.bsolve[st], Job{js, 0, k0, f, k0, k0 + nb, 0}, 1 + (k0 + kBwdCols - 1) / kBwdCols);
+            }
+            close_launch(lp.bsolve[st]);
         }
         open_launch(lp.outer);
         for (int32_t js : lp.large_nodes) {

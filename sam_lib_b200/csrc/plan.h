@@ -50,8 +50,11 @@ struct LevelPlan {
     std::vector<Launch> panel, inner;         // per panel step
     Launch outer;                             // update block, K = S
     Launch writeback;                         // S columns -> LNZ
-    std::vector<Launch> bwd_update;           // back solve: columns [0, k0) of each step
+    std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
+    std::vector<Launch> bsolve;               // back step: 1 diagonal CTA + column groups [0, k0)
 };
+
+constexpr int kBwdCols = 8;                   // columns per CTA in the back-solve update
 
 struct Plan {
     // sizes
