@@ -238,6 +238,7 @@ int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm) {
     if (c->resident && c->sm_host == sm && c->sm_fp == sm_fingerprint(sm, nsm)) return 0;
     if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return -4;
+    c->eng.invalidate_factor();
     c->sm_host = sm;
     c->sm_fp = sm_fingerprint(sm, nsm);
     c->resident = true;

@@ -67,6 +67,8 @@ struct PV {
     double* sn_faild;
     double* sn_faila;
     Stats* st;
+    const int64_t* linv_off;
+    double* linv;            // inverses of the unit-lower diagonal blocks
     double tol1;
 };
 
@@ -77,6 +79,8 @@ struct Engine::Dev {
     int64_t *lnz_off = nullptr, *rel_off = nullptr, *rbase = nullptr, *cptr = nullptr,
             *buf_off = nullptr, *upd_off = nullptr;
     Job* jobs = nullptr;
+    int64_t* linv_off = nullptr;
+    double* linv = nullptr;
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
     std::vector<int64_t> small_begin;            // per level offset into level_nodes
     int32_t* all_nodes = nullptr;                // all nodes of every level (solves)
@@ -158,11 +162,12 @@ __device__ __forceinline__ bool children_bad(const PV& P, int js) {
 // Pre-pass: original diagonal, zero test, trace (sprfc1.f:465-488)
 // ---------------------------------------------------------------------------
 __global__ void k_prepass(PV P, int64_t nsuper) {
-    for (int64_t js = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; js < nsuper;
-         js += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t js = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; js < nsuper;
+         js += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int s = P.S[js], f = P.F[js], fst = P.fst[js];
         const double* col = P.lnz + P.lnz_off[js];
-        for (int j = 0; j < s; ++j) {
+        for (int j = lane; j < s; j += 32) {
             const double a = col[lnz_col(j, f)];
             P.adiag[fst + j] = a;
             if (a == 0.0) {
@@ -335,22 +340,25 @@ __global__ void k_assemble(const Job* jobs, int64_t njobs, int64_t ntasks, PV P)
     }
 }
 
-// LDL' of one nb x nb diagonal block (right-looking, in shared memory),
-// pivot test / inertia / TOL(2) as SPRF17 (sprfc1.f:1272-1294).
+// LDL' of one nb x nb diagonal block, pivot test / inertia / TOL(2) as
+// SPRF17 (sprfc1.f:1272-1294).  256 threads on a 16x16 grid, each owning
+// rows i = tx + 16a and columns j = ty + 16b of the block; right-looking with
+// the unscaled column (a_ij -= a_ik * a_jk / d_k), scaled to L at the end.
+// Also forms X = L11^-1 (unit lower) for the panel TRSM and the solves.
 __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
+    // A holds L (lower) and, transposed in its strict upper part, X = L^-1
     __shared__ double A[kNB][kNB + 1];
-    __shared__ double w[kNB];
+    __shared__ double rdv[kNB];
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     if (P.sn_bad[js]) return;
     const int ld = P.buf_ld[js], fst = P.fst[js];
     double* front = P.arena + P.buf_off[js];
-    const int tid = threadIdx.x;
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-        const int i = e % nb, j = e / nb;
-        if (i >= j) A[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
-    }
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    for (int j = ty; j < nb; j += 16)
+        for (int i = tx; i < nb; i += 16)
+            if (i >= j) A[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
     __syncthreads();
     int neg = 0;
     double tmax = 0.0;
@@ -366,23 +374,45 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         if (d < 0.0) ++neg;
         tmax = fmax(tmax, ad / d);
         const double rd = 1.0 / d;
-        for (int i = k + 1 + tid; i < nb; i += blockDim.x) {
-            w[i] = A[i][k];
-            A[i][k] = A[i][k] * rd;
-        }
-        __syncthreads();
-        const int m = nb - k - 1;
-        for (int e = tid; e < m * m; e += blockDim.x) {
-            const int ii = e % m, jj = e / m;
-            if (ii >= jj) A[k + 1 + ii][k + 1 + jj] -= w[k + 1 + ii] * A[k + 1 + jj][k];
+        if (tid == 0) rdv[k] = rd;
+#pragma unroll
+        for (int a = 0; a < kNB / 16; ++a) {
+            const int i = tx + 16 * a;
+            if (i > k && i < nb) {
+                const double aik = A[i][k] * rd;
+#pragma unroll
+                for (int b = 0; b < kNB / 16; ++b) {
+                    const int j = ty + 16 * b;
+                    if (j > k && j <= i) A[i][j] -= aik * A[j][k];
+                }
+            }
         }
         __syncthreads();
     }
     if (failed < 0) {
-        for (int e = tid; e < nb * nb; e += blockDim.x) {
-            const int i = e % nb, j = e / nb;
-            if (i >= j) front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld] = A[i][j];
+        // L below the diagonal, d on it
+        for (int j = ty; j < nb; j += 16)
+            for (int i = tx; i < nb; i += 16)
+                if (i > j) A[i][j] *= rdv[j];
+        __syncthreads();
+        // X = L^-1 by columns: X[j][j] = 1, X[i][j] = -sum_{m=j}^{i-1} L[i][m] X[m][j];
+        // X[i][j] (i > j) is kept at A[j][i]
+        if (tid < nb) {
+            const int j = tid;
+            for (int i = j + 1; i < nb; ++i) {
+                double acc = -A[i][j];
+                for (int m = j + 1; m < i; ++m) acc -= A[i][m] * A[j][m];
+                A[j][i] = acc;
+            }
         }
+        __syncthreads();
+        double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
+        for (int j = ty; j < kNB; j += 16)
+            for (int i = tx; i < kNB; i += 16)
+                lv[i + j * kNB] = (i < nb && j < nb) ? (i > j ? A[j][i] : (i == j ? 1.0 : 0.0)) : 0.0;
+        for (int j = ty; j < nb; j += 16)
+            for (int i = tx; i < nb; i += 16)
+                if (i >= j) front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld] = A[i][j];
         for (int k = tid; k < nb; k += blockDim.x) P.dvec[fst + k0 + k] = A[k][k];
     }
     if (tid == 0) {
@@ -392,15 +422,26 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     }
 }
 
-// Panel TRSM: rows below the diagonal block, L21 = A21 L11^-T D^-1.
-// One CTA of kTRSMRows threads per row block, one thread per row.
-constexpr size_t kTrsmSmem = sizeof(double) * ((size_t)kNB * (kNB + 1) + (size_t)kNB * kTRSMRows + kNB);
+namespace gemm {
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+}  // namespace gemm
 
-__global__ void __launch_bounds__(kTRSMRows) k_trsm(const Job* jobs, int64_t njobs, PV P) {
+// Panel TRSM as a product with the stored inverse: for a 64-row block of the
+// rows below the diagonal block, W = A21 X' (X = L11^-1), L21 = W D^-1.
+// 128 threads = 2x2 warps of 32x32 DMMA tiles; the block is read completely
+// into shared memory before it is overwritten, so the update is in place.
+constexpr int kTrsmLds = kNB + 4;
+constexpr size_t kTrsmSmem = sizeof(double) * (2 * (size_t)kNB * kTrsmLds + kNB);
+
+__global__ void __launch_bounds__(128) k_trsm(const Job* jobs, int64_t njobs, PV P) {
     extern __shared__ double tsh[];
-    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(tsh);
-    double(*W)[kTRSMRows] = reinterpret_cast<double(*)[kTRSMRows]>(tsh + kNB * (kNB + 1));
-    double* rd = tsh + kNB * (kNB + 1) + kNB * kTRSMRows;
+    double(*As)[kTrsmLds] = reinterpret_cast<double(*)[kTrsmLds]>(tsh);              // As[m][i]
+    double(*Xs)[kTrsmLds] = reinterpret_cast<double(*)[kTrsmLds]>(tsh + kNB * kTrsmLds);  // Xs[m][c] = X[c][m]
+    double* rd = tsh + 2 * kNB * kTrsmLds;
     if (P.st->any_fail) return;
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
@@ -409,24 +450,76 @@ __global__ void __launch_bounds__(kTRSMRows) k_trsm(const Job* jobs, int64_t njo
     const int F = P.F[js], ld = P.buf_ld[js];
     const int r0 = jb.c0 + (int)(task - jb.task0) * kTRSMRows;
     double* front = P.arena + P.buf_off[js];
+    const double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int i = e % kNB, m = e / kNB;
+        As[m][i] = (m < nb && r0 + i < F) ? front[(int64_t)(r0 + i) + (int64_t)(k0 + m) * ld] : 0.0;
+        Xs[m][i] = lv[i + m * kNB];          // X[i][m]: row i (output column), col m
+    }
+    for (int c = tid; c < kNB; c += blockDim.x)
+        rd[c] = (c < nb) ? 1.0 / front[(int64_t)(k0 + c) * (ld + 1)] : 0.0;
+    __syncthreads();
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll 4
+    for (int k4 = 0; k4 < kNB; k4 += 4) {
+        const int kk = k4 + (lane & 3);
+        double av[4], bv[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) av[mi] = As[kk][wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) bv[ni] = Xs[kk][wn + ni * 8 + (lane >> 2)];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) gemm::dmma(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+        const int r = r0 + wm + mi * 8 + (lane >> 2);
+        if (r >= F) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = wn + ni * 8 + 2 * (lane & 3) + h;
+                if (c < nb) front[(int64_t)r + (int64_t)(k0 + c) * ld] = acc[mi][ni][h] * rd[c];
+            }
+    }
+}
+
+// Inverse of the unit-lower diagonal blocks straight from LNZ (used when the
+// factor in SM was not produced by this engine, e.g. a solve-only call).
+__global__ void __launch_bounds__(64) k_linv(const Job* jobs, PV P) {
+    __shared__ double L[kNB][kNB + 1];      // L strictly lower, X = L^-1 transposed above
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    const int F = P.F[js];
+    const double* base = P.lnz + P.lnz_off[js];
     const int tid = threadIdx.x;
     for (int e = tid; e < nb * nb; e += blockDim.x) {
         const int i = e % nb, j = e / nb;
-        if (i > j) L[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
+        if (i > j) L[i][j] = base[lnz_col(k0 + j, F) - (k0 + j) + (k0 + i)];
     }
-    for (int k = tid; k < nb; k += blockDim.x)
-        rd[k] = 1.0 / front[(int64_t)(k0 + k) * (ld + 1)];
-    const int i = r0 + tid;
-    const bool live = i < F;
-    if (live)
-        for (int c = 0; c < nb; ++c) W[c][tid] = front[(int64_t)i + (int64_t)(k0 + c) * ld];
     __syncthreads();
-    if (!live) return;
-    for (int c = 0; c < nb; ++c) {
-        double acc = W[c][tid];
-        for (int m = 0; m < c; ++m) acc -= W[m][tid] * L[c][m];
-        W[c][tid] = acc;
-        front[(int64_t)i + (int64_t)(k0 + c) * ld] = acc * rd[c];
+    if (tid < nb) {
+        const int j = tid;
+        for (int i = j + 1; i < nb; ++i) {
+            double acc = -L[i][j];
+            for (int m = j + 1; m < i; ++m) acc -= L[i][m] * L[j][m];
+            L[j][i] = acc;
+        }
+    }
+    __syncthreads();
+    double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int i = e % kNB, j = e / kNB;
+        lv[e] = (i < nb && j < nb) ? (i > j ? L[j][i] : (i == j ? 1.0 : 0.0)) : 0.0;
     }
 }
 
@@ -446,11 +539,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
 }  // namespace gemm
 
 __global__ void __launch_bounds__(128) k_gemm(const Job* jobs, int64_t njobs, PV P) {
@@ -721,14 +809,14 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     }
 }
 
-// One forward step of a large front: every CTA loads the unit-lower
-// diagonal block L11 and the block of w into shared memory and solves it
-// (redundantly; 64x64 is cheap), CTA 0 of the job stores the solved block in
-// ysol, the others update kTRSMRows rows below it (SPRFS5 + SPRFS6).
+// One forward step of a large front.  Every CTA computes the solved block
+// y = X w_block with the stored inverse X = L11^-1 (a 64x64 product in
+// shared memory, no sequential chain); CTA 0 of the job stores y in ysol,
+// the others update kTRSMRows rows below the block (SPRFS5 + SPRFS6).
 __global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
                                                         double* ysol, int nrhs) {
-    __shared__ double Ls[kNB][kNB + 1];
-    __shared__ double yb[kNB][kMaxRHS];
+    __shared__ double Xs[kNB][kNB + 1];
+    __shared__ double wb[kNB][kMaxRHS];
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -736,21 +824,32 @@ __global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t
     const int64_t vb = P.rbase[js] * nrhs;
     double* w = vbuf + vb;
     const double* base = P.lnz + P.lnz_off[js];
+    const double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
     const int tid = threadIdx.x;
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-        const int i = e % nb, j = e / nb;
-        if (i > j) Ls[i][j] = base[lnz_col(k0 + j, F) - (k0 + j) + (k0 + i)];
-    }
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
     for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int c = e % nb, r = e / nb;
-        yb[c][r] = w[(int64_t)r * F + k0 + c];
+        wb[c][r] = w[(int64_t)r * F + k0 + c];
     }
     __syncthreads();
-    for (int j = 0; j < nb - 1; ++j) {
-        if (tid > j && tid < nb)
-            for (int r = 0; r < nrhs; ++r) yb[tid][r] -= yb[j][r] * Ls[tid][j];
-        __syncthreads();
+    double sol[kMaxRHS];
+    if (tid < nb) {
+        const int c = tid;
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) {
+            double acc = 0.0;
+            if (r < nrhs)
+                for (int m = 0; m <= c; ++m) acc += Xs[c][m] * wb[m][r];
+            sol[r] = acc;
+        }
     }
+    __syncthreads();
+    if (tid < nb)
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) wb[tid][r] = sol[r];
+    __syncthreads();
+    double(*yb)[kMaxRHS] = wb;
     const int64_t u = task - jb.task0;
     if (u == 0) {
         for (int e = tid; e < nb * nrhs; e += blockDim.x) {
@@ -764,10 +863,12 @@ __global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t
     double acc[kMaxRHS];
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
+#pragma unroll 8
     for (int c = 0; c < nb; ++c) {
         const double l = base[lnz_col(k0 + c, F) - (k0 + c) + i];
 #pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) acc[r] -= l * yb[c][r];
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) acc[r] -= l * yb[c][r];
     }
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r)
@@ -836,14 +937,14 @@ __global__ void k_bwd_rect(const Job* jobs, int64_t njobs, int64_t ntasks, PV P,
     warp_col_dot(P, js, F, c, S, F, vbuf + P.rbase[js] * nrhs, nrhs);
 }
 
-// One back step of a large front: every CTA loads L11 and the block of w,
-// solves L11' x = w (redundantly, column-oriented in shared memory); CTA 0
-// stores x in xsol, the others apply x to kBwdCols columns m < k0 each
-// (one warp per column: w[m] -= L[k0:k1, m]' x), SPRBS6 in blocked form.
+// One back step of a large front: every CTA forms x = X' w_block with the
+// stored inverse; CTA 0 stores x in xsol, the others apply x to kBwdCols
+// columns m < k0 each (one warp per column: w[m] -= L[k0:k1, m]' x),
+// SPRBS6 in blocked form.
 __global__ void __launch_bounds__(256) k_bwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
                                                   double* xsol, int nrhs) {
-    __shared__ double Ls[kNB][kNB + 1];
-    __shared__ double xb[kNB][kMaxRHS];
+    __shared__ double Xs[kNB][kNB + 1];
+    __shared__ double wb[kNB][kMaxRHS];
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -851,21 +952,32 @@ __global__ void __launch_bounds__(256) k_bwd_step(const Job* jobs, int64_t njobs
     const int64_t vb = P.rbase[js] * nrhs;
     double* w = vbuf + vb;
     const double* base = P.lnz + P.lnz_off[js];
+    const double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-        const int i = e % nb, j = e / nb;
-        if (i > j) Ls[i][j] = base[lnz_col(k0 + j, F) - (k0 + j) + (k0 + i)];
-    }
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
     for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int c = e % nb, r = e / nb;
-        xb[c][r] = w[(int64_t)r * F + k0 + c];
+        wb[c][r] = w[(int64_t)r * F + k0 + c];
     }
     __syncthreads();
-    for (int c = nb - 1; c > 0; --c) {
-        if (tid < c)
-            for (int r = 0; r < nrhs; ++r) xb[tid][r] -= Ls[c][tid] * xb[c][r];
-        __syncthreads();
+    double sol[kMaxRHS];
+    if (tid < nb) {
+        const int c = tid;
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) {
+            double acc = 0.0;
+            if (r < nrhs)
+                for (int m = c; m < nb; ++m) acc += Xs[m][c] * wb[m][r];
+            sol[r] = acc;
+        }
     }
+    __syncthreads();
+    if (tid < nb)
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) wb[tid][r] = sol[r];
+    __syncthreads();
+    double(*xb)[kMaxRHS] = wb;
     const int64_t u = task - jb.task0;
     if (u == 0) {
         for (int e = tid; e < nb * nrhs; e += blockDim.x) {
@@ -883,7 +995,8 @@ __global__ void __launch_bounds__(256) k_bwd_step(const Job* jobs, int64_t njobs
     for (int c = lane; c < nb; c += 32) {
         const double l = cm[k0 + c];
 #pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) acc[r] += l * xb[c][r];
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) acc[r] += l * xb[c][r];
     }
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) {
@@ -934,8 +1047,11 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         dev_upload(o, &D.buf_ld, P_.buf_ld) || dev_upload(o, &D.lnz_off, P_.lnz_off) ||
         dev_upload(o, &D.rel_off, P_.rel_off) || dev_upload(o, &D.rbase, P_.rbase) ||
         dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
-        dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs))
+        dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs) ||
+        dev_upload(o, &D.linv_off, P_.linv_off))
         return -4;
+    CK(cudaMalloc((void**)&D.linv, std::max<int64_t>(P_.linv_doubles, 1) * sizeof(double)));
+    o.push_back(D.linv);
     std::vector<int32_t> small, all;
     D.small_begin.clear();
     D.all_begin.clear();
@@ -1003,6 +1119,8 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.sn_faild = D.sn_faild;
     v.sn_faila = D.sn_faila;
     v.st = D.st;
+    v.linv_off = D.linv_off;
+    v.linv = D.linv;
     v.tol1 = tol1;
     return v;
 }
@@ -1011,6 +1129,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     Dev& D = *d_;
     cudaStream_t s = stream_;
     PV pv = make_view(D, P_, d_sm, tol1);
+    linv_valid_ = false;
     Stats init{};
     init.first_zero = 0x7fffffff;
     CK(cudaMemcpyAsync(D.st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
@@ -1021,7 +1140,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     timing.gemm_launches = 0;
     timing.launches = 0;
     CK(cudaEventRecord(D.ev0, s));
-    k_prepass<<<(int)std::min<int64_t>((P_.nsuper + 255) / 256, 1184), 256, 0, s>>>(pv, P_.nsuper);
+    k_prepass<<<(int)std::min<int64_t>((P_.nsuper * 32 + 255) / 256, 4736), 256, 0, s>>>(pv, P_.nsuper);
     k_reduce<false><<<1, 1024, 0, s>>>(D.adiag, P_.neq, &D.st->trace);
     timing.launches += 2;
     std::vector<cudaEvent_t> gev;
@@ -1047,7 +1166,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
             k_diag<<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             ++timing.launches;
             if (pl.ntasks > 0) {
-                k_trsm<<<(int)pl.ntasks, kTRSMRows, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, pv);
+                k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, pv);
                 ++timing.launches;
             }
             const Launch& il = lp.inner[st];
@@ -1110,6 +1229,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
         res.tol3 = fa;
         return 0;
     }
+    linv_valid_ = true;
     res.numneg = hs.numneg;
     res.tol2 = (hs.tol2 != 0.0) ? 1.0 / hs.tol2 : 0.0;          // sprfc1.f:699-703
     res.tol3 = (hs.mindpos != 0.0) ? hs.trace / hs.mindpos : 0.0;  // sprfc1.f:704-708
@@ -1137,6 +1257,12 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     ensure_vectors(chunk);
     if (!D.vbuf || !D.vbuf2) return -4;
     CK(cudaEventRecord(D.ev0, s));
+    if (!linv_valid_) {
+        for (const LevelPlan& lp : P_.levels)
+            for (const Launch& pl : lp.panel)
+                if (pl.job_count > 0) k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
+        linv_valid_ = true;
+    }
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
         const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
         double* b = d_b + r0 * ldb;

@@ -39,6 +39,10 @@ public:
     int factor(double* d_sm, double tol1, FactorResult& res);
     // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
     int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
+    // The solves use the inverses of the diagonal blocks that factor() stores;
+    // after SM was replaced by a factor from elsewhere, call this so the next
+    // solve rebuilds them from LNZ.
+    void invalidate_factor() { linv_valid_ = false; }
     // Timing of the Schur-update kernels can be switched on (events around each launch).
     void set_profile(bool on) { profile_ = on; }
     Timing timing;
@@ -50,6 +54,7 @@ private:
     Plan P_;
     cudaStream_t stream_ = nullptr;
     bool profile_ = false;
+    bool linv_valid_ = false;
     std::unique_ptr<Dev> d_;
 };
 

@@ -220,6 +220,13 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
     }
     P.arena_doubles = arena.peak();
+    P.linv_off.assign(ns, -1);
+    P.linv_doubles = 0;
+    for (int64_t js = 0; js < ns; ++js)
+        if (P.F[js] > kSmallMaxF) {
+            P.linv_off[js] = P.linv_doubles;
+            P.linv_doubles += (int64_t)((P.S[js] + kNB - 1) / kNB) * kNB * kNB;
+        }
     // ---- batched launches of the large path
     P.jobs.clear();
     auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };

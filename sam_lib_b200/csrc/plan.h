@@ -19,7 +19,7 @@ namespace sprb {
 
 constexpr int kSmallMaxF = 176;     // fronts up to this order: one CTA, shared memory
 constexpr int kNB = 64;             // panel width of the blocked LDL' for large fronts
-constexpr int kTRSMRows = 128;      // rows per CTA in the panel (TRSM) kernel
+constexpr int kTRSMRows = 64;       // rows per CTA in the panel (TRSM) kernel
 constexpr int kTile = 64;           // Schur-update tile (rows x cols)
 constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
 
@@ -76,6 +76,10 @@ struct Plan {
     std::vector<int32_t> buf_ld;             // leading dimension of the front / update buffer
     std::vector<int64_t> upd_off;            // per node: where its update matrix (F-S)^2 starts
     int64_t arena_doubles = 0;
+    // inverses of the unit-lower diagonal blocks of the large fronts: block st
+    // of node js is the column-major kNB x kNB matrix at linv_off[js] + st*kNB*kNB
+    std::vector<int64_t> linv_off;
+    int64_t linv_doubles = 0;
     bool any_large = false;
     // levels and tasks
     std::vector<LevelPlan> levels;
