@@ -1,0 +1,350 @@
+#!/usr/bin/env python3
+"""Factor + solve benchmark of the SPR numeric phase on B200.
+
+Workload (one step): the numeric phase of SPR on the 48^3 hex8 elasticity box
+(E=1, nu=0.3, face x=0 clamped, 345,744 equations), i.e. the LDL'
+factorisation of SM plus forward/diagonal/back solves of 4 right-hand sides
+U[-1,1] (seed 1).  The symbolic structure is the reference's own (its MMD
+ordering, supernodes and symbolic factorisation, committed as
+tests/golden/structures/hex48.npz); SM is assembled by the library's SPRADM
+main add.  Synthetic, seeded data; no dataset is involved.
+
+  value  : GFLOP/s of factor+solve = (RINFO(3) + NRHS*RINFO(4)) / t, with SM
+           and B resident in HBM (device API), CUDA events on the engine's
+           stream, max over ranks; N>1 runs independent replicas (weak).
+  e2e    : the same metric through the Fortran-ABI call sprsol_(IOP=3) with
+           pinned host SM and B (H2D of SM, factor, D2H of the factor into SM,
+           H2D/D2H of B inside the timed region).
+  --impl reference : the reference's own CPU implementation (the translated
+           Fortran SPR from the oracle build) on all host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'factor+solve s & GFLOP/s, 350k-DOF hex elasticity; mixed+IR vs FP64 @1e-12'
+UNIT = 'GFLOP/s'
+N_MESH = 48
+NRHS = 4
+SAMPLE_N = 20          # bounded CPU sample: the 20^3 box of the same family
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--n', type=int, default=N_MESH)
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    return ap.parse_args()
+
+
+def config(n=N_MESH):
+    return {'workload': 'SPR numeric phase, %d^3 hex8 elasticity (E=1, nu=0.3, x=0 clamped), '
+                        'LDL\' factor + %d RHS solve' % (n, NRHS),
+            'mesh': '%dx%dx%d' % (n, n, n), 'nrhs': NRHS, 'rhs': 'U[-1,1] seed 1',
+            'ordering': 'reference MMD + supernodes (bit-exact structure)',
+            'l2': 'inputs larger than L2 (SM is %s)' % ('9.1 GB' if n == 48 else 'n^3-sized'),
+            'parallelism': 'replicas'}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference SPR path on a bounded sample (oracle build; baseline only)
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    n, reps = args
+    from oracle.refpipe import RefSystem
+    from sam_lib_b200.fe import HexBox, hex8_stiffness
+    rs = RefSystem(HexBox(n))
+    ke = hex8_stiffness()
+    sm0 = rs.assemble(lambda e: ke)
+    b0 = np.asfortranarray(np.random.default_rng(1).uniform(-1.0, 1.0, size=(rs.neq, NRHS)))
+    flops = float(rs.rinfo[2] + NRHS * (2.0 * rs.rinfo[3] + rs.neq))
+    times = []
+    for _ in range(reps):
+        sm = sm0.copy()
+        b = b0.copy(order='F')
+        t = time.perf_counter()
+        ierr, _, _ = rs.sprsol(3, sm, b)
+        times.append(time.perf_counter() - t)
+        assert ierr == 0
+    return flops, times
+
+
+def cpu_sample(nproc, reps):
+    """GFLOP/s of the reference SPRSOL(IOP=3) on the 20^3 sample, nproc processes."""
+    import multiprocessing as mp
+    if nproc == 1:
+        flops, times = _cpu_worker((SAMPLE_N, reps))
+        return flops, [times]
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_cpu_worker, [(SAMPLE_N, reps)] * nproc)
+    return res[0][0], [r[1] for r in res]
+
+
+def sample_desc(cores):
+    return ('reference SPRSOL IOP=3 (factor + %d-RHS solve) on the %d^3 hex8 box (26,460 eq) of the '
+            'same family, machine-translated Fortran SPR built with gcc -O2, %d process%s' %
+            (NRHS, SAMPLE_N, cores, '' if cores == 1 else 'es'))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.QUERY,
+                                       '--format=csv,noheader,nounits', '-lms', '200'],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(',') for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == 'active':
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': mx, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def dgemm_peak(torch):
+    """Measured cuBLAS DGEMM throughput (TFLOP/s): the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    b = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / ms / 1e9
+
+
+def read_traffic():
+    """dram bytes per Schur-update flop from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, 'profiles', 'k_gemm_traffic.txt')
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith('dram_bytes_per_flop'):
+            return float(line.split('=')[1])
+    return None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    nproc = os.cpu_count() or 1
+    flops, times = cpu_sample(nproc, args.warmup + args.steps)
+    per_step = [max(t[s] for t in times) for s in range(args.warmup, args.warmup + args.steps)]
+    t = float(np.mean(per_step))
+    value = nproc * flops / t / 1e9
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded hex8 meshes)',
+            'config': config(args.n),
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': nproc, 'kind': 'reference',
+                             'sample': sample_desc(nproc)},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    # CPU baseline first (rank 0, N=1 only), before the GPU is touched
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        flops_s, times = cpu_sample(1, 1)
+        t = times[0][0]
+        cpu = {'value': flops_s / t / 1e9, 'unit': UNIT, 'cores': 1, 'kind': 'reference',
+               'sample': sample_desc(1), 'sample_s': t}
+    import torch
+    import sam_lib_b200 as spr
+    from sam_lib_b200.system import HexSystem
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    hs = HexSystem(args.n)
+    sm = hs.assemble()
+    neq, nzerol = hs.neq, hs.nzerol
+    f = np.random.default_rng(1).uniform(-1.0, 1.0, size=(NRHS, neq))
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    stream = torch.cuda.Stream()
+    ds.set_stream(stream.cuda_stream)
+    d_sm0 = torch.from_numpy(sm).cuda()
+    d_sm = torch.empty_like(d_sm0)
+    d_b0 = torch.from_numpy(f).cuda()
+    d_b = torch.empty_like(d_b0)
+    info = ds.info()
+    flops = info['factor_flops'] + NRHS * info['solve_flops']
+
+    def step(timed):
+        with torch.cuda.stream(stream):
+            d_sm.copy_(d_sm0)
+            d_b.copy_(d_b0)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = ds.factor(d_sm)
+        ds.solve(d_sm, d_b, NRHS)
+        e1.record(stream)
+        e1.synchronize()
+        assert r['lierr'] == 0 and r['numneg'] == 0, r
+        inf = ds.info()
+        return e0.elapsed_time(e1), inf
+
+    for _ in range(args.warmup):
+        step(False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    ds.set_profile(True)
+    times, gemm_ms, fac_ms, sol_ms, launches = [], [], [], [], 0
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        ms, inf = step(True)
+        times.append(ms)
+        gemm_ms.append(inf['gemm_ms'])
+        fac_ms.append(inf['factor_ms'])
+        sol_ms.append(inf['solve_ms'])
+        launches += int(inf['launches'] + inf['solve_launches'])
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    ds.set_profile(False)
+    ms_step = float(np.mean(times))
+    if dist:
+        t = torch.tensor([ms_step], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * flops / (ms_step / 1e3) / 1e9
+    # accuracy of the last step: ||K x - f|| / ||f|| per RHS
+    x = d_b.cpu().numpy()
+    res = [float(np.linalg.norm(hs.matvec(x[r]) - f[r]) / np.linalg.norm(f[r])) for r in range(NRHS)]
+    # end to end through the Fortran ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        sm_pin0 = torch.from_numpy(sm).pin_memory()
+        sm_pin = torch.empty(sm.shape, dtype=torch.float64, pin_memory=True)
+        b_pin0 = torch.from_numpy(f.copy()).pin_memory()           # (NRHS, NEQ) == B(NEQ, NRHS)
+        b_pin = torch.empty(f.shape, dtype=torch.float64, pin_memory=True)
+        mspar = hs.mspar.copy()
+        e2e_t = []
+        for k in range(1 + min(args.steps, 3)):
+            sm_pin.copy_(sm_pin0)
+            b_pin.copy_(b_pin0)
+            smv, bv = sm_pin.numpy(), b_pin.numpy().T
+            tol = np.array([1.0e-12, 0.0, 0.0])
+            mspar[:] = hs.mspar
+            t = time.perf_counter()
+            ierr = spr.sprsol(3, mspar, hs.mtrees, hs.msifa, smv, bv, neq, NRHS, tol)
+            dt = time.perf_counter() - t
+            assert ierr == 0, ierr
+            if k > 0:                 # the first call also builds the context (plan, buffers)
+                e2e_t.append(dt)
+        spr.release_all()
+        xe = b_pin.numpy()
+        assert np.allclose(xe, x, rtol=1e-9, atol=1e-12)
+        te = float(np.mean(e2e_t))
+        bytes_io = 8 * (neq + nzerol) + 8 * neq * NRHS
+        e2e = {'value': world * flops / te / 1e9, 'unit': UNIT, 'h2d_bytes_per_step': bytes_io,
+               'd2h_bytes_per_step': bytes_io, 's_per_step': te}
+    peak = dgemm_peak(torch)
+    gemm_s = float(np.mean(gemm_ms)) / 1e3
+    achieved = info['gemm_flops'] / gemm_s / 1e12
+    tpf = read_traffic()
+    launches_per_step = inf['gemm_launches']
+    roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+            'frac': achieved / peak,
+            'traffic': (tpf * info['gemm_flops'] / launches_per_step) if tpf else None,
+            'kernel': 'k_gemm: FP64 Schur update C -= L D L\' (mma.sync m8n8k4 f64)',
+            'flops_per_launch': info['gemm_flops'] / launches_per_step,
+            'peak_source': 'measured in-run: cuBLAS DGEMM 8192^3 via torch.matmul float64 '
+                           '(MEASURED_PEAKS.json has no FP64 figure)',
+            'time_share': gemm_s / (ms_step / 1e3)}
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded hex8 mesh, reference structure)',
+                'config': config(args.n),
+                'factor_s': float(np.mean(fac_ms)) / 1e3, 'solve_s': float(np.mean(sol_ms)) / 1e3,
+                'factor_solve_s': ms_step / 1e3, 'factor_flops': info['factor_flops'],
+                'solve_flops_per_rhs': info['solve_flops'], 'residual': max(res),
+                'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches,
+                'clocks': clocks, 'wall_s_timed': t_wall}
+        print(json.dumps(line), flush=True)
+    del ds
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == '__main__':
+    main()

@@ -67,11 +67,24 @@ int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ld
                        int64_t nrhs, int which);
 /* info[0]=RINFO(3) factor flops [1]=solve flops per RHS [2]=front arena bytes
  * [3]=tree levels [4]=last factor ms [5]=last solve ms [6]=launches of the
- * last factorisation [7]=Schur-update launches. */
+ * last factorisation [7]=Schur-update launches [8]=Schur-update ms (profile
+ * mode) [9]=Schur-update algorithmic flops [10]=launches of the last solve
+ * [11]=NZEROL.  info must hold 12 doubles. */
 int spr_b200_info(void* handle, double* info);
+/* Profile mode: CUDA events around every Schur-update launch. */
+int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed); see abi.cpp. */
 int spr_b200_plan_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                         double* out);
+/* Host element assembly into LNZ, the SPRADM/SPRAD2 main add
+ * (src/SPR/spradm.f:818-859) for systems without constraint equations:
+ * SM(NEQ+K) += EM(I,J), J=1..NEDOF, I<=J, elements in order (bit-exact with
+ * SPRADM).  EM of element e = em_scale[e]*em, or the e-th matrix of em when
+ * em_scale is NULL.  MEQN as renumbered by SPRTRS/SPREQN (sprtrs.f:3762). */
+int spr_b200_assemble(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                      const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
+                      const SPR_INT* mmnpc, SPR_INT nel, SPR_INT nedof, const double* em,
+                      const double* em_scale, double* sm);
 /* Frees every device context cached by the Fortran entry points. */
 void spr_b200_release_all(void);
 

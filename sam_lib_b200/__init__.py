@@ -43,6 +43,8 @@ def load(int_kind=8):
         lib.spr_b200_solve_dev.restype = C.c_int
         lib.spr_b200_info.argtypes = [vp, vp]
         lib.spr_b200_info.restype = C.c_int
+        lib.spr_b200_set_profile.argtypes = [vp, C.c_int]
+        lib.spr_b200_set_profile.restype = C.c_int
         lib.spr_b200_release_all.argtypes = []
         lib.spr_b200_release_all.restype = None
         _libs[path] = lib
@@ -165,11 +167,14 @@ class DeviceSolver:
             raise RuntimeError('spr_b200_solve_dev failed with %d' % rc)
 
     def info(self):
-        out = np.zeros(8)
+        out = np.zeros(12)
         self.lib.spr_b200_info(self.h, _ptr(out))
         keys = ('factor_flops', 'solve_flops', 'arena_bytes', 'levels', 'factor_ms', 'solve_ms',
-                'launches', 'gemm_launches')
+                'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops', 'solve_launches', 'nzerol')
         return dict(zip(keys, out.tolist()))
+
+    def set_profile(self, on=True):
+        self.lib.spr_b200_set_profile(self.h, 1 if on else 0)
 
     def close(self):
         if self.h:

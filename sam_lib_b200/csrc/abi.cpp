@@ -14,6 +14,7 @@
 // of the factor keep working.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cinttypes>
 #include <cstdio>
 #include <cstring>
@@ -481,7 +482,9 @@ int SPR_API(spr_b200_solve_dev)(void* handle, const double* d_sm, double* d_b, i
 
 // info[0]=RINFO(3) factor flops, [1]=RINFO(4)-style solve flops per RHS,
 // [2]=front arena bytes, [3]=levels, [4]=last factor ms, [5]=last solve ms,
-// [6]=kernel launches of the last factorisation, [7]=Schur-update launches.
+// [6]=kernel launches of the last factorisation, [7]=Schur-update launches,
+// [8]=Schur-update ms (profile mode), [9]=Schur-update algorithmic flops,
+// [10]=kernel launches of the last solve, [11]=NZEROL.
 int SPR_API(spr_b200_info)(void* handle, double* info) {
     Engine* e = static_cast<Engine*>(handle);
     const sprb::Plan& p = e->plan();
@@ -493,6 +496,16 @@ int SPR_API(spr_b200_info)(void* handle, double* info) {
     info[5] = e->timing.solve_ms;
     info[6] = (double)e->timing.launches;
     info[7] = (double)e->timing.gemm_launches;
+    info[8] = e->timing.gemm_ms;
+    info[9] = p.gemm_flops;
+    info[10] = (double)e->timing.solve_launches;
+    info[11] = (double)p.nzerol;
+    return 0;
+}
+
+// Profile mode: CUDA events around every Schur-update launch (spr_b200_info[8]).
+int SPR_API(spr_b200_set_profile)(void* handle, int on) {
+    static_cast<Engine*>(handle)->set_profile(on != 0);
     return 0;
 }
 
@@ -526,6 +539,71 @@ int SPR_API(spr_b200_plan_check)(const I* mspar, const I* mtrees, const I* msifa
     out[8] = (double)nsmall;
     out[9] = (double)nlarge;
     out[10] = (double)p.jobs.size();
+    return 0;
+}
+
+// Element assembly into the packed LNZ of SM: the SPRADM/SPRAD2 main add
+// (src/SPR/spradm.f:818-859) for systems without constraint equations.
+// For every element in order, for J = 1..NEDOF and I = 1..J with both DOFs
+// free, SM(NEQ + K) += EM(I,J), K the LNZ position of (max eq, min eq).
+// EM of element e is em_scale[e] * em (one reference matrix) when em_scale is
+// given, else the e-th NEDOF x NEDOF column-major matrix of em.  Additions
+// happen in the reference's order, so SM matches SPRADM bit for bit.
+// Returns 0, or -3 when an element's DOF count differs from NEDOF.
+int SPR_API(spr_b200_assemble)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
+                               const I* mpmnpc, const I* mmnpc, I nel, I nedof, const double* em,
+                               const double* em_scale, double* sm) {
+    const int64_t neq = mspar[7], nsuper = mspar[10];
+    const I* xsuper = mtrees + (mspar[44] - 1);
+    const I* xlindx = mtrees + (mspar[45] - 1);
+    const I* lindx = msifa + (mspar[46] - 1);
+    const I* xlnz = msifa + (mspar[47] - 1);
+    std::vector<int32_t> colsn(neq);
+    for (int64_t js = 0; js < nsuper; ++js)
+        for (int64_t c = xsuper[js]; c < xsuper[js + 1]; ++c) colsn[c - 1] = (int32_t)js;
+    double* lnz = sm + neq;
+    std::vector<int64_t> eq(nedof);
+    std::vector<double> ems(em_scale ? (size_t)nedof * nedof : 0);
+    for (int64_t e = 0; e < nel; ++e) {
+        int64_t nd = 0;
+        for (int64_t p = mpmnpc[e]; p < mpmnpc[e + 1]; ++p) {
+            const int64_t node = mmnpc[p - 1];
+            for (int64_t d = madof[node - 1]; d < madof[node]; ++d) {
+                if (nd >= nedof) return -3;
+                eq[nd++] = meqn[d - 1];
+            }
+        }
+        if (nd != nedof) return -3;
+        const double* E;
+        if (em_scale) {
+            const double sc = em_scale[e];
+            for (int64_t k = 0; k < nedof * nedof; ++k) ems[k] = sc * em[k];
+            E = ems.data();
+        } else {
+            E = em + e * nedof * nedof;
+        }
+        for (int64_t J = 0; J < nedof; ++J) {
+            const int64_t jeq = eq[J];
+            if (jeq < 1) continue;
+            for (int64_t Iq = 0; Iq <= J; ++Iq) {
+                const int64_t ieq = eq[Iq];
+                if (ieq < 1) continue;
+                const int64_t col = std::min(ieq, jeq), row = std::max(ieq, jeq);
+                const int64_t js = colsn[col - 1];
+                const int64_t F = xlindx[js + 1] - xlindx[js];
+                const I* rows = lindx + (xlindx[js] - 1);
+                int64_t lo = col - xsuper[js], hi = F - 1;      // the row is at or below the column
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if ((int64_t)rows[mid] < row) lo = mid + 1;
+                    else hi = mid;
+                }
+                const int64_t jc = col - xsuper[js];
+                const int64_t k = (xlnz[js] - 1) + jc * F - (jc * (jc - 1)) / 2 + (lo - jc);
+                lnz[k] = lnz[k] + E[Iq + J * nedof];
+            }
+        }
+    }
     return 0;
 }
 

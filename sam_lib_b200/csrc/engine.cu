@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     // A holds L (lower) and, transposed in its strict upper part, X = L^-1
     __shared__ double A[kNB][kNB + 1];
     __shared__ double rdv[kNB];
+    __shared__ double adv[kNB];
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -359,13 +360,14 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     for (int j = ty; j < nb; j += 16)
         for (int i = tx; i < nb; i += 16)
             if (i >= j) A[i][j] = front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld];
+    for (int k = tid; k < nb; k += blockDim.x) adv[k] = P.adiag[fst + k0 + k];
     __syncthreads();
     int neg = 0;
     double tmax = 0.0;
     int failed = -1;
     for (int k = 0; k < nb; ++k) {
         const double d = A[k][k];
-        const double ad = P.adiag[fst + k0 + k];
+        const double ad = adv[k];
         if (fabs(d) <= P.tol1 * fabs(ad)) {
             failed = k;
             if (tid == 0) record_fail(P, js, k0 + k, d, ad);
@@ -1091,6 +1093,13 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     return 0;
 }
 
+static cudaEvent_t record_event(cudaStream_t s) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    return e;
+}
+
 static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     PV v;
     v.fst = D.fst;
@@ -1171,13 +1180,17 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
             }
             const Launch& il = lp.inner[st];
             if (il.ntasks > 0) {
+                if (profile_) gev.push_back(record_event(s));
                 k_gemm<<<(int)il.ntasks, 128, 0, s>>>(jobs + il.job_begin, il.job_count, pv);
+                if (profile_) gev.push_back(record_event(s));
                 ++timing.launches;
                 ++timing.gemm_launches;
             }
         }
         if (lp.outer.ntasks > 0) {
+            if (profile_) gev.push_back(record_event(s));
             k_gemm<<<(int)lp.outer.ntasks, 128, 0, s>>>(jobs + lp.outer.job_begin, lp.outer.job_count, pv);
+            if (profile_) gev.push_back(record_event(s));
             ++timing.launches;
             ++timing.gemm_launches;
         }
@@ -1196,6 +1209,12 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     CK(cudaMemcpyAsync(&hs, D.st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     CK(cudaEventElapsedTime(&timing.factor_ms, D.ev0, D.ev1));
+    for (size_t k = 0; k + 1 < gev.size(); k += 2) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, gev[k], gev[k + 1]);
+        timing.gemm_ms += ms;
+    }
+    for (cudaEvent_t e : gev) cudaEventDestroy(e);
     res = FactorResult();
     if (hs.zero_count > 0) {                       // sprfc1.f:474-488
         // the reference's pre-pass has already replaced D by the original diagonal
@@ -1257,10 +1276,14 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     ensure_vectors(chunk);
     if (!D.vbuf || !D.vbuf2) return -4;
     CK(cudaEventRecord(D.ev0, s));
+    int64_t nl = 0;
     if (!linv_valid_) {
         for (const LevelPlan& lp : P_.levels)
             for (const Launch& pl : lp.panel)
-                if (pl.job_count > 0) k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
+                if (pl.job_count > 0) {
+                    k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
+                    ++nl;
+                }
         linv_valid_ = true;
     }
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
@@ -1271,43 +1294,54 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
         if (which & 1) {
             for (size_t L = 0; L < P_.levels.size(); ++L) {
                 const LevelPlan& lp = P_.levels[L];
-                if (!lp.small_nodes.empty())
+                if (!lp.small_nodes.empty()) {
                     k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(D.level_nodes + D.small_begin[L],
                                                                                 pv, D.vbuf, b, ldb, nr);
+                    ++nl;
+                }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
                 k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
+                ++nl;
                 for (size_t st = 0; st < lp.fsolve.size(); ++st) {
                     const Launch& fl = lp.fsolve[st];
                     k_fwd_step<<<(int)fl.ntasks, kTRSMRows, 0, s>>>(jobs + fl.job_begin, fl.job_count, pv, D.vbuf,
                                                                     D.vbuf2, nr);
+                    ++nl;
                 }
                 const Launch& wb = lp.writeback;
                 k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
+                ++nl;
             }
         }
         if (which & 2) {
             for (size_t L = P_.levels.size(); L-- > 0;) {
                 const LevelPlan& lp = P_.levels[L];
-                if (!lp.small_nodes.empty())
+                if (!lp.small_nodes.empty()) {
                     k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(
                         D.level_nodes + D.small_begin[L], pv, D.vbuf, b, ldb, nr);
+                    ++nl;
+                }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
                 k_bwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
+                ++nl;
                 const Launch& wb = lp.writeback;
                 k_bwd_rect<<<blocks(wb.ntasks * 32), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                   D.vbuf, nr);
+                ++nl;
                 for (size_t st = lp.bsolve.size(); st-- > 0;) {
                     const Launch& bl = lp.bsolve[st];
                     k_bwd_step<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf, D.vbuf2,
                                                               nr);
+                    ++nl;
                 }
                 k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
+                ++nl;
             }
         }
     }
@@ -1315,6 +1349,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     CK(cudaEventElapsedTime(&timing.solve_ms, D.ev0, D.ev1));
+    timing.solve_launches = nl;
     return 0;
 }
 

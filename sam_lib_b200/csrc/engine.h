@@ -23,7 +23,7 @@ struct FactorResult {
 struct Timing {              // CUDA-event times of the last calls (ms)
     float factor_ms = 0.f, solve_ms = 0.f;
     float gemm_ms = 0.f;     // Schur-update kernels only (sum over launches)
-    int64_t gemm_launches = 0, launches = 0;
+    int64_t gemm_launches = 0, launches = 0, solve_launches = 0;
 };
 
 class Engine {

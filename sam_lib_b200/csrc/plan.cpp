@@ -237,6 +237,21 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         l.ntasks += ntask;
     };
     auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
+    P.gemm_flops = 0.0;
+    P.small_flops = 0.0;
+    for (int64_t js = 0; js < ns; ++js)
+        if (P.F[js] <= kSmallMaxF) {
+            const double s = P.S[js], f = P.F[js];
+            P.small_flops += ((f * f) + 2.0 * f) * s - 2.0 * (1.0 + f) * (s * (s + 1.0) / 2.0) +
+                             s * (s + 1.0) * (2.0 * s + 1.0) / 6.0;
+        }
+    // lower-triangle entries of rows [c0, r_end) x columns [c0, c_end), times 2K
+    auto update_flops = [](int32_t c0, int32_t c_end, int32_t r_end, int32_t k) -> double {
+        double e = 0.0;
+        const double n = c_end - c0, r = r_end - c0;
+        e = n * r - n * (n - 1.0) / 2.0;
+        return 2.0 * e * k;
+    };
     auto tiles = [](int32_t c0, int32_t c_end, int32_t r_end) -> int64_t {
         const int64_t nct = (c_end - c0 + kTile - 1) / kTile;
         const int64_t nr = (r_end - c0 + kTile - 1) / kTile;
@@ -275,6 +290,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 const int32_t c0 = k0 + nb;
                 if (c0 >= s) continue;
                 add_job(lp.inner[st], Job{js, c0, s, f, k0, k0 + nb, 0}, tiles(c0, s, f));
+                P.gemm_flops += update_flops(c0, s, f, nb);
             }
             close_launch(lp.inner[st]);
             open_launch(lp.fsolve[st]);
@@ -298,7 +314,10 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         open_launch(lp.outer);
         for (int32_t js : lp.large_nodes) {
             const int32_t s = P.S[js], f = P.F[js];
-            if (f > s) add_job(lp.outer, Job{js, s, f, f, 0, s, 0}, tiles(s, f, f));
+            if (f > s) {
+                add_job(lp.outer, Job{js, s, f, f, 0, s, 0}, tiles(s, f, f));
+                P.gemm_flops += update_flops(s, f, f, s);
+            }
         }
         close_launch(lp.outer);
         open_launch(lp.writeback);

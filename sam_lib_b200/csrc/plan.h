@@ -87,6 +87,8 @@ struct Plan {
     // statistics (the reference's own counters are recomputed for reporting)
     double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
+    double gemm_flops = 0.0;                 // algorithmic flops of the Schur-update launches
+    double small_flops = 0.0;                // factor flops done by the fused small-front kernel
 };
 
 // Builds the plan from the SPR control arrays.  Returns 0 on success or a
