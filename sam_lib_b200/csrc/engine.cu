@@ -525,13 +525,18 @@ __global__ void __launch_bounds__(64) k_linv(const Job* jobs, PV P) {
     }
 }
 
-// Schur update C -= L D L' on 64x64 lower-triangle tiles with FP64 DMMA
-// (mma.sync m8n8k4).  A = rows i of L scaled by D, B = rows j of L.
-// 128 threads = 2x2 warps of 32x32; K staged through shared memory in
-// double-buffered 16-wide slices with cp.async.
+// Schur update C -= L D L' on T x T lower-triangle tiles with FP64 DMMA
+// (mma.sync m8n8k4 f64).  A = rows i of L scaled by D (the scaling is applied
+// to the A fragments), B = rows j of L, both read from the front buffer.
+// Warps of WM x WN; K is staged through shared memory in 16-wide slices with
+// a STAGES-deep cp.async pipeline (16-byte copies of row pairs).
 namespace gemm {
-constexpr int BM = kTile, BN = kTile, BK = 16, LDS = BM + 4;
+constexpr int BK = 16;
 
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(src), "r"(bytes));
+}
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
     const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
     const int sz = valid ? 8 : 0;
@@ -541,23 +546,34 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+template <int T, int WM, int WN, int STAGES>
+struct Cfg {
+    static constexpr int NWM = T / WM, NWN = T / WN, NT = NWM * NWN * 32;
+    static constexpr int LDS = T + 4;                       // bank-conflict-free fragment reads
+    static constexpr int MI = WM / 8, NI = WN / 8;
+    static constexpr size_t smem = sizeof(double) * ((size_t)2 * STAGES * BK * LDS + (size_t)STAGES * BK);
+};
 }  // namespace gemm
 
-__global__ void __launch_bounds__(128) k_gemm(const Job* jobs, int64_t njobs, PV P) {
+template <int T, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__(gemm::Cfg<T, WM, WN, STAGES>::NT)
+k_gemm(const Job* jobs, int64_t njobs, PV P) {
     using namespace gemm;
-    __shared__ __align__(16) double As[2][BK][LDS];
-    __shared__ __align__(16) double Bs[2][BK][LDS];
-    __shared__ double Ds[2][BK];
+    using C = Cfg<T, WM, WN, STAGES>;
+    extern __shared__ __align__(16) double gsh[];
+    double* As = gsh;                                // [STAGES][BK][LDS]
+    double* Bs = As + STAGES * BK * C::LDS;
+    double* Ds = Bs + STAGES * BK * C::LDS;         // [STAGES][BK]
     if (P.st->any_fail) return;
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
     const int js = jb.node;
     if (P.sn_bad[js]) return;
-    const int F = P.F[js], ld = P.buf_ld[js];
+    const int ld = P.buf_ld[js];
     // decode the lower-triangle tile (column tile jt, row tile it >= jt)
     const int64_t u = task - jb.task0;
-    const int nct = (jb.c_end - jb.c0 + BN - 1) / BN;
-    const int nr = (jb.r_end - jb.c0 + BM - 1) / BM;
+    const int nct = (jb.c_end - jb.c0 + T - 1) / T;
+    const int nr = (jb.r_end - jb.c0 + T - 1) / T;
     int lo = 0, hi = nct - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -567,83 +583,107 @@ __global__ void __launch_bounds__(128) k_gemm(const Job* jobs, int64_t njobs, PV
     }
     const int jt = lo;
     const int it = jt + (int)(u - ((int64_t)jt * nr - ((int64_t)jt * (jt - 1)) / 2));
-    const int i0 = jb.c0 + it * BM, j0 = jb.c0 + jt * BN;
+    const int i0 = jb.c0 + it * T, j0 = jb.c0 + jt * T;
     const int r_end = jb.r_end, c_end = jb.c_end;
-    double* front = P.arena + P.buf_off[js];
+    const double* front = P.arena + P.buf_off[js];
+    double* frontw = P.arena + P.buf_off[js];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-    (void)F;
+    const int wm = (warp % C::NWM) * WM, wn = (warp / C::NWM) * WN;
 
-    double acc[4][4][2];
+    double acc[C::MI][C::NI][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < C::MI; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+        for (int b = 0; b < C::NI; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
     const int k_lo = jb.k_lo, k_hi = jb.k_hi;
     const int nk = (k_hi - k_lo + BK - 1) / BK;
+    // 16-byte copies need an even first row (the buffer base and ld are
+    // 32-byte multiples); tiles of jobs starting on an odd column use 8 bytes
+    const bool even = ((i0 | j0) & 1) == 0;
     auto load_stage = [&](int stage, int kt) {
         const int kb = k_lo + kt * BK;
+        double* as = As + stage * BK * C::LDS;
+        double* bs = Bs + stage * BK * C::LDS;
 #pragma unroll
-        for (int e = 0; e < (BM * BK) / 128; ++e) {
-            const int idx = tid + e * 128;
-            const int r = idx % BM, k = idx / BM;
-            const int kk = kb + k;
-            const bool kv = kk < k_hi;
-            const int ra = i0 + r, rb = j0 + r;
-            const double* ga = front + (int64_t)(kv ? kk : k_lo) * ld + (ra < r_end ? ra : i0);
-            const double* gb = front + (int64_t)(kv ? kk : k_lo) * ld + (rb < r_end ? rb : j0);
-            cp_async8(&As[stage][k][r], ga, kv && ra < r_end);
-            cp_async8(&Bs[stage][k][r], gb, kv && rb < r_end);
+        for (int e = 0; e < (T / 2 * BK + C::NT - 1) / C::NT; ++e) {
+            const int idx = tid + e * C::NT;
+            if (idx < T / 2 * BK) {
+                const int pr = idx % (T / 2), k = idx / (T / 2);
+                const int r = 2 * pr, kk = kb + k;
+                const bool kv = kk < k_hi;
+                const int64_t col = (int64_t)(kv ? kk : k_lo) * ld;
+                const int ra = i0 + r, rb = j0 + r;
+                const int na = kv ? max(0, min(2, r_end - ra)) : 0;
+                const int nbb = kv ? max(0, min(2, r_end - rb)) : 0;
+                if (even) {
+                    cp_async16(as + k * C::LDS + r, front + col + (na > 0 ? ra : i0), 8 * na);
+                    cp_async16(bs + k * C::LDS + r, front + col + (nbb > 0 ? rb : j0), 8 * nbb);
+                } else {
+                    cp_async8(as + k * C::LDS + r, front + col + (na > 0 ? ra : i0), na > 0);
+                    cp_async8(as + k * C::LDS + r + 1, front + col + (na > 1 ? ra + 1 : i0), na > 1);
+                    cp_async8(bs + k * C::LDS + r, front + col + (nbb > 0 ? rb : j0), nbb > 0);
+                    cp_async8(bs + k * C::LDS + r + 1, front + col + (nbb > 1 ? rb + 1 : j0), nbb > 1);
+                }
+            }
         }
         if (tid < BK) {
             const int kk = kb + tid;
-            Ds[stage][tid] = kk < k_hi ? front[(int64_t)kk * (ld + 1)] : 0.0;
+            cp_async8(Ds + stage * BK + tid, front + (int64_t)(kk < k_hi ? kk : k_lo) * (ld + 1), kk < k_hi);
         }
-        cp_async_commit();
     };
 
-    load_stage(0, 0);
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; ++st) {
+        if (st < nk) load_stage(st, st);
+        cp_async_commit();
+    }
     for (int kt = 0; kt < nk; ++kt) {
-        const int cur = kt & 1;
-        if (kt + 1 < nk) {
-            load_stage(cur ^ 1, kt + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        cp_async_wait<STAGES - 2>();
         __syncthreads();
+        const int nxt = kt + STAGES - 1;
+        if (nxt < nk) load_stage(nxt % STAGES, nxt);
+        cp_async_commit();
+        const int cur = kt % STAGES;
+        const double* as = As + cur * BK * C::LDS;
+        const double* bs = Bs + cur * BK * C::LDS;
+        const double* ds = Ds + cur * BK;
 #pragma unroll
         for (int k4 = 0; k4 < BK; k4 += 4) {
             const int kk = k4 + (lane & 3);
-            const double dk = Ds[cur][kk];
-            double a[4], b[4];
+            const double dk = ds[kk];
+            double a[C::MI], b[C::NI];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi) a[mi] = As[cur][kk][wm + mi * 8 + (lane >> 2)] * dk;
+            for (int mi = 0; mi < C::MI; ++mi) a[mi] = as[kk * C::LDS + wm + mi * 8 + (lane >> 2)] * dk;
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[cur][kk][wn + ni * 8 + (lane >> 2)];
+            for (int ni = 0; ni < C::NI; ++ni) b[ni] = bs[kk * C::LDS + wn + ni * 8 + (lane >> 2)];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
+            for (int mi = 0; mi < C::MI; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+                for (int ni = 0; ni < C::NI; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
     // epilogue: C -= acc on the lower part, inside [.., r_end) x [.., c_end)
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
+    for (int mi = 0; mi < C::MI; ++mi) {
         const int r = i0 + wm + mi * 8 + (lane >> 2);
         if (r >= r_end) continue;
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
+        for (int ni = 0; ni < C::NI; ++ni) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int c = j0 + wn + ni * 8 + 2 * (lane & 3) + h;
-                if (c < c_end && r >= c) front[(int64_t)r + (int64_t)c * ld] -= acc[mi][ni][h];
+                if (c < c_end && r >= c) frontw[(int64_t)r + (int64_t)c * ld] -= acc[mi][ni][h];
             }
         }
     }
 }
+
+using GemmBig = gemm::Cfg<kTileBig, 64, 32, 3>;
+using GemmSmall = gemm::Cfg<kTile, 32, 32, 3>;
+#define K_GEMM_BIG k_gemm<kTileBig, 64, 32, 3>
+#define K_GEMM_SMALL k_gemm<kTile, 32, 32, 3>
 
 // Store the S factored columns of a dense front into LNZ (sprfc1.f:630-637).
 __global__ void k_writeback(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {
@@ -1090,6 +1130,8 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     if ((size_t)smem_max < need) return -4;
     CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
+    CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     return 0;
 }
 
@@ -1132,6 +1174,19 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.linv = D.linv;
     v.tol1 = tol1;
     return v;
+}
+
+void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev) {
+    if (l.ntasks <= 0) return;
+    if (profile_) gev.push_back(record_event(s));
+    const Job* jobs = d_->jobs + l.job_begin;
+    if (l.tile == kTileBig)
+        K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, pv);
+    else
+        K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, pv);
+    if (profile_) gev.push_back(record_event(s));
+    ++timing.launches;
+    ++timing.gemm_launches;
 }
 
 int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
@@ -1178,22 +1233,9 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
                 k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, pv);
                 ++timing.launches;
             }
-            const Launch& il = lp.inner[st];
-            if (il.ntasks > 0) {
-                if (profile_) gev.push_back(record_event(s));
-                k_gemm<<<(int)il.ntasks, 128, 0, s>>>(jobs + il.job_begin, il.job_count, pv);
-                if (profile_) gev.push_back(record_event(s));
-                ++timing.launches;
-                ++timing.gemm_launches;
-            }
+            for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
         }
-        if (lp.outer.ntasks > 0) {
-            if (profile_) gev.push_back(record_event(s));
-            k_gemm<<<(int)lp.outer.ntasks, 128, 0, s>>>(jobs + lp.outer.job_begin, lp.outer.job_count, pv);
-            if (profile_) gev.push_back(record_event(s));
-            ++timing.launches;
-            ++timing.gemm_launches;
-        }
+        for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
         {
             const Launch& l = lp.writeback;
             const int64_t threads = l.ntasks * 32;

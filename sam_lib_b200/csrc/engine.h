@@ -49,6 +49,7 @@ public:
     struct Dev;              // device copies of the plan and work buffers
 
 private:
+    void launch_gemm(const Launch& l, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     void upload_plan();
     void ensure_vectors(int64_t nrhs);
     Plan P_;

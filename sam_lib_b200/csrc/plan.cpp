@@ -230,11 +230,11 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     // ---- batched launches of the large path
     P.jobs.clear();
     auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };
-    auto add_job = [&](Launch& l, Job j, int64_t ntask) {
-        if (ntask <= 0) return;
+    auto add_job = [&](Launch& l, Job j, int64_t ntask, bool keep_empty = false) {
+        if (ntask <= 0 && !keep_empty) return;
         j.task0 = l.ntasks;
         P.jobs.push_back(j);
-        l.ntasks += ntask;
+        l.ntasks += std::max<int64_t>(ntask, 0);
     };
     auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
     P.gemm_flops = 0.0;
@@ -252,9 +252,9 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         e = n * r - n * (n - 1.0) / 2.0;
         return 2.0 * e * k;
     };
-    auto tiles = [](int32_t c0, int32_t c_end, int32_t r_end) -> int64_t {
-        const int64_t nct = (c_end - c0 + kTile - 1) / kTile;
-        const int64_t nr = (r_end - c0 + kTile - 1) / kTile;
+    auto tiles_t = [](int32_t c0, int32_t c_end, int32_t r_end, int32_t t) -> int64_t {
+        const int64_t nct = (c_end - c0 + t - 1) / t;
+        const int64_t nr = (r_end - c0 + t - 1) / t;
         return nct * nr - nct * (nct - 1) / 2;
     };
     for (int32_t L = 0; L < nlev; ++L) {
@@ -268,9 +268,26 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (int32_t js : lp.large_nodes) smax = std::max(smax, P.S[js]);
         const int32_t nsteps = (smax + kNB - 1) / kNB;
         lp.panel.assign(nsteps, Launch());
-        lp.inner.assign(nsteps, Launch());
+        lp.update.assign(nsteps, std::vector<Launch>());
         lp.fsolve.assign(nsteps, Launch());
         lp.bsolve.assign(nsteps, Launch());
+        // Schur-update jobs of one step, split into a big-tile and a small-tile launch
+        auto emit_updates = [&](std::vector<Job>& jl, std::vector<Launch>& out) {
+            for (int pass = 0; pass < 2; ++pass) {
+                const int32_t tile = pass == 0 ? kTileBig : kTile;
+                Launch l;
+                l.tile = tile;
+                open_launch(l);
+                for (const Job& j : jl) {
+                    const bool big = (j.r_end - j.c0) >= 4 * kTileBig;
+                    if (big != (pass == 0)) continue;
+                    add_job(l, j, tiles_t(j.c0, j.c_end, j.r_end, tile));
+                }
+                close_launch(l);
+                l.tile = tile;
+                if (l.ntasks > 0) out.push_back(l);
+            }
+        };
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
@@ -279,20 +296,27 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
                 const int64_t nrb = (f - (k0 + nb) + kTRSMRows - 1) / kTRSMRows;
-                add_job(lp.panel[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, 1 + nrb);
+                add_job(lp.panel[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, nrb, true);
             }
             close_launch(lp.panel[st]);
-            open_launch(lp.inner[st]);
+            std::vector<Job> jl;
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
                 const int32_t c0 = k0 + nb;
-                if (c0 >= s) continue;
-                add_job(lp.inner[st], Job{js, c0, s, f, k0, k0 + nb, 0}, tiles(c0, s, f));
-                P.gemm_flops += update_flops(c0, s, f, nb);
+                const int32_t sp0 = (k0 / kSuperPanel) * kSuperPanel;
+                const int32_t sp1 = std::min(sp0 + kSuperPanel, s);
+                if (c0 < sp1) {                                     // inside the super-panel
+                    jl.push_back(Job{js, c0, sp1, f, k0, c0, 0});
+                    P.gemm_flops += update_flops(c0, sp1, f, nb);
+                }
+                if (c0 == sp1 && sp1 < s) {                          // trailing, K = 256
+                    jl.push_back(Job{js, sp1, s, f, sp0, sp1, 0});
+                    P.gemm_flops += update_flops(sp1, s, f, sp1 - sp0);
+                }
             }
-            close_launch(lp.inner[st]);
+            emit_updates(jl, lp.update[st]);
             open_launch(lp.fsolve[st]);
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
@@ -311,15 +335,18 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.bsolve[st]);
         }
-        open_launch(lp.outer);
-        for (int32_t js : lp.large_nodes) {
-            const int32_t s = P.S[js], f = P.F[js];
-            if (f > s) {
-                add_job(lp.outer, Job{js, s, f, f, 0, s, 0}, tiles(s, f, f));
-                P.gemm_flops += update_flops(s, f, f, s);
+        {
+            std::vector<Job> jl;
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (f > s) {
+                    jl.push_back(Job{js, s, f, f, 0, s, 0});
+                    P.gemm_flops += update_flops(s, f, f, s);
+                }
             }
+            lp.outer.clear();
+            emit_updates(jl, lp.outer);
         }
-        close_launch(lp.outer);
         open_launch(lp.writeback);
         for (int32_t js : lp.large_nodes)
             add_job(lp.writeback, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, P.S[js]);

@@ -20,7 +20,9 @@ namespace sprb {
 constexpr int kSmallMaxF = 176;     // fronts up to this order: one CTA, shared memory
 constexpr int kNB = 64;             // panel width of the blocked LDL' for large fronts
 constexpr int kTRSMRows = 64;       // rows per CTA in the panel (TRSM) kernel
-constexpr int kTile = 64;           // Schur-update tile (rows x cols)
+constexpr int kTile = 64;           // Schur-update tile of small updates (rows x cols)
+constexpr int kTileBig = 128;       // Schur-update tile of large updates
+constexpr int kSuperPanel = 256;    // trailing updates are applied per 256 columns (K = 256)
 constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
 
 // A job is one front's share of one batched launch.  Tasks inside a job are
@@ -29,8 +31,13 @@ constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front ass
 //   assembly / write-back : one task per column in [c0, c_end)
 //   panel (TRSM)          : task 0 = diagonal-block CTA, then row blocks of
 //                           kTRSMRows rows starting at c0 (= k_hi)
-//   Schur update          : lower-triangle 64x64 tiles of rows [c0, r_end) x
-//                           columns [c0, c_end), contraction over [k_lo, k_hi)
+//   Schur update          : lower-triangle tiles (Launch::tile) of rows
+//                           [c0, r_end) x columns [c0, c_end), contraction
+//                           over [k_lo, k_hi)
+// Blocked right-looking LDL' of the S fully-summed columns with two levels:
+// 64-wide panels (diagonal block + TRSM) whose updates stay inside their
+// 256-wide super-panel, one K=256 trailing update per super-panel for the
+// remaining fully-summed columns, and one K=S update of the (F-S) block.
 struct Job {
     int32_t node;
     int32_t c0, c_end, r_end;
@@ -40,6 +47,7 @@ struct Job {
 
 struct Launch {                      // a contiguous range of Plan::jobs
     int64_t job_begin = 0, job_count = 0, ntasks = 0;
+    int32_t tile = kTile;            // Schur-update launches: tile size of the decode
 };
 
 struct LevelPlan {
@@ -47,8 +55,9 @@ struct LevelPlan {
     std::vector<int32_t> large_nodes;        // fronts done by the blocked path
     int32_t small_maxF = 0;
     Launch assemble;                          // large fronts: extend-add into dense fronts
-    std::vector<Launch> panel, inner;         // per panel step
-    Launch outer;                             // update block, K = S
+    std::vector<Launch> panel;                // per panel step: diagonal block + TRSM
+    std::vector<std::vector<Launch>> update;  // per panel step: Schur updates (one launch per tile size)
+    std::vector<Launch> outer;                // update block, K = S (one launch per tile size)
     Launch writeback;                         // S columns -> LNZ
     std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
     std::vector<Launch> bsolve;               // back step: 1 diagonal CTA + column groups [0, k0)
