@@ -680,10 +680,19 @@ k_gemm(const Job* jobs, int64_t njobs, PV P) {
     }
 }
 
-using GemmBig = gemm::Cfg<kTileBig, 64, 32, 3>;
-using GemmSmall = gemm::Cfg<kTile, 32, 32, 3>;
-#define K_GEMM_BIG k_gemm<kTileBig, 64, 32, 3>
-#define K_GEMM_SMALL k_gemm<kTile, 32, 32, 3>
+#ifndef SPR_GEMM_BIG_WM
+#define SPR_GEMM_BIG_WM 32
+#endif
+#ifndef SPR_GEMM_BIG_WN
+#define SPR_GEMM_BIG_WN 32
+#endif
+#ifndef SPR_GEMM_STAGES
+#define SPR_GEMM_STAGES 3
+#endif
+using GemmBig = gemm::Cfg<kTileBig, SPR_GEMM_BIG_WM, SPR_GEMM_BIG_WN, SPR_GEMM_STAGES>;
+using GemmSmall = gemm::Cfg<kTile, 32, 32, SPR_GEMM_STAGES>;
+#define K_GEMM_BIG k_gemm<kTileBig, SPR_GEMM_BIG_WM, SPR_GEMM_BIG_WN, SPR_GEMM_STAGES>
+#define K_GEMM_SMALL k_gemm<kTile, 32, 32, SPR_GEMM_STAGES>
 
 // Store the S factored columns of a dense front into LNZ (sprfc1.f:630-637).
 __global__ void k_writeback(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {

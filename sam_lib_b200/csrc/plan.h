@@ -21,7 +21,10 @@ constexpr int kSmallMaxF = 176;     // fronts up to this order: one CTA, shared 
 constexpr int kNB = 64;             // panel width of the blocked LDL' for large fronts
 constexpr int kTRSMRows = 64;       // rows per CTA in the panel (TRSM) kernel
 constexpr int kTile = 64;           // Schur-update tile of small updates (rows x cols)
-constexpr int kTileBig = 128;       // Schur-update tile of large updates
+#ifndef SPR_TILE_BIG
+#define SPR_TILE_BIG 64
+#endif
+constexpr int kTileBig = SPR_TILE_BIG;   // Schur-update tile of large updates
 constexpr int kSuperPanel = 256;    // trailing updates are applied per 256 columns (K = 256)
 constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
 
