@@ -85,6 +85,21 @@ int spr_b200_assemble(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT
                       const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
                       const SPR_INT* mmnpc, SPR_INT nel, SPR_INT nedof, const double* em,
                       const double* em_scale, double* sm);
+/* No counterpart in the reference (SPR never touches device memory).
+ * LDL' of one dense symmetric front on the device, in place, for callers that
+ * must not allocate device memory (an application allocator owns it all, or
+ * an allocation would stall a time-critical loop): d_a (n x n, column-major,
+ * leading dimension lda % 4 == 0, 32-byte aligned, lower triangle used) is
+ * overwritten by L below the diagonal and d on it; d_d (n) receives d.  All
+ * scratch lives in one 5 MiB file-scope __device__ array, so n <= 8192
+ * (else -3); calls that overlap on the GPU race on that array; the first call
+ * on a device resolves its address and should precede any stream capture.
+ * Pivot test, inertia and TOL(2) as SPRF17 (sprfc1.f:1272-1294).
+ * out[0]=NUMNEG out[1]=first failing column (1-based, 0 if none)
+ * out[2]=that pivot out[3]=its original a_jj out[4]=max(a_jj/d_j).
+ * Returns 0, -2 (shape/alignment), -3 (too large) or -4 (CUDA error). */
+int spr_b200_dense_ldlt_noalloc(double* d_a, int64_t n, int64_t lda, double tol1, double* d_d,
+                                void* stream, double* out);
 /* Frees every device context cached by the Fortran entry points. */
 void spr_b200_release_all(void);
 

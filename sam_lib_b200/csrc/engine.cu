@@ -1404,4 +1404,138 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Blocked LDL' of one dense front with caller-provided scratch (no device
+// allocation).  Same kernels and step order as the large-front path of
+// Engine::factor for a front with S = F = n.
+// ---------------------------------------------------------------------------
+size_t dense_scratch_bytes(int64_t n) {
+    const int64_t nblk = (n + kNB - 1) / kNB;
+    const int64_t njobs = 3 * nblk;
+    size_t b = 0;
+    auto add = [&](size_t bytes) { b += (bytes + 255) / 256 * 256; };
+    add(sizeof(Stats));
+    add(sizeof(double) * n);                       // original diagonal
+    add(sizeof(double) * nblk * kNB * kNB);        // inverses of the diagonal blocks
+    add(sizeof(Job) * njobs);
+    add(sizeof(int32_t) * 16);                     // node arrays (one node)
+    add(sizeof(int64_t) * 8);
+    add(sizeof(double) * 4);
+    return b;
+}
+
+int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, double* d, void* scratch,
+                              size_t scratch_bytes, cudaStream_t s, double* out) {
+    if (n <= 0 || lda < n || (lda % 4) != 0 || ((uintptr_t)a % 32) != 0) return -2;
+    if (dense_scratch_bytes(n) > scratch_bytes) return -3;
+    const int64_t nblk = (n + kNB - 1) / kNB;
+    char* p = static_cast<char*>(scratch);
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += (bytes + 255) / 256 * 256;
+        return q;
+    };
+    Stats* st = reinterpret_cast<Stats*>(take(sizeof(Stats)));
+    double* adiag = reinterpret_cast<double*>(take(sizeof(double) * n));
+    double* linv = reinterpret_cast<double*>(take(sizeof(double) * nblk * kNB * kNB));
+    Job* jobs = reinterpret_cast<Job*>(take(sizeof(Job) * 3 * nblk));
+    int32_t* i32 = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 16));
+    int64_t* i64 = reinterpret_cast<int64_t*>(take(sizeof(int64_t) * 8));
+    double* f64 = reinterpret_cast<double*>(take(sizeof(double) * 4));
+    // node arrays: fst, S, F, buf_ld, sn_neg, sn_fail, sn_bad (int32); buf_off, linv_off (int64)
+    int32_t hi32[16] = {0, (int32_t)n, (int32_t)n, (int32_t)lda, 0, -1, 0};
+    int64_t hi64[8] = {0, 0};
+    Stats init{};
+    init.first_zero = 0x7fffffff;
+    // jobs of every step (host side, fixed-size per block, no allocation)
+    struct StepJobs {
+        int64_t panel_begin, panel_tasks, upd_begin, upd_jobs, upd_tasks;
+    };
+    constexpr int kMaxBlocks = 1024;
+    if (nblk > kMaxBlocks) return -3;
+    static thread_local Job hjobs[3 * kMaxBlocks];
+    static thread_local StepJobs steps[kMaxBlocks];
+    int64_t nj = 0;
+    auto tiles = [](int64_t c0, int64_t c_end, int64_t r_end) -> int64_t {
+        const int64_t nct = (c_end - c0 + kTile - 1) / kTile, nr = (r_end - c0 + kTile - 1) / kTile;
+        return nct * nr - nct * (nct - 1) / 2;
+    };
+    for (int64_t stp = 0; stp < nblk; ++stp) {
+        const int32_t k0 = (int32_t)(stp * kNB);
+        const int32_t nb = (int32_t)std::min<int64_t>(kNB, n - k0);
+        const int32_t c0 = k0 + nb;
+        StepJobs& sj = steps[stp];
+        sj.panel_begin = nj;
+        sj.panel_tasks = (n - c0 + kTRSMRows - 1) / kTRSMRows;
+        hjobs[nj++] = Job{0, c0, c0, (int32_t)n, k0, c0, 0};
+        sj.upd_begin = nj;
+        sj.upd_jobs = 0;
+        sj.upd_tasks = 0;
+        const int32_t sp0 = (k0 / kSuperPanel) * kSuperPanel;
+        const int32_t sp1 = (int32_t)std::min<int64_t>(sp0 + kSuperPanel, n);
+        if (c0 < sp1) {
+            hjobs[nj] = Job{0, c0, sp1, (int32_t)n, k0, c0, sj.upd_tasks};
+            sj.upd_tasks += tiles(c0, sp1, n);
+            ++nj;
+            ++sj.upd_jobs;
+        }
+        if (c0 == sp1 && sp1 < n) {
+            hjobs[nj] = Job{0, sp1, (int32_t)n, (int32_t)n, sp0, sp1, sj.upd_tasks};
+            sj.upd_tasks += tiles(sp1, n, n);
+            ++nj;
+            ++sj.upd_jobs;
+        }
+    }
+    CK(cudaMemcpyAsync(jobs, hjobs, sizeof(Job) * nj, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(i32, hi32, sizeof(hi32), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(i64, hi64, sizeof(hi64), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(f64, 0, sizeof(double) * 4, s));
+    // the pivot test compares with the diagonal before factorisation (sprfc1.f:1272-1279)
+    CK(cudaMemcpy2DAsync(adiag, sizeof(double), a, (lda + 1) * sizeof(double), sizeof(double), n,
+                         cudaMemcpyDeviceToDevice, s));
+    PV pv{};
+    pv.fst = i32 + 0;
+    pv.S = i32 + 1;
+    pv.F = i32 + 2;
+    pv.buf_ld = i32 + 3;
+    pv.sn_neg = i32 + 4;
+    pv.sn_fail = i32 + 5;
+    pv.sn_bad = i32 + 6;
+    pv.buf_off = i64 + 0;
+    pv.linv_off = i64 + 1;
+    pv.arena = a;
+    pv.dvec = d;
+    pv.lnz = nullptr;
+    pv.adiag = adiag;
+    pv.linv = linv;
+    pv.sn_faild = f64 + 0;
+    pv.sn_faila = f64 + 1;
+    pv.st = st;
+    pv.tol1 = tol1;
+    for (int64_t stp = 0; stp < nblk; ++stp) {
+        const StepJobs& sj = steps[stp];
+        k_diag<<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
+        if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, pv);
+        if (sj.upd_tasks > 0)
+            K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, pv);
+    }
+    CK(cudaGetLastError());
+    Stats hs;
+    int32_t hfail = -1;
+    double hf[2] = {0.0, 0.0};
+    CK(cudaMemcpyAsync(&hs, st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&hfail, i32 + 5, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hf, f64, sizeof(hf), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // out[0]=NUMNEG out[1]=first failing column (1-based, 0 if none) out[2]=failing pivot out[3]=its a_jj
+    // out[4]=max(a_jj/d_j)
+    out[0] = (double)hs.numneg;
+    out[1] = hs.pivot_fail ? (double)(hfail + 1) : 0.0;
+    out[2] = hf[0];
+    out[3] = hf[1];
+    out[4] = hs.tol2;
+    return 0;
+}
+
 }  // namespace sprb

@@ -59,4 +59,15 @@ private:
     std::unique_ptr<Dev> d_;
 };
 
+// Blocked LDL' of one dense front a (n x n, column-major, leading dimension
+// lda, lower triangle used) in place, with every scratch buffer carved out
+// of the caller's `scratch` (no device allocation).  d receives the pivots.
+// Returns 0, -2 for a bad shape/alignment (lda % 4 == 0 and a 32-byte
+// aligned are required), -3 when the scratch is too small, -4 on CUDA
+// errors.  out[0]=NUMNEG out[1]=first failing column (1-based, 0 if none)
+// out[2]=that pivot out[3]=its original a_jj out[4]=max(a_jj/d_j).
+size_t dense_scratch_bytes(int64_t n);
+int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, double* d, void* scratch,
+                              size_t scratch_bytes, cudaStream_t s, double* out);
+
 }  // namespace sprb
