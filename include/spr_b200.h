@@ -71,6 +71,10 @@ int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ld
  * mode) [9]=Schur-update algorithmic flops [10]=launches of the last solve
  * [11]=NZEROL.  info must hold 12 doubles. */
 int spr_b200_info(void* handle, double* info);
+/* Per-supernode negative-pivot counts and first failing column (-1 if none)
+ * of the last spr_b200_factor_dev (NSUPER entries each): per-system inertia
+ * of a forest of independent systems. */
+int spr_b200_sn_stats(void* handle, int32_t* neg, int32_t* fail);
 /* Profile mode: CUDA events around every Schur-update launch. */
 int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed); see abi.cpp. */

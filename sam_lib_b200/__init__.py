@@ -43,6 +43,8 @@ def load(int_kind=8):
         lib.spr_b200_solve_dev.restype = C.c_int
         lib.spr_b200_info.argtypes = [vp, vp]
         lib.spr_b200_info.restype = C.c_int
+        lib.spr_b200_sn_stats.argtypes = [vp, vp, vp]
+        lib.spr_b200_sn_stats.restype = C.c_int
         lib.spr_b200_set_profile.argtypes = [vp, C.c_int]
         lib.spr_b200_set_profile.restype = C.c_int
         lib.spr_b200_release_all.argtypes = []
@@ -172,6 +174,12 @@ class DeviceSolver:
         keys = ('factor_flops', 'solve_flops', 'arena_bytes', 'levels', 'factor_ms', 'solve_ms',
                 'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops', 'solve_launches', 'nzerol')
         return dict(zip(keys, out.tolist()))
+
+    def sn_stats(self, nsuper):
+        neg = np.zeros(nsuper, dtype=np.int32)
+        fail = np.zeros(nsuper, dtype=np.int32)
+        self.lib.spr_b200_sn_stats(self.h, _ptr(neg), _ptr(fail))
+        return neg, fail
 
     def set_profile(self, on=True):
         self.lib.spr_b200_set_profile(self.h, 1 if on else 0)

@@ -503,6 +503,12 @@ int SPR_API(spr_b200_info)(void* handle, double* info) {
     return 0;
 }
 
+// Per-supernode negative-pivot counts and first failing column (-1 if none)
+// of the last factorisation (host arrays of NSUPER entries).
+int SPR_API(spr_b200_sn_stats)(void* handle, int32_t* neg, int32_t* fail) {
+    return static_cast<Engine*>(handle)->sn_stats(neg, fail);
+}
+
 // Profile mode: CUDA events around every Schur-update launch (spr_b200_info[8]).
 int SPR_API(spr_b200_set_profile)(void* handle, int on) {
     static_cast<Engine*>(handle)->set_profile(on != 0);

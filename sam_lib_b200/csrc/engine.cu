@@ -1306,6 +1306,13 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     return 0;
 }
 
+int Engine::sn_stats(int32_t* neg, int32_t* fail) {
+    Dev& D = *d_;
+    CK(cudaMemcpy(neg, D.sn_neg, P_.nsuper * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fail, D.sn_fail, P_.nsuper * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
 void Engine::ensure_vectors(int64_t nrhs) {
     Dev& D = *d_;
     if (D.vbuf_rhs < nrhs) {

@@ -39,6 +39,8 @@ public:
     int factor(double* d_sm, double tol1, FactorResult& res);
     // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
     int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
+    // Per-supernode negative-pivot counts and failing column of the last factor().
+    int sn_stats(int32_t* neg, int32_t* fail);
     // The solves use the inverses of the diagonal blocks that factor() stores;
     // after SM was replaced by a factor from elsewhere, call this so the next
     // solve rebuilds them from LNZ.

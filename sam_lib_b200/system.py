@@ -80,3 +80,50 @@ class HexSystem:
         ye = np.einsum('ij,ejk->eik', self.ke, xe) * self.moduli[:, None, None]
         np.add.at(out, eq[m], ye[m])
         return out.reshape(x.shape)
+
+
+def diag_positions(mspar, mtrees, msifa):
+    """0-based index into SM of each equation's diagonal (inside LNZ), cf. SPRDG1."""
+    neq, ns = int(mspar[7]), int(mspar[10])
+    xs = mtrees[mspar[44] - 1: mspar[44] + ns]
+    xl = mtrees[mspar[45] - 1: mspar[45] + ns]
+    xlnz = msifa[mspar[47] - 1: mspar[47] + ns]
+    pos = np.empty(neq, dtype=np.int64)
+    for js in range(ns):
+        F = xl[js + 1] - xl[js]
+        j = np.arange(xs[js + 1] - xs[js])
+        pos[xs[js] - 1 + j] = neq + (xlnz[js] - 1) + j * F - (j * (j - 1)) // 2
+    return pos
+
+
+def shift_diagonal(sm, pos, mass, sigma):
+    """A - sigma*B for a diagonal B (SPRSHA KSB=2, src/SPR/sprsha.f:86-93)."""
+    out = sm.copy()
+    out[pos] -= sigma * mass
+    return out
+
+
+def sm_to_csr(mspar, mtrees, msifa, sm):
+    """Full symmetric scipy CSR of the matrix held (lower part) in LNZ, zeros dropped."""
+    import scipy.sparse as sp
+    neq, ns = int(mspar[7]), int(mspar[10])
+    xs = mtrees[mspar[44] - 1: mspar[44] + ns]
+    xl = mtrees[mspar[45] - 1: mspar[45] + ns]
+    lindx = msifa[mspar[46] - 1:]
+    xlnz = msifa[mspar[47] - 1: mspar[47] + ns]
+    rows, cols, vals = [], [], []
+    lnz = sm[neq:]
+    for js in range(ns):
+        F = int(xl[js + 1] - xl[js])
+        r = lindx[xl[js] - 1: xl[js + 1] - 1] - 1
+        p = int(xlnz[js] - 1)
+        for j in range(int(xs[js + 1] - xs[js])):
+            v = lnz[p: p + F - j]
+            nz = v != 0.0
+            rows.append(r[j:][nz])
+            cols.append(np.full(int(nz.sum()), xs[js] - 1 + j))
+            vals.append(v[nz])
+            p += F - j
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+    L = sp.coo_matrix((vals, (rows, cols)), shape=(neq, neq)).tocsr()
+    return (L + sp.tril(L, -1).T).tocsr()

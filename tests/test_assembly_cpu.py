@@ -35,3 +35,28 @@ def test_matvec_matches_dense():
     x = np.random.default_rng(0).standard_normal(hs.neq)
     K = dense_from_sm(rs, sm)
     assert np.allclose(hs.matvec(x), K @ x, rtol=1e-12, atol=1e-12)
+
+
+def test_forest_merge_matches_individual_systems_bitwise():
+    """Independent systems merged into one SPR forest: the oracle factors the
+    forest exactly as it factors each system (solutions bitwise equal)."""
+    from sam_lib_b200.workloads import config4
+    from sam_lib_b200.batch import Forest
+    from test_batched_gpu import oracle_solve
+    systems = config4()[:6]
+    fo = Forest([(s['hs'].mspar, s['hs'].mtrees, s['hs'].msifa) for s in systems])
+    sm = fo.merge_sm([s['sm'] for s in systems])
+    B = np.zeros((fo.neq, 16), order='F')
+    for i, s in enumerate(systems):
+        B[fo.eq_off[i]:fo.eq_off[i] + fo.neq_i[i]] = s['b']
+
+    class H:
+        mspar, mtrees, msifa, neq = fo.mspar, fo.mtrees, fo.msifa, fo.neq
+    ierr, nn, X = oracle_solve(H, sm, B)
+    assert ierr == 0
+    tot = 0
+    for i, s in enumerate(systems):
+        e, n1, x = oracle_solve(s['hs'], s['sm'], s['b'])
+        tot += n1
+        assert np.array_equal(x, X[fo.eq_off[i]:fo.eq_off[i] + fo.neq_i[i]])
+    assert nn == tot
