@@ -926,6 +926,211 @@ __global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t
         if (r < nrhs) w[(int64_t)r * F + i] = acc[r];
 }
 
+// Solve steps of kSolveBlock (256) columns.  Forward: one CTA per front
+// solves the block's unit-lower triangle (4 diagonal blocks of 64, each a
+// product with its stored inverse X, then the rows below it inside the
+// block), stores the block in ysol; then k_fwd_blk_upd applies it to every
+// row below the block (thread per row, SPRFS6).  Backward mirrors it.
+constexpr size_t kBlkDiagSmem = sizeof(double) * ((size_t)kNB * (kNB + 1) + 2 * (size_t)kSolveBlock * kMaxRHS);
+
+__global__ void __launch_bounds__(256) k_fwd_blk_diag(const Job* jobs, PV P, const double* vbuf, double* ysol,
+                                                      int nrhs) {
+    extern __shared__ double fsh[];
+    double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(fsh);
+    double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(fsh + kNB * (kNB + 1));
+    double(*t)[kMaxRHS] = y + kSolveBlock;
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js], nbk = k1 - k0;
+    const int64_t vb = P.rbase[js] * nrhs;
+    const double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        y[i][r] = w[(int64_t)r * F + k0 + i];
+    }
+    for (int j0 = 0; j0 < nbk; j0 += kNB) {
+        const int nb = min(kNB, nbk - j0);
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)((k0 + j0) / kNB) * kNB * kNB;
+        for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
+        __syncthreads();
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            double acc = 0.0;
+            for (int m = 0; m <= c; ++m) acc += Xs[c][m] * y[j0 + m][r];
+            t[c][r] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            y[j0 + c][r] = t[c][r];
+        }
+        __syncthreads();
+        for (int i = j0 + nb + tid; i < nbk; i += blockDim.x) {
+            double acc[kMaxRHS];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? y[i][r] : 0.0;
+#pragma unroll 8
+            for (int c = 0; c < nb; ++c) {
+                const int col = k0 + j0 + c;
+                const double l = base[lnz_col(col, F) - col + (k0 + i)];
+#pragma unroll
+                for (int r = 0; r < kMaxRHS; ++r)
+                    if (r < nrhs) acc[r] -= l * y[j0 + c][r];
+            }
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r)
+                if (r < nrhs) y[i][r] = acc[r];
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        ysol[vb + (int64_t)r * F + k0 + i] = y[i][r];
+    }
+}
+
+__global__ void __launch_bounds__(kSolveRows) k_fwd_blk_upd(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                            const double* ysol, int nrhs) {
+    __shared__ double y[kSolveBlock][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js], nbk = k1 - k0;
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    for (int e = threadIdx.x; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        y[i][r] = ysol[vb + (int64_t)r * F + k0 + i];
+    }
+    __syncthreads();
+    const int i = jb.c0 + (int)(task - jb.task0) * kSolveRows + threadIdx.x;
+    if (i >= F) return;
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
+#pragma unroll 8
+    for (int c = 0; c < nbk; ++c) {
+        const int col = k0 + c;
+        const double l = base[lnz_col(col, F) - col + i];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) acc[r] -= l * y[c][r];
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) w[(int64_t)r * F + i] = acc[r];
+}
+
+// w[m] -= sum_{c < n} L[row0 + c, m] x[c][.] by one warp (column m of L contiguous)
+__device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, const double (*x)[kMaxRHS],
+                                                  double* wm, int64_t F, int nrhs) {
+    const int lane = threadIdx.x & 31;
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    for (int c = lane; c < n; c += 32) {
+        const double l = cm_row0[c];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) acc[r] += l * x[c][r];
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) {
+        if (r >= nrhs) break;
+        double v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) wm[(int64_t)r * F] -= v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bwd_blk_diag(const Job* jobs, PV P, const double* vbuf, double* xsol,
+                                                      int nrhs) {
+    extern __shared__ double bsh[];
+    double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(bsh);
+    double(*x)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(bsh + kNB * (kNB + 1));
+    double(*t)[kMaxRHS] = x + kSolveBlock;
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js], nbk = k1 - k0;
+    const int64_t vb = P.rbase[js] * nrhs;
+    const double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        x[i][r] = w[(int64_t)r * F + k0 + i];
+    }
+    const int nsub = (nbk + kNB - 1) / kNB;
+    for (int jj = nsub - 1; jj >= 0; --jj) {
+        const int j0 = jj * kNB, nb = min(kNB, nbk - j0);
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)((k0 + j0) / kNB) * kNB * kNB;
+        for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
+        __syncthreads();
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            double acc = 0.0;
+            for (int m = c; m < nb; ++m) acc += Xs[m][c] * x[j0 + m][r];
+            t[c][r] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+            const int c = e % nb, r = e / nb;
+            x[j0 + c][r] = t[c][r];
+        }
+        __syncthreads();
+        // earlier columns of the block: x[q] -= L[k0+j0 : k0+j0+nb, k0+q]' x_j
+        for (int q = warp; q < j0; q += nwarp) {
+            const int col = k0 + q;
+            const double* cm = base + lnz_col(col, F) - col + (k0 + j0);
+            const int lane0 = lane;
+            double acc[kMaxRHS];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+            for (int c = lane0; c < nb; c += 32) {
+                const double l = cm[c];
+#pragma unroll
+                for (int r = 0; r < kMaxRHS; ++r)
+                    if (r < nrhs) acc[r] += l * x[j0 + c][r];
+            }
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r) {
+                if (r >= nrhs) break;
+                double v = acc[r];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) x[q][r] -= v;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        xsol[vb + (int64_t)r * F + k0 + i] = x[i][r];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                     const double* xsol, int nrhs) {
+    __shared__ double x[kSolveBlock][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js], nbk = k1 - k0;
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    for (int e = threadIdx.x; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        x[i][r] = xsol[vb + (int64_t)r * F + k0 + i];
+    }
+    __syncthreads();
+    const int m = (int)(task - jb.task0) * kBwdCols + (threadIdx.x >> 5);
+    if (m >= jb.c_end) return;
+    warp_col_dot_smem(base + lnz_col(m, F) - m + k0, nbk, x, w + m, F, nrhs);
+}
+
 // y_j /= d_j and scatter of the own rows (thread per column)
 __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* ysol, double* b,
                              int64_t ldb, int nrhs) {
@@ -1139,6 +1344,8 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     if ((size_t)smem_max < need) return -4;
     CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    CK(cudaFuncSetAttribute(k_fwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
+    CK(cudaFuncSetAttribute(k_bwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     return 0;
@@ -1362,11 +1569,16 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
-                for (size_t st = 0; st < lp.fsolve.size(); ++st) {
-                    const Launch& fl = lp.fsolve[st];
-                    k_fwd_step<<<(int)fl.ntasks, kTRSMRows, 0, s>>>(jobs + fl.job_begin, fl.job_count, pv, D.vbuf,
-                                                                    D.vbuf2, nr);
+                for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
+                    const Launch& fl = lp.fs_upd[sb];
+                    k_fwd_blk_diag<<<(int)fl.job_count, 256, kBlkDiagSmem, s>>>(jobs + fl.job_begin, pv, D.vbuf,
+                                                                               D.vbuf2, nr);
                     ++nl;
+                    if (fl.ntasks > 0) {
+                        k_fwd_blk_upd<<<(int)fl.ntasks, kSolveRows, 0, s>>>(jobs + fl.job_begin, fl.job_count, pv,
+                                                                             D.vbuf, D.vbuf2, nr);
+                        ++nl;
+                    }
                 }
                 const Launch& wb = lp.writeback;
                 k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
@@ -1391,11 +1603,16 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 k_bwd_rect<<<blocks(wb.ntasks * 32), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                   D.vbuf, nr);
                 ++nl;
-                for (size_t st = lp.bsolve.size(); st-- > 0;) {
-                    const Launch& bl = lp.bsolve[st];
-                    k_bwd_step<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf, D.vbuf2,
-                                                              nr);
+                for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
+                    const Launch& bl = lp.bs_upd[sb];
+                    k_bwd_blk_diag<<<(int)bl.job_count, 256, kBlkDiagSmem, s>>>(jobs + bl.job_begin, pv, D.vbuf,
+                                                                               D.vbuf2, nr);
                     ++nl;
+                    if (bl.ntasks > 0) {
+                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf,
+                                                                     D.vbuf2, nr);
+                        ++nl;
+                    }
                 }
                 k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);

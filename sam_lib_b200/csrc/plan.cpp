@@ -335,6 +335,28 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.bsolve[st]);
         }
+        const int32_t nsb = (smax + kSolveBlock - 1) / kSolveBlock;
+        lp.fs_upd.assign(nsb, Launch());
+        lp.bs_upd.assign(nsb, Launch());
+        for (int32_t sb = 0; sb < nsb; ++sb) {
+            const int32_t k0 = sb * kSolveBlock;
+            open_launch(lp.fs_upd[sb]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t k1 = std::min(k0 + kSolveBlock, s);
+                add_job(lp.fs_upd[sb], Job{js, k1, k1, f, k0, k1, 0}, (f - k1 + kSolveRows - 1) / kSolveRows, true);
+            }
+            close_launch(lp.fs_upd[sb]);
+            open_launch(lp.bs_upd[sb]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t k1 = std::min(k0 + kSolveBlock, s);
+                add_job(lp.bs_upd[sb], Job{js, 0, k0, f, k0, k1, 0}, (k0 + kBwdCols - 1) / kBwdCols, true);
+            }
+            close_launch(lp.bs_upd[sb]);
+        }
         {
             std::vector<Job> jl;
             for (int32_t js : lp.large_nodes) {

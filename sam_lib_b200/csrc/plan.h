@@ -64,9 +64,15 @@ struct LevelPlan {
     Launch writeback;                         // S columns -> LNZ
     std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
     std::vector<Launch> bsolve;               // back step: 1 diagonal CTA + column groups [0, k0)
+    // solves in kSolveBlock-wide steps: per step, the diagonal-block launch uses
+    // the job list (one CTA per job), the update launch its tasks
+    std::vector<Launch> fs_upd;               // rows [k1, F) below the block, kSolveRows per task
+    std::vector<Launch> bs_upd;               // columns [0, k0) before the block, kBwdCols per task
 };
 
 constexpr int kBwdCols = 8;                   // columns per CTA in the back-solve update
+constexpr int kSolveBlock = 256;              // width of a solve step (4 diagonal blocks of kNB)
+constexpr int kSolveRows = 128;               // rows per CTA in the forward update
 
 struct Plan {
     // sizes
