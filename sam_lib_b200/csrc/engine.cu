@@ -69,6 +69,8 @@ struct PV {
     Stats* st;
     const int64_t* linv_off;
     double* linv;            // inverses of the unit-lower diagonal blocks
+    const int64_t* xinv_off;
+    double* xinv;            // inverses of the kSolveBlock-wide diagonal blocks
     double tol1;
 };
 
@@ -81,6 +83,8 @@ struct Engine::Dev {
     Job* jobs = nullptr;
     int64_t* linv_off = nullptr;
     double* linv = nullptr;
+    int64_t* xinv_off = nullptr;
+    double* xinv = nullptr;
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
     std::vector<int64_t> small_begin;            // per level offset into level_nodes
     int32_t* all_nodes = nullptr;                // all nodes of every level (solves)
@@ -1131,6 +1135,277 @@ __global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t nj
     warp_col_dot_smem(base + lnz_col(m, F) - m + k0, nbk, x, w + m, F, nrhs);
 }
 
+// Inverse X = L_blk^-1 of one kSolveBlock-wide unit-lower diagonal block of a
+// large front, from the stored 64x64 inverses: X_jj = inv(L_jj),
+// X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj (64x64 tiles, FP64 CUDA cores).
+// Written column-major (ld = nb) into xinv; used by the block solves.
+constexpr size_t kInvSmem = sizeof(double) * 3 * (size_t)kNB * (kNB + 1);
+
+__device__ void tile_mm(const double (*A)[kNB + 1], const double (*B)[kNB + 1], double acc[4][4], int tid) {
+    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
+    for (int k = 0; k < kNB; ++k) {
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = A[r0 + u][k];
+            b[u] = B[k][c0 + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_inv_block(const Job* jobs, PV P) {
+    extern __shared__ double ish[];
+    double(*As)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(ish);
+    double(*Bs)[kNB + 1] = As + kNB;
+    double(*Ts)[kNB + 1] = Bs + kNB;
+    const Job& jb = jobs[blockIdx.x];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    if (P.sn_bad && P.sn_bad[js]) return;
+    const int F = P.F[js];
+    const double* base = P.lnz + P.lnz_off[js];
+    const double* lv0 = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
+    double* X = P.xinv + P.xinv_off[js] + (int64_t)(k0 / kSolveBlock) * kSolveBlock * kSolveBlock;
+    const int tid = threadIdx.x;
+    const int q = (nb + kNB - 1) / kNB;
+    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
+    auto xat = [&](int i, int j) -> double& { return X[(int64_t)i + (int64_t)j * nb]; };
+    for (int j = 0; j < q; ++j) {
+        const int sj = min(kNB, nb - kNB * j);
+        // diagonal block and the zero blocks above it
+        for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+            const int a = e % kNB, b = e / kNB;
+            if (a < sj && b < sj) xat(kNB * j + a, kNB * j + b) = lv0[(int64_t)j * kNB * kNB + e];
+        }
+        for (int i = 0; i < j; ++i)
+            for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+                const int a = e % kNB, b = e / kNB;
+                if (kNB * i + a < nb && b < sj) xat(kNB * i + a, kNB * j + b) = 0.0;
+            }
+        __syncthreads();
+        for (int i = j + 1; i < q; ++i) {
+            const int si = min(kNB, nb - kNB * i);
+            double acc[4][4] = {};
+            for (int k = j; k < i; ++k) {
+                const int sk = min(kNB, nb - kNB * k);
+                for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+                    const int a = e % kNB, b = e / kNB;
+                    const int row = k0 + kNB * i + a, col = k0 + kNB * k + b;
+                    As[a][b] = (a < si && b < sk) ? base[lnz_col(col, F) - col + row] : 0.0;
+                    Bs[a][b] = (a < sk && b < sj) ? xat(kNB * k + a, kNB * j + b) : 0.0;
+                }
+                __syncthreads();
+                tile_mm(As, Bs, acc, tid);
+                __syncthreads();
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Ts[r0 + u][c0 + v] = acc[u][v];
+            for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+                const int a = e % kNB, b = e / kNB;
+                As[a][b] = (a < si && b < si) ? lv0[(int64_t)i * kNB * kNB + e] : 0.0;
+            }
+            __syncthreads();
+            double acc2[4][4] = {};
+            tile_mm(As, Ts, acc2, tid);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    if (r0 + u < si && c0 + v < sj) xat(kNB * i + r0 + u, kNB * j + c0 + v) = -acc2[u][v];
+            __syncthreads();
+        }
+    }
+}
+
+// y_block = X w_block: 32 rows per CTA, 8 warps split the columns
+constexpr size_t kMvSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + 8 * 32 * (kMaxRHS + 1));
+
+__global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+                                                    double* ysol, int nrhs) {
+    extern __shared__ double msh[];
+    double(*wb)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(msh);
+    double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(msh + kSolveBlock * kMaxRHS);
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    const int F = P.F[js];
+    const int64_t vb = P.rbase[js] * nrhs;
+    const double* w = vbuf + vb;
+    const double* X = P.xinv + P.xinv_off[js] + (int64_t)(k0 / kSolveBlock) * kSolveBlock * kSolveBlock;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+        const int i = e % nb, r = e / nb;
+        wb[i][r] = w[(int64_t)r * F + k0 + i];
+    }
+    __syncthreads();
+    const int i = (int)(task - jb.task0) * 32 + lane;
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    if (i < nb) {
+        const int m1 = min(32 * warp + 32, i + 1);
+        for (int m = 32 * warp; m < m1; ++m) {
+            const double x = X[(int64_t)i + (int64_t)m * nb];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r)
+                if (r < nrhs) acc[r] += x * wb[m][r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) part[warp][lane][r] = acc[r];
+    __syncthreads();
+    if (warp == 0 && i < nb)
+        for (int r = 0; r < nrhs; ++r) {
+            double v = 0.0;
+            for (int g = 0; g < 8; ++g) v += part[g][lane][r];
+            ysol[vb + (int64_t)r * F + k0 + i] = v;
+        }
+}
+
+// x_block = X' w_block: 32 columns per CTA, 4 per warp, lanes over rows
+__global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+                                                    double* xsol, int nrhs) {
+    __shared__ double wb[kSolveBlock][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
+    const int F = P.F[js];
+    const int64_t vb = P.rbase[js] * nrhs;
+    const double* w = vbuf + vb;
+    const double* X = P.xinv + P.xinv_off[js] + (int64_t)(k0 / kSolveBlock) * kSolveBlock * kSolveBlock;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
+        const int i = e % nb, r = e / nb;
+        wb[i][r] = w[(int64_t)r * F + k0 + i];
+    }
+    __syncthreads();
+    for (int cc = 0; cc < 4; ++cc) {
+        const int c = (int)(task - jb.task0) * 32 + warp * 4 + cc;
+        if (c >= nb) break;
+        double acc[kMaxRHS];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+        for (int m = c + lane; m < nb; m += 32) {
+            const double x = X[(int64_t)m + (int64_t)c * nb];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r)
+                if (r < nrhs) acc[r] += x * wb[m][r];
+        }
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) {
+            if (r >= nrhs) break;
+            double v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) xsol[vb + (int64_t)r * F + k0 + c] = v;
+        }
+    }
+}
+
+// rows below a solve block: w[i] -= L[i, k0:k1] y, 32 rows x 8 column groups per CTA
+__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+                                                      const double* ysol, int nrhs) {
+    extern __shared__ double ush[];
+    double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(ush);
+    double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(ush + kSolveBlock * kMaxRHS);
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
+    const int F = P.F[js], nbk = k1 - k0;
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
+        const int i = e % nbk, r = e / nbk;
+        y[i][r] = ysol[vb + (int64_t)r * F + k0 + i];
+    }
+    __syncthreads();
+    const int i = jb.c0 + (int)(task - jb.task0) * kSolveRows + lane;
+    double acc[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    if (i < F) {
+        const int c1 = min(32 * warp + 32, nbk);
+#pragma unroll 8
+        for (int c = 32 * warp; c < c1; ++c) {
+            const int col = k0 + c;
+            const double l = base[lnz_col(col, F) - col + i];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r)
+                if (r < nrhs) acc[r] += l * y[c][r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) part[warp][lane][r] = acc[r];
+    __syncthreads();
+    if (warp == 0 && i < F)
+        for (int r = 0; r < nrhs; ++r) {
+            double v = 0.0;
+            for (int g = 0; g < 8; ++g) v += part[g][lane][r];
+            w[(int64_t)r * F + i] -= v;
+        }
+}
+
+// back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F] for 32 columns per
+// CTA (4 per warp); the vector is staged through shared memory in 256-row chunks
+__global__ void __launch_bounds__(256) k_bwd_rect2(const Job* jobs, int64_t njobs, PV P, double* vbuf, int nrhs) {
+    __shared__ double ws[256][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int F = P.F[js], S = P.S[js];
+    const int64_t vb = P.rbase[js] * nrhs;
+    double* w = vbuf + vb;
+    const double* base = P.lnz + P.lnz_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cbase = (int)(task - jb.task0) * kRectCols + warp * 4;
+    double acc[4][kMaxRHS];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) acc[a][r] = 0.0;
+    for (int r0 = S; r0 < F; r0 += 256) {
+        const int nr = min(256, F - r0);
+        __syncthreads();
+        for (int e = tid; e < nr * nrhs; e += blockDim.x) {
+            const int i = e % nr, r = e / nr;
+            ws[i][r] = w[(int64_t)r * F + r0 + i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int c = cbase + a;
+            if (c >= S) break;
+            const double* cc = base + lnz_col(c, F) - c + r0;
+            for (int i = lane; i < nr; i += 32) {
+                const double l = cc[i];
+#pragma unroll
+                for (int r = 0; r < kMaxRHS; ++r)
+                    if (r < nrhs) acc[a][r] += l * ws[i][r];
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int c = cbase + a;
+        if (c >= S) break;
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) {
+            if (r >= nrhs) break;
+            double v = acc[a][r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) w[(int64_t)r * F + c] -= v;
+        }
+    }
+}
+
 // y_j /= d_j and scatter of the own rows (thread per column)
 __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* ysol, double* b,
                              int64_t ldb, int nrhs) {
@@ -1304,8 +1579,10 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         dev_upload(o, &D.rel_off, P_.rel_off) || dev_upload(o, &D.rbase, P_.rbase) ||
         dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
         dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs) ||
-        dev_upload(o, &D.linv_off, P_.linv_off))
+        dev_upload(o, &D.linv_off, P_.linv_off) || dev_upload(o, &D.xinv_off, P_.xinv_off))
         return -4;
+    CK(cudaMalloc((void**)&D.xinv, std::max<int64_t>(P_.xinv_doubles, 1) * sizeof(double)));
+    o.push_back(D.xinv);
     CK(cudaMalloc((void**)&D.linv, std::max<int64_t>(P_.linv_doubles, 1) * sizeof(double)));
     o.push_back(D.linv);
     std::vector<int32_t> small, all;
@@ -1344,6 +1621,9 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     if ((size_t)smem_max < need) return -4;
     CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
+    CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
+    CK(cudaFuncSetAttribute(k_inv_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
     CK(cudaFuncSetAttribute(k_bwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
@@ -1388,6 +1668,8 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.st = D.st;
     v.linv_off = D.linv_off;
     v.linv = D.linv;
+    v.xinv_off = D.xinv_off;
+    v.xinv = D.xinv;
     v.tol1 = tol1;
     return v;
 }
@@ -1458,6 +1740,10 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
             k_writeback<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, l.ntasks, pv);
             ++timing.launches;
         }
+    }
+    if (P_.inv_blocks.job_count > 0) {
+        k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pv);
+        ++timing.launches;
     }
     k_reduce<true><<<1, 1024, 0, s>>>(pv.dvec, P_.neq, &D.st->mindpos);
     ++timing.launches;
@@ -1549,6 +1835,12 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                     k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
                     ++nl;
                 }
+        if (P_.inv_blocks.job_count > 0) {
+            PV pvi = pv;
+            pvi.sn_bad = nullptr;
+            k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pvi);
+            ++nl;
+        }
         linv_valid_ = true;
     }
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
@@ -1570,13 +1862,14 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
-                    const Launch& fl = lp.fs_upd[sb];
-                    k_fwd_blk_diag<<<(int)fl.job_count, 256, kBlkDiagSmem, s>>>(jobs + fl.job_begin, pv, D.vbuf,
-                                                                               D.vbuf2, nr);
+                    const Launch& ml = lp.blk_mv[sb];
+                    k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, pv, D.vbuf,
+                                                                 D.vbuf2, nr);
                     ++nl;
+                    const Launch& fl = lp.fs_upd[sb];
                     if (fl.ntasks > 0) {
-                        k_fwd_blk_upd<<<(int)fl.ntasks, kSolveRows, 0, s>>>(jobs + fl.job_begin, fl.job_count, pv,
-                                                                             D.vbuf, D.vbuf2, nr);
+                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kMvSmem, s>>>(jobs + fl.job_begin, fl.job_count, pv,
+                                                                       D.vbuf, D.vbuf2, nr);
                         ++nl;
                     }
                 }
@@ -1600,14 +1893,16 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 const Launch& wb = lp.writeback;
-                k_bwd_rect<<<blocks(wb.ntasks * 32), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
-                                                                  D.vbuf, nr);
+                const Launch& rl = lp.rect;
+                if (rl.ntasks > 0)
+                    k_bwd_rect2<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, pv, D.vbuf, nr);
                 ++nl;
                 for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
-                    const Launch& bl = lp.bs_upd[sb];
-                    k_bwd_blk_diag<<<(int)bl.job_count, 256, kBlkDiagSmem, s>>>(jobs + bl.job_begin, pv, D.vbuf,
-                                                                               D.vbuf2, nr);
+                    const Launch& ml = lp.blk_mv[sb];
+                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, pv, D.vbuf,
+                                                                 D.vbuf2, nr);
                     ++nl;
+                    const Launch& bl = lp.bs_upd[sb];
                     if (bl.ntasks > 0) {
                         k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf,
                                                                      D.vbuf2, nr);

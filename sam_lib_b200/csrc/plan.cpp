@@ -220,6 +220,15 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
     }
     P.arena_doubles = arena.peak();
+    P.xinv_off.assign(ns, -1);
+    P.xinv_doubles = 0;
+    for (int64_t js = 0; js < ns; ++js)
+        if (P.F[js] > kSmallMaxF) {
+            const int64_t nsb = (P.S[js] + kSolveBlock - 1) / kSolveBlock;
+            const int64_t last = P.S[js] - (nsb - 1) * kSolveBlock;
+            P.xinv_off[js] = P.xinv_doubles;
+            P.xinv_doubles += ((nsb - 1) * kSolveBlock * kSolveBlock + last * last + 31) / 32 * 32;
+        }
     P.linv_off.assign(ns, -1);
     P.linv_doubles = 0;
     for (int64_t js = 0; js < ns; ++js)
@@ -338,8 +347,17 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         const int32_t nsb = (smax + kSolveBlock - 1) / kSolveBlock;
         lp.fs_upd.assign(nsb, Launch());
         lp.bs_upd.assign(nsb, Launch());
+        lp.blk_mv.assign(nsb, Launch());
         for (int32_t sb = 0; sb < nsb; ++sb) {
             const int32_t k0 = sb * kSolveBlock;
+            open_launch(lp.blk_mv[sb]);
+            for (int32_t js : lp.large_nodes) {
+                const int32_t s = P.S[js], f = P.F[js];
+                if (k0 >= s) continue;
+                const int32_t k1 = std::min(k0 + kSolveBlock, s);
+                add_job(lp.blk_mv[sb], Job{js, k0, k1, f, k0, k1, 0}, (k1 - k0 + 31) / 32);
+            }
+            close_launch(lp.blk_mv[sb]);
             open_launch(lp.fs_upd[sb]);
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
@@ -357,6 +375,12 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.bs_upd[sb]);
         }
+        open_launch(lp.rect);
+        for (int32_t js : lp.large_nodes) {
+            const int32_t s = P.S[js], f = P.F[js];
+            if (f > s) add_job(lp.rect, Job{js, 0, s, f, s, f, 0}, (s + kRectCols - 1) / kRectCols);
+        }
+        close_launch(lp.rect);
         {
             std::vector<Job> jl;
             for (int32_t js : lp.large_nodes) {
@@ -374,6 +398,14 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             add_job(lp.writeback, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, P.S[js]);
         close_launch(lp.writeback);
     }
+    open_launch(P.inv_blocks);
+    for (int64_t js = 0; js < ns; ++js) {
+        if (P.F[js] <= kSmallMaxF) continue;
+        for (int32_t k0 = 0; k0 < P.S[js]; k0 += kSolveBlock)
+            add_job(P.inv_blocks, Job{(int32_t)js, k0, std::min(k0 + kSolveBlock, P.S[js]), P.F[js], k0,
+                                      std::min(k0 + kSolveBlock, P.S[js]), 0}, 1);
+    }
+    close_launch(P.inv_blocks);
     return 0;
 }
 

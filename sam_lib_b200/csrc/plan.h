@@ -68,11 +68,14 @@ struct LevelPlan {
     // the job list (one CTA per job), the update launch its tasks
     std::vector<Launch> fs_upd;               // rows [k1, F) below the block, kSolveRows per task
     std::vector<Launch> bs_upd;               // columns [0, k0) before the block, kBwdCols per task
+    std::vector<Launch> blk_mv;               // product with the block inverse, 32 rows/columns per task
+    Launch rect;                              // back solve, rows [S, F): 32 columns per task
 };
 
 constexpr int kBwdCols = 8;                   // columns per CTA in the back-solve update
 constexpr int kSolveBlock = 256;              // width of a solve step (4 diagonal blocks of kNB)
-constexpr int kSolveRows = 128;               // rows per CTA in the forward update
+constexpr int kSolveRows = 32;                // rows per CTA in the forward update (x 8 column groups)
+constexpr int kRectCols = 32;                 // columns per CTA in the back-solve rectangle
 
 struct Plan {
     // sizes
@@ -98,6 +101,12 @@ struct Plan {
     // of node js is the column-major kNB x kNB matrix at linv_off[js] + st*kNB*kNB
     std::vector<int64_t> linv_off;
     int64_t linv_doubles = 0;
+    // inverses of the kSolveBlock-wide unit-lower diagonal blocks (the solves):
+    // block b of node js is column-major nb x nb (nb = min(kSolveBlock, S - b*kSolveBlock))
+    // at xinv_off[js] + b*kSolveBlock*kSolveBlock
+    std::vector<int64_t> xinv_off;
+    int64_t xinv_doubles = 0;
+    Launch inv_blocks;                        // one task per (large front, solve block)
     bool any_large = false;
     // levels and tasks
     std::vector<LevelPlan> levels;
