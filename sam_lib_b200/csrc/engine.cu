@@ -71,6 +71,7 @@ struct PV {
     double* linv;            // inverses of the unit-lower diagonal blocks
     const int64_t* xinv_off;
     double* xinv;            // inverses of the kSolveBlock-wide diagonal blocks
+    const int64_t* rect_off;
     double tol1;
 };
 
@@ -85,6 +86,8 @@ struct Engine::Dev {
     double* linv = nullptr;
     int64_t* xinv_off = nullptr;
     double* xinv = nullptr;
+    int64_t* rect_off = nullptr;
+    double* pbuf = nullptr;                      // back-solve rectangle partial sums
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
     std::vector<int64_t> small_begin;            // per level offset into level_nodes
     int32_t* all_nodes = nullptr;                // all nodes of every level (solves)
@@ -1353,26 +1356,34 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
         }
 }
 
-// back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F] for 32 columns per
-// CTA (4 per warp); the vector is staged through shared memory in 256-row chunks
-__global__ void __launch_bounds__(256) k_bwd_rect2(const Job* jobs, int64_t njobs, PV P, double* vbuf, int nrhs) {
+// back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F].  Phase 1: one
+// CTA per (32 columns, kRectRows rows) writes partial dot products (one warp
+// per column, 4 columns per warp, the vector staged in shared memory);
+// phase 2 (k_bwd_rect_sum) adds the partials of each column in a fixed order,
+// so the result is deterministic.
+__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+                                                       double* pbuf, int nrhs) {
     __shared__ double ws[256][kMaxRHS];
     const int64_t task = blockIdx.x;
     const Job& jb = jobs[find_job(jobs, njobs, task)];
     const int js = jb.node;
     const int F = P.F[js], S = P.S[js];
+    const int ncc = jb.k_hi;
+    const int64_t u = task - jb.task0;
+    const int cc = (int)(u % ncc), rc = (int)(u / ncc);
     const int64_t vb = P.rbase[js] * nrhs;
-    double* w = vbuf + vb;
+    const double* w = vbuf + vb;
     const double* base = P.lnz + P.lnz_off[js];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int cbase = (int)(task - jb.task0) * kRectCols + warp * 4;
+    const int cbase = cc * kRectCols + warp * 4;
+    const int rbeg = S + rc * kRectRows, rend = min(F, rbeg + kRectRows);
     double acc[4][kMaxRHS];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int r = 0; r < kMaxRHS; ++r) acc[a][r] = 0.0;
-    for (int r0 = S; r0 < F; r0 += 256) {
-        const int nr = min(256, F - r0);
+    for (int r0 = rbeg; r0 < rend; r0 += 256) {
+        const int nr = min(256, rend - r0);
         __syncthreads();
         for (int e = tid; e < nr * nrhs; e += blockDim.x) {
             const int i = e % nr, r = e / nr;
@@ -1383,15 +1394,16 @@ __global__ void __launch_bounds__(256) k_bwd_rect2(const Job* jobs, int64_t njob
         for (int a = 0; a < 4; ++a) {
             const int c = cbase + a;
             if (c >= S) break;
-            const double* cc = base + lnz_col(c, F) - c + r0;
+            const double* col = base + lnz_col(c, F) - c + r0;
             for (int i = lane; i < nr; i += 32) {
-                const double l = cc[i];
+                const double l = col[i];
 #pragma unroll
                 for (int r = 0; r < kMaxRHS; ++r)
                     if (r < nrhs) acc[a][r] += l * ws[i][r];
             }
         }
     }
+    double* part = pbuf + (P.rect_off[js] + (int64_t)rc * S) * kMaxRHS;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int c = cbase + a;
@@ -1401,8 +1413,27 @@ __global__ void __launch_bounds__(256) k_bwd_rect2(const Job* jobs, int64_t njob
             if (r >= nrhs) break;
             double v = acc[a][r];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) w[(int64_t)r * F + c] -= v;
+            if (lane == 0) part[(int64_t)c * kMaxRHS + r] = v;
         }
+    }
+}
+
+__global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+                               const double* pbuf, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const int js = jb.node;
+    const int F = P.F[js], S = P.S[js];
+    if (F <= S) return;
+    const int c = (int)(task - jb.task0);
+    const int nrc = (F - S + kRectRows - 1) / kRectRows;
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const double* part = pbuf + P.rect_off[js] * kMaxRHS;
+    for (int r = 0; r < nrhs; ++r) {
+        double v = 0.0;
+        for (int k = 0; k < nrc; ++k) v += part[((int64_t)k * S + c) * kMaxRHS + r];
+        w[(int64_t)r * F + c] -= v;
     }
 }
 
@@ -1579,8 +1610,11 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         dev_upload(o, &D.rel_off, P_.rel_off) || dev_upload(o, &D.rbase, P_.rbase) ||
         dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
         dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs) ||
-        dev_upload(o, &D.linv_off, P_.linv_off) || dev_upload(o, &D.xinv_off, P_.xinv_off))
+        dev_upload(o, &D.linv_off, P_.linv_off) || dev_upload(o, &D.xinv_off, P_.xinv_off) ||
+        dev_upload(o, &D.rect_off, P_.rect_off))
         return -4;
+    CK(cudaMalloc((void**)&D.pbuf, std::max<int64_t>(P_.rect_entries, 1) * kMaxRHS * sizeof(double)));
+    o.push_back(D.pbuf);
     CK(cudaMalloc((void**)&D.xinv, std::max<int64_t>(P_.xinv_doubles, 1) * sizeof(double)));
     o.push_back(D.xinv);
     CK(cudaMalloc((void**)&D.linv, std::max<int64_t>(P_.linv_doubles, 1) * sizeof(double)));
@@ -1670,6 +1704,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.linv = D.linv;
     v.xinv_off = D.xinv_off;
     v.xinv = D.xinv;
+    v.rect_off = D.rect_off;
     v.tol1 = tol1;
     return v;
 }
@@ -1894,9 +1929,14 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 ++nl;
                 const Launch& wb = lp.writeback;
                 const Launch& rl = lp.rect;
-                if (rl.ntasks > 0)
-                    k_bwd_rect2<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, pv, D.vbuf, nr);
-                ++nl;
+                if (rl.ntasks > 0) {
+                    k_bwd_rect_part<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, pv, D.vbuf,
+                                                                    D.pbuf, nr);
+                    ++nl;
+                    k_bwd_rect_sum<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                                                                      D.vbuf, D.pbuf, nr);
+                    ++nl;
+                }
                 for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
                     const Launch& ml = lp.blk_mv[sb];
                     k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, pv, D.vbuf,

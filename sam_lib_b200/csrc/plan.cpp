@@ -238,6 +238,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         }
     // ---- batched launches of the large path
     P.jobs.clear();
+    P.rect_off.assign(ns, 0);
+    P.rect_entries = 0;
     auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };
     auto add_job = [&](Launch& l, Job j, int64_t ntask, bool keep_empty = false) {
         if (ntask <= 0 && !keep_empty) return;
@@ -376,10 +378,17 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             close_launch(lp.bs_upd[sb]);
         }
         open_launch(lp.rect);
+        int64_t roff = 0;
         for (int32_t js : lp.large_nodes) {
             const int32_t s = P.S[js], f = P.F[js];
-            if (f > s) add_job(lp.rect, Job{js, 0, s, f, s, f, 0}, (s + kRectCols - 1) / kRectCols);
+            if (f <= s) continue;
+            const int64_t nrc = (f - s + kRectRows - 1) / kRectRows;
+            const int64_t ncc = (s + kRectCols - 1) / kRectCols;
+            P.rect_off[js] = roff;
+            roff += nrc * s;
+            add_job(lp.rect, Job{js, 0, s, f, (int32_t)nrc, (int32_t)ncc, 0}, nrc * ncc);
         }
+        P.rect_entries = std::max(P.rect_entries, roff);
         close_launch(lp.rect);
         {
             std::vector<Job> jl;

@@ -76,6 +76,7 @@ constexpr int kBwdCols = 8;                   // columns per CTA in the back-sol
 constexpr int kSolveBlock = 256;              // width of a solve step (4 diagonal blocks of kNB)
 constexpr int kSolveRows = 32;                // rows per CTA in the forward update (x 8 column groups)
 constexpr int kRectCols = 32;                 // columns per CTA in the back-solve rectangle
+constexpr int kRectRows = 1024;               // rows per CTA in the back-solve rectangle
 
 struct Plan {
     // sizes
@@ -107,6 +108,10 @@ struct Plan {
     std::vector<int64_t> xinv_off;
     int64_t xinv_doubles = 0;
     Launch inv_blocks;                        // one task per (large front, solve block)
+    // back-solve rectangle partial sums: node js uses rect_off[js] .. + nchunk*S entries
+    // (each kMaxRHS doubles) of a scratch of rect_entries entries (max over levels)
+    std::vector<int64_t> rect_off;
+    int64_t rect_entries = 0;
     bool any_large = false;
     // levels and tasks
     std::vector<LevelPlan> levels;
