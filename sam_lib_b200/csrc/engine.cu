@@ -724,118 +724,84 @@ __global__ void k_writeback(const Job* jobs, int64_t njobs, int64_t ntasks, PV P
 // vector are its update vector for the parent.
 // ---------------------------------------------------------------------------
 constexpr int kSolveThreads = 256;
-constexpr int kSolveBlk = 32;
+
+// Small fronts (F <= kSmallMaxF): the front vector lives in shared memory.
+constexpr size_t kSmallSolveSmem = sizeof(double) * (size_t)kSmallMaxF * kMaxRHS;
 
 __global__ void __launch_bounds__(kSolveThreads)
 k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
+    extern __shared__ double wsm[];           // w[i * nrhs + r]
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
+    double* wg = vbuf + P.rbase[js] * nrhs;   // update rows for the parent (r*F + i)
     const double* Lb = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x;
     // gather: own rows from b, plus the children's update vectors (SPRFB1 + extend-add)
-    for (int i = tid; i < F; i += blockDim.x) {
+    for (int e = tid; e < F * nrhs; e += blockDim.x) {
+        const int i = e % F, r = e / F;
+        double v = (i < S) ? b[(int64_t)(fst + i) + r * ldb] : 0.0;
         const int64_t e0 = P.cptr[P.rbase[js] + i], e1 = P.cptr[P.rbase[js] + i + 1];
-        for (int r = 0; r < nrhs; ++r) {
-            double v = (i < S) ? b[(int64_t)(fst + i) + r * ldb] : 0.0;
-            for (int64_t e = e0; e < e1; ++e) {
-                const int c = P.cchild[e], t = P.ct[e];
-                const int fc = P.F[c];
-                v += vbuf[P.rbase[c] * nrhs + (int64_t)r * fc + P.S[c] + t];
-            }
-            w[(int64_t)r * F + i] = v;
+        for (int64_t q = e0; q < e1; ++q) {
+            const int c = P.cchild[q], t = P.ct[q];
+            v += vbuf[P.rbase[c] * nrhs + (int64_t)r * P.F[c] + P.S[c] + t];
         }
+        wsm[i * nrhs + r] = v;
     }
     __syncthreads();
-    for (int jb = 0; jb < S; jb += kSolveBlk) {
-        const int je = min(jb + kSolveBlk, S);
-        // triangle of the block (SPRFS5 :600-608), one warp
-        if (tid < 32) {
-            for (int j = jb; j < je; ++j) {
-                const double* cj = Lb + lnz_col(j, F) - j;
-                const int i = j + 1 + lane;
-                if (i < je)
-                    for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= w[(int64_t)r * F + j] * cj[i];
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        // rectangle below the block (SPRFS6)
-        for (int i = je + tid; i < F; i += blockDim.x) {
-            double acc[kMaxRHS];
-            for (int r = 0; r < nrhs; ++r) acc[r] = w[(int64_t)r * F + i];
-            for (int j = jb; j < je; ++j) {
-                const double l = Lb[lnz_col(j, F) - j + i];
-                for (int r = 0; r < nrhs; ++r) acc[r] -= w[(int64_t)r * F + j] * l;
-            }
-            for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = acc[r];
+    // column j eliminates all rows below it (SPRFS5 triangle + SPRFS6 rectangle)
+    for (int j = 0; j < S; ++j) {
+        const double* cj = Lb + lnz_col(j, F) - j;
+        const int m = F - j - 1;
+        for (int e = tid; e < m * nrhs; e += blockDim.x) {
+            const int i = j + 1 + e % m, r = e / m;
+            wsm[i * nrhs + r] -= wsm[j * nrhs + r] * cj[i];
         }
         __syncthreads();
     }
-    // diagonal (SPRFS5 :622-625) and scatter of the own rows (SPRFB2)
-    for (int j = tid; j < S; j += blockDim.x) {
-        const double d = Lb[lnz_col(j, F)];
-        for (int r = 0; r < nrhs; ++r) {
-            const double y = w[(int64_t)r * F + j] / d;
-            w[(int64_t)r * F + j] = y;
-            b[(int64_t)(fst + j) + r * ldb] = y;
+    // diagonal (SPRFS5 :622-625), own rows to b, update rows to the parent
+    for (int e = tid; e < F * nrhs; e += blockDim.x) {
+        const int i = e % F, r = e / F;
+        if (i < S) {
+            const double y = wsm[i * nrhs + r] / Lb[lnz_col(i, F)];
+            b[(int64_t)(fst + i) + r * ldb] = y;
+        } else {
+            wg[(int64_t)r * F + i] = wsm[i * nrhs + r];
         }
     }
 }
 
 __global__ void __launch_bounds__(kSolveThreads)
 k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
-    __shared__ double part[kSolveBlk][kMaxRHS];
+    extern __shared__ double wsm[];           // w[i * nrhs + r]
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
-    double* w = vbuf + P.rbase[js] * nrhs;
     const double* Lb = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-    // gather: own rows (forward result) and the ancestors' solved rows.  The
-    // row list of front js starts at rbase[js] (LINDX is the concatenation of
-    // the fronts' row lists, XLINDX(js) - 1 == sum of the previous F).
-    for (int i = tid; i < F; i += blockDim.x) {
+    const int tid = threadIdx.x;
+    (void)vbuf;
+    // own rows (forward result) and the ancestors' solved rows; the row list
+    // of front js starts at rbase[js] (LINDX concatenates the row lists)
+    for (int e = tid; e < F * nrhs; e += blockDim.x) {
+        const int i = e % F, r = e / F;
         const int row = (i < S) ? (fst + i) : P.rows[P.rbase[js] + i];
-        for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = b[(int64_t)row + r * ldb];
+        wsm[i * nrhs + r] = b[(int64_t)row + r * ldb];
     }
     __syncthreads();
-    const int nblk = (S + kSolveBlk - 1) / kSolveBlk;
-    for (int bi = nblk - 1; bi >= 0; --bi) {
-        const int jb = bi * kSolveBlk, je = min(jb + kSolveBlk, S);
-        // contributions of the rows below the block (SPRBS6 dot products)
-        for (int c = jb + warp; c < je; c += nwarp) {
-            const double* cc = Lb + lnz_col(c, F) - c;
-            double acc[kMaxRHS];
-            for (int r = 0; r < nrhs; ++r) acc[r] = 0.0;
-            for (int i = je + lane; i < F; i += 32) {
-                const double l = cc[i];
-                for (int r = 0; r < nrhs; ++r) acc[r] += l * w[(int64_t)r * F + i];
-            }
-            for (int r = 0; r < nrhs; ++r) {
-                double v = acc[r];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) part[c - jb][r] = v;
-            }
-        }
+    // x_j = w_j - sum_{i>j} L_ij x_i (SPRBS6): 16 lanes per right-hand side
+    const int r = tid >> 4, li = tid & 15;
+    for (int j = S - 1; j >= 0; --j) {
+        const double* cj = Lb + lnz_col(j, F) - j;
+        double v = 0.0;
+        if (r < nrhs)
+            for (int i = j + 1 + li; i < F; i += 16) v += cj[i] * wsm[i * nrhs + r];
+        for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         __syncthreads();
-        // triangle of the block, bottom-up, one warp
-        if (tid < 32) {
-            for (int c = je - 1; c >= jb; --c) {
-                const double* cc = Lb + lnz_col(c, F) - c;
-                for (int r = 0; r < nrhs; ++r) {
-                    double v = 0.0;
-                    const int i = c + 1 + lane;
-                    if (i < je) v = cc[i] * w[(int64_t)r * F + i];
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0) w[(int64_t)r * F + c] -= part[c - jb][r] + v;
-                }
-                __syncwarp();
-            }
-        }
+        if (r < nrhs && li == 0) wsm[j * nrhs + r] -= v;
         __syncthreads();
     }
-    for (int j = tid; j < S; j += blockDim.x)
-        for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = w[(int64_t)r * F + j];
+    for (int e = tid; e < S * nrhs; e += blockDim.x) {
+        const int i = e % S, rr = e / S;
+        b[(int64_t)(fst + i) + rr * ldb] = wsm[i * nrhs + rr];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1887,7 +1853,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
             for (size_t L = 0; L < P_.levels.size(); ++L) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
-                    k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(D.level_nodes + D.small_begin[L],
+                    k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(D.level_nodes + D.small_begin[L],
                                                                                 pv, D.vbuf, b, ldb, nr);
                     ++nl;
                 }
@@ -1918,7 +1884,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
             for (size_t L = P_.levels.size(); L-- > 0;) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
-                    k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, 0, s>>>(
+                    k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(
                         D.level_nodes + D.small_begin[L], pv, D.vbuf, b, ldb, nr);
                     ++nl;
                 }
