@@ -86,6 +86,7 @@ struct Engine::Dev {
     double* linv = nullptr;
     int64_t* xinv_off = nullptr;
     double* xinv = nullptr;
+    int32_t* task_map = nullptr;
     int64_t* rect_off = nullptr;
     double* pbuf = nullptr;                      // back-solve rectangle partial sums
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
@@ -140,6 +141,12 @@ __device__ __forceinline__ int64_t find_job(const Job* jobs, int64_t n, int64_t 
         else hi = mid - 1;
     }
     return lo;
+}
+
+// job of a task: one load from the launch's task map, or a binary search
+// over the jobs' first tasks when no map is given
+__device__ __forceinline__ const Job& job_of(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t t) {
+    return tmap ? jobs[tmap[t]] : jobs[find_job(jobs, njobs, t)];
 }
 
 // packed lower, column-major, order F: column j holds rows j..F-1
@@ -309,7 +316,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
 // ---------------------------------------------------------------------------
 
 // A large front whose child failed (or depends on a failure) is skipped.
-__global__ void k_poison(const Job* jobs, int64_t njobs, PV P) {
+__global__ void k_poison(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     const int js = jobs[j].node;
@@ -317,12 +324,12 @@ __global__ void k_poison(const Job* jobs, int64_t njobs, PV P) {
 }
 
 // Extend-add into a dense column-major front: one warp per front column.
-__global__ void k_assemble(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {
+__global__ void k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P) {
     if (P.st->any_fail) return;
     const int lane = threadIdx.x & 31;
     const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     if (P.sn_bad[js]) return;
     const int j = jb.c0 + (int)(task - jb.task0);
@@ -446,14 +453,14 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 constexpr int kTrsmLds = kNB + 4;
 constexpr size_t kTrsmSmem = sizeof(double) * (2 * (size_t)kNB * kTrsmLds + kNB);
 
-__global__ void __launch_bounds__(128) k_trsm(const Job* jobs, int64_t njobs, PV P) {
+__global__ void __launch_bounds__(128) k_trsm(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
     extern __shared__ double tsh[];
     double(*As)[kTrsmLds] = reinterpret_cast<double(*)[kTrsmLds]>(tsh);              // As[m][i]
     double(*Xs)[kTrsmLds] = reinterpret_cast<double(*)[kTrsmLds]>(tsh + kNB * kTrsmLds);  // Xs[m][c] = X[c][m]
     double* rd = tsh + 2 * kNB * kTrsmLds;
     if (P.st->any_fail) return;
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     if (P.sn_bad[js]) return;
     const int F = P.F[js], ld = P.buf_ld[js];
@@ -564,7 +571,7 @@ struct Cfg {
 
 template <int T, int WM, int WN, int STAGES>
 __global__ void __launch_bounds__(gemm::Cfg<T, WM, WN, STAGES>::NT)
-k_gemm(const Job* jobs, int64_t njobs, PV P) {
+k_gemm(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
     using namespace gemm;
     using C = Cfg<T, WM, WN, STAGES>;
     extern __shared__ __align__(16) double gsh[];
@@ -573,7 +580,7 @@ k_gemm(const Job* jobs, int64_t njobs, PV P) {
     double* Ds = Bs + STAGES * BK * C::LDS;         // [STAGES][BK]
     if (P.st->any_fail) return;
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     if (P.sn_bad[js]) return;
     const int ld = P.buf_ld[js];
@@ -702,12 +709,12 @@ using GemmSmall = gemm::Cfg<kTile, 32, 32, SPR_GEMM_STAGES>;
 #define K_GEMM_SMALL k_gemm<kTile, 32, 32, SPR_GEMM_STAGES>
 
 // Store the S factored columns of a dense front into LNZ (sprfc1.f:630-637).
-__global__ void k_writeback(const Job* jobs, int64_t njobs, int64_t ntasks, PV P) {
+__global__ void k_writeback(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P) {
     if (P.st->any_fail) return;
     const int lane = threadIdx.x & 31;
     const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     if (P.sn_bad[js]) return;
     const int j = jb.c0 + (int)(task - jb.task0);
@@ -813,11 +820,11 @@ __device__ __forceinline__ const double* lcol(const PV& P, int js, int F, int j)
 }
 
 // gather of the forward sweep: own rows of B plus the children's update vectors
-__global__ void k_fwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+__global__ void k_fwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
                              const double* b, int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int i = (int)(task - jb.task0);
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
@@ -833,169 +840,11 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     }
 }
 
-// One forward step of a large front.  Every CTA computes the solved block
-// y = X w_block with the stored inverse X = L11^-1 (a 64x64 product in
-// shared memory, no sequential chain); CTA 0 of the job stores y in ysol,
-// the others update kTRSMRows rows below the block (SPRFS5 + SPRFS6).
-__global__ void __launch_bounds__(kTRSMRows) k_fwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
-                                                        double* ysol, int nrhs) {
-    __shared__ double Xs[kNB][kNB + 1];
-    __shared__ double wb[kNB][kMaxRHS];
-    const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
-    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
-    const int F = P.F[js];
-    const int64_t vb = P.rbase[js] * nrhs;
-    double* w = vbuf + vb;
-    const double* base = P.lnz + P.lnz_off[js];
-    const double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
-    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-        const int c = e % nb, r = e / nb;
-        wb[c][r] = w[(int64_t)r * F + k0 + c];
-    }
-    __syncthreads();
-    double sol[kMaxRHS];
-    if (tid < nb) {
-        const int c = tid;
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) {
-            double acc = 0.0;
-            if (r < nrhs)
-                for (int m = 0; m <= c; ++m) acc += Xs[c][m] * wb[m][r];
-            sol[r] = acc;
-        }
-    }
-    __syncthreads();
-    if (tid < nb)
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) wb[tid][r] = sol[r];
-    __syncthreads();
-    double(*yb)[kMaxRHS] = wb;
-    const int64_t u = task - jb.task0;
-    if (u == 0) {
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            ysol[vb + (int64_t)r * F + k0 + c] = yb[c][r];
-        }
-        return;
-    }
-    const int i = jb.c0 + (int)(u - 1) * kTRSMRows + tid;
-    if (i >= F) return;
-    double acc[kMaxRHS];
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
-#pragma unroll 8
-    for (int c = 0; c < nb; ++c) {
-        const double l = base[lnz_col(k0 + c, F) - (k0 + c) + i];
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) acc[r] -= l * yb[c][r];
-    }
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r)
-        if (r < nrhs) w[(int64_t)r * F + i] = acc[r];
-}
-
 // Solve steps of kSolveBlock (256) columns.  Forward: one CTA per front
 // solves the block's unit-lower triangle (4 diagonal blocks of 64, each a
 // product with its stored inverse X, then the rows below it inside the
 // block), stores the block in ysol; then k_fwd_blk_upd applies it to every
 // row below the block (thread per row, SPRFS6).  Backward mirrors it.
-constexpr size_t kBlkDiagSmem = sizeof(double) * ((size_t)kNB * (kNB + 1) + 2 * (size_t)kSolveBlock * kMaxRHS);
-
-__global__ void __launch_bounds__(256) k_fwd_blk_diag(const Job* jobs, PV P, const double* vbuf, double* ysol,
-                                                      int nrhs) {
-    extern __shared__ double fsh[];
-    double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(fsh);
-    double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(fsh + kNB * (kNB + 1));
-    double(*t)[kMaxRHS] = y + kSolveBlock;
-    const Job& jb = jobs[blockIdx.x];
-    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
-    const int F = P.F[js], nbk = k1 - k0;
-    const int64_t vb = P.rbase[js] * nrhs;
-    const double* w = vbuf + vb;
-    const double* base = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x;
-    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
-        const int i = e % nbk, r = e / nbk;
-        y[i][r] = w[(int64_t)r * F + k0 + i];
-    }
-    for (int j0 = 0; j0 < nbk; j0 += kNB) {
-        const int nb = min(kNB, nbk - j0);
-        const double* lv = P.linv + P.linv_off[js] + (int64_t)((k0 + j0) / kNB) * kNB * kNB;
-        for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
-        __syncthreads();
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            double acc = 0.0;
-            for (int m = 0; m <= c; ++m) acc += Xs[c][m] * y[j0 + m][r];
-            t[c][r] = acc;
-        }
-        __syncthreads();
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            y[j0 + c][r] = t[c][r];
-        }
-        __syncthreads();
-        for (int i = j0 + nb + tid; i < nbk; i += blockDim.x) {
-            double acc[kMaxRHS];
-#pragma unroll
-            for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? y[i][r] : 0.0;
-#pragma unroll 8
-            for (int c = 0; c < nb; ++c) {
-                const int col = k0 + j0 + c;
-                const double l = base[lnz_col(col, F) - col + (k0 + i)];
-#pragma unroll
-                for (int r = 0; r < kMaxRHS; ++r)
-                    if (r < nrhs) acc[r] -= l * y[j0 + c][r];
-            }
-#pragma unroll
-            for (int r = 0; r < kMaxRHS; ++r)
-                if (r < nrhs) y[i][r] = acc[r];
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
-        const int i = e % nbk, r = e / nbk;
-        ysol[vb + (int64_t)r * F + k0 + i] = y[i][r];
-    }
-}
-
-__global__ void __launch_bounds__(kSolveRows) k_fwd_blk_upd(const Job* jobs, int64_t njobs, PV P, double* vbuf,
-                                                            const double* ysol, int nrhs) {
-    __shared__ double y[kSolveBlock][kMaxRHS];
-    const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
-    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
-    const int F = P.F[js], nbk = k1 - k0;
-    const int64_t vb = P.rbase[js] * nrhs;
-    double* w = vbuf + vb;
-    const double* base = P.lnz + P.lnz_off[js];
-    for (int e = threadIdx.x; e < nbk * nrhs; e += blockDim.x) {
-        const int i = e % nbk, r = e / nbk;
-        y[i][r] = ysol[vb + (int64_t)r * F + k0 + i];
-    }
-    __syncthreads();
-    const int i = jb.c0 + (int)(task - jb.task0) * kSolveRows + threadIdx.x;
-    if (i >= F) return;
-    double acc[kMaxRHS];
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) acc[r] = (r < nrhs) ? w[(int64_t)r * F + i] : 0.0;
-#pragma unroll 8
-    for (int c = 0; c < nbk; ++c) {
-        const int col = k0 + c;
-        const double l = base[lnz_col(col, F) - col + i];
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) acc[r] -= l * y[c][r];
-    }
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r)
-        if (r < nrhs) w[(int64_t)r * F + i] = acc[r];
-}
 
 // w[m] -= sum_{c < n} L[row0 + c, m] x[c][.] by one warp (column m of L contiguous)
 __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, const double (*x)[kMaxRHS],
@@ -1019,76 +868,11 @@ __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, 
     }
 }
 
-__global__ void __launch_bounds__(256) k_bwd_blk_diag(const Job* jobs, PV P, const double* vbuf, double* xsol,
-                                                      int nrhs) {
-    extern __shared__ double bsh[];
-    double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(bsh);
-    double(*x)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(bsh + kNB * (kNB + 1));
-    double(*t)[kMaxRHS] = x + kSolveBlock;
-    const Job& jb = jobs[blockIdx.x];
-    const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
-    const int F = P.F[js], nbk = k1 - k0;
-    const int64_t vb = P.rbase[js] * nrhs;
-    const double* w = vbuf + vb;
-    const double* base = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
-        const int i = e % nbk, r = e / nbk;
-        x[i][r] = w[(int64_t)r * F + k0 + i];
-    }
-    const int nsub = (nbk + kNB - 1) / kNB;
-    for (int jj = nsub - 1; jj >= 0; --jj) {
-        const int j0 = jj * kNB, nb = min(kNB, nbk - j0);
-        const double* lv = P.linv + P.linv_off[js] + (int64_t)((k0 + j0) / kNB) * kNB * kNB;
-        for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
-        __syncthreads();
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            double acc = 0.0;
-            for (int m = c; m < nb; ++m) acc += Xs[m][c] * x[j0 + m][r];
-            t[c][r] = acc;
-        }
-        __syncthreads();
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            x[j0 + c][r] = t[c][r];
-        }
-        __syncthreads();
-        // earlier columns of the block: x[q] -= L[k0+j0 : k0+j0+nb, k0+q]' x_j
-        for (int q = warp; q < j0; q += nwarp) {
-            const int col = k0 + q;
-            const double* cm = base + lnz_col(col, F) - col + (k0 + j0);
-            const int lane0 = lane;
-            double acc[kMaxRHS];
-#pragma unroll
-            for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
-            for (int c = lane0; c < nb; c += 32) {
-                const double l = cm[c];
-#pragma unroll
-                for (int r = 0; r < kMaxRHS; ++r)
-                    if (r < nrhs) acc[r] += l * x[j0 + c][r];
-            }
-#pragma unroll
-            for (int r = 0; r < kMaxRHS; ++r) {
-                if (r >= nrhs) break;
-                double v = acc[r];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) x[q][r] -= v;
-            }
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
-        const int i = e % nbk, r = e / nbk;
-        xsol[vb + (int64_t)r * F + k0 + i] = x[i][r];
-    }
-}
-
-__global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+__global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
                                                      const double* xsol, int nrhs) {
     __shared__ double x[kSolveBlock][kMaxRHS];
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
     const int F = P.F[js], nbk = k1 - k0;
     const int64_t vb = P.rbase[js] * nrhs;
@@ -1194,13 +978,13 @@ __global__ void __launch_bounds__(256) k_inv_block(const Job* jobs, PV P) {
 // y_block = X w_block: 32 rows per CTA, 8 warps split the columns
 constexpr size_t kMvSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + 8 * 32 * (kMaxRHS + 1));
 
-__global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+__global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
                                                     double* ysol, int nrhs) {
     extern __shared__ double msh[];
     double(*wb)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(msh);
     double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(msh + kSolveBlock * kMaxRHS);
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
     const int64_t vb = P.rbase[js] * nrhs;
@@ -1238,11 +1022,11 @@ __global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njo
 }
 
 // x_block = X' w_block: 32 columns per CTA, 4 per warp, lanes over rows
-__global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+__global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
                                                     double* xsol, int nrhs) {
     __shared__ double wb[kSolveBlock][kMaxRHS];
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
     const int64_t vb = P.rbase[js] * nrhs;
@@ -1277,13 +1061,13 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
 }
 
 // rows below a solve block: w[i] -= L[i, k0:k1] y, 32 rows x 8 column groups per CTA
-__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, PV P, double* vbuf,
+__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
                                                       const double* ysol, int nrhs) {
     extern __shared__ double ush[];
     double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(ush);
     double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(ush + kSolveBlock * kMaxRHS);
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
     const int F = P.F[js], nbk = k1 - k0;
     const int64_t vb = P.rbase[js] * nrhs;
@@ -1327,11 +1111,11 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
 // per column, 4 columns per warp, the vector staged in shared memory);
 // phase 2 (k_bwd_rect_sum) adds the partials of each column in a fixed order,
 // so the result is deterministic.
-__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, PV P, const double* vbuf,
+__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
                                                        double* pbuf, int nrhs) {
     __shared__ double ws[256][kMaxRHS];
     const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int F = P.F[js], S = P.S[js];
     const int ncc = jb.k_hi;
@@ -1384,11 +1168,11 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     }
 }
 
-__global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+__global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
                                const double* pbuf, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int F = P.F[js], S = P.S[js];
     if (F <= S) return;
@@ -1404,11 +1188,11 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, int64_t ntasks, P
 }
 
 // y_j /= d_j and scatter of the own rows (thread per column)
-__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* ysol, double* b,
+__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, const double* ysol, double* b,
                              int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
@@ -1418,11 +1202,11 @@ __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
 }
 
 // gather of the back sweep: own rows (forward result) and ancestors' solution
-__global__ void k_bwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf,
+__global__ void k_bwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
                              const double* b, int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int i = (int)(task - jb.task0);
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
@@ -1431,115 +1215,12 @@ __global__ void k_bwd_gather(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
     for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] = b[(int64_t)row + r * ldb];
 }
 
-// w[c] -= sum over rows [lo, hi) of L[i,c] w[i]; one warp per column c
-__device__ __forceinline__ void warp_col_dot(const PV& P, int js, int F, int c, int lo, int hi, double* w,
-                                             int nrhs) {
-    const int lane = threadIdx.x & 31;
-    const double* cc = lcol(P, js, F, c);
-    double acc[kMaxRHS];
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
-    for (int i = lo + lane; i < hi; i += 32) {
-        const double l = cc[i];
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) acc[r] += l * w[(int64_t)r * F + i];
-    }
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) {
-        if (r >= nrhs) break;
-        double v = acc[r];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) w[(int64_t)r * F + c] -= v;
-    }
-}
 
-// rectangle: contributions of the update rows [S, F) to every column c < S
-__global__ void k_bwd_rect(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, double* vbuf, int nrhs) {
-    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
-    const int js = jb.node;
-    const int c = (int)(task - jb.task0);
-    const int F = P.F[js], S = P.S[js];
-    warp_col_dot(P, js, F, c, S, F, vbuf + P.rbase[js] * nrhs, nrhs);
-}
-
-// One back step of a large front: every CTA forms x = X' w_block with the
-// stored inverse; CTA 0 stores x in xsol, the others apply x to kBwdCols
-// columns m < k0 each (one warp per column: w[m] -= L[k0:k1, m]' x),
-// SPRBS6 in blocked form.
-__global__ void __launch_bounds__(256) k_bwd_step(const Job* jobs, int64_t njobs, PV P, double* vbuf,
-                                                  double* xsol, int nrhs) {
-    __shared__ double Xs[kNB][kNB + 1];
-    __shared__ double wb[kNB][kMaxRHS];
-    const int64_t task = blockIdx.x;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
-    const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
-    const int F = P.F[js];
-    const int64_t vb = P.rbase[js] * nrhs;
-    double* w = vbuf + vb;
-    const double* base = P.lnz + P.lnz_off[js];
-    const double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < kNB * kNB; e += blockDim.x) Xs[e % kNB][e / kNB] = lv[e];
-    for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-        const int c = e % nb, r = e / nb;
-        wb[c][r] = w[(int64_t)r * F + k0 + c];
-    }
-    __syncthreads();
-    double sol[kMaxRHS];
-    if (tid < nb) {
-        const int c = tid;
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) {
-            double acc = 0.0;
-            if (r < nrhs)
-                for (int m = c; m < nb; ++m) acc += Xs[m][c] * wb[m][r];
-            sol[r] = acc;
-        }
-    }
-    __syncthreads();
-    if (tid < nb)
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) wb[tid][r] = sol[r];
-    __syncthreads();
-    double(*xb)[kMaxRHS] = wb;
-    const int64_t u = task - jb.task0;
-    if (u == 0) {
-        for (int e = tid; e < nb * nrhs; e += blockDim.x) {
-            const int c = e % nb, r = e / nb;
-            xsol[vb + (int64_t)r * F + k0 + c] = xb[c][r];
-        }
-        return;
-    }
-    const int m = (int)(u - 1) * kBwdCols + warp;
-    if (m >= k0) return;
-    const double* cm = base + lnz_col(m, F) - m;       // column m, indexed by row
-    double acc[kMaxRHS];
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
-    for (int c = lane; c < nb; c += 32) {
-        const double l = cm[k0 + c];
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) acc[r] += l * xb[c][r];
-    }
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) {
-        if (r >= nrhs) break;
-        double v = acc[r];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) w[(int64_t)r * F + m] -= v;
-    }
-}
-
-__global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV P, const double* xsol, double* b,
+__global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, const double* xsol, double* b,
                              int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
-    const Job& jb = jobs[find_job(jobs, njobs, task)];
+    const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
@@ -1550,6 +1231,7 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, int64_t ntasks, PV 
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
+#define TMAP(l) ((l).map_begin >= 0 ? d_->task_map + (l).map_begin : nullptr)
 Engine::Engine() : d_(new Dev()) {}
 
 Engine::~Engine() {
@@ -1577,7 +1259,7 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
         dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs) ||
         dev_upload(o, &D.linv_off, P_.linv_off) || dev_upload(o, &D.xinv_off, P_.xinv_off) ||
-        dev_upload(o, &D.rect_off, P_.rect_off))
+        dev_upload(o, &D.rect_off, P_.rect_off) || dev_upload(o, &D.task_map, P_.task_map))
         return -4;
     CK(cudaMalloc((void**)&D.pbuf, std::max<int64_t>(P_.rect_entries, 1) * kMaxRHS * sizeof(double)));
     o.push_back(D.pbuf);
@@ -1624,8 +1306,6 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
     CK(cudaFuncSetAttribute(k_inv_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
-    CK(cudaFuncSetAttribute(k_fwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
-    CK(cudaFuncSetAttribute(k_bwd_blk_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkDiagSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     return 0;
@@ -1680,9 +1360,9 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     if (profile_) gev.push_back(record_event(s));
     const Job* jobs = d_->jobs + l.job_begin;
     if (l.tile == kTileBig)
-        K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, pv);
+        K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
     else
-        K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, pv);
+        K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
     if (profile_) gev.push_back(record_event(s));
     ++timing.launches;
     ++timing.gemm_launches;
@@ -1719,9 +1399,9 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
         const Job* jobs = D.jobs;
         {
             const Launch& l = lp.assemble;
-            k_poison<<<(int)((l.job_count + 127) / 128), 128, 0, s>>>(jobs + l.job_begin, l.job_count, pv);
+            k_poison<<<(int)((l.job_count + 127) / 128), 128, 0, s>>>(jobs + l.job_begin, l.job_count, TMAP(l), pv);
             const int64_t threads = l.ntasks * 32;
-            k_assemble<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, l.ntasks, pv);
+            k_assemble<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, TMAP(l), l.ntasks, pv);
             ++timing.launches;
         }
         for (size_t st = 0; st < lp.panel.size(); ++st) {
@@ -1729,7 +1409,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
             k_diag<<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             ++timing.launches;
             if (pl.ntasks > 0) {
-                k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, pv);
+                k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, TMAP(pl), pv);
                 ++timing.launches;
             }
             for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
@@ -1738,7 +1418,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
         {
             const Launch& l = lp.writeback;
             const int64_t threads = l.ntasks * 32;
-            k_writeback<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, l.ntasks, pv);
+            k_writeback<<<(int)((threads + 255) / 256), 256, 0, s>>>(jobs + l.job_begin, l.job_count, TMAP(l), l.ntasks, pv);
             ++timing.launches;
         }
     }
@@ -1859,23 +1539,23 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
-                k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
+                k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, TMAP(ga), ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
                     const Launch& ml = lp.blk_mv[sb];
-                    k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, pv, D.vbuf,
+                    k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
                     const Launch& fl = lp.fs_upd[sb];
                     if (fl.ntasks > 0) {
-                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kMvSmem, s>>>(jobs + fl.job_begin, fl.job_count, pv,
+                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kMvSmem, s>>>(jobs + fl.job_begin, fl.job_count, TMAP(fl), pv,
                                                                        D.vbuf, D.vbuf2, nr);
                         ++nl;
                     }
                 }
                 const Launch& wb = lp.writeback;
-                k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
                 ++nl;
             }
@@ -1890,32 +1570,32 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
-                k_bwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, ga.ntasks, pv,
+                k_bwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, TMAP(ga), ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 const Launch& wb = lp.writeback;
                 const Launch& rl = lp.rect;
                 if (rl.ntasks > 0) {
-                    k_bwd_rect_part<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, pv, D.vbuf,
+                    k_bwd_rect_part<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, TMAP(rl), pv, D.vbuf,
                                                                     D.pbuf, nr);
                     ++nl;
-                    k_bwd_rect_sum<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                    k_bwd_rect_sum<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                       D.vbuf, D.pbuf, nr);
                     ++nl;
                 }
                 for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
                     const Launch& ml = lp.blk_mv[sb];
-                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, pv, D.vbuf,
+                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
                     const Launch& bl = lp.bs_upd[sb];
                     if (bl.ntasks > 0) {
-                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, pv, D.vbuf,
+                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, TMAP(bl), pv, D.vbuf,
                                                                      D.vbuf2, nr);
                         ++nl;
                     }
                 }
-                k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, wb.ntasks, pv,
+                k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
                 ++nl;
             }
@@ -2041,9 +1721,10 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     for (int64_t stp = 0; stp < nblk; ++stp) {
         const StepJobs& sj = steps[stp];
         k_diag<<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
-        if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, pv);
+        if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, nullptr, pv);
         if (sj.upd_tasks > 0)
-            K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, pv);
+            K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, nullptr,
+                                                                                 pv);
     }
     CK(cudaGetLastError());
     Stats hs;

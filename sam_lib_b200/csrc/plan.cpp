@@ -407,6 +407,28 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             add_job(lp.writeback, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, P.S[js]);
         close_launch(lp.writeback);
     }
+    // task -> job maps of every launch
+    P.task_map.clear();
+    auto build_map = [&](Launch& l) {
+        l.map_begin = (int64_t)P.task_map.size();
+        for (int64_t j = 0; j < l.job_count; ++j) {
+            const int64_t t0 = P.jobs[l.job_begin + j].task0;
+            const int64_t t1 = (j + 1 < l.job_count) ? P.jobs[l.job_begin + j + 1].task0 : l.ntasks;
+            for (int64_t t = t0; t < t1; ++t) P.task_map.push_back((int32_t)j);
+        }
+    };
+    for (LevelPlan& lp : P.levels) {
+        build_map(lp.assemble);
+        build_map(lp.writeback);
+        build_map(lp.rect);
+        for (Launch& l : lp.panel) build_map(l);
+        for (auto& v : lp.update)
+            for (Launch& l : v) build_map(l);
+        for (Launch& l : lp.outer) build_map(l);
+        for (Launch& l : lp.fs_upd) build_map(l);
+        for (Launch& l : lp.bs_upd) build_map(l);
+        for (Launch& l : lp.blk_mv) build_map(l);
+    }
     open_launch(P.inv_blocks);
     for (int64_t js = 0; js < ns; ++js) {
         if (P.F[js] <= kSmallMaxF) continue;

@@ -51,6 +51,7 @@ struct Job {
 struct Launch {                      // a contiguous range of Plan::jobs
     int64_t job_begin = 0, job_count = 0, ntasks = 0;
     int32_t tile = kTile;            // Schur-update launches: tile size of the decode
+    int64_t map_begin = -1;          // task -> job map of this launch in Plan::task_map
 };
 
 struct LevelPlan {
@@ -116,6 +117,9 @@ struct Plan {
     // levels and tasks
     std::vector<LevelPlan> levels;
     std::vector<Job> jobs;
+    // for every launch: the job (relative to Launch::job_begin) of each task,
+    // so a CTA finds its job with one load instead of a binary search
+    std::vector<int32_t> task_map;
     // statistics (the reference's own counters are recomputed for reporting)
     double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
