@@ -732,18 +732,21 @@ __global__ void k_writeback(const Job* jobs, int64_t njobs, const int32_t* tmap,
 // ---------------------------------------------------------------------------
 constexpr int kSolveThreads = 256;
 
-// Small fronts (F <= kSmallMaxF): the front vector lives in shared memory.
-constexpr size_t kSmallSolveSmem = sizeof(double) * (size_t)kSmallMaxF * kMaxRHS;
+// Small fronts (F <= kSmallMaxF): the front vector and one 32-column block of
+// L live in shared memory; per block, one warp solves the 32x32 triangle and
+// all threads apply the block to the rows below it (3 barriers per block).
+constexpr int kSmallBlk = 32;
+constexpr size_t kSmallSolveSmem = sizeof(double) * ((size_t)kSmallMaxF * kMaxRHS + (size_t)kSmallMaxF * (kSmallBlk + 1));
 
 __global__ void __launch_bounds__(kSolveThreads)
 k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
-    extern __shared__ double wsm[];           // w[i * nrhs + r]
+    extern __shared__ double wsm[];           // w[i * nrhs + r], then Ls[(i - j0) * (kSmallBlk + 1) + c]
+    double* Ls = wsm + kSmallMaxF * kMaxRHS;
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* wg = vbuf + P.rbase[js] * nrhs;   // update rows for the parent (r*F + i)
     const double* Lb = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x;
-    // gather: own rows from b, plus the children's update vectors (SPRFB1 + extend-add)
+    const int tid = threadIdx.x, lane = tid & 31;
     for (int e = tid; e < F * nrhs; e += blockDim.x) {
         const int i = e % F, r = e / F;
         double v = (i < S) ? b[(int64_t)(fst + i) + r * ldb] : 0.0;
@@ -754,36 +757,46 @@ k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int 
         }
         wsm[i * nrhs + r] = v;
     }
-    __syncthreads();
-    // column j eliminates all rows below it (SPRFS5 triangle + SPRFS6 rectangle)
-    for (int j = 0; j < S; ++j) {
-        const double* cj = Lb + lnz_col(j, F) - j;
-        const int m = F - j - 1;
-        for (int e = tid; e < m * nrhs; e += blockDim.x) {
-            const int i = j + 1 + e % m, r = e / m;
-            wsm[i * nrhs + r] -= wsm[j * nrhs + r] * cj[i];
+    for (int j0 = 0; j0 < S; j0 += kSmallBlk) {
+        const int nb = min(kSmallBlk, S - j0), m = F - j0;
+        for (int e = tid; e < m * nb; e += blockDim.x) {
+            const int i = e % m, c = e / m;
+            Ls[i * (kSmallBlk + 1) + c] = (i > c) ? Lb[lnz_col(j0 + c, F) - (j0 + c) + (j0 + i)] : 0.0;
+        }
+        __syncthreads();
+        if (tid < 32) {                       // triangle of the block (SPRFS5 :600-608)
+            for (int c = 0; c < nb - 1; ++c) {
+                for (int e = lane; e < (nb - c - 1) * nrhs; e += 32) {
+                    const int i = c + 1 + e % (nb - c - 1), r = e / (nb - c - 1);
+                    wsm[(j0 + i) * nrhs + r] -= wsm[(j0 + c) * nrhs + r] * Ls[i * (kSmallBlk + 1) + c];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < (m - nb) * nrhs; e += blockDim.x) {   // rectangle (SPRFS6)
+            const int i = nb + e % (m - nb), r = e / (m - nb);
+            double v = wsm[(j0 + i) * nrhs + r];
+            for (int c = 0; c < nb; ++c) v -= Ls[i * (kSmallBlk + 1) + c] * wsm[(j0 + c) * nrhs + r];
+            wsm[(j0 + i) * nrhs + r] = v;
         }
         __syncthreads();
     }
-    // diagonal (SPRFS5 :622-625), own rows to b, update rows to the parent
     for (int e = tid; e < F * nrhs; e += blockDim.x) {
         const int i = e % F, r = e / F;
-        if (i < S) {
-            const double y = wsm[i * nrhs + r] / Lb[lnz_col(i, F)];
-            b[(int64_t)(fst + i) + r * ldb] = y;
-        } else {
-            wg[(int64_t)r * F + i] = wsm[i * nrhs + r];
-        }
+        if (i < S) b[(int64_t)(fst + i) + r * ldb] = wsm[i * nrhs + r] / Lb[lnz_col(i, F)];
+        else wg[(int64_t)r * F + i] = wsm[i * nrhs + r];
     }
 }
 
 __global__ void __launch_bounds__(kSolveThreads)
 k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
-    extern __shared__ double wsm[];           // w[i * nrhs + r]
+    extern __shared__ double wsm[];
+    double* Ls = wsm + kSmallMaxF * kMaxRHS;
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     const double* Lb = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     (void)vbuf;
     // own rows (forward result) and the ancestors' solved rows; the row list
     // of front js starts at rbase[js] (LINDX concatenates the row lists)
@@ -792,19 +805,34 @@ k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int
         const int row = (i < S) ? (fst + i) : P.rows[P.rbase[js] + i];
         wsm[i * nrhs + r] = b[(int64_t)row + r * ldb];
     }
-    __syncthreads();
-    // x_j = w_j - sum_{i>j} L_ij x_i (SPRBS6): 16 lanes per right-hand side
-    const int r = tid >> 4, li = tid & 15;
-    for (int j = S - 1; j >= 0; --j) {
-        const double* cj = Lb + lnz_col(j, F) - j;
-        double v = 0.0;
-        if (r < nrhs)
-            for (int i = j + 1 + li; i < F; i += 16) v += cj[i] * wsm[i * nrhs + r];
-        for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int nblk = (S + kSmallBlk - 1) / kSmallBlk;
+    for (int bi = nblk - 1; bi >= 0; --bi) {
+        const int j0 = bi * kSmallBlk, nb = min(kSmallBlk, S - j0), m = F - j0;
         __syncthreads();
-        if (r < nrhs && li == 0) wsm[j * nrhs + r] -= v;
+        for (int e = tid; e < m * nb; e += blockDim.x) {
+            const int i = e % m, c = e / m;
+            Ls[i * (kSmallBlk + 1) + c] = (i > c) ? Lb[lnz_col(j0 + c, F) - (j0 + c) + (j0 + i)] : 0.0;
+        }
         __syncthreads();
+        for (int e = tid; e < nb * nrhs; e += blockDim.x) {         // rows below the block (SPRBS6)
+            const int c = e % nb, r = e / nb;
+            double v = 0.0;
+            for (int i = nb; i < m; ++i) v += Ls[i * (kSmallBlk + 1) + c] * wsm[(j0 + i) * nrhs + r];
+            wsm[(j0 + c) * nrhs + r] -= v;
+        }
+        __syncthreads();
+        if (tid < 32) {                       // triangle of the block, bottom-up
+            for (int c = nb - 2; c >= 0; --c) {
+                if (lane < nrhs) {
+                    double v = 0.0;
+                    for (int i = c + 1; i < nb; ++i) v += Ls[i * (kSmallBlk + 1) + c] * wsm[(j0 + i) * nrhs + lane];
+                    wsm[(j0 + c) * nrhs + lane] -= v;
+                }
+                __syncwarp();
+            }
+        }
     }
+    __syncthreads();
     for (int e = tid; e < S * nrhs; e += blockDim.x) {
         const int i = e % S, rr = e / S;
         b[(int64_t)(fst + i) + rr * ldb] = wsm[i * nrhs + rr];
@@ -977,6 +1005,7 @@ __global__ void __launch_bounds__(256) k_inv_block(const Job* jobs, PV P) {
 
 // y_block = X w_block: 32 rows per CTA, 8 warps split the columns
 constexpr size_t kMvSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + 8 * 32 * (kMaxRHS + 1));
+constexpr size_t kUpdSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + (size_t)128 * (kMaxRHS + 1));
 
 __global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
                                                     double* ysol, int nrhs) {
@@ -1060,12 +1089,13 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
     }
 }
 
-// rows below a solve block: w[i] -= L[i, k0:k1] y, 32 rows x 8 column groups per CTA
-__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
-                                                      const double* ysol, int nrhs) {
+// rows below a solve block: w[i] -= L[i, k0:k1] y; 128 rows per CTA, the two
+// halves of the 256 columns summed through shared memory
+__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+                                                      double* vbuf, const double* ysol, int nrhs) {
     extern __shared__ double ush[];
     double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(ush);
-    double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(ush + kSolveBlock * kMaxRHS);
+    double(*part)[kMaxRHS + 1] = reinterpret_cast<double(*)[kMaxRHS + 1]>(ush + kSolveBlock * kMaxRHS);
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
@@ -1073,20 +1103,22 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
     const int64_t vb = P.rbase[js] * nrhs;
     double* w = vbuf + vb;
     const double* base = P.lnz + P.lnz_off[js];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
         const int i = e % nbk, r = e / nbk;
         y[i][r] = ysol[vb + (int64_t)r * F + k0 + i];
     }
     __syncthreads();
-    const int i = jb.c0 + (int)(task - jb.task0) * kSolveRows + lane;
+    const int row = tid & (kSolveRows - 1), half = tid / kSolveRows;
+    const int i = jb.c0 + (int)(task - jb.task0) * kSolveRows + row;
     double acc[kMaxRHS];
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+    const int hc = (nbk + 1) / 2;
     if (i < F) {
-        const int c1 = min(32 * warp + 32, nbk);
+        const int c0 = half * hc, c1 = min(nbk, c0 + hc);
 #pragma unroll 8
-        for (int c = 32 * warp; c < c1; ++c) {
+        for (int c = c0; c < c1; ++c) {
             const int col = k0 + c;
             const double l = base[lnz_col(col, F) - col + i];
 #pragma unroll
@@ -1094,26 +1126,24 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
                 if (r < nrhs) acc[r] += l * y[c][r];
         }
     }
+    if (half == 1)
 #pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r)
-        if (r < nrhs) part[warp][lane][r] = acc[r];
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) part[row][r] = acc[r];
     __syncthreads();
-    if (warp == 0 && i < F)
-        for (int r = 0; r < nrhs; ++r) {
-            double v = 0.0;
-            for (int g = 0; g < 8; ++g) v += part[g][lane][r];
-            w[(int64_t)r * F + i] -= v;
-        }
+    if (half == 0 && i < F)
+        for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= acc[r] + part[row][r];
 }
 
 // back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F].  Phase 1: one
-// CTA per (32 columns, kRectRows rows) writes partial dot products (one warp
-// per column, 4 columns per warp, the vector staged in shared memory);
-// phase 2 (k_bwd_rect_sum) adds the partials of each column in a fixed order,
-// so the result is deterministic.
-__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
-                                                       double* pbuf, int nrhs) {
-    __shared__ double ws[256][kMaxRHS];
+// CTA per (kRectCols columns, kRectRows rows) stages its rows of the vector in
+// shared memory once and writes one partial dot product per column (a warp
+// per column at a time, 32 columns per warp); phase 2 (k_bwd_rect_sum) adds
+// the partials of each column in a fixed order, so the result is
+// deterministic.
+__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+                                                       const double* vbuf, double* pbuf, int nrhs) {
+    __shared__ double ws[kRectRows][kMaxRHS];
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
@@ -1125,43 +1155,31 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     const double* w = vbuf + vb;
     const double* base = P.lnz + P.lnz_off[js];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int cbase = cc * kRectCols + warp * 4;
-    const int rbeg = S + rc * kRectRows, rend = min(F, rbeg + kRectRows);
-    double acc[4][kMaxRHS];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) acc[a][r] = 0.0;
-    for (int r0 = rbeg; r0 < rend; r0 += 256) {
-        const int nr = min(256, rend - r0);
-        __syncthreads();
-        for (int e = tid; e < nr * nrhs; e += blockDim.x) {
-            const int i = e % nr, r = e / nr;
-            ws[i][r] = w[(int64_t)r * F + r0 + i];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int c = cbase + a;
-            if (c >= S) break;
-            const double* col = base + lnz_col(c, F) - c + r0;
-            for (int i = lane; i < nr; i += 32) {
-                const double l = col[i];
-#pragma unroll
-                for (int r = 0; r < kMaxRHS; ++r)
-                    if (r < nrhs) acc[a][r] += l * ws[i][r];
-            }
-        }
+    const int rbeg = S + rc * kRectRows, nr = min(kRectRows, F - rbeg);
+    for (int e = tid; e < nr * nrhs; e += blockDim.x) {
+        const int i = e % nr, r = e / nr;
+        ws[i][r] = w[(int64_t)r * F + rbeg + i];
     }
+    __syncthreads();
     double* part = pbuf + (P.rect_off[js] + (int64_t)rc * S) * kMaxRHS;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int c = cbase + a;
+    const int cw = kRectCols / 8;
+    for (int a = 0; a < cw; ++a) {
+        const int c = cc * kRectCols + warp * cw + a;
         if (c >= S) break;
+        const double* col = base + lnz_col(c, F) - c + rbeg;
+        double acc[kMaxRHS];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+        for (int i = lane; i < nr; i += 32) {
+            const double l = col[i];
+#pragma unroll
+            for (int r = 0; r < kMaxRHS; ++r)
+                if (r < nrhs) acc[r] += l * ws[i][r];
+        }
 #pragma unroll
         for (int r = 0; r < kMaxRHS; ++r) {
             if (r >= nrhs) break;
-            double v = acc[a][r];
+            double v = acc[r];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) part[(int64_t)c * kMaxRHS + r] = v;
         }
@@ -1304,7 +1322,9 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
-    CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
+    CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
+    CK(cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSolveSmem));
+    CK(cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSolveSmem));
     CK(cudaFuncSetAttribute(k_inv_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
@@ -1549,7 +1569,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                     ++nl;
                     const Launch& fl = lp.fs_upd[sb];
                     if (fl.ntasks > 0) {
-                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kMvSmem, s>>>(jobs + fl.job_begin, fl.job_count, TMAP(fl), pv,
+                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kUpdSmem, s>>>(jobs + fl.job_begin, fl.job_count, TMAP(fl), pv,
                                                                        D.vbuf, D.vbuf2, nr);
                         ++nl;
                     }
