@@ -1250,9 +1250,33 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
 // Engine
 // ---------------------------------------------------------------------------
 #define TMAP(l) ((l).map_begin >= 0 ? d_->task_map + (l).map_begin : nullptr)
-Engine::Engine() : d_(new Dev()) {}
+Engine::Engine() : d_(new Dev()) {
+    const char* e = getenv("SPR_B200_GRAPHS");
+    use_graphs_ = !(e && e[0] == '0');
+}
+
+cudaGraphExec_t Engine::find_graph(const GraphKey& k) {
+    for (auto& g : graphs_)
+        if (g.key == k) return g.exec;
+    return nullptr;
+}
+
+int64_t Engine::graph_launches(const GraphKey& k) {
+    for (auto& g : graphs_)
+        if (g.key == k) return g.launches;
+    return 0;
+}
+
+void Engine::store_graph(const GraphKey& k, cudaGraphExec_t exec, int64_t launches) {
+    if (graphs_.size() >= 16) {
+        cudaGraphExecDestroy(graphs_.front().exec);
+        graphs_.erase(graphs_.begin());
+    }
+    graphs_.push_back(GraphEntry{k, exec, launches});
+}
 
 Engine::~Engine() {
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     if (!d_) return;
     for (void* p : d_->owned) cudaFree(p);
     if (d_->arena) cudaFree(d_->arena);
@@ -1388,25 +1412,12 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     ++timing.gemm_launches;
 }
 
-int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
+void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_t>& gev) {
     Dev& D = *d_;
-    cudaStream_t s = stream_;
-    PV pv = make_view(D, P_, d_sm, tol1);
-    linv_valid_ = false;
-    Stats init{};
-    init.first_zero = 0x7fffffff;
-    CK(cudaMemcpyAsync(D.st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(D.sn_neg, 0, P_.nsuper * sizeof(int32_t), s));
-    CK(cudaMemsetAsync(D.sn_fail, 0xff, P_.nsuper * sizeof(int32_t), s));
-    CK(cudaMemsetAsync(D.sn_bad, 0, P_.nsuper * sizeof(int32_t), s));
-    timing.gemm_ms = 0.f;
-    timing.gemm_launches = 0;
     timing.launches = 0;
-    CK(cudaEventRecord(D.ev0, s));
     k_prepass<<<(int)std::min<int64_t>((P_.nsuper * 32 + 255) / 256, 4736), 256, 0, s>>>(pv, P_.nsuper);
     k_reduce<false><<<1, 1024, 0, s>>>(D.adiag, P_.neq, &D.st->trace);
     timing.launches += 2;
-    std::vector<cudaEvent_t> gev;
     for (size_t L = 0; L < P_.levels.size(); ++L) {
         const LevelPlan& lp = P_.levels[L];
         if (!lp.small_nodes.empty()) {
@@ -1448,6 +1459,43 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     }
     k_reduce<true><<<1, 1024, 0, s>>>(pv.dvec, P_.neq, &D.st->mindpos);
     ++timing.launches;
+}
+
+int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    PV pv = make_view(D, P_, d_sm, tol1);
+    linv_valid_ = false;
+    Stats init{};
+    init.first_zero = 0x7fffffff;
+    CK(cudaMemcpyAsync(D.st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(D.sn_neg, 0, P_.nsuper * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(D.sn_fail, 0xff, P_.nsuper * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(D.sn_bad, 0, P_.nsuper * sizeof(int32_t), s));
+    timing.gemm_ms = 0.f;
+    timing.gemm_launches = 0;
+    CK(cudaEventRecord(D.ev0, s));
+    std::vector<cudaEvent_t> gev;
+    // the legacy default stream cannot be captured: graphs need a stream of our own
+    const bool graph = use_graphs_ && !profile_ && s != nullptr;
+    if (graph) {
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, 0, 0};
+        cudaGraphExec_t exec = find_graph(key);
+        if (!exec) {
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            enqueue_factor(pv, s, gev);
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamEndCapture(s, &g));
+            CK(cudaGraphInstantiate(&exec, g, 0));
+            cudaGraphDestroy(g);
+            store_graph(key, exec, timing.launches);
+        } else {
+            timing.launches = graph_launches(key);
+        }
+        CK(cudaGraphLaunch(exec, s));
+    } else {
+        enqueue_factor(pv, s, gev);
+    }
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());
     Stats hs;
@@ -1520,30 +1568,10 @@ void Engine::ensure_vectors(int64_t nrhs) {
     }
 }
 
-int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which) {
+void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ldb, int64_t nrhs, int which,
+                           int64_t& nl) {
     Dev& D = *d_;
-    cudaStream_t s = stream_;
-    PV pv = make_view(D, P_, const_cast<double*>(d_sm), 0.0);
     const int64_t chunk = std::min<int64_t>(nrhs, kMaxRHS);
-    ensure_vectors(chunk);
-    if (!D.vbuf || !D.vbuf2) return -4;
-    CK(cudaEventRecord(D.ev0, s));
-    int64_t nl = 0;
-    if (!linv_valid_) {
-        for (const LevelPlan& lp : P_.levels)
-            for (const Launch& pl : lp.panel)
-                if (pl.job_count > 0) {
-                    k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
-                    ++nl;
-                }
-        if (P_.inv_blocks.job_count > 0) {
-            PV pvi = pv;
-            pvi.sn_bad = nullptr;
-            k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pvi);
-            ++nl;
-        }
-        linv_valid_ = true;
-    }
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
         const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
         double* b = d_b + r0 * ldb;
@@ -1620,6 +1648,50 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                 ++nl;
             }
         }
+    }
+}
+
+int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    PV pv = make_view(D, P_, const_cast<double*>(d_sm), 0.0);
+    const int64_t chunk = std::min<int64_t>(nrhs, kMaxRHS);
+    ensure_vectors(chunk);
+    if (!D.vbuf || !D.vbuf2) return -4;
+    CK(cudaEventRecord(D.ev0, s));
+    int64_t nl = 0;
+    if (!linv_valid_) {
+        for (const LevelPlan& lp : P_.levels)
+            for (const Launch& pl : lp.panel)
+                if (pl.job_count > 0) {
+                    k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
+                    ++nl;
+                }
+        if (P_.inv_blocks.job_count > 0) {
+            PV pvi = pv;
+            pvi.sn_bad = nullptr;
+            k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pvi);
+            ++nl;
+        }
+        linv_valid_ = true;
+    }
+    if (use_graphs_ && s != nullptr) {
+        const GraphKey key{(const void*)d_sm, (const void*)d_b, (double)ldb, nrhs, which, (int64_t)(uintptr_t)D.vbuf};
+        cudaGraphExec_t exec = find_graph(key);
+        if (!exec) {
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            enqueue_solve(pv, s, d_b, ldb, nrhs, which, nl);
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamEndCapture(s, &g));
+            CK(cudaGraphInstantiate(&exec, g, 0));
+            cudaGraphDestroy(g);
+            store_graph(key, exec, nl);
+        } else {
+            nl += graph_launches(key);
+        }
+        CK(cudaGraphLaunch(exec, s));
+    } else {
+        enqueue_solve(pv, s, d_b, ldb, nrhs, which, nl);
     }
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());

@@ -47,10 +47,37 @@ public:
     void invalidate_factor() { linv_valid_ = false; }
     // Timing of the Schur-update kernels can be switched on (events around each launch).
     void set_profile(bool on) { profile_ = on; }
+    // CUDA-graph replay of the factor/solve launch sequences (on by default;
+    // SPR_B200_GRAPHS=0 or set_graphs(false) launches kernel by kernel).
+    void set_graphs(bool on) { use_graphs_ = on; }
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
 
 private:
+    struct GraphKey {
+        const void* a;
+        const void* b;
+        double x;
+        int64_t n;
+        int w;
+        int64_t v;
+        bool operator==(const GraphKey& o) const {
+            return a == o.a && b == o.b && x == o.x && n == o.n && w == o.w && v == o.v;
+        }
+    };
+    struct GraphEntry {
+        GraphKey key;
+        cudaGraphExec_t exec;
+        int64_t launches;
+    };
+    cudaGraphExec_t find_graph(const GraphKey& k);
+    int64_t graph_launches(const GraphKey& k);
+    void store_graph(const GraphKey& k, cudaGraphExec_t exec, int64_t launches);
+    void enqueue_factor(const struct PV& pv, cudaStream_t s, std::vector<cudaEvent_t>& gev);
+    void enqueue_solve(const struct PV& pv, cudaStream_t s, double* d_b, int64_t ldb, int64_t nrhs, int which,
+                       int64_t& nl);
+    std::vector<GraphEntry> graphs_;
+    bool use_graphs_ = true;
     void launch_gemm(const Launch& l, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     void upload_plan();
     void ensure_vectors(int64_t nrhs);
