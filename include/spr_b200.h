@@ -75,6 +75,21 @@ int spr_b200_info(void* handle, double* info);
  * of the last spr_b200_factor_dev (NSUPER entries each): per-system inertia
  * of a forest of independent systems. */
 int spr_b200_sn_stats(void* handle, int32_t* neg, int32_t* fail);
+/* Factorisation mode of the device API: 0 = FP64 (default, the drop-in
+ * semantics), 1 = mixed precision (Schur updates of the large fronts as
+ * 3xTF32 split products, FP64 diagonal blocks/TRSM/storage); pair mode 1
+ * with spr_b200_refine against the FP64 matrix (spr_b200_build_residual). */
+int spr_b200_set_mode(void* handle, int mode);
+/* Residual operator for refinement: compacts the FP64 matrix held in an
+ * assembled (not yet factored) device SM into a CSR (the product SPRPRQ forms
+ * from the packed pattern, sprprm.f:243-325). */
+int spr_b200_build_residual(void* handle, const double* d_sm_assembled);
+/* Iterative refinement on a factored device SM: x = solve(b); while the
+ * normwise backward error max|r|/(||K||inf max|x| + max|b|) > tol and fewer
+ * than maxit corrections: x += solve(b - K x).  out[0]=corrections
+ * out[1]=backward error out[2]=solve ms.  b, x: ld x nrhs, device. */
+int spr_b200_refine(void* handle, const double* d_sm, const double* d_b, double* d_x, int64_t ld,
+                    int64_t nrhs, double tol, int maxit, double* out);
 /* Profile mode: CUDA events around every Schur-update launch. */
 int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed); see abi.cpp. */
@@ -104,6 +119,27 @@ int spr_b200_assemble(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT
  * Returns 0, -2 (shape/alignment), -3 (too large) or -4 (CUDA error). */
 int spr_b200_dense_ldlt_noalloc(double* d_a, int64_t n, int64_t lda, double tol1, double* d_d,
                                 void* stream, double* out);
+/* ---- element-level device operations (no reference counterpart for the
+ * gradient; the assembly is SPRADM's main add) ---- */
+/* Builds the gather plan of the SPRADM main add (spradm.f:818-859) and the
+ * element equation map for one structure and SAM element topology (MEQN,
+ * MADOF, MPMNPC, MMNPC as SPRADM takes them; every element has nedof <= 32
+ * DOFs, nel < 2^22).  0, -2 (limits), -3 (DOF count or pattern mismatch). */
+int spr_b200_elem_open(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                       const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
+                       const SPR_INT* mmnpc, SPR_INT nel, SPR_INT nedof, void** handle);
+void spr_b200_elem_close(void* handle);
+/* Device SM = 0 then the SPRADM main add of every element: EM_e =
+ * d_scale[e]*d_em (one nedof x nedof column-major matrix) or, with d_scale
+ * NULL, the e-th matrix of d_em.  Bit-exact with spr_b200_assemble. */
+int spr_b200_elem_assemble(void* handle, double* d_sm, const double* d_em, const double* d_scale,
+                           void* stream);
+/* Adjoint element gradient: d_grad[e] = -sum_q lam_q,e^T dK_e u_q,e with
+ * dK_e = d_dscale[e]*d_em, or the e-th matrix of d_em when d_dscale is NULL;
+ * u, lam: ld x nrhs device arrays in equation order (constrained DOFs are
+ * skipped).  With lam solving K lam = dL/du this is dL/dtheta_e. */
+int spr_b200_elem_grad(void* handle, const double* d_u, const double* d_lam, int64_t ld, int64_t nrhs,
+                       const double* d_em, const double* d_dscale, double* d_grad, void* stream);
 /* Frees every device context cached by the Fortran entry points. */
 void spr_b200_release_all(void);
 

@@ -45,6 +45,12 @@ def load(int_kind=8):
         lib.spr_b200_info.restype = C.c_int
         lib.spr_b200_sn_stats.argtypes = [vp, vp, vp]
         lib.spr_b200_sn_stats.restype = C.c_int
+        lib.spr_b200_build_residual.argtypes = [vp, vp]
+        lib.spr_b200_build_residual.restype = C.c_int
+        lib.spr_b200_refine.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_int64, C.c_double, C.c_int, vp]
+        lib.spr_b200_refine.restype = C.c_int
+        lib.spr_b200_set_mode.argtypes = [vp, C.c_int]
+        lib.spr_b200_set_mode.restype = C.c_int
         lib.spr_b200_set_profile.argtypes = [vp, C.c_int]
         lib.spr_b200_set_profile.restype = C.c_int
         lib.spr_b200_release_all.argtypes = []
@@ -180,6 +186,24 @@ class DeviceSolver:
         fail = np.zeros(nsuper, dtype=np.int32)
         self.lib.spr_b200_sn_stats(self.h, _ptr(neg), _ptr(fail))
         return neg, fail
+
+    def build_residual(self, d_sm_assembled):
+        rc = self.lib.spr_b200_build_residual(self.h, C.c_void_p(self._dev(d_sm_assembled)))
+        if rc != 0:
+            raise RuntimeError('spr_b200_build_residual failed with %d' % rc)
+
+    def refine(self, d_sm, d_b, d_x, nrhs, tol=1e-12, maxit=30, ld=None):
+        """Iterative refinement; returns (corrections, backward error, solve ms)."""
+        ld = self.neq if ld is None else ld
+        out = np.zeros(3)
+        rc = self.lib.spr_b200_refine(self.h, C.c_void_p(self._dev(d_sm)), C.c_void_p(self._dev(d_b)),
+                                      C.c_void_p(self._dev(d_x)), ld, nrhs, tol, maxit, _ptr(out))
+        if rc != 0:
+            raise RuntimeError('spr_b200_refine failed with %d' % rc)
+        return int(out[0]), float(out[1]), float(out[2])
+
+    def set_mode(self, mixed):
+        self.lib.spr_b200_set_mode(self.h, 1 if mixed else 0)
 
     def set_profile(self, on=True):
         self.lib.spr_b200_set_profile(self.h, 1 if on else 0)

@@ -17,7 +17,7 @@ NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 COMMON = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-O3']
 
-ENGINE_SOURCES = ['engine.cu', 'plan.cpp', 'noalloc.cu']
+ENGINE_SOURCES = ['engine.cu', 'plan.cpp', 'noalloc.cu', 'elements.cu']
 
 
 def _run(cmd):

@@ -24,6 +24,7 @@
 #include <tuple>
 #include <vector>
 
+#include "elements.h"
 #include "engine.h"
 
 #ifndef SPR_INT
@@ -509,6 +510,26 @@ int SPR_API(spr_b200_sn_stats)(void* handle, int32_t* neg, int32_t* fail) {
     return static_cast<Engine*>(handle)->sn_stats(neg, fail);
 }
 
+// Residual operator of iterative refinement: CSR of the FP64 matrix held in
+// the assembled (not yet factored) device SM.
+int SPR_API(spr_b200_build_residual)(void* handle, const double* d_sm_assembled) {
+    return static_cast<Engine*>(handle)->build_residual(d_sm_assembled);
+}
+
+// Iterative refinement on a factored device SM: x = solve(b), then
+// x += solve(b - K x) until the normwise backward error <= tol.
+// out[0] = correction steps, out[1] = backward error, out[2] = solve ms.
+int SPR_API(spr_b200_refine)(void* handle, const double* d_sm, const double* d_b, double* d_x, int64_t ld,
+                             int64_t nrhs, double tol, int maxit, double* out) {
+    return static_cast<Engine*>(handle)->refine(d_sm, d_b, d_x, ld, nrhs, tol, maxit, out);
+}
+
+// Factorisation mode: 0 = FP64 (the drop-in), 1 = mixed (3xTF32 Schur updates).
+int SPR_API(spr_b200_set_mode)(void* handle, int mode) {
+    static_cast<Engine*>(handle)->set_mixed(mode == 1);
+    return 0;
+}
+
 // Profile mode: CUDA events around every Schur-update launch (spr_b200_info[8]).
 int SPR_API(spr_b200_set_profile)(void* handle, int on) {
     static_cast<Engine*>(handle)->set_profile(on != 0);
@@ -611,6 +632,40 @@ int SPR_API(spr_b200_assemble)(const I* mspar, const I* mtrees, const I* msifa, 
         }
     }
     return 0;
+}
+
+// Element-level device operations (assembly gather, adjoint element gradient)
+// on one structure and one SAM element topology.
+int SPR_API(spr_b200_elem_open)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
+                                const I* mpmnpc, const I* mmnpc, I nel, I nedof, void** handle) {
+    if (nel < 0) return -2;
+    std::vector<int64_t> ms(60, 0);
+    for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
+    std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
+    std::vector<int64_t> pn = widen(mpmnpc, nel + 1);
+    std::vector<int64_t> mn = widen(mmnpc, pn[nel] - 1);
+    int64_t nnod = 0;
+    for (int64_t v : mn) nnod = std::max(nnod, v);
+    std::vector<int64_t> ad = widen(madof, nnod + 1);
+    std::vector<int64_t> eq = widen(meqn, nnod > 0 ? ad[nnod] - 1 : 0);
+    std::unique_ptr<sprb::Elements> e(new sprb::Elements());
+    const int rc = e->open(ms.data(), mt.data(), mf.data(), eq.data(), ad.data(), pn.data(), mn.data(), nel, nedof);
+    if (rc != 0) return rc;
+    *handle = e.release();
+    return 0;
+}
+
+void SPR_API(spr_b200_elem_close)(void* handle) { delete static_cast<sprb::Elements*>(handle); }
+
+int SPR_API(spr_b200_elem_assemble)(void* handle, double* d_sm, const double* d_em, const double* d_scale,
+                                    void* stream) {
+    return static_cast<sprb::Elements*>(handle)->assemble(d_sm, d_em, d_scale, (cudaStream_t)stream);
+}
+
+int SPR_API(spr_b200_elem_grad)(void* handle, const double* d_u, const double* d_lam, int64_t ld, int64_t nrhs,
+                                const double* d_em, const double* d_dscale, double* d_grad, void* stream) {
+    return static_cast<sprb::Elements*>(handle)->grad(d_u, d_lam, ld, nrhs, d_em, d_dscale, d_grad,
+                                                      (cudaStream_t)stream);
 }
 
 // Releases every cached context (device memory of the Fortran entry points).

@@ -708,6 +708,178 @@ using GemmSmall = gemm::Cfg<kTile, 32, 32, SPR_GEMM_STAGES>;
 #define K_GEMM_BIG k_gemm<kTileBig, SPR_GEMM_BIG_WM, SPR_GEMM_BIG_WN, SPR_GEMM_STAGES>
 #define K_GEMM_SMALL k_gemm<kTile, 32, 32, SPR_GEMM_STAGES>
 
+// Mixed-precision Schur update: C -= L D L' with 3xTF32 split products on
+// the tensor cores (mma.sync m16n8k8 tf32, FP32 accumulation inside each
+// 64-wide slice of K, FP64 accumulation across slices and in C).  Each FP64
+// operand a is rounded to FP32, then split a = hi + lo with hi = tf32(a),
+// lo = tf32(a - hi); the product uses hi*hi + hi*lo + lo*hi.
+namespace x3 {
+__device__ __forceinline__ uint32_t tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split(double v, uint32_t& hi, uint32_t& lo) {
+    const float f = (float)v;
+    hi = tf32(f);
+    lo = tf32(f - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+}  // namespace x3
+
+__global__ void __launch_bounds__(128) k_gemm_x3(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
+    using namespace gemm;
+    constexpr int T = kTile, STAGES = 3, LDS = T + 4;
+    extern __shared__ __align__(16) double gsh[];
+    double* As = gsh;
+    double* Bs = As + STAGES * BK * LDS;
+    double* Ds = Bs + STAGES * BK * LDS;
+    if (P.st->any_fail) return;
+    const int64_t task = blockIdx.x;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int ld = P.buf_ld[js];
+    const int64_t u = task - jb.task0;
+    const int nct = (jb.c_end - jb.c0 + T - 1) / T;
+    const int nr = (jb.r_end - jb.c0 + T - 1) / T;
+    int lo = 0, hi = nct - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t pre = (int64_t)mid * nr - ((int64_t)mid * (mid - 1)) / 2;
+        if (pre <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const int jt = lo;
+    const int it = jt + (int)(u - ((int64_t)jt * nr - ((int64_t)jt * (jt - 1)) / 2));
+    const int i0 = jb.c0 + it * T, j0 = jb.c0 + jt * T;
+    const int r_end = jb.r_end, c_end = jb.c_end;
+    const double* front = P.arena + P.buf_off[js];
+    double* frontw = P.arena + P.buf_off[js];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    float acc[2][4][4];
+    double acc64[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                acc[a][b][c] = 0.f;
+                acc64[a][b][c] = 0.0;
+            }
+    const int k_lo = jb.k_lo, k_hi = jb.k_hi;
+    const int nk = (k_hi - k_lo + BK - 1) / BK;
+    const bool even = ((i0 | j0) & 1) == 0;
+    auto load_stage = [&](int stage, int kt) {
+        const int kb = k_lo + kt * BK;
+        double* as = As + stage * BK * LDS;
+        double* bs = Bs + stage * BK * LDS;
+#pragma unroll
+        for (int e = 0; e < (T / 2 * BK + 127) / 128; ++e) {
+            const int idx = tid + e * 128;
+            if (idx < T / 2 * BK) {
+                const int pr = idx % (T / 2), k = idx / (T / 2);
+                const int r = 2 * pr, kk = kb + k;
+                const bool kv = kk < k_hi;
+                const int64_t col = (int64_t)(kv ? kk : k_lo) * ld;
+                const int ra = i0 + r, rb = j0 + r;
+                const int na = kv ? max(0, min(2, r_end - ra)) : 0;
+                const int nbb = kv ? max(0, min(2, r_end - rb)) : 0;
+                if (even) {
+                    cp_async16(as + k * LDS + r, front + col + (na > 0 ? ra : i0), 8 * na);
+                    cp_async16(bs + k * LDS + r, front + col + (nbb > 0 ? rb : j0), 8 * nbb);
+                } else {
+                    cp_async8(as + k * LDS + r, front + col + (na > 0 ? ra : i0), na > 0);
+                    cp_async8(as + k * LDS + r + 1, front + col + (na > 1 ? ra + 1 : i0), na > 1);
+                    cp_async8(bs + k * LDS + r, front + col + (nbb > 0 ? rb : j0), nbb > 0);
+                    cp_async8(bs + k * LDS + r + 1, front + col + (nbb > 1 ? rb + 1 : j0), nbb > 1);
+                }
+            }
+        }
+        if (tid < BK) {
+            const int kk = kb + tid;
+            cp_async8(Ds + stage * BK + tid, front + (int64_t)(kk < k_hi ? kk : k_lo) * (ld + 1), kk < k_hi);
+        }
+    };
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; ++st) {
+        if (st < nk) load_stage(st, st);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        const int nxt = kt + STAGES - 1;
+        if (nxt < nk) load_stage(nxt % STAGES, nxt);
+        cp_async_commit();
+        const int cur = kt % STAGES;
+        const double* as = As + cur * BK * LDS;
+        const double* bs = Bs + cur * BK * LDS;
+        const double* ds = Ds + cur * BK;
+#pragma unroll
+        for (int k8 = 0; k8 < BK; k8 += 8) {
+            const double d0 = ds[k8 + t], d1 = ds[k8 + t + 4];
+            uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                const int r0 = wm + mi * 16 + g;
+                x3::split(as[(k8 + t) * LDS + r0] * d0, ah[mi][0], al[mi][0]);
+                x3::split(as[(k8 + t) * LDS + r0 + 8] * d0, ah[mi][1], al[mi][1]);
+                x3::split(as[(k8 + t + 4) * LDS + r0] * d1, ah[mi][2], al[mi][2]);
+                x3::split(as[(k8 + t + 4) * LDS + r0 + 8] * d1, ah[mi][3], al[mi][3]);
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+                const int c = wn + ni * 8 + g;
+                x3::split(bs[(k8 + t) * LDS + c], bh[ni][0], bl[ni][0]);
+                x3::split(bs[(k8 + t + 4) * LDS + c], bh[ni][1], bl[ni][1]);
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) {
+                    x3::mma(acc[mi][ni], al[mi], bh[ni][0], bh[ni][1]);
+                    x3::mma(acc[mi][ni], ah[mi], bl[ni][0], bl[ni][1]);
+                    x3::mma(acc[mi][ni], ah[mi], bh[ni][0], bh[ni][1]);
+                }
+        }
+        if ((kt & 3) == 3 || kt == nk - 1) {           // FP64 accumulation across 64-wide K slices
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        acc64[a][b][c] += (double)acc[a][b][c];
+                        acc[a][b][c] = 0.f;
+                    }
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = i0 + wm + mi * 16 + g + 8 * h;
+            if (r >= r_end) continue;
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int c = j0 + wn + ni * 8 + 2 * t + q;
+                    if (c < c_end && r >= c) frontw[(int64_t)r + (int64_t)c * ld] -= acc64[mi][ni][2 * h + q];
+                }
+        }
+}
+
 // Store the S factored columns of a dense front into LNZ (sprfc1.f:630-637).
 __global__ void k_writeback(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P) {
     if (P.st->any_fail) return;
@@ -1247,6 +1419,109 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
 }
 
 // ---------------------------------------------------------------------------
+// Residual of the FP64 matrix for iterative refinement (the product SPRPRQ
+// forms from the packed pattern, src/SPR/sprprm.f:243-325): the nonzeros of
+// the assembled LNZ are compacted once into a full symmetric CSR with rows
+// sorted by column, so r = b - K x is a deterministic warp-per-row SpMV.
+// ---------------------------------------------------------------------------
+__global__ void k_csr_count(PV P, int64_t nsuper, int* rowcnt) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t js = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; js < nsuper;
+         js += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+        const int32_t* rows = P.rows + P.rbase[js];
+        const double* col = P.lnz + P.lnz_off[js];
+        for (int j = 0; j < S; ++j) {
+            const double* cj = col + lnz_col(j, F) - j;
+            for (int i = j + lane; i < F; i += 32)
+                if (cj[i] != 0.0) {
+                    atomicAdd(&rowcnt[rows[i]], 1);
+                    if (i != j) atomicAdd(&rowcnt[fst + j], 1);
+                }
+        }
+    }
+}
+
+__global__ void k_csr_fill(PV P, int64_t nsuper, int* fillpos, int32_t* ci, double* cv) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t js = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; js < nsuper;
+         js += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+        const int32_t* rows = P.rows + P.rbase[js];
+        const double* col = P.lnz + P.lnz_off[js];
+        for (int j = 0; j < S; ++j) {
+            const double* cj = col + lnz_col(j, F) - j;
+            for (int i = j + lane; i < F; i += 32) {
+                const double a = cj[i];
+                if (a == 0.0) continue;
+                const int row = rows[i];
+                int p = atomicAdd(&fillpos[row], 1);
+                ci[p] = fst + j;
+                cv[p] = a;
+                if (i != j) {
+                    p = atomicAdd(&fillpos[fst + j], 1);
+                    ci[p] = row;
+                    cv[p] = a;
+                }
+            }
+        }
+    }
+}
+
+// insertion sort of each row by column (rows are short: ~81 entries for hex8)
+__global__ void k_csr_sort(const int64_t* rowptr, int64_t neq, int32_t* ci, double* cv, double* rowabs) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= neq) return;
+    const int64_t p0 = rowptr[r], p1 = rowptr[r + 1];
+    double sabs = 0.0;
+    for (int64_t p = p0 + 1; p < p1; ++p) {
+        const int32_t c = ci[p];
+        const double v = cv[p];
+        int64_t q = p - 1;
+        while (q >= p0 && ci[q] > c) {
+            ci[q + 1] = ci[q];
+            cv[q + 1] = cv[q];
+            --q;
+        }
+        ci[q + 1] = c;
+        cv[q + 1] = v;
+    }
+    for (int64_t p = p0; p < p1; ++p) sabs += fabs(cv[p]);
+    rowabs[r] = sabs;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// r = b - K x per right-hand side (warp per row); norms[3r..3r+2] = max|r|, max|x|, max|b|
+__global__ void k_residual(const int64_t* rowptr, const int32_t* ci, const double* cv, int64_t neq, const double* b,
+                           const double* x, double* r, int64_t ld, int nrhs, double* norms) {
+    const int lane = threadIdx.x & 31;
+    const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (row >= neq) return;
+    const int64_t p0 = rowptr[row], p1 = rowptr[row + 1];
+    for (int q = 0; q < nrhs; ++q) {
+        const double* xq = x + q * ld;
+        double acc = 0.0;
+        for (int64_t p = p0 + lane; p < p1; p += 32) acc += cv[p] * xq[ci[p]];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            const double bi = b[row + q * ld], ri = bi - acc;
+            r[row + q * ld] = ri;
+            atomic_max_nonneg(&norms[3 * q], fabs(ri));
+            atomic_max_nonneg(&norms[3 * q + 1], fabs(xq[row]));
+            atomic_max_nonneg(&norms[3 * q + 2], fabs(bi));
+        }
+    }
+}
+
+__global__ void k_axpy(double* x, const double* d, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) x[i] += d[i];
+}
+
+// ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
 #define TMAP(l) ((l).map_begin >= 0 ? d_->task_map + (l).map_begin : nullptr)
@@ -1277,6 +1552,11 @@ void Engine::store_graph(const GraphKey& k, cudaGraphExec_t exec, int64_t launch
 
 Engine::~Engine() {
     for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    if (csr_.rowptr) cudaFree(csr_.rowptr);
+    if (csr_.ci) cudaFree(csr_.ci);
+    if (csr_.cv) cudaFree(csr_.cv);
+    if (csr_.rowabs) cudaFree(csr_.rowabs);
+    if (rbuf_) cudaFree(rbuf_);
     if (!d_) return;
     for (void* p : d_->owned) cudaFree(p);
     if (d_->arena) cudaFree(d_->arena);
@@ -1352,6 +1632,7 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(k_inv_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
+    CK(cudaFuncSetAttribute(k_gemm_x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     return 0;
 }
 
@@ -1403,7 +1684,9 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     if (l.ntasks <= 0) return;
     if (profile_) gev.push_back(record_event(s));
     const Job* jobs = d_->jobs + l.job_begin;
-    if (l.tile == kTileBig)
+    if (mixed_)
+        k_gemm_x3<<<(int)l.ntasks, 128, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
+    else if (l.tile == kTileBig)
         K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
     else
         K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
@@ -1479,7 +1762,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     // the legacy default stream cannot be captured: graphs need a stream of our own
     const bool graph = use_graphs_ && !profile_ && s != nullptr;
     if (graph) {
-        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, 0, 0};
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, mixed_ ? 1 : 0, 0};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1833,6 +2116,103 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     out[2] = hf[0];
     out[3] = hf[1];
     out[4] = hs.tol2;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Iterative refinement against the FP64 matrix
+// ---------------------------------------------------------------------------
+int Engine::build_residual(const double* d_sm_assembled) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    PV pv = make_view(D, P_, const_cast<double*>(d_sm_assembled), 0.0);
+    const int64_t neq = P_.neq;
+    int* cnt = nullptr;
+    CK(cudaMalloc((void**)&cnt, (neq + 1) * sizeof(int)));
+    CK(cudaMemsetAsync(cnt, 0, (neq + 1) * sizeof(int), s));
+    const int grid = (int)std::min<int64_t>((P_.nsuper * 32 + 255) / 256, 4736);
+    k_csr_count<<<grid, 256, 0, s>>>(pv, P_.nsuper, cnt);
+    std::vector<int> hc(neq);
+    CK(cudaMemcpyAsync(hc.data(), cnt, neq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<int64_t> rp(neq + 1, 0);
+    for (int64_t i = 0; i < neq; ++i) rp[i + 1] = rp[i] + hc[i];
+    const int64_t nnz = rp[neq];
+    if (csr_.rowptr) cudaFree(csr_.rowptr);
+    if (csr_.ci) cudaFree(csr_.ci);
+    if (csr_.cv) cudaFree(csr_.cv);
+    if (csr_.rowabs) cudaFree(csr_.rowabs);
+    CK(cudaMalloc((void**)&csr_.rowptr, (neq + 1) * sizeof(int64_t)));
+    CK(cudaMalloc((void**)&csr_.ci, std::max<int64_t>(nnz, 1) * sizeof(int32_t)));
+    CK(cudaMalloc((void**)&csr_.cv, std::max<int64_t>(nnz, 1) * sizeof(double)));
+    CK(cudaMalloc((void**)&csr_.rowabs, neq * sizeof(double)));
+    CK(cudaMemcpyAsync(csr_.rowptr, rp.data(), (neq + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    std::vector<int> fp(rp.begin(), rp.end() - 1);
+    CK(cudaMemcpyAsync(cnt, fp.data(), neq * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_csr_fill<<<grid, 256, 0, s>>>(pv, P_.nsuper, cnt, csr_.ci, csr_.cv);
+    k_csr_sort<<<(int)((neq + 255) / 256), 256, 0, s>>>(csr_.rowptr, neq, csr_.ci, csr_.cv, csr_.rowabs);
+    std::vector<double> ra(neq);
+    CK(cudaMemcpyAsync(ra.data(), csr_.rowabs, neq * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    cudaFree(cnt);
+    csr_.norm_inf = 0.0;
+    for (double v : ra) csr_.norm_inf = std::max(csr_.norm_inf, v);
+    csr_.nnz = nnz;
+    return 0;
+}
+
+int Engine::residual(const double* d_b, const double* d_x, double* d_r, int64_t ld, int64_t nrhs, double* berr) {
+    if (!csr_.rowptr) return -2;
+    cudaStream_t s = stream_;
+    double* norms = nullptr;
+    CK(cudaMalloc((void**)&norms, 3 * nrhs * sizeof(double)));
+    CK(cudaMemsetAsync(norms, 0, 3 * nrhs * sizeof(double), s));
+    const int64_t neq = P_.neq;
+    k_residual<<<(int)((neq * 32 + 255) / 256), 256, 0, s>>>(csr_.rowptr, csr_.ci, csr_.cv, neq, d_b, d_x, d_r, ld,
+                                                            (int)nrhs, norms);
+    std::vector<double> h(3 * nrhs);
+    CK(cudaMemcpyAsync(h.data(), norms, 3 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    cudaFree(norms);
+    double worst = 0.0;
+    for (int64_t q = 0; q < nrhs; ++q) {
+        const double den = csr_.norm_inf * h[3 * q + 1] + h[3 * q + 2];
+        worst = std::max(worst, den > 0.0 ? h[3 * q] / den : 0.0);
+    }
+    *berr = worst;
+    return 0;
+}
+
+int Engine::refine(const double* d_sm, const double* d_b, double* d_x, int64_t ld, int64_t nrhs, double tol,
+                   int maxit, double* out) {
+    Dev& D = *d_;
+    cudaStream_t s = stream_;
+    const int64_t n = ld * nrhs;
+    if (rbuf_cap_ < n) {
+        if (rbuf_) cudaFree(rbuf_);
+        rbuf_ = nullptr;
+        rbuf_cap_ = 0;
+        CK(cudaMalloc((void**)&rbuf_, n * sizeof(double)));
+        rbuf_cap_ = n;
+    }
+    (void)D;
+    CK(cudaMemcpyAsync(d_x, d_b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (solve(d_sm, d_x, ld, nrhs, 3) != 0) return -4;
+    float solve_ms = timing.solve_ms;
+    double berr = 0.0;
+    int it = 0;
+    for (;;) {
+        if (residual(d_b, d_x, rbuf_, ld, nrhs, &berr) != 0) return -4;
+        if (berr <= tol || it >= maxit) break;
+        if (solve(d_sm, rbuf_, ld, nrhs, 3) != 0) return -4;
+        solve_ms += timing.solve_ms;
+        k_axpy<<<(int)((n + 255) / 256), 256, 0, s>>>(d_x, rbuf_, n);
+        ++it;
+    }
+    CK(cudaStreamSynchronize(s));
+    out[0] = it;
+    out[1] = berr;
+    out[2] = solve_ms;
     return 0;
 }
 

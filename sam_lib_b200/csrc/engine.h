@@ -39,6 +39,15 @@ public:
     int factor(double* d_sm, double tol1, FactorResult& res);
     // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
     int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
+    // Iterative refinement (mixed precision): build_residual() compacts the
+    // assembled (unfactored) SM into a CSR of the FP64 matrix; refine() runs
+    // x = solve(b), then r = b - K x, x += solve(r) until the normwise
+    // backward error max|r| / (||K||inf max|x| + max|b|) <= tol.
+    // out[0] = correction steps, out[1] = final backward error, out[2] = solve ms.
+    int build_residual(const double* d_sm_assembled);
+    int residual(const double* d_b, const double* d_x, double* d_r, int64_t ld, int64_t nrhs, double* berr);
+    int refine(const double* d_sm, const double* d_b, double* d_x, int64_t ld, int64_t nrhs, double tol, int maxit,
+               double* out);
     // Per-supernode negative-pivot counts and failing column of the last factor().
     int sn_stats(int32_t* neg, int32_t* fail);
     // The solves use the inverses of the diagonal blocks that factor() stores;
@@ -50,6 +59,10 @@ public:
     // CUDA-graph replay of the factor/solve launch sequences (on by default;
     // SPR_B200_GRAPHS=0 or set_graphs(false) launches kernel by kernel).
     void set_graphs(bool on) { use_graphs_ = on; }
+    // Mixed precision: the Schur updates of the large fronts in 3xTF32 (FP64
+    // diagonal blocks, TRSM, small fronts and storage); see k_gemm_x3.
+    void set_mixed(bool on) { mixed_ = on; }
+    bool mixed() const { return mixed_; }
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
 
@@ -78,6 +91,17 @@ private:
                        int64_t& nl);
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
+    bool mixed_ = false;
+    struct Csr {
+        int64_t* rowptr = nullptr;
+        int32_t* ci = nullptr;
+        double* cv = nullptr;
+        double* rowabs = nullptr;
+        int64_t nnz = 0;
+        double norm_inf = 0.0;
+    } csr_;
+    double* rbuf_ = nullptr;
+    int64_t rbuf_cap_ = 0;
     void launch_gemm(const Launch& l, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     void upload_plan();
     void ensure_vectors(int64_t nrhs);
