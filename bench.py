@@ -49,6 +49,8 @@ def parse():
     ap.add_argument('--n', type=int, default=N_MESH)
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-forms', action='store_true',
+                    help='skip the mixed+IR, batched and adjoint measurements')
     return ap.parse_args()
 
 
@@ -180,6 +182,151 @@ def read_traffic():
         if line.startswith('dram_bytes_per_flop'):
             return float(line.split('=')[1])
     return None
+
+
+# ---------------------------------------------------------------------------
+# the three further forms (each one timed with CUDA events on its stream)
+# ---------------------------------------------------------------------------
+def _ev(torch):
+    return torch.cuda.Event(enable_timing=True)
+
+
+def form_mixed_ir(torch, spr, n, emod, reps=2):
+    """FP64 factor+solve against mixed (3xTF32 Schur updates) factor + FP64
+    iterative refinement to a normwise backward error of 1e-12, same system."""
+    from sam_lib_b200.adjoint import ElementOps
+    from sam_lib_b200.fe import element_moduli
+    from sam_lib_b200.system import HexSystem
+    hs = HexSystem(n, moduli=element_moduli(n ** 3, emod, seed=2))
+    ops = ElementOps(hs)
+    d_sm0 = torch.empty(hs.neq + hs.nzerol, dtype=torch.float64, device='cuda')
+    ops.assemble(d_sm0, torch.from_numpy(hs.ke.ravel(order='F').copy()).cuda(),
+                 torch.from_numpy(hs.moduli).cuda())
+    ops.close()
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    st = torch.cuda.Stream()
+    ds.set_stream(st.cuda_stream)
+    ds.build_residual(d_sm0)
+    b = torch.from_numpy(np.random.default_rng(1).uniform(-1.0, 1.0, size=(NRHS, hs.neq))).cuda()
+    d_sm, x, x64 = torch.empty_like(d_sm0), torch.empty_like(b), torch.empty_like(b)
+    out = {}
+    for mode in (0, 1):
+        ds.set_mode(bool(mode))
+        ts = []
+        for r in range(reps + 1):
+            with torch.cuda.stream(st):
+                d_sm.copy_(d_sm0)
+            st.synchronize()
+            e0, e1 = _ev(torch), _ev(torch)
+            e0.record(st)
+            fr = ds.factor(d_sm)
+            fac_ms = ds.info()['factor_ms']
+            if mode == 0:
+                with torch.cuda.stream(st):
+                    x64.copy_(b)
+                ds.solve(d_sm, x64, NRHS)
+                e1.record(st)
+                e1.synchronize()
+                it, berr, _ = ds.refine(d_sm, b, x, NRHS, tol=1e-12, maxit=0)
+            else:
+                it, berr, _ = ds.refine(d_sm, b, x, NRHS, tol=1e-12, maxit=30)
+                e1.record(st)
+                e1.synchronize()
+            assert fr['lierr'] == 0, fr
+            if r > 0:
+                ts.append(e0.elapsed_time(e1))
+        out[mode] = {'factor_solve_s': float(np.mean(ts)) / 1e3, 'factor_s': fac_ms / 1e3,
+                     'ir_corrections': it, 'backward_error': berr, 'numneg': fr['numneg']}
+    ds.set_mode(False)
+    rel = float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64))
+    del ds
+    torch.cuda.empty_cache()
+    return {'system': '%d^3 hex8, E %s (seed 2), %d RHS U[-1,1] seed 1' % (
+                n, 'log-uniform [1,1e4]' if emod == 'loguniform' else '= 1', NRHS),
+            'fp64': out[0], 'mixed_ir': out[1], 'tol': 1e-12,
+            'speedup_mixed_ir_vs_fp64': out[0]['factor_solve_s'] / out[1]['factor_solve_s'],
+            'numneg_equal': out[0]['numneg'] == out[1]['numneg'],
+            'rel_diff_vs_fp64_gpu_solution': rel}
+
+
+def form_batched(torch, reps=3):
+    """512 uneven shifted (indefinite) systems, 16 RHS each, as one forest."""
+    from sam_lib_b200.batch import BatchSolver
+    from sam_lib_b200.workloads import config4
+    bs = BatchSolver(config4())
+    ds = bs.ds
+    st = torch.cuda.Stream()
+    ds.set_stream(st.cuda_stream)
+    ds.build_residual(bs.sm0)
+    x = torch.empty_like(bs.b0)
+    out = {}
+    for mode in (0, 1):
+        ds.set_mode(bool(mode))
+        ts = []
+        for r in range(reps + 1):
+            with torch.cuda.stream(st):
+                bs.sm.copy_(bs.sm0)
+                bs.b.copy_(bs.b0)
+            st.synchronize()
+            e0, e1 = _ev(torch), _ev(torch)
+            e0.record(st)
+            fr = ds.factor(bs.sm)
+            if mode == 0:
+                ds.solve(bs.sm, bs.b, bs.nrhs)
+                e1.record(st)
+                e1.synchronize()
+                it, berr, _ = ds.refine(bs.sm, bs.b0, x, bs.nrhs, tol=1e-12, maxit=0)
+            else:
+                it, berr, _ = ds.refine(bs.sm, bs.b0, x, bs.nrhs, tol=1e-12, maxit=30)
+                e1.record(st)
+                e1.synchronize()
+            if r > 0:
+                ts.append(e0.elapsed_time(e1))
+        t = float(np.mean(ts)) / 1e3
+        out['fp64' if mode == 0 else 'fp32_ir'] = {
+            'systems_per_s': bs.forest.nsys / t, 's_per_batch': t, 'ir_corrections': it,
+            'backward_error': berr, 'numneg_total': fr['numneg'],
+            'indefinite_systems': int(np.count_nonzero(bs.numneg() > 0))}
+    ds.set_mode(False)
+    del bs, ds
+    torch.cuda.empty_cache()
+    out['workload'] = ('512 boxes n~U{3..12} (seed 3), K - sigma M, sigma = U[0.5,2] x lambda1, '
+                       '16 RHS each, merged forest (%s)' % 'one launch per kernel per tree level')
+    return out
+
+
+def form_adjoint(torch, reps=3):
+    """32^3 SIMP compliance: forward (assemble + factor + solve) vs forward + backward."""
+    from sam_lib_b200.adjoint import SimpModel, simp_solve, simp_workload
+    hs, theta, f = simp_workload(32, seed=4)
+    model = SimpModel(hs)
+    th = torch.tensor(theta, device='cuda', requires_grad=True)
+    ft = torch.tensor(f, device='cuda')
+    fw, fb = [], []
+    for r in range(reps + 1):
+        torch.cuda.synchronize()
+        e0, e1 = _ev(torch), _ev(torch)
+        e0.record()
+        with torch.no_grad():
+            torch.dot(ft, simp_solve(th, ft, model))
+        e1.record()
+        e1.synchronize()
+        th.grad = None
+        torch.cuda.synchronize()
+        e2, e3 = _ev(torch), _ev(torch)
+        e2.record()
+        torch.dot(ft, simp_solve(th, ft, model)).backward()
+        e3.record()
+        e3.synchronize()
+        if r > 0:
+            fw.append(e0.elapsed_time(e1))
+            fb.append(e2.elapsed_time(e3))
+    res = {'workload': '32^3 hex8 SIMP E=theta^3, theta~U[0.2,1] seed 4, tip load, L = f^T u',
+           'forward_s': float(np.mean(fw)) / 1e3, 'forward_backward_s': float(np.mean(fb)) / 1e3}
+    res['backward_over_forward'] = res['forward_backward_s'] / res['forward_s'] - 1.0
+    del model
+    torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -318,6 +465,13 @@ def run_ours(args, rank, world, local_rank):
             'peak_source': 'measured in-run: cuBLAS DGEMM 8192^3 via torch.matmul float64 '
                            '(MEASURED_PEAKS.json has no FP64 figure)',
             'time_share': gemm_s / (ms_step / 1e3)}
+    del ds, d_sm0, d_sm, d_b0, d_b
+    torch.cuda.empty_cache()
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms and args.n == N_MESH:
+        forms = {'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
+                 'mixed_ir_uniform': form_mixed_ir(torch, spr, N_MESH, 'uniform'),
+                 'batched': form_batched(torch), 'adjoint': form_adjoint(torch)}
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
@@ -327,9 +481,8 @@ def run_ours(args, rank, world, local_rank):
                 'factor_solve_s': ms_step / 1e3, 'factor_flops': info['factor_flops'],
                 'solve_flops_per_rhs': info['solve_flops'], 'residual': max(res),
                 'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches,
-                'clocks': clocks, 'wall_s_timed': t_wall}
+                'clocks': clocks, 'wall_s_timed': t_wall, 'forms': forms}
         print(json.dumps(line), flush=True)
-    del ds
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -76,9 +76,12 @@ int spr_b200_info(void* handle, double* info);
  * of a forest of independent systems. */
 int spr_b200_sn_stats(void* handle, int32_t* neg, int32_t* fail);
 /* Factorisation mode of the device API: 0 = FP64 (default, the drop-in
- * semantics), 1 = mixed precision (Schur updates of the large fronts as
- * 3xTF32 split products, FP64 diagonal blocks/TRSM/storage); pair mode 1
- * with spr_b200_refine against the FP64 matrix (spr_b200_build_residual). */
+ * semantics); 1 = mixed precision, the Schur updates of the large fronts as
+ * 3xTF32 split products on the tcgen05 tensor cores with FP32 accumulation
+ * (FP64 diagonal blocks, TRSM, small fronts and storage); 2 = the same split
+ * products through mma.sync (FP64 accumulation every 64 columns).  Pair modes
+ * 1 and 2 with spr_b200_refine against the FP64 matrix
+ * (spr_b200_build_residual).  Returns -2 for an unknown mode. */
 int spr_b200_set_mode(void* handle, int mode);
 /* Residual operator for refinement: compacts the FP64 matrix held in an
  * assembled (not yet factored) device SM into a CSR (the product SPRPRQ forms

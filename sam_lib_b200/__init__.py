@@ -203,7 +203,10 @@ class DeviceSolver:
         return int(out[0]), float(out[1]), float(out[2])
 
     def set_mode(self, mixed):
-        self.lib.spr_b200_set_mode(self.h, 1 if mixed else 0)
+        """0/False = FP64, 1/True = 3xTF32 on tcgen05, 2 = 3xTF32 through mma.sync."""
+        rc = self.lib.spr_b200_set_mode(self.h, int(mixed))
+        if rc != 0:
+            raise ValueError('unknown factorisation mode %r' % (mixed,))
 
     def set_profile(self, on=True):
         self.lib.spr_b200_set_profile(self.h, 1 if on else 0)

@@ -526,7 +526,8 @@ int SPR_API(spr_b200_refine)(void* handle, const double* d_sm, const double* d_b
 
 // Factorisation mode: 0 = FP64 (the drop-in), 1 = mixed (3xTF32 Schur updates).
 int SPR_API(spr_b200_set_mode)(void* handle, int mode) {
-    static_cast<Engine*>(handle)->set_mixed(mode == 1);
+    if (mode < 0 || mode > 2) return -2;
+    static_cast<Engine*>(handle)->set_mixed(mode);
     return 0;
 }
 

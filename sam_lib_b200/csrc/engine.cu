@@ -17,6 +17,7 @@
 // assembled into dense column-major buffers in HBM and factored with a
 // blocked right-looking LDL' (diagonal block, panel TRSM, FP64 DMMA Schur
 // update), all fronts of the level batched into each launch.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,6 +53,7 @@ struct Stats {
     double tol2;             // max(a_jj / d_j), sprfc1.f:1284
     double trace;            // sum a_jj, sprfc1.f:483
     double mindpos;          // smallest positive pivot, sprfc1.f:690-697
+    int tc_timeout;          // a tensor-core update CTA gave up waiting (see tc_gemm.cuh)
 };
 
 struct PV {
@@ -109,6 +111,9 @@ struct Engine::Dev {
     int64_t bbuf_rhs = 0;
     std::vector<void*> owned;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // tensor-core (mixed) updates: operand slabs and the TMA map over them
+    float* slab = nullptr;
+    alignas(64) CUtensorMap slab_map;
 };
 
 template <typename T>
@@ -731,6 +736,8 @@ __device__ __forceinline__ void mma(float* c, const uint32_t* a, uint32_t b0, ui
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 }  // namespace x3
+
+#include "tc_gemm.cuh"
 
 __global__ void __launch_bounds__(128) k_gemm_x3(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
     using namespace gemm;
@@ -1633,8 +1640,41 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     CK(cudaFuncSetAttribute(k_gemm_x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
+    CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kSmem));
     return 0;
 }
+
+// Operand slabs of the tensor-core updates and the 2-D TMA map over them:
+// [slab_rows][32] fp32, box 32 x 128 rows, 128-byte swizzle.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int Engine::ensure_slabs() {
+    Dev& D = *d_;
+    if (D.slab) return 0;
+    const int64_t rows = std::max<int64_t>(P_.slab_rows, tc::kTM);
+    if (rows >= (int64_t(1) << 31)) return -3;                 // TMA row coordinates are 32-bit
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+        return -4;
+    CK(cudaMalloc((void**)&D.slab, rows * tc::kBK * sizeof(float)));
+    const cuuint64_t dims[2] = {(cuuint64_t)tc::kBK, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)tc::kBK * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)tc::kBK, (cuuint32_t)tc::kTM};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = ((EncodeTiledFn)fn)(&D.slab_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, D.slab, dims, strides,
+                                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        cudaFree(D.slab);
+        D.slab = nullptr;
+        return -4;
+    }
+    return 0;
+}
+
 
 static cudaEvent_t record_event(cudaStream_t s) {
     cudaEvent_t e = nullptr;
@@ -1684,7 +1724,7 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     if (l.ntasks <= 0) return;
     if (profile_) gev.push_back(record_event(s));
     const Job* jobs = d_->jobs + l.job_begin;
-    if (mixed_)
+    if (mixed_ == 2)
         k_gemm_x3<<<(int)l.ntasks, 128, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
     else if (l.tile == kTileBig)
         K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
@@ -1692,6 +1732,19 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
         K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
     if (profile_) gev.push_back(record_event(s));
     ++timing.launches;
+    ++timing.gemm_launches;
+}
+
+void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev) {
+    if (t.gemm.ntasks <= 0) return;
+    Dev& D = *d_;
+    if (profile_) gev.push_back(record_event(s));
+    k_split_tc<<<(int)t.split.ntasks, 256, 0, s>>>(D.jobs + t.split.job_begin, t.split.job_count, TMAP(t.split), pv,
+                                                   D.slab);
+    k_gemm_tc<<<(int)t.gemm.ntasks, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count,
+                                                                  TMAP(t.gemm), pv, D.slab_map);
+    if (profile_) gev.push_back(record_event(s));
+    timing.launches += 2;
     ++timing.gemm_launches;
 }
 
@@ -1726,9 +1779,15 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, TMAP(pl), pv);
                 ++timing.launches;
             }
-            for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            if (mixed_ == 1)
+                for (const TcLaunch& t : lp.update_tc[st]) launch_tc(t, s, pv, gev);
+            else
+                for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
         }
-        for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
+        if (mixed_ == 1)
+            for (const TcLaunch& t : lp.outer_tc) launch_tc(t, s, pv, gev);
+        else
+            for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
         {
             const Launch& l = lp.writeback;
             const int64_t threads = l.ntasks * 32;
@@ -1749,6 +1808,10 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     cudaStream_t s = stream_;
     PV pv = make_view(D, P_, d_sm, tol1);
     linv_valid_ = false;
+    if (mixed_ == 1) {
+        const int rc = ensure_slabs();
+        if (rc != 0) return rc;
+    }
     Stats init{};
     init.first_zero = 0x7fffffff;
     CK(cudaMemcpyAsync(D.st, &init, sizeof(Stats), cudaMemcpyHostToDevice, s));
@@ -1762,7 +1825,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     // the legacy default stream cannot be captured: graphs need a stream of our own
     const bool graph = use_graphs_ && !profile_ && s != nullptr;
     if (graph) {
-        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, mixed_ ? 1 : 0, 0};
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, mixed_, 0};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1792,6 +1855,10 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     }
     for (cudaEvent_t e : gev) cudaEventDestroy(e);
     res = FactorResult();
+    if (hs.tc_timeout) {
+        fprintf(stderr, "spr_b200: a tensor-core update gave up waiting for its operands\n");
+        return -4;
+    }
     if (hs.zero_count > 0) {                       // sprfc1.f:474-488
         // the reference's pre-pass has already replaced D by the original diagonal
         CK(cudaMemcpy(pv.dvec, D.adiag, P_.neq * sizeof(double), cudaMemcpyDeviceToDevice));

@@ -59,10 +59,11 @@ public:
     // CUDA-graph replay of the factor/solve launch sequences (on by default;
     // SPR_B200_GRAPHS=0 or set_graphs(false) launches kernel by kernel).
     void set_graphs(bool on) { use_graphs_ = on; }
-    // Mixed precision: the Schur updates of the large fronts in 3xTF32 (FP64
-    // diagonal blocks, TRSM, small fronts and storage); see k_gemm_x3.
-    void set_mixed(bool on) { mixed_ = on; }
-    bool mixed() const { return mixed_; }
+    // Mixed precision: the Schur updates of the large fronts as 3xTF32 split
+    // products (FP64 diagonal blocks, TRSM, small fronts and storage).
+    // 0 = FP64, 1 = tcgen05 tensor cores (k_gemm_tc), 2 = mma.sync (k_gemm_x3).
+    void set_mixed(int mode) { mixed_ = mode; }
+    int mixed() const { return mixed_; }
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
 
@@ -91,7 +92,9 @@ private:
                        int64_t& nl);
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
-    bool mixed_ = false;
+    int mixed_ = 0;
+    int ensure_slabs();
+    void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     struct Csr {
         int64_t* rowptr = nullptr;
         int32_t* ci = nullptr;

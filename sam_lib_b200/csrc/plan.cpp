@@ -249,6 +249,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     };
     auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
     P.gemm_flops = 0.0;
+    P.slab_rows = 0;
     P.small_flops = 0.0;
     for (int64_t js = 0; js < ns; ++js)
         if (P.F[js] <= kSmallMaxF) {
@@ -299,6 +300,33 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 if (l.ntasks > 0) out.push_back(l);
             }
         };
+        // the same jobs for the tensor-core path: slabs of W = L D and L as
+        // FP32 hi/lo pairs (4 arrays of K blocks of [rows][32])
+        lp.update_tc.assign(nsteps, std::vector<TcLaunch>());
+        auto emit_tc = [&](std::vector<Job> jl, std::vector<TcLaunch>& out) {
+            if (jl.empty()) return;
+            int64_t rows = 0;
+            for (Job& j : jl) {
+                const int64_t np = (int64_t)(j.r_end - j.c0 + kTcTile - 1) / kTcTile * kTcTile;
+                const int64_t nkb = (j.k_hi - j.k_lo + kTcBK - 1) / kTcBK;
+                j.slab = rows;
+                rows += 4 * nkb * np;
+            }
+            TcLaunch t;
+            open_launch(t.split);
+            for (const Job& j : jl) {
+                const int64_t np = (int64_t)(j.r_end - j.c0 + kTcTile - 1) / kTcTile * kTcTile;
+                const int64_t nkb = (j.k_hi - j.k_lo + kTcBK - 1) / kTcBK;
+                add_job(t.split, j, (np / 32) * nkb);
+            }
+            close_launch(t.split);
+            open_launch(t.gemm);
+            for (const Job& j : jl) add_job(t.gemm, j, tiles_t(j.c0, j.c_end, j.r_end, kTcTile));
+            close_launch(t.gemm);
+            t.gemm.tile = kTcTile;
+            P.slab_rows = std::max(P.slab_rows, rows);
+            out.push_back(t);
+        };
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
@@ -328,6 +356,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 }
             }
             emit_updates(jl, lp.update[st]);
+            emit_tc(jl, lp.update_tc[st]);
             open_launch(lp.fsolve[st]);
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
@@ -401,6 +430,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             lp.outer.clear();
             emit_updates(jl, lp.outer);
+            lp.outer_tc.clear();
+            emit_tc(jl, lp.outer_tc);
         }
         open_launch(lp.writeback);
         for (int32_t js : lp.large_nodes)
@@ -425,6 +456,15 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (auto& v : lp.update)
             for (Launch& l : v) build_map(l);
         for (Launch& l : lp.outer) build_map(l);
+        for (auto& v : lp.update_tc)
+            for (TcLaunch& t : v) {
+                build_map(t.split);
+                build_map(t.gemm);
+            }
+        for (TcLaunch& t : lp.outer_tc) {
+            build_map(t.split);
+            build_map(t.gemm);
+        }
         for (Launch& l : lp.fs_upd) build_map(l);
         for (Launch& l : lp.bs_upd) build_map(l);
         for (Launch& l : lp.blk_mv) build_map(l);

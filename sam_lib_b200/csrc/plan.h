@@ -46,12 +46,22 @@ struct Job {
     int32_t c0, c_end, r_end;
     int32_t k_lo, k_hi;
     int64_t task0;                   // first task of this job within its launch
+    int64_t slab = 0;                // tensor-core updates: first row of the job's operand slabs
 };
 
 struct Launch {                      // a contiguous range of Plan::jobs
     int64_t job_begin = 0, job_count = 0, ntasks = 0;
     int32_t tile = kTile;            // Schur-update launches: tile size of the decode
     int64_t map_begin = -1;          // task -> job map of this launch in Plan::task_map
+};
+
+// A tensor-core Schur-update launch: the split of the panel into FP32 hi/lo
+// operand slabs, then the 128x128-tile update (one task per lower tile).
+constexpr int kTcTile = 128;
+constexpr int kTcBK = 32;
+struct TcLaunch {
+    Launch split;                    // one task per 32 rows x 32 columns of each job's panel
+    Launch gemm;                     // one task per lower 128x128 tile of each job's block
 };
 
 struct LevelPlan {
@@ -71,6 +81,8 @@ struct LevelPlan {
     std::vector<Launch> bs_upd;               // columns [0, k0) before the block, kBwdCols per task
     std::vector<Launch> blk_mv;               // product with the block inverse, 32 rows/columns per task
     Launch rect;                              // back solve, rows [S, F): 32 columns per task
+    std::vector<std::vector<TcLaunch>> update_tc;   // mixed precision: the updates of each step
+    std::vector<TcLaunch> outer_tc;                 // mixed precision: the K = S update
 };
 
 constexpr int kBwdCols = 8;                   // columns per CTA in the back-solve update
@@ -124,6 +136,7 @@ struct Plan {
     double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
     double gemm_flops = 0.0;                 // algorithmic flops of the Schur-update launches
+    int64_t slab_rows = 0;                   // largest operand-slab need of one tensor-core launch (128-byte rows)
     double small_flops = 0.0;                // factor flops done by the fused small-front kernel
 };
 

@@ -1,0 +1,333 @@
+// Mixed-precision Schur update on the 5th-generation tensor cores (sm_100a).
+//
+//     C(rows, cols) -= (L D)(rows, K) * L(cols, K)'        (LMMY18, lmmy18.f:5-192)
+//
+// as 3xTF32 split products: x = hi + lo with hi = tf32(x), lo = tf32(x - hi),
+// and A*B ~ A_lo*B_hi + A_hi*B_lo + A_hi*B_hi accumulated in FP32 in tensor
+// memory; the FP64 front is updated once per tile at the end.
+//
+// Two kernels per Schur-update launch:
+//   k_split_tc  reads the FP64 panel columns [k_lo, k_hi) of rows [c0, r_end)
+//               of each front and writes four K-major FP32 slabs (W_hi, W_lo,
+//               L_hi, L_lo; W = L D) of 32-column blocks, [row][32] floats, rows
+//               padded to a multiple of 128 and K to a multiple of 32 with
+//               zeros, into the slab arena (one 128-byte row per slab row);
+//   k_gemm_tc   one CTA per 128x128 lower tile of the update block: a TMA
+//               producer warp streams the four 128x32 operand tiles of each K
+//               block into a 3-stage shared-memory ring (128-byte swizzle), one
+//               thread issues tcgen05.mma kind::tf32 (M=N=128, K=8) into a
+//               128-column TMEM accumulator and releases stages with
+//               tcgen05.commit, and four epilogue warps read the accumulator
+//               with tcgen05.ld and subtract it from the FP64 front (lower
+//               triangle only: the upper triangle of diagonal blocks holds
+//               L11^-1 of later panels).
+// Every mbarrier wait is bounded by a time limit; a wait that gives up sets
+// Stats::tc_timeout, the CTA skips its remaining work, frees its TMEM and
+// returns (the host turns the flag into an error).
+#pragma once
+#include <cuda.h>
+
+namespace tc {
+
+constexpr int kTM = 128;                  // M = N of the tile and of the MMA
+constexpr int kBK = 32;                     // K block: 32 fp32 = one 128-byte swizzle row
+constexpr int kStages = 3;
+constexpr int kOperandBytes = kTM * kBK * 4;          // 16 KB: one 128x32 fp32 tile
+constexpr int kStageBytes = 4 * kOperandBytes;           // A_hi, A_lo, B_hi, B_lo
+constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024 + 256;
+constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2-5 epilogue
+constexpr uint32_t kTmemCols = 128;
+constexpr unsigned long long kWaitNs = 2000000000ull;    // 2 s per wait
+
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTM >> 3) << 17) |
+                            ((uint32_t)(kTM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase of the given parity; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try(bar, parity)) return true;
+        if (now_ns() - t0 > kWaitNs) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(dst),
+        "l"(map), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: 8-row groups 1024 B apart (SBO),
+// descriptor version 1 (sm_100), layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns: thread t receives lane t's columns.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ int64_t padded_rows(const Job& jb) {
+    return ((int64_t)(jb.r_end - jb.c0) + kTM - 1) / kTM * kTM;
+}
+__device__ __forceinline__ int k_blocks(const Job& jb) { return (jb.k_hi - jb.k_lo + kBK - 1) / kBK; }
+
+}  // namespace tc
+
+// Split kernel: one CTA (256 threads) per 32-row x 32-column block of a job's
+// panel; the transpose goes through shared memory so that both the FP64
+// reads (column-major front) and the FP32 slab writes (row-major) coalesce.
+__global__ void __launch_bounds__(256) k_split_tc(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+                                                   float* slab) {
+    __shared__ float sw[2][32][33];
+    __shared__ float sl[2][32][33];
+    if (P.st->any_fail) return;
+    const int64_t task = blockIdx.x;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int64_t np = tc::padded_rows(jb);
+    const int nkb = tc::k_blocks(jb);
+    const int64_t u = task - jb.task0;
+    const int kb = (int)(u % nkb);
+    const int rb = (int)(u / nkb);
+    const int ld = P.buf_ld[js];
+    const double* front = P.arena + P.buf_off[js];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    // read: thread (tx = row, ty + 8 q = column)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int kc = ty + 8 * q;
+        const int k = jb.k_lo + kb * tc::kBK + kc;
+        const int r = jb.c0 + rb * 32 + tx;
+        double l = 0.0, d = 0.0;
+        if (k < jb.k_hi && r < jb.r_end) {
+            l = front[(int64_t)k * ld + r];
+            d = front[(int64_t)k * (ld + 1)];
+        }
+        const double w = l * d;
+        const float wh = tc::to_tf32((float)w), lh = tc::to_tf32((float)l);
+        sw[0][kc][tx] = wh;
+        sw[1][kc][tx] = tc::to_tf32((float)(w - (double)wh));
+        sl[0][kc][tx] = lh;
+        sl[1][kc][tx] = tc::to_tf32((float)(l - (double)lh));
+    }
+    __syncthreads();
+    // write: thread (tx = column, ty + 8 q = row); slab a at row base
+    // jb.slab + (a * nkb + kb) * np
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int rr = ty + 8 * q;
+        const int64_t row = (int64_t)rb * 32 + rr;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float v = a < 2 ? sw[a][tx][rr] : sl[a - 2][tx][rr];
+            slab[(jb.slab + ((int64_t)a * nkb + kb) * np + row) * tc::kBK + tx] = v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(tc::kThreads, 1)
+    k_gemm_tc(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const __grid_constant__ CUtensorMap tm) {
+    using namespace tc;
+    extern __shared__ uint8_t tc_raw[];
+    __shared__ uint64_t bars[2 * kStages + 1];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    if (P.st->any_fail) return;
+    const int64_t task = blockIdx.x;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // tile decode: column tile jt, row tile it >= jt (lower tiles of the block)
+    const int64_t u = task - jb.task0;
+    const int nct = (jb.c_end - jb.c0 + kTM - 1) / kTM;
+    const int nr = (jb.r_end - jb.c0 + kTM - 1) / kTM;
+    int lo = 0, hi = nct - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t pre = (int64_t)mid * nr - ((int64_t)mid * (mid - 1)) / 2;
+        if (pre <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const int jt = lo;
+    const int it = jt + (int)(u - ((int64_t)jt * nr - ((int64_t)jt * (jt - 1)) / 2));
+    const int i0 = jb.c0 + it * kTM, j0 = jb.c0 + jt * kTM;
+    const int64_t np = padded_rows(jb);
+    const int nkb = k_blocks(jb);
+
+    const uint32_t base = (smem_u32(tc_raw) + 1023u) & ~1023u;
+    const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[kStages]), accb = smem_u32(&bars[2 * kStages]);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(accb, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        const int ya = (int)(jb.slab + (i0 - jb.c0)), yb = (int)(jb.slab + (j0 - jb.c0));
+        int issued = 0;
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % kStages;
+            const uint32_t ph = (uint32_t)(kb / kStages) & 1u;
+            if (kb >= kStages && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                failed = 1;
+                break;
+            }
+            if (*(volatile int*)&failed) break;
+            const uint32_t st = base + (uint32_t)s * kStageBytes;
+            const uint32_t fb = full0 + 8 * s;
+            mbar_expect_tx(fb, kStageBytes);
+            const int64_t off = (int64_t)kb * np;
+            tma_load_2d(st, &tm, fb, 0, (int)(ya + off));                                   // W_hi
+            tma_load_2d(st + kOperandBytes, &tm, fb, 0, (int)(ya + off + (int64_t)nkb * np));      // W_lo
+            tma_load_2d(st + 2 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 2 * (int64_t)nkb * np));  // L_hi
+            tma_load_2d(st + 3 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 3 * (int64_t)nkb * np));  // L_lo
+            ++issued;
+        }
+        // drain: every issued stage must have landed before the CTA can exit
+        for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
+            mbar_wait(full0 + 8 * (kb % kStages), (uint32_t)(kb / kStages) & 1u);
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % kStages;
+            if (!mbar_wait(full0 + 8 * s, (uint32_t)(kb / kStages) & 1u) || *(volatile int*)&failed) {
+                failed = 1;
+                break;
+            }
+            fence_after_sync();
+            const uint32_t st = base + (uint32_t)s * kStageBytes;
+            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + kOperandBytes);
+            const uint64_t bh = sw128_desc(st + 2 * kOperandBytes), bl = sw128_desc(st + 3 * kOperandBytes);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 8; ++kk) {
+                const uint64_t adv = (uint64_t)(kk * 32) >> 4;     // 8 tf32 = 32 bytes along K
+                mma_tf32(tmem, al + adv, bh + adv, (kb | kk) != 0);
+                mma_tf32(tmem, ah + adv, bl + adv, 1u);
+                mma_tf32(tmem, ah + adv, bh + adv, 1u);
+            }
+            mma_commit(empty0 + 8 * s);
+        }
+        mma_commit(accb);               // arrives once every MMA issued above has completed
+    } else if (warp >= 2) {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile rows
+        const int q = warp & 3;
+        const bool ok = mbar_wait(accb, 0);
+        fence_after_sync();
+        if (ok && !*(volatile int*)&failed && nkb > 0) {
+            const int r = i0 + 32 * q + lane;
+            const int ld = P.buf_ld[js];
+            double* front = P.arena + P.buf_off[js];
+            for (int c = 0; c < kTM / 32; ++c) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
+                if (r < jb.r_end) {
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        const int col = j0 + 32 * c + t;
+                        if (col < jb.c_end && r >= col)
+                            front[(int64_t)r + (int64_t)col * ld] -= (double)__uint_as_float(v[t]);
+                    }
+                }
+            }
+        } else if (!ok) {
+            failed = 1;
+        }
+        fence_before_sync();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && failed) atomicExch(&P.st->tc_timeout, 1);
+    if (warp == 1) {
+        fence_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}

@@ -1,8 +1,10 @@
 """Mixed precision: 3xTF32 Schur updates with FP64 iterative refinement.
 
 The factor of the large fronts uses split-TF32 products (three tensor-core
-products per update, FP32 accumulation per 64-wide slice, FP64 across
-slices); diagonal blocks, pivots, TRSM and storage stay FP64.  Refinement
+products per update): mode 1 on tcgen05 (TMA-fed, FP32 accumulation in
+tensor memory over the whole update), mode 2 through mma.sync (FP32
+accumulation per 64-wide slice, FP64 across slices); diagonal blocks,
+pivots, TRSM and storage stay FP64.  Refinement
 runs against the FP64 matrix (CSR compacted from the assembled SM on the
 device) until the normwise backward error
 
@@ -43,9 +45,10 @@ def _host_berr(K, x, b):
                for q in range(b.shape[1]))
 
 
+@pytest.mark.parametrize('mode', [1, 2])
 @pytest.mark.parametrize('n,emod,sigma_factor', [(16, 'uniform', 0.0), (16, 'loguniform', 0.0),
                                                  (20, 'uniform', 2.5)])
-def test_mixed_factor_refined_to_fp64_backward_error(n, emod, sigma_factor):
+def test_mixed_factor_refined_to_fp64_backward_error(n, emod, sigma_factor, mode):
     import torch
     import sam_lib_b200 as spr
     hs, sm, K = _system(n, emod, sigma_factor)
@@ -67,7 +70,7 @@ def test_mixed_factor_refined_to_fp64_backward_error(n, emod, sigma_factor):
     assert it0 == 0 and berr64 <= 1e-13
 
     # mixed factor + refinement
-    ds.set_mode(True)
+    ds.set_mode(mode)
     d_mx = d_sm0.clone()
     rmx = ds.factor(d_mx)
     ds.set_mode(False)
