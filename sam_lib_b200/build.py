@@ -34,7 +34,7 @@ def _newer(target, deps):
 
 def build(verbose_ptxas=False):
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.h')]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.h', '.cuh'))]
     objs = []
     for src in ENGINE_SOURCES:
         s = os.path.join(CSRC, src)

@@ -144,6 +144,36 @@ __device__ __forceinline__ int64_t padded_rows(const Job& jb) {
 }
 __device__ __forceinline__ int k_blocks(const Job& jb) { return (jb.k_hi - jb.k_lo + kBK - 1) / kBK; }
 
+// Lower tiles (it >= jt) of an nr x nct tile grid in groups of kGroup
+// column tiles: inside a group the order is row by row, so the CTAs that run
+// together share a few row panels (A) and a few column panels (B) and the
+// operand slabs are served from L2 instead of HBM.
+constexpr int kGroup = 8;
+__device__ __forceinline__ void tile_of(int64_t u, int nct, int nr, int& it, int& jt) {
+    int g0 = 0;
+    for (;;) {
+        const int w = min(kGroup, nct - g0);
+        const int64_t tri = (int64_t)w * (w - 1) / 2;
+        const int64_t cnt = tri + (int64_t)(nr - g0 - (w - 1)) * w;
+        if (u < cnt || g0 + w >= nct) {
+            if (u < tri) {
+                int a = (int)((sqrt(8.0 * (double)u + 1.0) - 1.0) * 0.5);
+                while ((int64_t)(a + 1) * (a + 2) / 2 <= u) ++a;
+                while ((int64_t)a * (a + 1) / 2 > u) --a;
+                it = g0 + a;
+                jt = g0 + (int)(u - (int64_t)a * (a + 1) / 2);
+            } else {
+                const int64_t v = u - tri;
+                it = g0 + (w - 1) + (int)(v / w);
+                jt = g0 + (int)(v % w);
+            }
+            return;
+        }
+        u -= cnt;
+        g0 += w;
+    }
+}
+
 }  // namespace tc
 
 // Split kernel: one CTA (256 threads) per 32-row x 32-column block of a job's
@@ -213,18 +243,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (P.sn_bad[js]) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // tile decode: column tile jt, row tile it >= jt (lower tiles of the block)
-    const int64_t u = task - jb.task0;
-    const int nct = (jb.c_end - jb.c0 + kTM - 1) / kTM;
-    const int nr = (jb.r_end - jb.c0 + kTM - 1) / kTM;
-    int lo = 0, hi = nct - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        const int64_t pre = (int64_t)mid * nr - ((int64_t)mid * (mid - 1)) / 2;
-        if (pre <= u) lo = mid;
-        else hi = mid - 1;
-    }
-    const int jt = lo;
-    const int it = jt + (int)(u - ((int64_t)jt * nr - ((int64_t)jt * (jt - 1)) / 2));
+    int it, jt;
+    tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
     const int i0 = jb.c0 + it * kTM, j0 = jb.c0 + jt * kTM;
     const int64_t np = padded_rows(jb);
     const int nkb = k_blocks(jb);
@@ -311,11 +331,19 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 uint32_t v[32];
                 tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
                 if (r < jb.r_end) {
+                    // all loads of the chunk first (independent), then the stores
+                    double cv[32];
+                    const double* src = front + (int64_t)r + (int64_t)(j0 + 32 * c) * ld;
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        const int col = j0 + 32 * c + t;
+                        cv[t] = (col < jb.c_end && r >= col) ? __ldcg(src + (int64_t)t * ld) : 0.0;
+                    }
 #pragma unroll
                     for (int t = 0; t < 32; ++t) {
                         const int col = j0 + 32 * c + t;
                         if (col < jb.c_end && r >= col)
-                            front[(int64_t)r + (int64_t)col * ld] -= (double)__uint_as_float(v[t]);
+                            front[(int64_t)r + (int64_t)col * ld] = cv[t] - (double)__uint_as_float(v[t]);
                     }
                 }
             }
