@@ -416,17 +416,28 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
             for (int i = tx; i < nb; i += 16)
                 if (i > j) A[i][j] *= rdv[j];
         __syncthreads();
-        // X = L^-1 by columns: X[j][j] = 1, X[i][j] = -sum_{m=j}^{i-1} L[i][m] X[m][j];
-        // X[i][j] (i > j) is kept at A[j][i]
-        if (tid < nb) {
-            const int j = tid;
-            for (int i = j + 1; i < nb; ++i) {
-                double acc = -A[i][j];
-                for (int m = j + 1; m < i; ++m) acc -= A[i][m] * A[j][m];
-                A[j][i] = acc;
-            }
-        }
+        // X = L^-1 by a column sweep: X = I, then for m = 0..nb-1 every
+        // X[i][j] with i > m >= j loses L[i][m] X[m][j] (X[m][j] is final at
+        // step m); X[i][j] (i > j) is kept at A[j][i], X[m][m] = 1
+        for (int j = ty; j < kNB; j += 16)
+            for (int i = tx; i < kNB; i += 16)
+                if (i > j) A[j][i] = 0.0;
         __syncthreads();
+        for (int m = 0; m < nb - 1; ++m) {
+#pragma unroll
+            for (int a = 0; a < kNB / 16; ++a) {
+                const int i = tx + 16 * a;
+                if (i > m && i < nb) {
+                    const double lim = A[i][m];
+#pragma unroll
+                    for (int b = 0; b < kNB / 16; ++b) {
+                        const int j = ty + 16 * b;
+                        if (j <= m) A[j][i] -= lim * (j == m ? 1.0 : A[j][m]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
         double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
         for (int j = ty; j < kNB; j += 16)
             for (int i = tx; i < kNB; i += 16)
