@@ -1590,6 +1590,11 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     if (rc != 0) return rc;
     Dev& D = *d_;
     auto& o = D.owned;
+    {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+    }
     if (dev_upload(o, &D.fst, P_.fst) || dev_upload(o, &D.S, P_.S) || dev_upload(o, &D.F, P_.F) ||
         dev_upload(o, &D.child_ptr, P_.child_ptr) || dev_upload(o, &D.child, P_.child) ||
         dev_upload(o, &D.rows, P_.rows) || dev_upload(o, &D.rel, P_.rel) ||
@@ -1752,8 +1757,9 @@ void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vec
     if (profile_) gev.push_back(record_event(s));
     k_split_tc<<<(int)t.split.ntasks, 256, 0, s>>>(D.jobs + t.split.job_begin, t.split.job_count, TMAP(t.split), pv,
                                                    D.slab);
-    k_gemm_tc<<<(int)t.gemm.ntasks, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count,
-                                                                  TMAP(t.gemm), pv, D.slab_map);
+    const int grid = (int)std::min<int64_t>(t.gemm.ntasks, sm_count_);
+    k_gemm_tc<<<grid, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count, TMAP(t.gemm),
+                                                    t.gemm.ntasks, pv, D.slab_map);
     if (profile_) gev.push_back(record_event(s));
     timing.launches += 2;
     ++timing.gemm_launches;

@@ -93,6 +93,7 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     int mixed_ = 0;
+    int sm_count_ = 148;
     int ensure_slabs();
     void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     struct Csr {

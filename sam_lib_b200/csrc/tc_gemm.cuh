@@ -36,7 +36,8 @@ constexpr int kOperandBytes = kTM * kBK * 4;          // 16 KB: one 128x32 fp32 
 constexpr int kStageBytes = 4 * kOperandBytes;           // A_hi, A_lo, B_hi, B_lo
 constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024 + 256;
 constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2-5 epilogue
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 512;       // FP32 accumulator pair [0,256) + FP64 sums [256,512)
+constexpr int kChunk = 8;                   // K blocks (256 columns) per FP32 accumulation
 constexpr unsigned long long kWaitNs = 2000000000ull;    // 2 s per wait
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128
@@ -131,6 +132,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
           "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
 }
 
 __device__ __forceinline__ float to_tf32(float x) {
@@ -229,34 +242,33 @@ __global__ void __launch_bounds__(256) k_split_tc(const Job* jobs, int64_t njobs
     }
 }
 
+// Persistent: CTA b takes the tasks b, b + gridDim.x, ...; the stage ring and
+// the accumulator pair run on across tiles, so the epilogue of one tile
+// overlaps the MMAs of the next.  The FP32 accumulation runs over chunks of
+// kChunk K blocks; between chunks the epilogue warps add the chunk into FP64
+// partial sums kept in tensor memory, and the last chunk goes to the front.
 __global__ void __launch_bounds__(tc::kThreads, 1)
-    k_gemm_tc(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const __grid_constant__ CUtensorMap tm) {
+    k_gemm_tc(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P,
+              const __grid_constant__ CUtensorMap tm) {
     using namespace tc;
     extern __shared__ uint8_t tc_raw[];
-    __shared__ uint64_t bars[2 * kStages + 1];
+    __shared__ uint64_t bars[2 * kStages + 4];
     __shared__ uint32_t tmem_slot;
     __shared__ int failed;
     if (P.st->any_fail) return;
-    const int64_t task = blockIdx.x;
-    const Job& jb = job_of(jobs, njobs, tmap, task);
-    const int js = jb.node;
-    if (P.sn_bad[js]) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // tile decode: column tile jt, row tile it >= jt (lower tiles of the block)
-    int it, jt;
-    tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
-    const int i0 = jb.c0 + it * kTM, j0 = jb.c0 + jt * kTM;
-    const int64_t np = padded_rows(jb);
-    const int nkb = k_blocks(jb);
-
     const uint32_t base = (smem_u32(tc_raw) + 1023u) & ~1023u;
-    const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[kStages]), accb = smem_u32(&bars[2 * kStages]);
+    const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[kStages]);
+    const uint32_t accf0 = smem_u32(&bars[2 * kStages]), acce0 = smem_u32(&bars[2 * kStages + 2]);
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
-        mbar_init(accb, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accf0 + 8 * b, 1);
+            mbar_init(acce0 + 8 * b, 4);                  // one arrival per epilogue warp
+        }
         failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -272,85 +284,161 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const uint32_t tmem = tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // TMA producer
-        const int ya = (int)(jb.slab + (i0 - jb.c0)), yb = (int)(jb.slab + (j0 - jb.c0));
-        int issued = 0;
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % kStages;
-            const uint32_t ph = (uint32_t)(kb / kStages) & 1u;
-            if (kb >= kStages && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
-                failed = 1;
-                break;
+        // ---- TMA producer: K blocks of every tile, continuing ring position
+        int64_t g = 0;
+        for (int64_t task = blockIdx.x; task < ntasks && !*(volatile int*)&failed; task += gridDim.x) {
+            const Job& jb = job_of(jobs, njobs, tmap, task);
+            if (P.sn_bad[jb.node]) continue;
+            int it, jt;
+            tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
+            const int64_t np = padded_rows(jb);
+            const int nkb = k_blocks(jb);
+            const int64_t ya = jb.slab + (int64_t)it * kTM, yb = jb.slab + (int64_t)jt * kTM;
+            for (int kb = 0; kb < nkb; ++kb, ++g) {
+                const int s = (int)(g % kStages);
+                const uint32_t ph = (uint32_t)(g / kStages) & 1u;
+                if (g >= kStages && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                    failed = 1;
+                    break;
+                }
+                const uint32_t st = base + (uint32_t)s * kStageBytes;
+                const uint32_t fb = full0 + 8 * s;
+                mbar_expect_tx(fb, kStageBytes);
+                const int64_t off = (int64_t)kb * np, arr = (int64_t)nkb * np;
+                tma_load_2d(st, &tm, fb, 0, (int)(ya + off));                                  // W_hi
+                tma_load_2d(st + kOperandBytes, &tm, fb, 0, (int)(ya + off + arr));               // W_lo
+                tma_load_2d(st + 2 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 2 * arr));       // L_hi
+                tma_load_2d(st + 3 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 3 * arr));       // L_lo
             }
-            if (*(volatile int*)&failed) break;
-            const uint32_t st = base + (uint32_t)s * kStageBytes;
-            const uint32_t fb = full0 + 8 * s;
-            mbar_expect_tx(fb, kStageBytes);
-            const int64_t off = (int64_t)kb * np;
-            tma_load_2d(st, &tm, fb, 0, (int)(ya + off));                                   // W_hi
-            tma_load_2d(st + kOperandBytes, &tm, fb, 0, (int)(ya + off + (int64_t)nkb * np));      // W_lo
-            tma_load_2d(st + 2 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 2 * (int64_t)nkb * np));  // L_hi
-            tma_load_2d(st + 3 * kOperandBytes, &tm, fb, 0, (int)(yb + off + 3 * (int64_t)nkb * np));  // L_lo
-            ++issued;
         }
-        // drain: every issued stage must have landed before the CTA can exit
-        for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
-            mbar_wait(full0 + 8 * (kb % kStages), (uint32_t)(kb / kStages) & 1u);
+        // drain: the last kStages issued stages must have landed before exit
+        for (int64_t q = (g > kStages ? g - kStages : 0); q < g; ++q)
+            mbar_wait(full0 + 8 * (int)(q % kStages), (uint32_t)(q / kStages) & 1u);
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % kStages;
-            if (!mbar_wait(full0 + 8 * s, (uint32_t)(kb / kStages) & 1u) || *(volatile int*)&failed) {
-                failed = 1;
-                break;
-            }
-            fence_after_sync();
-            const uint32_t st = base + (uint32_t)s * kStageBytes;
-            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + kOperandBytes);
-            const uint64_t bh = sw128_desc(st + 2 * kOperandBytes), bl = sw128_desc(st + 3 * kOperandBytes);
+        // ---- MMA issuer: chunks of kChunk K blocks into alternating accumulators
+        int64_t g = 0, h = 0;
+        for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
+            const Job& jb = job_of(jobs, njobs, tmap, task);
+            if (P.sn_bad[jb.node]) continue;
+            const int nkb = k_blocks(jb);
+            bool stop = false;
+            for (int c0 = 0; c0 < nkb && !stop; c0 += kChunk, ++h) {
+                const int b = (int)(h & 1);
+                const int64_t use = h >> 1;
+                if (use >= 1 && !mbar_wait(acce0 + 8 * b, (uint32_t)((use - 1) & 1))) {
+                    failed = 1;
+                    stop = true;
+                    break;
+                }
+                fence_after_sync();
+                const uint32_t acc = tmem + (uint32_t)(b * kTM);
+                const int c1 = min(nkb, c0 + kChunk);
+                for (int kb = c0; kb < c1; ++kb, ++g) {
+                    const int s = (int)(g % kStages);
+                    if (!mbar_wait(full0 + 8 * s, (uint32_t)(g / kStages) & 1u) || *(volatile int*)&failed) {
+                        failed = 1;
+                        stop = true;
+                        break;
+                    }
+                    fence_after_sync();
+                    const uint32_t st = base + (uint32_t)s * kStageBytes;
+                    const uint64_t ah = sw128_desc(st), al = sw128_desc(st + kOperandBytes);
+                    const uint64_t bh = sw128_desc(st + 2 * kOperandBytes), bl = sw128_desc(st + 3 * kOperandBytes);
 #pragma unroll
-            for (int kk = 0; kk < kBK / 8; ++kk) {
-                const uint64_t adv = (uint64_t)(kk * 32) >> 4;     // 8 tf32 = 32 bytes along K
-                mma_tf32(tmem, al + adv, bh + adv, (kb | kk) != 0);
-                mma_tf32(tmem, ah + adv, bl + adv, 1u);
-                mma_tf32(tmem, ah + adv, bh + adv, 1u);
+                    for (int kk = 0; kk < kBK / 8; ++kk) {
+                        const uint64_t adv = (uint64_t)(kk * 32) >> 4;     // 8 tf32 = 32 bytes along K
+                        mma_tf32(acc, al + adv, bh + adv, (kb != c0 || kk != 0) ? 1u : 0u);
+                        mma_tf32(acc, ah + adv, bl + adv, 1u);
+                        mma_tf32(acc, ah + adv, bh + adv, 1u);
+                    }
+                    mma_commit(empty0 + 8 * s);
+                }
+                mma_commit(accf0 + 8 * b);      // arrives when this chunk's MMAs are done
             }
-            mma_commit(empty0 + 8 * s);
+            if (stop) break;
         }
-        mma_commit(accb);               // arrives once every MMA issued above has completed
     } else if (warp >= 2) {
-        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile rows
+        // ---- epilogue: warp w owns TMEM lanes 32 (w % 4) .. + 31 (tile rows)
         const int q = warp & 3;
-        const bool ok = mbar_wait(accb, 0);
-        fence_after_sync();
-        if (ok && !*(volatile int*)&failed && nkb > 0) {
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+        int64_t h = 0;
+        for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
+            const Job& jb = job_of(jobs, njobs, tmap, task);
+            const int js = jb.node;
+            if (P.sn_bad[js]) continue;
+            int it, jt;
+            tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
+            const int i0 = jb.c0 + it * kTM, j0 = jb.c0 + jt * kTM;
+            const int nkb = k_blocks(jb);
+            const int nch = (nkb + kChunk - 1) / kChunk;
             const int r = i0 + 32 * q + lane;
             const int ld = P.buf_ld[js];
             double* front = P.arena + P.buf_off[js];
-            for (int c = 0; c < kTM / 32; ++c) {
-                uint32_t v[32];
-                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
-                if (r < jb.r_end) {
-                    // all loads of the chunk first (independent), then the stores
-                    double cv[32];
-                    const double* src = front + (int64_t)r + (int64_t)(j0 + 32 * c) * ld;
+            bool stop = false;
+            for (int c = 0; c < nch; ++c, ++h) {
+                const int b = (int)(h & 1);
+                if (!mbar_wait(accf0 + 8 * b, (uint32_t)((h >> 1) & 1)) || *(volatile int*)&failed) {
+                    failed = 1;
+                    stop = true;
+                    break;
+                }
+                fence_after_sync();
+                const uint32_t acc = lane_base + (uint32_t)(b * kTM);
+                const uint32_t acc64 = lane_base + (uint32_t)(2 * kTM);
+                for (int cc = 0; cc < kTM / 32; ++cc) {
+                    uint32_t v[32];
+                    tmem_ld32(acc + (uint32_t)(32 * cc), v);
+                    double sum[32];
+                    if (c == 0) {
 #pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        const int col = j0 + 32 * c + t;
-                        cv[t] = (col < jb.c_end && r >= col) ? __ldcg(src + (int64_t)t * ld) : 0.0;
+                        for (int t = 0; t < 32; ++t) sum[t] = (double)__uint_as_float(v[t]);
+                    } else {
+                        uint32_t w0[32], w1[32];
+                        tmem_ld32(acc64 + (uint32_t)(64 * cc), w0);
+                        tmem_ld32(acc64 + (uint32_t)(64 * cc + 32), w1);
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) {
+                            sum[t] = __hiloint2double((int)w0[2 * t + 1], (int)w0[2 * t]) +
+                                     (double)__uint_as_float(v[t]);
+                            sum[16 + t] = __hiloint2double((int)w1[2 * t + 1], (int)w1[2 * t]) +
+                                          (double)__uint_as_float(v[16 + t]);
+                        }
                     }
+                    if (c + 1 < nch) {
+                        // keep the FP64 partial sums in TMEM (two 32-bit columns each)
+                        uint32_t w0[32], w1[32];
 #pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        const int col = j0 + 32 * c + t;
-                        if (col < jb.c_end && r >= col)
-                            front[(int64_t)r + (int64_t)col * ld] = cv[t] - (double)__uint_as_float(v[t]);
+                        for (int t = 0; t < 16; ++t) {
+                            w0[2 * t] = (uint32_t)__double2loint(sum[t]);
+                            w0[2 * t + 1] = (uint32_t)__double2hiint(sum[t]);
+                            w1[2 * t] = (uint32_t)__double2loint(sum[16 + t]);
+                            w1[2 * t + 1] = (uint32_t)__double2hiint(sum[16 + t]);
+                        }
+                        tmem_st32(acc64 + (uint32_t)(64 * cc), w0);
+                        tmem_st32(acc64 + (uint32_t)(64 * cc + 32), w1);
+                    } else if (r < jb.r_end) {
+                        // all loads of the chunk first (independent), then the stores
+                        double cv[32];
+                        const double* src = front + (int64_t)r + (int64_t)(j0 + 32 * cc) * ld;
+#pragma unroll
+                        for (int t = 0; t < 32; ++t) {
+                            const int col = j0 + 32 * cc + t;
+                            cv[t] = (col < jb.c_end && r >= col) ? __ldcg(src + (int64_t)t * ld) : 0.0;
+                        }
+#pragma unroll
+                        for (int t = 0; t < 32; ++t) {
+                            const int col = j0 + 32 * cc + t;
+                            if (col < jb.c_end && r >= col) front[(int64_t)r + (int64_t)col * ld] = cv[t] - sum[t];
+                        }
                     }
                 }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                fence_before_sync();
+                __syncwarp();
+                if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce0 + 8 * b) : "memory");
             }
-        } else if (!ok) {
-            failed = 1;
+            if (stop) break;
         }
-        fence_before_sync();
     }
     __syncthreads();
     if (threadIdx.x == 0 && failed) atomicExch(&P.st->tc_timeout, 1);
