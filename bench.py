@@ -49,6 +49,10 @@ def parse():
     ap.add_argument('--n', type=int, default=N_MESH)
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--case', choices=['fp64', 'mixed'], default=None,
+                    help='profiling case: only WARMUP+STEPS factorisations of the n^3 box in that mode')
+    ap.add_argument('--phases', action='store_true',
+                    help='with --case: CUDA events between launch groups, time by phase')
     ap.add_argument('--no-forms', action='store_true',
                     help='skip the mixed+IR, batched and adjoint measurements')
     return ap.parse_args()
@@ -173,6 +177,18 @@ def dgemm_peak(torch):
     return 2.0 * n ** 3 / ms / 1e9
 
 
+def tf32_peak():
+    """Dense TF32 tensor peak: half the measured bf16 burst rate (tcgen05 kind::tf32
+    runs at half the kind::f16 rate), else half the fallback bf16 figure."""
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(p) as f:
+            bf16 = float(json.load(f)['bf16_tflops'])
+        return bf16 / 2.0, 'measured bf16 burst %.1f TFLOP/s (MEASURED_PEAKS.json) / 2' % bf16
+    except Exception:
+        return 1590.0 / 2.0, 'fallback bf16 1590 TFLOP/s / 2'
+
+
 def read_traffic():
     """dram bytes per Schur-update flop from the committed ncu summary, if any."""
     p = os.path.join(ROOT, 'profiles', 'k_gemm_traffic.txt')
@@ -237,13 +253,31 @@ def form_mixed_ir(torch, spr, n, emod, reps=2):
                 ts.append(e0.elapsed_time(e1))
         out[mode] = {'factor_solve_s': float(np.mean(ts)) / 1e3, 'factor_s': fac_ms / 1e3,
                      'ir_corrections': it, 'backward_error': berr, 'numneg': fr['numneg']}
+    # roofline of the tensor-core update (split + k_gemm_tc launches, CUDA
+    # events around each launch pair) in one more mixed factorisation
+    ds.set_mode(1)
+    ds.set_profile(True)
+    with torch.cuda.stream(st):
+        d_sm.copy_(d_sm0)
+    st.synchronize()
+    ds.factor(d_sm)
+    inf = ds.info()
+    ds.set_profile(False)
     ds.set_mode(False)
+    tf32_flops = 3.0 * inf['gemm_flops']
+    peak, src = tf32_peak()
+    achieved = tf32_flops / (inf['gemm_ms'] / 1e3) / 1e12
+    roof_tc = {'bound': 'tensor', 'kernel': 'k_split_tc + k_gemm_tc: 3xTF32 Schur update (tcgen05.mma kind::tf32, '
+                                            'TMA, TMEM accumulators)',
+               'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
+               'flops': 'TF32 tensor flops = 3 products x algorithmic update flops (%.4g)' % inf['gemm_flops'],
+               'peak_source': src, 'time_s': inf['gemm_ms'] / 1e3, 'launch_pairs': inf['gemm_launches']}
     rel = float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64))
     del ds
     torch.cuda.empty_cache()
     return {'system': '%d^3 hex8, E %s (seed 2), %d RHS U[-1,1] seed 1' % (
                 n, 'log-uniform [1,1e4]' if emod == 'loguniform' else '= 1', NRHS),
-            'fp64': out[0], 'mixed_ir': out[1], 'tol': 1e-12,
+            'fp64': out[0], 'mixed_ir': out[1], 'tol': 1e-12, 'roofline_tc': roof_tc,
             'speedup_mixed_ir_vs_fp64': out[0]['factor_solve_s'] / out[1]['factor_solve_s'],
             'numneg_equal': out[0]['numneg'] == out[1]['numneg'],
             'rel_diff_vs_fp64_gpu_solution': rel}
@@ -488,8 +522,40 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_case(args):
+    """Factorisations only (no solve, e2e, CPU leg or forms): the command the
+    committed ncu summaries were captured with."""
+    import torch
+    import sam_lib_b200 as spr
+    from sam_lib_b200.system import HexSystem
+    hs = HexSystem(args.n)
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    st = torch.cuda.Stream()
+    ds.set_stream(st.cuda_stream)
+    ds.set_mode(1 if args.case == 'mixed' else 0)
+    ds.set_profile(args.phases)
+    d_sm0 = torch.from_numpy(hs.assemble()).cuda()
+    d_sm = torch.empty_like(d_sm0)
+    ms = []
+    for k in range(args.warmup + args.steps):
+        with torch.cuda.stream(st):
+            d_sm.copy_(d_sm0)
+        st.synchronize()
+        r = ds.factor(d_sm)
+        assert r['lierr'] == 0, r
+        if k >= args.warmup:
+            ms.append(ds.info()['factor_ms'])
+    line = {'case': args.case, 'n': args.n, 'factor_ms': ms}
+    if args.phases:
+        line['phase_ms'] = ds.phase_ms()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args)
+        return
     rank = int(os.environ.get('RANK', '0'))
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))

@@ -93,6 +93,10 @@ int spr_b200_build_residual(void* handle, const double* d_sm_assembled);
  * out[1]=backward error out[2]=solve ms.  b, x: ld x nrhs, device. */
 int spr_b200_refine(void* handle, const double* d_sm, const double* d_b, double* d_x, int64_t ld,
                     int64_t nrhs, double tol, int maxit, double* out);
+/* Profile mode only: last factorisation's time by phase, out[0..8] = pre-pass,
+ * small fronts, extend-add, diagonal blocks, panel TRSM, in-panel/trailing
+ * updates, K = S update, write-back, end (ms). */
+int spr_b200_phase_ms(void* handle, double* out);
 /* Profile mode: CUDA events around every Schur-update launch. */
 int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed); see abi.cpp. */

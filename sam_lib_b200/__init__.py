@@ -51,6 +51,8 @@ def load(int_kind=8):
         lib.spr_b200_refine.restype = C.c_int
         lib.spr_b200_set_mode.argtypes = [vp, C.c_int]
         lib.spr_b200_set_mode.restype = C.c_int
+        lib.spr_b200_phase_ms.argtypes = [vp, vp]
+        lib.spr_b200_phase_ms.restype = C.c_int
         lib.spr_b200_set_profile.argtypes = [vp, C.c_int]
         lib.spr_b200_set_profile.restype = C.c_int
         lib.spr_b200_release_all.argtypes = []
@@ -207,6 +209,14 @@ class DeviceSolver:
         rc = self.lib.spr_b200_set_mode(self.h, int(mixed))
         if rc != 0:
             raise ValueError('unknown factorisation mode %r' % (mixed,))
+
+    def phase_ms(self):
+        """Profile mode: last factorisation's time by phase (ms)."""
+        out = np.zeros(9)
+        self.lib.spr_b200_phase_ms(self.h, _ptr(out))
+        keys = ('prepass', 'small_fronts', 'extend_add', 'diag', 'trsm', 'updates', 'outer_update',
+                'writeback', 'end')
+        return dict(zip(keys, out.tolist()))
 
     def set_profile(self, on=True):
         self.lib.spr_b200_set_profile(self.h, 1 if on else 0)

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "plan.h"
@@ -24,6 +25,10 @@ struct Timing {              // CUDA-event times of the last calls (ms)
     float factor_ms = 0.f, solve_ms = 0.f;
     float gemm_ms = 0.f;     // Schur-update kernels only (sum over launches)
     int64_t gemm_launches = 0, launches = 0, solve_launches = 0;
+    // profile mode: factor time by phase (CUDA events between launch groups):
+    // 0 pre-pass, 1 small fronts, 2 extend-add, 3 diagonal blocks, 4 panel
+    // TRSM, 5 in-panel/trailing updates, 6 K = S update, 7 write-back, 8 end
+    float phase_ms[9] = {};
 };
 
 class Engine {
@@ -93,6 +98,7 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     int mixed_ = 0;
+    std::vector<std::pair<int, cudaEvent_t>> marks_;
     int sm_count_ = 148;
     int ensure_slabs();
     void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
