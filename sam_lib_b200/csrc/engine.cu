@@ -1788,18 +1788,6 @@ int Engine::ensure_slabs() {
 }
 
 
-// Profile mode: holds the stream for a fixed time so that the host can queue
-// the launch sequence ahead of the GPU (the phase events then time the
-// kernels back to back rather than the host's launch rate).
-__global__ void k_hold(unsigned long long ns) {
-    unsigned long long t0, t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    do {
-        __nanosleep(10000);
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    } while (t - t0 < ns);
-}
-
 static cudaEvent_t record_event(cudaStream_t s) {
     cudaEvent_t e = nullptr;
     cudaEventCreate(&e);
@@ -1957,7 +1945,6 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     CK(cudaMemsetAsync(D.sn_bad, 0, P_.nsuper * sizeof(int32_t), s));
     timing.gemm_ms = 0.f;
     timing.gemm_launches = 0;
-    if (profile_) k_hold<<<1, 32, 0, s>>>(300000000ull);
     CK(cudaEventRecord(D.ev0, s));
     std::vector<cudaEvent_t> gev;
     // the legacy default stream cannot be captured: graphs need a stream of our own
