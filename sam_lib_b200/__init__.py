@@ -212,10 +212,11 @@ class DeviceSolver:
 
     def phase_ms(self):
         """Profile mode: last factorisation's time by phase (ms)."""
-        out = np.zeros(9)
+        out = np.zeros(20)
         self.lib.spr_b200_phase_ms(self.h, _ptr(out))
         keys = ('prepass', 'small_fronts', 'extend_add', 'diag', 'trsm', 'updates', 'outer_update',
-                'writeback', 'end')
+                'writeback', 'end', 'fwd_small', 'fwd_gather', 'fwd_blocks', 'fwd_rect', 'fwd_finish',
+                'bwd_small', 'bwd_gather', 'bwd_rect', 'bwd_blk_mv', 'bwd_blk_upd', 'bwd_finish')
         return dict(zip(keys, out.tolist()))
 
     def set_profile(self, on=True):

@@ -534,10 +534,11 @@ int SPR_API(spr_b200_set_mode)(void* handle, int mode) {
 // Profile mode: CUDA events around every Schur-update launch (spr_b200_info[8]).
 // Profile mode only: factor time of the last factorisation by phase
 // (out[0..8]: pre-pass, small fronts, extend-add, diagonal blocks, panel
-// TRSM, in-panel/trailing updates, K = S update, write-back, end).
+// TRSM, in-panel/trailing updates, K = S update, write-back, end) and of the
+// last solve (out[9..19], see Timing::phase_ms).
 int SPR_API(spr_b200_phase_ms)(void* handle, double* out) {
     const auto& t = static_cast<Engine*>(handle)->timing;
-    for (int k = 0; k < 9; ++k) out[k] = t.phase_ms[k];
+    for (int k = 0; k < 20; ++k) out[k] = t.phase_ms[k];
     return 0;
 }
 

@@ -74,6 +74,7 @@ struct PV {
     const int64_t* xinv_off;
     double* xinv;            // inverses of the kSolveBlock-wide diagonal blocks
     const int64_t* rect_off;
+    const int64_t* fwd_off;
     double tol1;
 };
 
@@ -90,6 +91,7 @@ struct Engine::Dev {
     double* xinv = nullptr;
     int32_t* task_map = nullptr;
     int64_t* rect_off = nullptr;
+    int64_t* fwd_off = nullptr;
     double* pbuf = nullptr;                      // back-solve rectangle partial sums
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
     std::vector<int64_t> small_begin;            // per level offset into level_nodes
@@ -1161,7 +1163,7 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap
 // row below the block (thread per row, SPRFS6).  Backward mirrors it.
 
 // w[m] -= sum_{c < n} L[row0 + c, m] x[c][.] by one warp (column m of L contiguous)
-__device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, const double (*x)[kMaxRHS],
+__device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, const double (*x)[kSolveBlock],
                                                   double* wm, int64_t F, int nrhs) {
     const int lane = threadIdx.x & 31;
     double acc[kMaxRHS];
@@ -1171,7 +1173,7 @@ __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, 
         const double l = cm_row0[c];
 #pragma unroll
         for (int r = 0; r < kMaxRHS; ++r)
-            if (r < nrhs) acc[r] += l * x[c][r];
+            if (r < nrhs) acc[r] += l * x[r][c];
     }
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) {
@@ -1184,7 +1186,7 @@ __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, 
 
 __global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
                                                      const double* xsol, int nrhs) {
-    __shared__ double x[kSolveBlock][kMaxRHS];
+    __shared__ double x[kMaxRHS][kSolveBlock];      // RHS-major: lanes read consecutive rows
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
@@ -1194,7 +1196,7 @@ __global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t nj
     const double* base = P.lnz + P.lnz_off[js];
     for (int e = threadIdx.x; e < nbk * nrhs; e += blockDim.x) {
         const int i = e % nbk, r = e / nbk;
-        x[i][r] = xsol[vb + (int64_t)r * F + k0 + i];
+        x[r][i] = xsol[vb + (int64_t)r * F + k0 + i];
     }
     __syncthreads();
     const int m = (int)(task - jb.task0) * kBwdCols + (threadIdx.x >> 5);
@@ -1339,7 +1341,7 @@ __global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njo
 // x_block = X' w_block: 32 columns per CTA, 4 per warp, lanes over rows
 __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
                                                     double* xsol, int nrhs) {
-    __shared__ double wb[kSolveBlock][kMaxRHS];
+    __shared__ double wb[kMaxRHS][kSolveBlock];     // RHS-major: lanes read consecutive rows
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -1350,7 +1352,7 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int i = e % nb, r = e / nb;
-        wb[i][r] = w[(int64_t)r * F + k0 + i];
+        wb[r][i] = w[(int64_t)r * F + k0 + i];
     }
     __syncthreads();
     for (int cc = 0; cc < 4; ++cc) {
@@ -1363,7 +1365,7 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
             const double x = X[(int64_t)m + (int64_t)c * nb];
 #pragma unroll
             for (int r = 0; r < kMaxRHS; ++r)
-                if (r < nrhs) acc[r] += x * wb[m][r];
+                if (r < nrhs) acc[r] += x * wb[r][m];
         }
 #pragma unroll
         for (int r = 0; r < kMaxRHS; ++r) {
@@ -1401,7 +1403,8 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
     const int hc = (nbk + 1) / 2;
-    if (i < F) {
+    const int r_end = jb.r_end;
+    if (i < r_end) {
         const int c0 = half * hc, c1 = min(nbk, c0 + hc);
 #pragma unroll 8
         for (int c = c0; c < c1; ++c) {
@@ -1417,8 +1420,70 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
         for (int r = 0; r < kMaxRHS; ++r)
             if (r < nrhs) part[row][r] = acc[r];
     __syncthreads();
-    if (half == 0 && i < F)
+    if (half == 0 && i < r_end)
         for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= acc[r] + part[row][r];
+}
+
+// forward sweep, rows [S, F): w[i] -= sum_{c < S} L[i][c] y[c].  Phase 1: one
+// CTA per (kRectRows rows, kRectCols columns) tile, a thread per row, writes
+// the tile's partial sums; phase 2 (k_fwd_rect_sum) adds the column tiles'
+// partials of each row in a fixed order (deterministic).
+template <int NR>
+__global__ void __launch_bounds__(256) k_fwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+                                                       const double* ysol, double* pbuf, int nrhs) {
+    __shared__ double ys[kRectCols][kMaxRHS];
+    const int64_t task = blockIdx.x;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    const int F = P.F[js], S = P.S[js];
+    const int ncc = jb.k_hi;
+    const int64_t u = task - jb.task0;
+    const int cc = (int)(u % ncc), rc = (int)(u / ncc);
+    const int64_t vb = P.rbase[js] * nrhs;
+    const int tid = threadIdx.x;
+    const int rbeg = S + rc * kRectRows, nr = min(kRectRows, F - rbeg);
+    const int cbeg = cc * kRectCols, ncol = min(kRectCols, S - cbeg);
+    for (int e = tid; e < ncol * nrhs; e += blockDim.x) {
+        const int c = e % ncol, r = e / ncol;
+        ys[c][r] = ysol[vb + (int64_t)r * F + cbeg + c];
+    }
+    __syncthreads();
+    if (tid >= nr) return;
+    const int i = rbeg + tid;
+    const double* base = P.lnz + P.lnz_off[js];
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+#pragma unroll 16
+    for (int c = 0; c < ncol; ++c) {
+        const int col = cbeg + c;
+        const double l = __ldcs(base + lnz_col(col, F) - col + i);
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) acc[r] += l * ys[c][r];
+    }
+    double* part = pbuf + (P.fwd_off[js] + (int64_t)cc * (F - S) + (i - S)) * kMaxRHS;
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+        if (r < nrhs) part[r] = acc[r];
+}
+
+__global__ void k_fwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
+                               const double* pbuf, int nrhs) {
+    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (task >= ntasks) return;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    const int F = P.F[js], S = P.S[js];
+    const int row = S + (int)(task - jb.task0);
+    const int ncc = (S + kRectCols - 1) / kRectCols;
+    double* w = vbuf + P.rbase[js] * nrhs;
+    const double* part = pbuf + P.fwd_off[js] * kMaxRHS;
+    for (int r = 0; r < nrhs; ++r) {
+        double v = 0.0;
+        for (int k = 0; k < ncc; ++k) v += part[((int64_t)k * (F - S) + (row - S)) * kMaxRHS + r];
+        w[(int64_t)r * F + row] -= v;
+    }
 }
 
 // back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F].  Phase 1: one
@@ -1427,9 +1492,10 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
 // per column at a time, 32 columns per warp); phase 2 (k_bwd_rect_sum) adds
 // the partials of each column in a fixed order, so the result is
 // deterministic.
+template <int NR>
 __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
                                                        const double* vbuf, double* pbuf, int nrhs) {
-    __shared__ double ws[kRectRows][kMaxRHS];
+    __shared__ double ws[kMaxRHS][kRectRows];
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
@@ -1444,31 +1510,50 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     const int rbeg = S + rc * kRectRows, nr = min(kRectRows, F - rbeg);
     for (int e = tid; e < nr * nrhs; e += blockDim.x) {
         const int i = e % nr, r = e / nr;
-        ws[i][r] = w[(int64_t)r * F + rbeg + i];
+        ws[r][i] = w[(int64_t)r * F + rbeg + i];
     }
     __syncthreads();
     double* part = pbuf + (P.rect_off[js] + (int64_t)rc * S) * kMaxRHS;
     const int cw = kRectCols / 8;
-    for (int a = 0; a < cw; ++a) {
-        const int c = cc * kRectCols + warp * cw + a;
-        if (c >= S) break;
-        const double* col = base + lnz_col(c, F) - c + rbeg;
-        double acc[kMaxRHS];
+    // four columns at a time per warp: 4 x 8 loads in flight per lane
+    for (int a = 0; a < cw; a += 4) {
+        const int c0 = cc * kRectCols + warp * cw + a;
+        if (c0 >= S) break;
+        const double* col[4];
+        bool cv[4];
 #pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) acc[r] = 0.0;
+        for (int q = 0; q < 4; ++q) {
+            cv[q] = c0 + q < S;
+            const int c = cv[q] ? c0 + q : c0;
+            col[q] = base + lnz_col(c, F) - c + rbeg;
+        }
+        double acc[4][NR];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[q][r] = 0.0;
+#pragma unroll 2
         for (int i = lane; i < nr; i += 32) {
-            const double l = col[i];
+            double l[4];
 #pragma unroll
-            for (int r = 0; r < kMaxRHS; ++r)
-                if (r < nrhs) acc[r] += l * ws[i][r];
+            for (int q = 0; q < 4; ++q) l[q] = __ldcs(col[q] + i);
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) {
+                    const double x = ws[r][i];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q][r] += l[q] * x;
+                }
         }
 #pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) {
-            if (r >= nrhs) break;
-            double v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) part[(int64_t)c * kMaxRHS + r] = v;
-        }
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                if (r >= nrhs) break;
+                double v = acc[q][r];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && cv[q]) part[(int64_t)(c0 + q) * kMaxRHS + r] = v;
+            }
     }
 }
 
@@ -1700,9 +1785,11 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         dev_upload(o, &D.cptr, P_.cptr) || dev_upload(o, &D.buf_off, P_.buf_off) ||
         dev_upload(o, &D.upd_off, P_.upd_off) || dev_upload(o, &D.jobs, P_.jobs) ||
         dev_upload(o, &D.linv_off, P_.linv_off) || dev_upload(o, &D.xinv_off, P_.xinv_off) ||
-        dev_upload(o, &D.rect_off, P_.rect_off) || dev_upload(o, &D.task_map, P_.task_map))
+        dev_upload(o, &D.rect_off, P_.rect_off) || dev_upload(o, &D.fwd_off, P_.fwd_off) ||
+        dev_upload(o, &D.task_map, P_.task_map))
         return -4;
-    CK(cudaMalloc((void**)&D.pbuf, std::max<int64_t>(P_.rect_entries, 1) * kMaxRHS * sizeof(double)));
+    CK(cudaMalloc((void**)&D.pbuf,
+                  std::max<int64_t>(std::max(P_.rect_entries, P_.fwd_entries), 1) * kMaxRHS * sizeof(double)));
     o.push_back(D.pbuf);
     CK(cudaMalloc((void**)&D.xinv, std::max<int64_t>(P_.xinv_doubles, 1) * sizeof(double)));
     o.push_back(D.xinv);
@@ -1828,6 +1915,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.xinv_off = D.xinv_off;
     v.xinv = D.xinv;
     v.rect_off = D.rect_off;
+    v.fwd_off = D.fwd_off;
     v.tol1 = tol1;
     return v;
 }
@@ -1979,7 +2067,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
         timing.gemm_ms += ms;
     }
     for (cudaEvent_t e : gev) cudaEventDestroy(e);
-    for (float& x : timing.phase_ms) x = 0.f;
+    for (int k = 0; k < 9; ++k) timing.phase_ms[k] = 0.f;
     for (size_t k = 0; k < marks_.size(); ++k) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, marks_[k].second, k + 1 < marks_.size() ? marks_[k + 1].second : D.ev1);
@@ -2054,6 +2142,9 @@ void Engine::ensure_vectors(int64_t nrhs) {
 void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ldb, int64_t nrhs, int which,
                            int64_t& nl) {
     Dev& D = *d_;
+    auto mark = [&](int phase) {
+        if (profile_) marks_.emplace_back(9 + phase, record_event(s));
+    };
     const int64_t chunk = std::min<int64_t>(nrhs, kMaxRHS);
     for (int64_t r0 = 0; r0 < nrhs; r0 += chunk) {
         const int nr = (int)std::min<int64_t>(chunk, nrhs - r0);
@@ -2064,17 +2155,20 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
             for (size_t L = 0; L < P_.levels.size(); ++L) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
+                    mark(0);
                     k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(D.level_nodes + D.small_begin[L],
                                                                                 pv, D.vbuf, b, ldb, nr);
                     ++nl;
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
+                mark(1);
                 k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, TMAP(ga), ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
                     const Launch& ml = lp.blk_mv[sb];
+                    mark(2);
                     k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
@@ -2085,7 +2179,22 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                         ++nl;
                     }
                 }
+                const Launch& rl = lp.rect;
+                if (rl.ntasks > 0) {
+                    mark(3);
+                    if (nr <= 4)
+                        k_fwd_rect_part<4><<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, TMAP(rl),
+                                                                          pv, D.vbuf2, D.pbuf, nr);
+                    else
+                        k_fwd_rect_part<kMaxRHS><<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count,
+                                                                                TMAP(rl), pv, D.vbuf2, D.pbuf, nr);
+                    const Launch& rr = lp.rect_rows;
+                    k_fwd_rect_sum<<<blocks(rr.ntasks), 256, 0, s>>>(jobs + rr.job_begin, rr.job_count, TMAP(rr),
+                                                                      rr.ntasks, pv, D.vbuf, D.pbuf, nr);
+                    nl += 2;
+                }
                 const Launch& wb = lp.writeback;
+                mark(4);
                 k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
                 ++nl;
@@ -2095,20 +2204,27 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
             for (size_t L = P_.levels.size(); L-- > 0;) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
+                    mark(5);
                     k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(
                         D.level_nodes + D.small_begin[L], pv, D.vbuf, b, ldb, nr);
                     ++nl;
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
+                mark(6);
                 k_bwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, TMAP(ga), ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 const Launch& wb = lp.writeback;
                 const Launch& rl = lp.rect;
                 if (rl.ntasks > 0) {
-                    k_bwd_rect_part<<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, TMAP(rl), pv, D.vbuf,
-                                                                    D.pbuf, nr);
+                    mark(7);
+                    if (nr <= 4)
+                        k_bwd_rect_part<4><<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count, TMAP(rl),
+                                                                          pv, D.vbuf, D.pbuf, nr);
+                    else
+                        k_bwd_rect_part<kMaxRHS><<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count,
+                                                                                TMAP(rl), pv, D.vbuf, D.pbuf, nr);
                     ++nl;
                     k_bwd_rect_sum<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                       D.vbuf, D.pbuf, nr);
@@ -2116,16 +2232,19 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 }
                 for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
                     const Launch& ml = lp.blk_mv[sb];
+                    mark(8);
                     k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
                     const Launch& bl = lp.bs_upd[sb];
                     if (bl.ntasks > 0) {
+                        mark(9);
                         k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, TMAP(bl), pv, D.vbuf,
                                                                      D.vbuf2, nr);
                         ++nl;
                     }
                 }
+                mark(10);
                 k_bwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                D.vbuf2, b, ldb, nr);
                 ++nl;
@@ -2158,7 +2277,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
         }
         linv_valid_ = true;
     }
-    if (use_graphs_ && s != nullptr) {
+    if (use_graphs_ && !profile_ && s != nullptr) {
         const GraphKey key{(const void*)d_sm, (const void*)d_b, (double)ldb, nrhs, which, (int64_t)(uintptr_t)D.vbuf};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
@@ -2181,6 +2300,16 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     CK(cudaStreamSynchronize(s));
     CK(cudaEventElapsedTime(&timing.solve_ms, D.ev0, D.ev1));
     timing.solve_launches = nl;
+    if (profile_) {
+        for (int k = 9; k < 20; ++k) timing.phase_ms[k] = 0.f;
+        for (size_t k = 0; k < marks_.size(); ++k) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, marks_[k].second, k + 1 < marks_.size() ? marks_[k + 1].second : D.ev1);
+            timing.phase_ms[marks_[k].first] += ms;
+            cudaEventDestroy(marks_[k].second);
+        }
+        marks_.clear();
+    }
     return 0;
 }
 

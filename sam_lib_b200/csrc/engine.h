@@ -27,8 +27,12 @@ struct Timing {              // CUDA-event times of the last calls (ms)
     int64_t gemm_launches = 0, launches = 0, solve_launches = 0;
     // profile mode: factor time by phase (CUDA events between launch groups):
     // 0 pre-pass, 1 small fronts, 2 extend-add, 3 diagonal blocks, 4 panel
-    // TRSM, 5 in-panel/trailing updates, 6 K = S update, 7 write-back, 8 end
-    float phase_ms[9] = {};
+    // TRSM, 5 in-panel/trailing updates, 6 K = S update, 7 write-back, 8 end;
+    // solve: 9 small-front forward, 10 forward gather, 11 forward blocks
+    // (block products and in-block updates), 12 forward rectangles, 13 forward finish, 14 small-front
+    // back, 15 back gather, 16 back rectangles, 17 back block products,
+    // 18 back in-block updates, 19 back finish
+    float phase_ms[20] = {};
 };
 
 class Engine {

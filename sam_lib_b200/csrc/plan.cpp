@@ -240,6 +240,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     P.jobs.clear();
     P.rect_off.assign(ns, 0);
     P.rect_entries = 0;
+    P.fwd_off.assign(ns, 0);
+    P.fwd_entries = 0;
     auto open_launch = [&](Launch& l) { l.job_begin = (int64_t)P.jobs.size(); l.ntasks = 0; };
     auto add_job = [&](Launch& l, Job j, int64_t ntask, bool keep_empty = false) {
         if (ntask <= 0 && !keep_empty) return;
@@ -394,7 +396,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t k1 = std::min(k0 + kSolveBlock, s);
-                add_job(lp.fs_upd[sb], Job{js, k1, k1, f, k0, k1, 0}, (f - k1 + kSolveRows - 1) / kSolveRows, true);
+                // rows [k1, S) of the diagonal part; rows [S, F) go to the rectangle launch
+                add_job(lp.fs_upd[sb], Job{js, k1, k1, s, k0, k1, 0}, (s - k1 + kSolveRows - 1) / kSolveRows, true);
             }
             close_launch(lp.fs_upd[sb]);
             open_launch(lp.bs_upd[sb]);
@@ -407,7 +410,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             close_launch(lp.bs_upd[sb]);
         }
         open_launch(lp.rect);
-        int64_t roff = 0;
+        int64_t roff = 0, foff = 0;
         for (int32_t js : lp.large_nodes) {
             const int32_t s = P.S[js], f = P.F[js];
             if (f <= s) continue;
@@ -415,10 +418,19 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             const int64_t ncc = (s + kRectCols - 1) / kRectCols;
             P.rect_off[js] = roff;
             roff += nrc * s;
+            P.fwd_off[js] = foff;
+            foff += ncc * (f - s);
             add_job(lp.rect, Job{js, 0, s, f, (int32_t)nrc, (int32_t)ncc, 0}, nrc * ncc);
         }
         P.rect_entries = std::max(P.rect_entries, roff);
+        P.fwd_entries = std::max(P.fwd_entries, foff);
         close_launch(lp.rect);
+        open_launch(lp.rect_rows);
+        for (int32_t js : lp.large_nodes) {
+            const int32_t s = P.S[js], f = P.F[js];
+            if (f > s) add_job(lp.rect_rows, Job{js, s, f, f, 0, 0, 0}, f - s);
+        }
+        close_launch(lp.rect_rows);
         {
             std::vector<Job> jl;
             for (int32_t js : lp.large_nodes) {
@@ -452,6 +464,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         build_map(lp.assemble);
         build_map(lp.writeback);
         build_map(lp.rect);
+        build_map(lp.rect_rows);
         for (Launch& l : lp.panel) build_map(l);
         for (auto& v : lp.update)
             for (Launch& l : v) build_map(l);

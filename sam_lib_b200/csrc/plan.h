@@ -80,7 +80,8 @@ struct LevelPlan {
     std::vector<Launch> fs_upd;               // rows [k1, F) below the block, kSolveRows per task
     std::vector<Launch> bs_upd;               // columns [0, k0) before the block, kBwdCols per task
     std::vector<Launch> blk_mv;               // product with the block inverse, 32 rows/columns per task
-    Launch rect;                              // back solve, rows [S, F): 32 columns per task
+    Launch rect;                              // rectangle rows [S, F): one task per 256 x 256 tile
+    Launch rect_rows;                         // forward solve, rows [S, F): one task per row
     std::vector<std::vector<TcLaunch>> update_tc;   // mixed precision: the updates of each step
     std::vector<TcLaunch> outer_tc;                 // mixed precision: the K = S update
 };
@@ -125,6 +126,8 @@ struct Plan {
     // (each kMaxRHS doubles) of a scratch of rect_entries entries (max over levels)
     std::vector<int64_t> rect_off;
     int64_t rect_entries = 0;
+    std::vector<int64_t> fwd_off;            // forward-sweep rectangle partials, per level
+    int64_t fwd_entries = 0;
     bool any_large = false;
     // levels and tasks
     std::vector<LevelPlan> levels;
