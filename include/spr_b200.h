@@ -96,9 +96,8 @@ int spr_b200_refine(void* handle, const double* d_sm, const double* d_b, double*
 /* Profile mode only: last factorisation's time by phase, out[0..8] = pre-pass,
  * small fronts, extend-add, diagonal blocks, panel TRSM, in-panel/trailing
  * updates, K = S update, write-back, end; last solve's, out[9..19] =
- * forward: small fronts, gather, block products, rectangle updates, finish;
- * back: small fronts, gather, rectangles, block products, in-block updates,
- * finish (ms).  out holds 20 doubles. */
+ * forward: small fronts, gather, blocks, rectangles, finish;
+ * back: small fronts, gather, rectangles, blocks, (unused), finish (ms).  out holds 20 doubles. */
 int spr_b200_phase_ms(void* handle, double* out);
 /* Profile mode: CUDA events around every Schur-update launch. */
 int spr_b200_set_profile(void* handle, int on);

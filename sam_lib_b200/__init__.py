@@ -216,7 +216,7 @@ class DeviceSolver:
         self.lib.spr_b200_phase_ms(self.h, _ptr(out))
         keys = ('prepass', 'small_fronts', 'extend_add', 'diag', 'trsm', 'updates', 'outer_update',
                 'writeback', 'end', 'fwd_small', 'fwd_gather', 'fwd_blocks', 'fwd_rect', 'fwd_finish',
-                'bwd_small', 'bwd_gather', 'bwd_rect', 'bwd_blk_mv', 'bwd_blk_upd', 'bwd_finish')
+                'bwd_small', 'bwd_gather', 'bwd_rect', 'bwd_blocks', 'unused', 'bwd_finish')
         return dict(zip(keys, out.tolist()))
 
     def set_profile(self, on=True):

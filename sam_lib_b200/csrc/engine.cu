@@ -1180,14 +1180,15 @@ __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, 
         if (r >= nrhs) break;
         double v = acc[r];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) wm[(int64_t)r * F] -= v;
+        if (lane == 0) wm[(int64_t)r * F] = __ldcg(wm + (int64_t)r * F) - v;
     }
 }
 
-__global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
-                                                     const double* xsol, int nrhs) {
-    __shared__ double x[kMaxRHS][kSolveBlock];      // RHS-major: lanes read consecutive rows
-    const int64_t task = blockIdx.x;
+// In-block update of the back sweep: w[m] -= L[k0:k1, m]' x_block for the
+// columns m in [0, k0) of the block's front (kBwdCols columns per task).
+__device__ void bwd_blk_upd_task(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t task, const PV& P,
+                                 double* vbuf, const double* xsol, int nrhs, double* sh) {
+    double(*x)[kSolveBlock] = reinterpret_cast<double(*)[kSolveBlock]>(sh);     // RHS-major
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
     const int F = P.F[js], nbk = k1 - k0;
@@ -1196,12 +1197,20 @@ __global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t nj
     const double* base = P.lnz + P.lnz_off[js];
     for (int e = threadIdx.x; e < nbk * nrhs; e += blockDim.x) {
         const int i = e % nbk, r = e / nbk;
-        x[r][i] = xsol[vb + (int64_t)r * F + k0 + i];
+        x[r][i] = __ldcg(xsol + vb + (int64_t)r * F + k0 + i);
     }
     __syncthreads();
     const int m = (int)(task - jb.task0) * kBwdCols + (threadIdx.x >> 5);
     if (m >= jb.c_end) return;
     warp_col_dot_smem(base + lnz_col(m, F) - m + k0, nbk, x, w + m, F, nrhs);
+}
+
+constexpr size_t kBwdSmem = sizeof(double) * (size_t)kMaxRHS * kSolveBlock;
+
+__global__ void __launch_bounds__(256) k_bwd_blk_upd(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, double* vbuf,
+                                                     const double* xsol, int nrhs) {
+    extern __shared__ double bsh[];
+    bwd_blk_upd_task(jobs, njobs, tmap, blockIdx.x, P, vbuf, xsol, nrhs, bsh);
 }
 
 // Inverse X = L_blk^-1 of one kSolveBlock-wide unit-lower diagonal block of a
@@ -1295,12 +1304,10 @@ __global__ void __launch_bounds__(256) k_inv_block(const Job* jobs, PV P) {
 constexpr size_t kMvSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + 8 * 32 * (kMaxRHS + 1));
 constexpr size_t kUpdSmem = sizeof(double) * ((size_t)kSolveBlock * kMaxRHS + (size_t)128 * (kMaxRHS + 1));
 
-__global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
-                                                    double* ysol, int nrhs) {
-    extern __shared__ double msh[];
+__device__ void fwd_blk_mv_task(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t task, const PV& P,
+                                const double* vbuf, double* ysol, int nrhs, double* msh) {
     double(*wb)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(msh);
     double(*part)[32][kMaxRHS + 1] = reinterpret_cast<double(*)[32][kMaxRHS + 1]>(msh + kSolveBlock * kMaxRHS);
-    const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
@@ -1310,7 +1317,7 @@ __global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njo
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int i = e % nb, r = e / nb;
-        wb[i][r] = w[(int64_t)r * F + k0 + i];
+        wb[i][r] = __ldcg(w + (int64_t)r * F + k0 + i);
     }
     __syncthreads();
     const int i = (int)(task - jb.task0) * 32 + lane;
@@ -1338,11 +1345,16 @@ __global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njo
         }
 }
 
+__global__ void __launch_bounds__(256) k_fwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
+                                                    double* ysol, int nrhs) {
+    extern __shared__ double msh[];
+    fwd_blk_mv_task(jobs, njobs, tmap, blockIdx.x, P, vbuf, ysol, nrhs, msh);
+}
+
 // x_block = X' w_block: 32 columns per CTA, 4 per warp, lanes over rows
-__global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
-                                                    double* xsol, int nrhs) {
-    __shared__ double wb[kMaxRHS][kSolveBlock];     // RHS-major: lanes read consecutive rows
-    const int64_t task = blockIdx.x;
+__device__ void bwd_blk_mv_task(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t task, const PV& P,
+                                const double* vbuf, double* xsol, int nrhs, double* sh) {
+    double(*wb)[kSolveBlock] = reinterpret_cast<double(*)[kSolveBlock]>(sh);     // RHS-major
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
     const int F = P.F[js];
@@ -1352,7 +1364,7 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nb * nrhs; e += blockDim.x) {
         const int i = e % nb, r = e / nb;
-        wb[r][i] = w[(int64_t)r * F + k0 + i];
+        wb[r][i] = __ldcg(w + (int64_t)r * F + k0 + i);
     }
     __syncthreads();
     for (int cc = 0; cc < 4; ++cc) {
@@ -1377,14 +1389,18 @@ __global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njo
     }
 }
 
+__global__ void __launch_bounds__(256) k_bwd_blk_mv(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P, const double* vbuf,
+                                                    double* xsol, int nrhs) {
+    extern __shared__ double bsh[];
+    bwd_blk_mv_task(jobs, njobs, tmap, blockIdx.x, P, vbuf, xsol, nrhs, bsh);
+}
+
 // rows below a solve block: w[i] -= L[i, k0:k1] y; 128 rows per CTA, the two
 // halves of the 256 columns summed through shared memory
-__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
-                                                      double* vbuf, const double* ysol, int nrhs) {
-    extern __shared__ double ush[];
+__device__ void fwd_blk_upd2_task(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t task, const PV& P,
+                                  double* vbuf, const double* ysol, int nrhs, double* ush) {
     double(*y)[kMaxRHS] = reinterpret_cast<double(*)[kMaxRHS]>(ush);
     double(*part)[kMaxRHS + 1] = reinterpret_cast<double(*)[kMaxRHS + 1]>(ush + kSolveBlock * kMaxRHS);
-    const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, k1 = jb.k_hi;
     const int F = P.F[js], nbk = k1 - k0;
@@ -1394,7 +1410,7 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
     const int tid = threadIdx.x;
     for (int e = tid; e < nbk * nrhs; e += blockDim.x) {
         const int i = e % nbk, r = e / nbk;
-        y[i][r] = ysol[vb + (int64_t)r * F + k0 + i];
+        y[i][r] = __ldcg(ysol + vb + (int64_t)r * F + k0 + i);
     }
     __syncthreads();
     const int row = tid & (kSolveRows - 1), half = tid / kSolveRows;
@@ -1421,8 +1437,17 @@ __global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t n
             if (r < nrhs) part[row][r] = acc[r];
     __syncthreads();
     if (half == 0 && i < r_end)
-        for (int r = 0; r < nrhs; ++r) w[(int64_t)r * F + i] -= acc[r] + part[row][r];
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) w[(int64_t)r * F + i] = __ldcg(w + (int64_t)r * F + i) - (acc[r] + part[row][r]);
 }
+
+__global__ void __launch_bounds__(256) k_fwd_blk_upd2(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+                                                      double* vbuf, const double* ysol, int nrhs) {
+    extern __shared__ double ush[];
+    fwd_blk_upd2_task(jobs, njobs, tmap, blockIdx.x, P, vbuf, ysol, nrhs, ush);
+}
+
 
 // forward sweep, rows [S, F): w[i] -= sum_{c < S} L[i][c] y[c].  Phase 1: one
 // CTA per (kRectRows rows, kRectCols columns) tile, a thread per row, writes
@@ -2166,9 +2191,9 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 k_fwd_gather<<<blocks(ga.ntasks), 256, 0, s>>>(jobs + ga.job_begin, ga.job_count, TMAP(ga), ga.ntasks, pv,
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
+                mark(2);
                 for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
                     const Launch& ml = lp.blk_mv[sb];
-                    mark(2);
                     k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
@@ -2230,16 +2255,15 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                                                                       D.vbuf, D.pbuf, nr);
                     ++nl;
                 }
+                mark(8);
                 for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
                     const Launch& ml = lp.blk_mv[sb];
-                    mark(8);
-                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, 0, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
+                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, kBwdSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
                                                                  D.vbuf2, nr);
                     ++nl;
                     const Launch& bl = lp.bs_upd[sb];
                     if (bl.ntasks > 0) {
-                        mark(9);
-                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, 0, s>>>(jobs + bl.job_begin, bl.job_count, TMAP(bl), pv, D.vbuf,
+                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, kBwdSmem, s>>>(jobs + bl.job_begin, bl.job_count, TMAP(bl), pv, D.vbuf,
                                                                      D.vbuf2, nr);
                         ++nl;
                     }

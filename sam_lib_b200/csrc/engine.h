@@ -30,8 +30,8 @@ struct Timing {              // CUDA-event times of the last calls (ms)
     // TRSM, 5 in-panel/trailing updates, 6 K = S update, 7 write-back, 8 end;
     // solve: 9 small-front forward, 10 forward gather, 11 forward blocks
     // (block products and in-block updates), 12 forward rectangles, 13 forward finish, 14 small-front
-    // back, 15 back gather, 16 back rectangles, 17 back block products,
-    // 18 back in-block updates, 19 back finish
+    // back, 15 back gather, 16 back rectangles, 17 back blocks (block
+    // products and in-block updates), 18 unused, 19 back finish
     float phase_ms[20] = {};
 };
 
