@@ -49,7 +49,7 @@ def parse():
     ap.add_argument('--n', type=int, default=N_MESH)
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
-    ap.add_argument('--case', choices=['fp64', 'mixed'], default=None,
+    ap.add_argument('--case', choices=['fp64', 'mixed', 'batched'], default=None,
                     help='profiling case: only WARMUP+STEPS factorisations of the n^3 box in that mode')
     ap.add_argument('--phases', action='store_true',
                     help='with --case: CUDA events between launch groups, time by phase')
@@ -530,14 +530,21 @@ def run_case(args):
     committed ncu summaries were captured with."""
     import torch
     import sam_lib_b200 as spr
-    from sam_lib_b200.system import HexSystem
-    hs = HexSystem(args.n)
-    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    if args.case == 'batched':
+        from sam_lib_b200.batch import BatchSolver
+        from sam_lib_b200.workloads import config4
+        bs = BatchSolver(config4())
+        ds, d_sm0, nrhs, neq = bs.ds, bs.sm0, bs.nrhs, bs.forest.neq
+    else:
+        from sam_lib_b200.system import HexSystem
+        hs = HexSystem(args.n)
+        ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+        d_sm0 = torch.from_numpy(hs.assemble()).cuda()
+        nrhs, neq = NRHS, hs.neq
     st = torch.cuda.Stream()
     ds.set_stream(st.cuda_stream)
     ds.set_mode(1 if args.case == 'mixed' else 0)
     ds.set_profile(args.phases)
-    d_sm0 = torch.from_numpy(hs.assemble()).cuda()
     d_sm = torch.empty_like(d_sm0)
     ms = []
     for k in range(args.warmup + args.steps):
@@ -550,8 +557,8 @@ def run_case(args):
             ms.append(ds.info()['factor_ms'])
     line = {'case': args.case, 'n': args.n, 'factor_ms': ms}
     if args.phases:
-        b = torch.from_numpy(np.random.default_rng(1).uniform(-1.0, 1.0, size=(NRHS, hs.neq))).cuda()
-        ds.solve(d_sm, b, NRHS)
+        b = torch.from_numpy(np.random.default_rng(1).uniform(-1.0, 1.0, size=(nrhs, neq))).cuda()
+        ds.solve(d_sm, b, nrhs)
         line['solve_ms'] = ds.info()['solve_ms']
     if args.phases:
         line['phase_ms'] = ds.phase_ms()

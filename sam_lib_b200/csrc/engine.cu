@@ -1163,6 +1163,31 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap
 // row below the block (thread per row, SPRFS6).  Backward mirrors it.
 
 // w[m] -= sum_{c < n} L[row0 + c, m] x[c][.] by one warp (column m of L contiguous)
+// Reduce-scatter of NR per-lane partial sums over a warp: halving exchanges
+// (NR/2 + NR/4 + ... shuffles) then full sums over the remaining lane bits.
+// Returns the total of partial index `rhs`; the lanes whose remaining bits
+// are zero (lane & (first_rem * 2 - 1)) == 0 hold distinct totals.
+template <int NR>
+__device__ __forceinline__ double warp_reduce_scatter(double (&v)[NR], int lane, int& rhs, int& owner_mask) {
+    int base = 0, o = 16;
+#pragma unroll
+    for (int h = NR / 2; h >= 1; h >>= 1, o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int j = 0; j < h; ++j) {
+            const double send = up ? v[j] : v[j + h];
+            const double keep = up ? v[j + h] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+        if (up) base += h;
+    }
+    owner_mask = 2 * o - 1;
+#pragma unroll
+    for (; o >= 1; o >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    rhs = base;
+    return v[0];
+}
+
 __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, const double (*x)[kSolveBlock],
                                                   double* wm, int64_t F, int nrhs) {
     const int lane = threadIdx.x & 31;
@@ -1175,13 +1200,9 @@ __device__ __forceinline__ void warp_col_dot_smem(const double* cm_row0, int n, 
         for (int r = 0; r < kMaxRHS; ++r)
             if (r < nrhs) acc[r] += l * x[r][c];
     }
-#pragma unroll
-    for (int r = 0; r < kMaxRHS; ++r) {
-        if (r >= nrhs) break;
-        double v = acc[r];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) wm[(int64_t)r * F] = __ldcg(wm + (int64_t)r * F) - v;
-    }
+    int r, om;
+    const double v = warp_reduce_scatter<kMaxRHS>(acc, lane, r, om);
+    if ((lane & om) == 0 && r < nrhs) wm[(int64_t)r * F] = __ldcg(wm + (int64_t)r * F) - v;
 }
 
 // In-block update of the back sweep: w[m] -= L[k0:k1, m]' x_block for the
@@ -1379,13 +1400,9 @@ __device__ void bwd_blk_mv_task(const Job* jobs, int64_t njobs, const int32_t* t
             for (int r = 0; r < kMaxRHS; ++r)
                 if (r < nrhs) acc[r] += x * wb[r][m];
         }
-#pragma unroll
-        for (int r = 0; r < kMaxRHS; ++r) {
-            if (r >= nrhs) break;
-            double v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) xsol[vb + (int64_t)r * F + k0 + c] = v;
-        }
+        int r, om;
+        const double v = warp_reduce_scatter<kMaxRHS>(acc, lane, r, om);
+        if ((lane & om) == 0 && r < nrhs) xsol[vb + (int64_t)r * F + k0 + c] = v;
     }
 }
 
@@ -1540,45 +1557,43 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     __syncthreads();
     double* part = pbuf + (P.rect_off[js] + (int64_t)rc * S) * kMaxRHS;
     const int cw = kRectCols / 8;
-    // four columns at a time per warp: 4 x 8 loads in flight per lane
-    for (int a = 0; a < cw; a += 4) {
+    // CG columns at a time per warp (CG x 8 loads in flight per lane)
+    constexpr int CG = NR <= 4 ? 4 : 2;
+    for (int a = 0; a < cw; a += CG) {
         const int c0 = cc * kRectCols + warp * cw + a;
         if (c0 >= S) break;
-        const double* col[4];
-        bool cv[4];
+        const double* col[CG];
+        bool cv[CG];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < CG; ++q) {
             cv[q] = c0 + q < S;
             const int c = cv[q] ? c0 + q : c0;
             col[q] = base + lnz_col(c, F) - c + rbeg;
         }
-        double acc[4][NR];
+        double acc[CG][NR];
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < CG; ++q)
 #pragma unroll
             for (int r = 0; r < NR; ++r) acc[q][r] = 0.0;
 #pragma unroll 2
         for (int i = lane; i < nr; i += 32) {
-            double l[4];
+            double l[CG];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) l[q] = __ldcs(col[q] + i);
+            for (int q = 0; q < CG; ++q) l[q] = __ldcs(col[q] + i);
 #pragma unroll
             for (int r = 0; r < NR; ++r)
                 if (r < nrhs) {
                     const double x = ws[r][i];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[q][r] += l[q] * x;
+                    for (int q = 0; q < CG; ++q) acc[q][r] += l[q] * x;
                 }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                if (r >= nrhs) break;
-                double v = acc[q][r];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && cv[q]) part[(int64_t)(c0 + q) * kMaxRHS + r] = v;
-            }
+        for (int q = 0; q < CG; ++q) {
+            int r, om;
+            const double v = warp_reduce_scatter<NR>(acc[q], lane, r, om);
+            if ((lane & om) == 0 && cv[q] && r < nrhs) part[(int64_t)(c0 + q) * kMaxRHS + r] = v;
+        }
     }
 }
 
