@@ -116,6 +116,10 @@ struct Engine::Dev {
     // tensor-core (mixed) updates: operand slabs and the TMA map over them
     float* slab = nullptr;
     alignas(64) CUtensorMap slab_map;
+    float* slab_far = nullptr;                   // slabs of the side-stream launches
+    alignas(64) CUtensorMap slab_map_far;
+    cudaStream_t side = nullptr;                 // side stream: trailing updates beyond the next super-panel
+    std::vector<cudaEvent_t> evpool;             // fork/join events of one factorisation
 };
 
 template <typename T>
@@ -1791,6 +1795,10 @@ void Engine::store_graph(const GraphKey& k, cudaGraphExec_t exec, int64_t launch
 
 Engine::~Engine() {
     for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    for (cudaEvent_t e : d_->evpool) cudaEventDestroy(e);
+    if (d_->side) cudaStreamDestroy(d_->side);
+    if (d_->slab) cudaFree(d_->slab);
+    if (d_->slab_far) cudaFree(d_->slab_far);
     if (csr_.rowptr) cudaFree(csr_.rowptr);
     if (csr_.ci) cudaFree(csr_.ci);
     if (csr_.cv) cudaFree(csr_.cv);
@@ -1815,6 +1823,17 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         int dev = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+    }
+    {
+        // side stream and the fork/join events of one factorisation (two per
+        // step that forks a far update)
+        size_t nev = 0;
+        for (const LevelPlan& lp : P_.levels)
+            for (size_t st = 0; st < lp.far.size(); ++st)
+                if (!lp.far[st].empty() || !lp.far_tc[st].empty()) nev += 2;
+        CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+        D.evpool.resize(nev);
+        for (cudaEvent_t& e : D.evpool) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     if (dev_upload(o, &D.fst, P_.fst) || dev_upload(o, &D.S, P_.S) || dev_upload(o, &D.F, P_.F) ||
         dev_upload(o, &D.child_ptr, P_.child_ptr) || dev_upload(o, &D.child, P_.child) ||
@@ -1889,28 +1908,37 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int Engine::ensure_slabs() {
-    Dev& D = *d_;
-    if (D.slab) return 0;
-    const int64_t rows = std::max<int64_t>(P_.slab_rows, tc::kTM);
+static int make_slab(int64_t rows_needed, float** slab, CUtensorMap* map) {
+    const int64_t rows = std::max<int64_t>(rows_needed, tc::kTM);
     if (rows >= (int64_t(1) << 31)) return -3;                 // TMA row coordinates are 32-bit
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
         return -4;
-    CK(cudaMalloc((void**)&D.slab, rows * tc::kBK * sizeof(float)));
+    CK(cudaMalloc((void**)slab, rows * tc::kBK * sizeof(float)));
     const cuuint64_t dims[2] = {(cuuint64_t)tc::kBK, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)tc::kBK * sizeof(float)};
     const cuuint32_t box[2] = {(cuuint32_t)tc::kBK, (cuuint32_t)tc::kTM};
     const cuuint32_t es[2] = {1, 1};
-    const CUresult r = ((EncodeTiledFn)fn)(&D.slab_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, D.slab, dims, strides,
-                                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+    const CUresult r = ((EncodeTiledFn)fn)(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, *slab, dims, strides, box, es,
+                                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
-        cudaFree(D.slab);
-        D.slab = nullptr;
+        cudaFree(*slab);
+        *slab = nullptr;
         return -4;
     }
+    return 0;
+}
+
+int Engine::ensure_slabs() {
+    Dev& D = *d_;
+    if (D.slab && D.slab_far) return 0;
+    if (!D.slab) {
+        const int rc = make_slab(P_.slab_rows, &D.slab, &D.slab_map);
+        if (rc != 0) return rc;
+    }
+    if (!D.slab_far) return make_slab(P_.slab_rows_far, &D.slab_far, &D.slab_map_far);
     return 0;
 }
 
@@ -1975,15 +2003,18 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     ++timing.gemm_launches;
 }
 
-void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev) {
+void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev, bool far) {
     if (t.gemm.ntasks <= 0) return;
     Dev& D = *d_;
     if (profile_) gev.push_back(record_event(s));
     k_split_tc<<<(int)t.split.ntasks, 256, 0, s>>>(D.jobs + t.split.job_begin, t.split.job_count, TMAP(t.split), pv,
-                                                   D.slab);
-    const int grid = (int)std::min<int64_t>(t.gemm.ntasks, sm_count_);
+                                                   far ? D.slab_far : D.slab);
+    // a side-stream launch leaves a quarter of the SMs to the panel chain
+    // (a persistent tensor-core CTA holds most of an SM's shared memory)
+    const int cap = far ? std::max(1, sm_count_ - sm_count_ / 4) : sm_count_;
+    const int grid = (int)std::min<int64_t>(t.gemm.ntasks, cap);
     k_gemm_tc<<<grid, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count, TMAP(t.gemm),
-                                                    t.gemm.ntasks, pv, D.slab_map);
+                                                    t.gemm.ntasks, pv, far ? D.slab_map_far : D.slab_map);
     if (profile_) gev.push_back(record_event(s));
     timing.launches += 2;
     ++timing.gemm_launches;
@@ -1994,6 +2025,17 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
     timing.launches = 0;
     auto mark = [&](int phase) {
         if (profile_) marks_.emplace_back(phase, record_event(s));
+    };
+    // side stream for the trailing-update columns beyond the next super-panel
+    // (profile mode keeps everything on one stream so the events time it)
+    cudaStream_t u = (profile_ || !D.side) ? s : D.side;
+    size_t evi = 0;
+    cudaEvent_t far_done = nullptr;
+    auto join_far = [&]() {
+        if (far_done) {
+            cudaStreamWaitEvent(s, far_done, 0);
+            far_done = nullptr;
+        }
     };
     mark(0);
     k_prepass<<<(int)std::min<int64_t>((P_.nsuper * 32 + 255) / 256, 4736), 256, 0, s>>>(pv, P_.nsuper);
@@ -2028,12 +2070,33 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, TMAP(pl), pv);
                 ++timing.launches;
             }
+            const bool has_far = mixed_ == 1 ? !lp.far_tc[st].empty() : !lp.far[st].empty();
+            if (has_far && u != s) {
+                // the super-panel is final: fork the far columns of its trailing update
+                cudaEvent_t e = D.evpool[evi++];
+                cudaEventRecord(e, s);
+                cudaStreamWaitEvent(u, e, 0);
+            }
             mark(5);
+            // a trailing update's next-super-panel columns were also updated by
+            // the previous super-panel's far launch: wait for it first
+            if ((st + 1) % (kSuperPanel / kNB) == 0) join_far();
             if (mixed_ == 1)
                 for (const TcLaunch& t : lp.update_tc[st]) launch_tc(t, s, pv, gev);
             else
                 for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            if (has_far) {
+                if (mixed_ == 1)
+                    for (const TcLaunch& t : lp.far_tc[st]) launch_tc(t, u, pv, gev, true);
+                else
+                    for (const Launch& fl : lp.far[st]) launch_gemm(fl, u, pv, gev);
+                if (u != s) {
+                    far_done = D.evpool[evi++];
+                    cudaEventRecord(far_done, u);
+                }
+            }
         }
+        join_far();
         mark(6);
         if (mixed_ == 1)
             for (const TcLaunch& t : lp.outer_tc) launch_tc(t, s, pv, gev);

@@ -105,7 +105,8 @@ private:
     std::vector<std::pair<int, cudaEvent_t>> marks_;
     int sm_count_ = 148;
     int ensure_slabs();
-    void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
+    void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev,
+                   bool far = false);
     struct Csr {
         int64_t* rowptr = nullptr;
         int32_t* ci = nullptr;

@@ -252,6 +252,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
     P.gemm_flops = 0.0;
     P.slab_rows = 0;
+    P.slab_rows_far = 0;
     P.small_flops = 0.0;
     for (int64_t js = 0; js < ns; ++js)
         if (P.F[js] <= kSmallMaxF) {
@@ -305,7 +306,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         // the same jobs for the tensor-core path: slabs of W = L D and L as
         // FP32 hi/lo pairs (4 arrays of K blocks of [rows][32])
         lp.update_tc.assign(nsteps, std::vector<TcLaunch>());
-        auto emit_tc = [&](std::vector<Job> jl, std::vector<TcLaunch>& out) {
+        auto emit_tc = [&](std::vector<Job> jl, std::vector<TcLaunch>& out, int64_t& slab_max) {
             if (jl.empty()) return;
             int64_t rows = 0;
             for (Job& j : jl) {
@@ -326,9 +327,11 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             for (const Job& j : jl) add_job(t.gemm, j, tiles_t(j.c0, j.c_end, j.r_end, kTcTile));
             close_launch(t.gemm);
             t.gemm.tile = kTcTile;
-            P.slab_rows = std::max(P.slab_rows, rows);
+            slab_max = std::max(slab_max, rows);
             out.push_back(t);
         };
+        lp.far.assign(nsteps, std::vector<Launch>());
+        lp.far_tc.assign(nsteps, std::vector<TcLaunch>());
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
@@ -340,7 +343,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 add_job(lp.panel[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, nrb, true);
             }
             close_launch(lp.panel[st]);
-            std::vector<Job> jl;
+            std::vector<Job> jl, jfar;
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
@@ -353,12 +356,21 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                     P.gemm_flops += update_flops(c0, sp1, f, nb);
                 }
                 if (c0 == sp1 && sp1 < s) {                          // trailing, K = 256
-                    jl.push_back(Job{js, sp1, s, f, sp0, sp1, 0});
-                    P.gemm_flops += update_flops(sp1, s, f, sp1 - sp0);
+                    // the next super-panel's columns now; the columns beyond
+                    // it on the side stream, overlapping that super-panel
+                    const int32_t sp2 = std::min(sp1 + kSuperPanel, s);
+                    jl.push_back(Job{js, sp1, sp2, f, sp0, sp1, 0});
+                    P.gemm_flops += update_flops(sp1, sp2, f, sp1 - sp0);
+                    if (sp2 < s) {
+                        jfar.push_back(Job{js, sp2, s, f, sp0, sp1, 0});
+                        P.gemm_flops += update_flops(sp2, s, f, sp1 - sp0);
+                    }
                 }
             }
             emit_updates(jl, lp.update[st]);
-            emit_tc(jl, lp.update_tc[st]);
+            emit_tc(jl, lp.update_tc[st], P.slab_rows);
+            emit_updates(jfar, lp.far[st]);
+            emit_tc(jfar, lp.far_tc[st], P.slab_rows_far);
             open_launch(lp.fsolve[st]);
             for (int32_t js : lp.large_nodes) {
                 const int32_t s = P.S[js], f = P.F[js];
@@ -443,7 +455,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             lp.outer.clear();
             emit_updates(jl, lp.outer);
             lp.outer_tc.clear();
-            emit_tc(jl, lp.outer_tc);
+            emit_tc(jl, lp.outer_tc, P.slab_rows);
         }
         open_launch(lp.writeback);
         for (int32_t js : lp.large_nodes)
@@ -470,6 +482,13 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             for (Launch& l : v) build_map(l);
         for (Launch& l : lp.outer) build_map(l);
         for (auto& v : lp.update_tc)
+            for (TcLaunch& t : v) {
+                build_map(t.split);
+                build_map(t.gemm);
+            }
+        for (auto& v : lp.far)
+            for (Launch& l : v) build_map(l);
+        for (auto& v : lp.far_tc)
             for (TcLaunch& t : v) {
                 build_map(t.split);
                 build_map(t.gemm);

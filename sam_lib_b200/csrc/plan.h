@@ -83,6 +83,9 @@ struct LevelPlan {
     Launch rect;                              // rectangle rows [S, F): one task per 256 x 256 tile
     Launch rect_rows;                         // forward solve, rows [S, F): one task per row
     std::vector<std::vector<TcLaunch>> update_tc;   // mixed precision: the updates of each step
+    // trailing update columns beyond the next super-panel (side stream)
+    std::vector<std::vector<Launch>> far;
+    std::vector<std::vector<TcLaunch>> far_tc;
     std::vector<TcLaunch> outer_tc;                 // mixed precision: the K = S update
 };
 
@@ -140,6 +143,7 @@ struct Plan {
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
     double gemm_flops = 0.0;                 // algorithmic flops of the Schur-update launches
     int64_t slab_rows = 0;                   // largest operand-slab need of one tensor-core launch (128-byte rows)
+    int64_t slab_rows_far = 0;               // the same for the side-stream launches
     double small_flops = 0.0;                // factor flops done by the fused small-front kernel
 };
 
