@@ -787,18 +787,37 @@ k_gemm(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
         }
     }
     cp_async_wait<0>();
-    // epilogue: C -= acc on the lower part, inside [.., r_end) x [.., c_end)
+    // epilogue: C -= acc on the lower part, inside [.., r_end) x [.., c_end);
+    // in two halves of the warp tile, each with its loads ahead of its
+    // stores, so that the loads overlap instead of waiting one latency each
+    constexpr int MH = C::MI > 1 ? C::MI / 2 : 1;
 #pragma unroll
-    for (int mi = 0; mi < C::MI; ++mi) {
-        const int r = i0 + wm + mi * 8 + (lane >> 2);
-        if (r >= r_end) continue;
+    for (int m0 = 0; m0 < C::MI; m0 += MH) {
+        double cv[MH][C::NI][2];
 #pragma unroll
-        for (int ni = 0; ni < C::NI; ++ni) {
+        for (int q = 0; q < MH; ++q) {
+            const int r = i0 + wm + (m0 + q) * 8 + (lane >> 2);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int c = j0 + wn + ni * 8 + 2 * (lane & 3) + h;
-                if (c < c_end && r >= c) frontw[(int64_t)r + (int64_t)c * ld] -= acc[mi][ni][h];
-            }
+            for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = j0 + wn + ni * 8 + 2 * (lane & 3) + h;
+                    cv[q][ni][h] =
+                        (r < r_end && c < c_end && r >= c) ? __ldcg(front + (int64_t)r + (int64_t)c * ld) : 0.0;
+                }
+        }
+#pragma unroll
+        for (int q = 0; q < MH; ++q) {
+            const int r = i0 + wm + (m0 + q) * 8 + (lane >> 2);
+            if (r >= r_end) continue;
+#pragma unroll
+            for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = j0 + wn + ni * 8 + 2 * (lane & 3) + h;
+                    if (c < c_end && r >= c)
+                        frontw[(int64_t)r + (int64_t)c * ld] = cv[q][ni][h] - acc[m0 + q][ni][h];
+                }
         }
     }
 }
