@@ -2030,7 +2030,7 @@ void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vec
                                                    far ? D.slab_far : D.slab);
     // a side-stream launch leaves a quarter of the SMs to the panel chain
     // (a persistent tensor-core CTA holds most of an SM's shared memory)
-    const int cap = far ? std::max(1, sm_count_ - sm_count_ / 4) : sm_count_;
+    const int cap = (far && !profile_) ? std::max(1, sm_count_ - sm_count_ / 4) : sm_count_;
     const int grid = (int)std::min<int64_t>(t.gemm.ntasks, cap);
     k_gemm_tc<<<grid, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count, TMAP(t.gemm),
                                                     t.gemm.ntasks, pv, far ? D.slab_map_far : D.slab_map);
