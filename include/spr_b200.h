@@ -99,6 +99,10 @@ int spr_b200_refine(void* handle, const double* d_sm, const double* d_b, double*
  * forward: small fronts, gather, blocks, rectangles, finish;
  * back: small fronts, gather, rectangles, blocks, (unused), finish (ms).  out holds 20 doubles. */
 int spr_b200_phase_ms(void* handle, double* out);
+/* Mixed mode: out[0] = algorithmic flops of the Schur updates that run on the
+ * tensor cores (trailing columns beyond the next super-panel, K = S updates),
+ * out[1] = their split + tensor-core time in the last profiled factor (ms). */
+int spr_b200_tc_stats(void* handle, double* out);
 /* Profile mode: CUDA events around every Schur-update launch. */
 int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed); see abi.cpp. */

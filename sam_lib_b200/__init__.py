@@ -51,6 +51,8 @@ def load(int_kind=8):
         lib.spr_b200_refine.restype = C.c_int
         lib.spr_b200_set_mode.argtypes = [vp, C.c_int]
         lib.spr_b200_set_mode.restype = C.c_int
+        lib.spr_b200_tc_stats.argtypes = [vp, vp]
+        lib.spr_b200_tc_stats.restype = C.c_int
         lib.spr_b200_phase_ms.argtypes = [vp, vp]
         lib.spr_b200_phase_ms.restype = C.c_int
         lib.spr_b200_set_profile.argtypes = [vp, C.c_int]
@@ -209,6 +211,12 @@ class DeviceSolver:
         rc = self.lib.spr_b200_set_mode(self.h, int(mixed))
         if rc != 0:
             raise ValueError('unknown factorisation mode %r' % (mixed,))
+
+    def tc_stats(self):
+        """Mixed mode: (tensor-core update flops, their time in the last profiled factor, ms)."""
+        out = np.zeros(2)
+        self.lib.spr_b200_tc_stats(self.h, _ptr(out))
+        return float(out[0]), float(out[1])
 
     def phase_ms(self):
         """Profile mode: last factorisation's time by phase (ms)."""

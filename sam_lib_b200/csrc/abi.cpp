@@ -542,6 +542,16 @@ int SPR_API(spr_b200_phase_ms)(void* handle, double* out) {
     return 0;
 }
 
+// Mixed mode: out[0] = algorithmic flops of the updates that run on tensor
+// cores (far trailing columns and K = S updates), out[1] = their split +
+// tensor-core time in the last profiled factorisation (ms).
+int SPR_API(spr_b200_tc_stats)(void* handle, double* out) {
+    const Engine* e = static_cast<Engine*>(handle);
+    out[0] = e->plan().tc_flops;
+    out[1] = e->timing.tc_ms;
+    return 0;
+}
+
 int SPR_API(spr_b200_set_profile)(void* handle, int on) {
     static_cast<Engine*>(handle)->set_profile(on != 0);
     return 0;

@@ -2025,7 +2025,10 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
 void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev, bool far) {
     if (t.gemm.ntasks <= 0) return;
     Dev& D = *d_;
-    if (profile_) gev.push_back(record_event(s));
+    if (profile_) {
+        tc_pairs_.push_back(gev.size());
+        gev.push_back(record_event(s));
+    }
     k_split_tc<<<(int)t.split.ntasks, 256, 0, s>>>(D.jobs + t.split.job_begin, t.split.job_count, TMAP(t.split), pv,
                                                    far ? D.slab_far : D.slab);
     // a side-stream launch leaves a quarter of the SMs to the panel chain
@@ -2100,10 +2103,11 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             // a trailing update's next-super-panel columns were also updated by
             // the previous super-panel's far launch: wait for it first
             if ((st + 1) % (kSuperPanel / kNB) == 0) join_far();
-            if (mixed_ == 1)
-                for (const TcLaunch& t : lp.update_tc[st]) launch_tc(t, s, pv, gev);
-            else
-                for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            // the updates inside the panel chain (K = 64 in-super-panel columns,
+            // the next super-panel's K = 256 columns) are small and on the
+            // critical path: the FP64 kernel's 64x64 tiles start sooner than
+            // the split + tensor-core pair, so they stay FP64 in both modes
+            for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
             if (has_far) {
                 if (mixed_ == 1)
                     for (const TcLaunch& t : lp.far_tc[st]) launch_tc(t, u, pv, gev, true);
@@ -2155,6 +2159,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     CK(cudaMemsetAsync(D.sn_bad, 0, P_.nsuper * sizeof(int32_t), s));
     timing.gemm_ms = 0.f;
     timing.gemm_launches = 0;
+    tc_pairs_.clear();
     CK(cudaEventRecord(D.ev0, s));
     std::vector<cudaEvent_t> gev;
     // the legacy default stream cannot be captured: graphs need a stream of our own
@@ -2183,11 +2188,18 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     CK(cudaMemcpyAsync(&hs, D.st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     CK(cudaEventElapsedTime(&timing.factor_ms, D.ev0, D.ev1));
+    timing.tc_ms = 0.f;
+    size_t tp = 0;
     for (size_t k = 0; k + 1 < gev.size(); k += 2) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, gev[k], gev[k + 1]);
         timing.gemm_ms += ms;
+        if (tp < tc_pairs_.size() && tc_pairs_[tp] == k) {
+            timing.tc_ms += ms;
+            ++tp;
+        }
     }
+    tc_pairs_.clear();
     for (cudaEvent_t e : gev) cudaEventDestroy(e);
     for (int k = 0; k < 9; ++k) timing.phase_ms[k] = 0.f;
     for (size_t k = 0; k < marks_.size(); ++k) {

@@ -24,6 +24,7 @@ struct FactorResult {
 struct Timing {              // CUDA-event times of the last calls (ms)
     float factor_ms = 0.f, solve_ms = 0.f;
     float gemm_ms = 0.f;     // Schur-update kernels only (sum over launches)
+    float tc_ms = 0.f;       // of those, the split + tensor-core launch pairs
     int64_t gemm_launches = 0, launches = 0, solve_launches = 0;
     // profile mode: factor time by phase (CUDA events between launch groups):
     // 0 pre-pass, 1 small fronts, 2 extend-add, 3 diagonal blocks, 4 panel
@@ -103,6 +104,7 @@ private:
     bool use_graphs_ = true;
     int mixed_ = 0;
     std::vector<std::pair<int, cudaEvent_t>> marks_;
+    std::vector<size_t> tc_pairs_;        // profile mode: event pairs of the tensor-core launches
     int sm_count_ = 148;
     int ensure_slabs();
     void launch_tc(const TcLaunch& t, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev,

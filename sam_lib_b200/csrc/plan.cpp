@@ -251,6 +251,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     };
     auto close_launch = [&](Launch& l) { l.job_count = (int64_t)P.jobs.size() - l.job_begin; };
     P.gemm_flops = 0.0;
+    P.tc_flops = 0.0;
     P.slab_rows = 0;
     P.slab_rows_far = 0;
     P.small_flops = 0.0;
@@ -303,9 +304,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 if (l.ntasks > 0) out.push_back(l);
             }
         };
-        // the same jobs for the tensor-core path: slabs of W = L D and L as
-        // FP32 hi/lo pairs (4 arrays of K blocks of [rows][32])
-        lp.update_tc.assign(nsteps, std::vector<TcLaunch>());
+        // the far and K = S updates for the tensor-core path: slabs of W = L D
+        // and L as FP32 hi/lo pairs (4 arrays of K blocks of [rows][32])
         auto emit_tc = [&](std::vector<Job> jl, std::vector<TcLaunch>& out, int64_t& slab_max) {
             if (jl.empty()) return;
             int64_t rows = 0;
@@ -364,11 +364,11 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                     if (sp2 < s) {
                         jfar.push_back(Job{js, sp2, s, f, sp0, sp1, 0});
                         P.gemm_flops += update_flops(sp2, s, f, sp1 - sp0);
+                        P.tc_flops += update_flops(sp2, s, f, sp1 - sp0);
                     }
                 }
             }
             emit_updates(jl, lp.update[st]);
-            emit_tc(jl, lp.update_tc[st], P.slab_rows);
             emit_updates(jfar, lp.far[st]);
             emit_tc(jfar, lp.far_tc[st], P.slab_rows_far);
             open_launch(lp.fsolve[st]);
@@ -450,6 +450,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 if (f > s) {
                     jl.push_back(Job{js, s, f, f, 0, s, 0});
                     P.gemm_flops += update_flops(s, f, f, s);
+                    P.tc_flops += update_flops(s, f, f, s);
                 }
             }
             lp.outer.clear();
@@ -481,11 +482,6 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (auto& v : lp.update)
             for (Launch& l : v) build_map(l);
         for (Launch& l : lp.outer) build_map(l);
-        for (auto& v : lp.update_tc)
-            for (TcLaunch& t : v) {
-                build_map(t.split);
-                build_map(t.gemm);
-            }
         for (auto& v : lp.far)
             for (Launch& l : v) build_map(l);
         for (auto& v : lp.far_tc)

@@ -82,7 +82,6 @@ struct LevelPlan {
     std::vector<Launch> blk_mv;               // product with the block inverse, 32 rows/columns per task
     Launch rect;                              // rectangle rows [S, F): one task per 256 x 256 tile
     Launch rect_rows;                         // forward solve, rows [S, F): one task per row
-    std::vector<std::vector<TcLaunch>> update_tc;   // mixed precision: the updates of each step
     // trailing update columns beyond the next super-panel (side stream)
     std::vector<std::vector<Launch>> far;
     std::vector<std::vector<TcLaunch>> far_tc;
@@ -142,6 +141,7 @@ struct Plan {
     double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
     double gemm_flops = 0.0;                 // algorithmic flops of the Schur-update launches
+    double tc_flops = 0.0;                   // of those, the updates the mixed mode runs on tensor cores
     int64_t slab_rows = 0;                   // largest operand-slab need of one tensor-core launch (128-byte rows)
     int64_t slab_rows_far = 0;               // the same for the side-stream launches
     double small_flops = 0.0;                // factor flops done by the fused small-front kernel

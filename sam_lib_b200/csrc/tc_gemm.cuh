@@ -4,7 +4,9 @@
 //
 // as 3xTF32 split products: x = hi + lo with hi = tf32(x), lo = tf32(x - hi),
 // and A*B ~ A_lo*B_hi + A_hi*B_lo + A_hi*B_hi accumulated in FP32 in tensor
-// memory; the FP64 front is updated once per tile at the end.
+// memory over 256-column chunks, FP64 across chunks.  The mixed mode runs the
+// K = S updates and the trailing-update columns beyond the next super-panel
+// here; the updates inside the panel chain stay on the FP64 kernel.
 //
 // Two kernels per Schur-update launch:
 //   k_split_tc  reads the FP64 panel columns [k_lo, k_hi) of rows [c0, r_end)
@@ -12,15 +14,15 @@
 //               L_hi, L_lo; W = L D) of 32-column blocks, [row][32] floats, rows
 //               padded to a multiple of 128 and K to a multiple of 32 with
 //               zeros, into the slab arena (one 128-byte row per slab row);
-//   k_gemm_tc   one CTA per 128x128 lower tile of the update block: a TMA
-//               producer warp streams the four 128x32 operand tiles of each K
-//               block into a 3-stage shared-memory ring (128-byte swizzle), one
-//               thread issues tcgen05.mma kind::tf32 (M=N=128, K=8) into a
-//               128-column TMEM accumulator and releases stages with
-//               tcgen05.commit, and four epilogue warps read the accumulator
-//               with tcgen05.ld and subtract it from the FP64 front (lower
-//               triangle only: the upper triangle of diagonal blocks holds
-//               L11^-1 of later panels).
+//   k_gemm_tc   persistent CTAs over the lower 128x128 tiles of the update
+//               block: a TMA producer warp streams the four 128x32 operand
+//               tiles of each K block into a 3-stage shared-memory ring
+//               (128-byte swizzle), one thread issues tcgen05.mma kind::tf32
+//               (M=N=128, K=8) into two alternating 128-column TMEM
+//               accumulators and releases stages with tcgen05.commit, and four
+//               epilogue warps add each chunk into FP64 sums kept in TMEM and
+//               subtract the last one from the FP64 front (lower triangle only:
+//               the upper triangle of diagonal blocks holds L11^-1 of later panels).
 // Every mbarrier wait is bounded by a time limit; a wait that gives up sets
 // Stats::tc_timeout, the CTA skips its remaining work, frees its TMEM and
 // returns (the host turns the flag into an error).
