@@ -99,6 +99,15 @@ int spr_b200_refine(void* handle, const double* d_sm, const double* d_b, double*
  * forward: small fronts, gather, blocks, rectangles, finish;
  * back: small fronts, gather, rectangles, blocks, (unused), finish (ms).  out holds 20 doubles. */
 int spr_b200_phase_ms(void* handle, double* out);
+/* No reference counterpart.  Autotuner of the mixed-precision factorisation:
+ * it times candidate choices (which Schur-update launches run on the tensor
+ * cores, by a minimum of algorithmic flops; how many SMs the side-stream
+ * launches may take), each on a copy of the assembled device SM (one extra
+ * SM-sized buffer is allocated for the duration), and keeps the fastest for
+ * later factorisations.  out[0] = chosen minimum flops, out[1] = chosen
+ * quarters of the SMs, out[2] = its factor ms, out[3] = the default's,
+ * out[4] = candidates tried. */
+int spr_b200_autotune(void* handle, const double* d_sm_assembled, double* out);
 /* Mixed mode: out[0] = algorithmic flops of the Schur updates that run on the
  * tensor cores (trailing columns beyond the next super-panel, K = S updates),
  * out[1] = their split + tensor-core time in the last profiled factor (ms). */

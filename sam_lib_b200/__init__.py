@@ -51,6 +51,8 @@ def load(int_kind=8):
         lib.spr_b200_refine.restype = C.c_int
         lib.spr_b200_set_mode.argtypes = [vp, C.c_int]
         lib.spr_b200_set_mode.restype = C.c_int
+        lib.spr_b200_autotune.argtypes = [vp, vp, vp]
+        lib.spr_b200_autotune.restype = C.c_int
         lib.spr_b200_tc_stats.argtypes = [vp, vp]
         lib.spr_b200_tc_stats.restype = C.c_int
         lib.spr_b200_phase_ms.argtypes = [vp, vp]
@@ -211,6 +213,15 @@ class DeviceSolver:
         rc = self.lib.spr_b200_set_mode(self.h, int(mixed))
         if rc != 0:
             raise ValueError('unknown factorisation mode %r' % (mixed,))
+
+    def autotune(self, d_sm_assembled):
+        """Mixed-mode autotuner on a copy of the assembled SM; returns the choice and times."""
+        out = np.zeros(5)
+        rc = self.lib.spr_b200_autotune(self.h, C.c_void_p(self._dev(d_sm_assembled)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError('spr_b200_autotune failed with %d' % rc)
+        return dict(tc_min_flops=out[0], far_sm_quarters=int(out[1]), factor_ms=out[2], default_ms=out[3],
+                    candidates=int(out[4]))
 
     def tc_stats(self):
         """Mixed mode: (tensor-core update flops, their time in the last profiled factor, ms)."""

@@ -542,6 +542,12 @@ int SPR_API(spr_b200_phase_ms)(void* handle, double* out) {
     return 0;
 }
 
+// Mixed-mode autotuner: which Schur updates run on the tensor cores and how
+// many SMs the side-stream launches take, timed on a copy of the assembled SM.
+int SPR_API(spr_b200_autotune)(void* handle, const double* d_sm_assembled, double* out) {
+    return static_cast<Engine*>(handle)->autotune(d_sm_assembled, out);
+}
+
 // Mixed mode: out[0] = algorithmic flops of the updates that run on tensor
 // cores (far trailing columns and K = S updates), out[1] = their split +
 // tensor-core time in the last profiled factorisation (ms).

@@ -2033,7 +2033,7 @@ void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vec
                                                    far ? D.slab_far : D.slab);
     // a side-stream launch leaves a quarter of the SMs to the panel chain
     // (a persistent tensor-core CTA holds most of an SM's shared memory)
-    const int cap = (far && !profile_) ? std::max(1, sm_count_ - sm_count_ / 4) : sm_count_;
+    const int cap = (far && !profile_) ? std::max(1, sm_count_ * far_cap_q_ / 4) : sm_count_;
     const int grid = (int)std::min<int64_t>(t.gemm.ntasks, cap);
     k_gemm_tc<<<grid, tc::kThreads, tc::kSmem, s>>>(D.jobs + t.gemm.job_begin, t.gemm.job_count, TMAP(t.gemm),
                                                     t.gemm.ntasks, pv, far ? D.slab_map_far : D.slab_map);
@@ -2092,7 +2092,8 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 k_trsm<<<(int)pl.ntasks, 128, kTrsmSmem, s>>>(jobs + pl.job_begin, pl.job_count, TMAP(pl), pv);
                 ++timing.launches;
             }
-            const bool has_far = mixed_ == 1 ? !lp.far_tc[st].empty() : !lp.far[st].empty();
+            const bool has_far = !lp.far[st].empty() || !lp.far_tc[st].empty();
+            const bool far_tc = mixed_ == 1 && lp.far_flops[st] >= tc_min_flops_;
             if (has_far && u != s) {
                 // the super-panel is final: fork the far columns of its trailing update
                 cudaEvent_t e = D.evpool[evi++];
@@ -2109,7 +2110,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             // the split + tensor-core pair, so they stay FP64 in both modes
             for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
             if (has_far) {
-                if (mixed_ == 1)
+                if (far_tc)
                     for (const TcLaunch& t : lp.far_tc[st]) launch_tc(t, u, pv, gev, true);
                 else
                     for (const Launch& fl : lp.far[st]) launch_gemm(fl, u, pv, gev);
@@ -2121,7 +2122,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         }
         join_far();
         mark(6);
-        if (mixed_ == 1)
+        if (mixed_ == 1 && lp.outer_flops >= tc_min_flops_)
             for (const TcLaunch& t : lp.outer_tc) launch_tc(t, s, pv, gev);
         else
             for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
@@ -2165,7 +2166,8 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     // the legacy default stream cannot be captured: graphs need a stream of our own
     const bool graph = use_graphs_ && !profile_ && s != nullptr;
     if (graph) {
-        const GraphKey key{(const void*)d_sm, nullptr, tol1, 0, mixed_, 0};
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_,
+                           (int64_t)std::min(tc_min_flops_, 9.0e18)};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2578,6 +2580,69 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     out[2] = hf[0];
     out[3] = hf[1];
     out[4] = hs.tol2;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the mixed-mode factorisation: which Schur updates go to the
+// tensor cores (launches of at least tc_min_flops; the rest stay on the FP64
+// kernel) and how many SMs the side-stream tensor-core launches may take.
+// Every candidate factors a copy of the assembled SM twice (the second,
+// graph-replayed pass is timed); the fastest is kept.  out[0] = chosen
+// tc_min_flops, out[1] = chosen quarters of the SMs, out[2] = its factor ms,
+// out[3] = factor ms of the default choice, out[4] = candidates tried.
+// ---------------------------------------------------------------------------
+int Engine::autotune(const double* d_sm_assembled, double* out) {
+    const int64_t n = P_.neq + P_.nzerol;
+    double* work = nullptr;
+    CK(cudaMalloc((void**)&work, n * sizeof(double)));
+    const int mode0 = mixed_;
+    const double t0 = tc_min_flops_;
+    const int q0 = far_cap_q_;
+    mixed_ = 1;
+    const double mins[] = {0.0, 1.0e9, 1.0e10, 1.0e11, 1.0e300};
+    const int caps[] = {2, 3, 4};
+    double best = 1e300, best_min = 0.0, def_ms = 0.0;
+    int best_cap = 3, tried = 0, rc = 0;
+    for (double m : mins)
+        for (int q : caps) {
+            if (m >= 1.0e300 && q != 3) continue;              // no tensor-core launches: the cap is moot
+            tc_min_flops_ = m;
+            far_cap_q_ = q;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && rc == 0; ++rep) {
+                if (cudaMemcpyAsync(work, d_sm_assembled, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_) !=
+                    cudaSuccess) {
+                    rc = -4;
+                    break;
+                }
+                FactorResult r;
+                rc = factor(work, 1.0e-12, r);
+                ms = timing.factor_ms;
+            }
+            if (rc != 0) break;
+            ++tried;
+            if (m == 0.0 && q == 3) def_ms = ms;
+            if (ms < best) {
+                best = ms;
+                best_min = m;
+                best_cap = q;
+            }
+        }
+    cudaFree(work);
+    mixed_ = mode0;
+    if (rc != 0) {
+        tc_min_flops_ = t0;
+        far_cap_q_ = q0;
+        return rc;
+    }
+    tc_min_flops_ = best_min;
+    far_cap_q_ = best_cap;
+    out[0] = best_min;
+    out[1] = best_cap;
+    out[2] = best;
+    out[3] = def_ms;
+    out[4] = tried;
     return 0;
 }
 

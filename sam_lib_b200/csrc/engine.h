@@ -58,6 +58,9 @@ public:
     int residual(const double* d_b, const double* d_x, double* d_r, int64_t ld, int64_t nrhs, double* berr);
     int refine(const double* d_sm, const double* d_b, double* d_x, int64_t ld, int64_t nrhs, double tol, int maxit,
                double* out);
+    // Mixed mode autotuner (see engine.cu): times candidate engine choices on a
+    // copy of the assembled SM and keeps the fastest.  out: 5 doubles.
+    int autotune(const double* d_sm_assembled, double* out);
     // Per-supernode negative-pivot counts and failing column of the last factor().
     int sn_stats(int32_t* neg, int32_t* fail);
     // The solves use the inverses of the diagonal blocks that factor() stores;
@@ -103,6 +106,8 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     int mixed_ = 0;
+    double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
+    int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
     std::vector<std::pair<int, cudaEvent_t>> marks_;
     std::vector<size_t> tc_pairs_;        // profile mode: event pairs of the tensor-core launches
     int sm_count_ = 148;

@@ -332,6 +332,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         };
         lp.far.assign(nsteps, std::vector<Launch>());
         lp.far_tc.assign(nsteps, std::vector<TcLaunch>());
+        lp.far_flops.assign(nsteps, 0.0);
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
@@ -365,6 +366,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                         jfar.push_back(Job{js, sp2, s, f, sp0, sp1, 0});
                         P.gemm_flops += update_flops(sp2, s, f, sp1 - sp0);
                         P.tc_flops += update_flops(sp2, s, f, sp1 - sp0);
+                        lp.far_flops[st] += update_flops(sp2, s, f, sp1 - sp0);
                     }
                 }
             }
@@ -451,6 +453,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                     jl.push_back(Job{js, s, f, f, 0, s, 0});
                     P.gemm_flops += update_flops(s, f, f, s);
                     P.tc_flops += update_flops(s, f, f, s);
+                    lp.outer_flops += update_flops(s, f, f, s);
                 }
             }
             lp.outer.clear();

@@ -85,6 +85,8 @@ struct LevelPlan {
     // trailing update columns beyond the next super-panel (side stream)
     std::vector<std::vector<Launch>> far;
     std::vector<std::vector<TcLaunch>> far_tc;
+    std::vector<double> far_flops;            // algorithmic flops of each step's far launches
+    double outer_flops = 0.0;                 // and of the K = S update
     std::vector<TcLaunch> outer_tc;                 // mixed precision: the K = S update
 };
 

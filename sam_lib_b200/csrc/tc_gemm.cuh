@@ -163,7 +163,10 @@ __device__ __forceinline__ int k_blocks(const Job& jb) { return (jb.k_hi - jb.k_
 // column tiles: inside a group the order is row by row, so the CTAs that run
 // together share a few row panels (A) and a few column panels (B) and the
 // operand slabs are served from L2 instead of HBM.
-constexpr int kGroup = 8;
+#ifndef SPR_TC_GROUP
+#define SPR_TC_GROUP 8
+#endif
+constexpr int kGroup = SPR_TC_GROUP;
 __device__ __forceinline__ void tile_of(int64_t u, int nct, int nr, int& it, int& jt) {
     int g0 = 0;
     for (;;) {

@@ -93,3 +93,33 @@ def test_mixed_factor_refined_to_fp64_backward_error(n, emod, sigma_factor, mode
     xr = x64.cpu().numpy().T
     assert np.linalg.norm(x - xr) <= (1e-9 if emod == 'uniform' else 1e-5) * np.linalg.norm(xr)
     ds.close()
+
+
+def test_autotune_keeps_refinement_to_fp64_backward_error():
+    """The autotuner picks the tensor-core/FP64 split of the mixed factor on a
+    copy of the assembled SM; the chosen setting still refines to 1e-12 with
+    the FP64 factor's inertia."""
+    import torch
+    import sam_lib_b200 as spr
+    hs, sm, K = _system(20, 'uniform', 2.5)
+    nrhs = 2
+    b = np.random.default_rng(3).uniform(-1.0, 1.0, size=(hs.neq, nrhs))
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    st = torch.cuda.Stream()
+    ds.set_stream(st.cuda_stream)
+    d_sm0 = torch.from_numpy(sm).cuda()
+    ds.build_residual(d_sm0)
+    ref = ds.factor(d_sm0.clone())
+    tuned = ds.autotune(d_sm0)
+    assert tuned['candidates'] == 13 and tuned['factor_ms'] > 0 and tuned['far_sm_quarters'] in (2, 3, 4)
+    assert np.array_equal(d_sm0.cpu().numpy(), sm)                  # the caller's SM is untouched
+    ds.set_mode(1)
+    d_mx = d_sm0.clone()
+    r = ds.factor(d_mx)
+    assert r['numneg'] == ref['numneg'] and r['lierr'] == 0
+    d_b = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    d_x = torch.empty_like(d_b)
+    it, berr, _ = ds.refine(d_mx, d_b, d_x, nrhs, tol=1e-12, maxit=20)
+    assert berr <= 1e-12, (it, berr)
+    assert _host_berr(K, d_x.cpu().numpy().T, b) <= 2e-12
+    ds.close()
