@@ -265,7 +265,16 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
         const int ld = P.buf_ld[c];
         for (int t = warp; t < q; t += nwarp) {
             const int pj = rel[t];
-            for (int r = t + lane; r < q; r += 32) A[pk(rel[r], pj, F)] += U[r + (int64_t)t * ld];
+            const double* Ut = U + (int64_t)t * ld;
+            int r = t + lane;
+            for (; r + 32 < q; r += 64) {
+                const int p0 = pk(rel[r], pj, F), p1 = pk(rel[r + 32], pj, F);
+                const double u0 = __ldcg(Ut + r), u1 = __ldcg(Ut + r + 32);
+                const double a0 = A[p0], a1 = A[p1];
+                A[p0] = a0 + u0;
+                A[p1] = a1 + u1;
+            }
+            if (r < q) A[pk(rel[r], pj, F)] += Ut[r];
         }
         __syncthreads();
     }
@@ -292,8 +301,18 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
         __syncthreads();
         for (int j = k + 1 + warp; j < F; j += nwarp) {
             const double ljk = A[pk(j, k, F)];
-            const int cj = pk(j, j, F) - j;
-            for (int i = j + lane; i < F; i += 32) A[cj + i] -= wcol[i] * ljk;
+            double* cj = A + pk(j, j, F) - j;
+            // loads of four rows ahead of their stores (shared-memory latency overlaps)
+            int i = j + lane;
+            for (; i + 96 < F; i += 128) {
+                const double a0 = cj[i], a1 = cj[i + 32], a2 = cj[i + 64], a3 = cj[i + 96];
+                const double w0 = wcol[i], w1 = wcol[i + 32], w2 = wcol[i + 64], w3 = wcol[i + 96];
+                cj[i] = a0 - w0 * ljk;
+                cj[i + 32] = a1 - w1 * ljk;
+                cj[i + 64] = a2 - w2 * ljk;
+                cj[i + 96] = a3 - w3 * ljk;
+            }
+            for (; i < F; i += 32) cj[i] -= wcol[i] * ljk;
         }
         __syncthreads();
     }
@@ -1048,13 +1067,18 @@ constexpr int kSolveThreads = 256;
 // all threads apply the block to the rows below it (3 barriers per block).
 constexpr int kSmallBlk = 32;
 constexpr size_t kSmallSolveSmem = sizeof(double) * ((size_t)kSmallMaxF * kMaxRHS + (size_t)kSmallMaxF * (kSmallBlk + 1));
+// shared memory of one small-front solve CTA: the front vector (F x nrhs) and
+// one 32-column block of L (F x 33)
+inline size_t small_solve_smem(int maxF, int nrhs) {
+    return sizeof(double) * ((size_t)maxF * nrhs + (size_t)maxF * (kSmallBlk + 1));
+}
 
 __global__ void __launch_bounds__(kSolveThreads)
 k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
     extern __shared__ double wsm[];           // w[i * nrhs + r], then Ls[(i - j0) * (kSmallBlk + 1) + c]
-    double* Ls = wsm + kSmallMaxF * kMaxRHS;
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* Ls = wsm + (size_t)F * nrhs;
     double* wg = vbuf + P.rbase[js] * nrhs;   // update rows for the parent (r*F + i)
     const double* Lb = P.lnz + P.lnz_off[js];
     const int tid = threadIdx.x, lane = tid & 31;
@@ -1103,9 +1127,9 @@ k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int 
 __global__ void __launch_bounds__(kSolveThreads)
 k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
     extern __shared__ double wsm[];
-    double* Ls = wsm + kSmallMaxF * kMaxRHS;
     const int js = nodes[blockIdx.x];
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
+    double* Ls = wsm + (size_t)F * nrhs;
     const double* Lb = P.lnz + P.lnz_off[js];
     const int tid = threadIdx.x, lane = tid & 31;
     (void)vbuf;
@@ -2067,10 +2091,12 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         const LevelPlan& lp = P_.levels[L];
         if (!lp.small_nodes.empty()) {
             mark(1);
-            const int F = lp.small_maxF;
-            const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
-            k_small_front<<<(int)lp.small_nodes.size(), 256, smem, s>>>(D.level_nodes + D.small_begin[L], pv);
-            ++timing.launches;
+            for (const LevelPlan::SmallClass& c : lp.small_classes) {
+                const int F = c.maxF;
+                const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
+                k_small_front<<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
+                ++timing.launches;
+            }
         }
         if (lp.large_nodes.empty()) continue;
         const Job* jobs = D.jobs;
@@ -2292,9 +2318,11 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
                     mark(0);
-                    k_forward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(D.level_nodes + D.small_begin[L],
-                                                                                pv, D.vbuf, b, ldb, nr);
-                    ++nl;
+                    for (const LevelPlan::SmallClass& c : lp.small_classes) {
+                        k_forward<<<c.count, kSolveThreads, small_solve_smem(c.maxF, nr), s>>>(
+                            D.level_nodes + D.small_begin[L] + c.begin, pv, D.vbuf, b, ldb, nr);
+                        ++nl;
+                    }
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;
@@ -2341,9 +2369,11 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
                     mark(5);
-                    k_backward<<<(int)lp.small_nodes.size(), kSolveThreads, kSmallSolveSmem, s>>>(
-                        D.level_nodes + D.small_begin[L], pv, D.vbuf, b, ldb, nr);
-                    ++nl;
+                    for (const LevelPlan::SmallClass& c : lp.small_classes) {
+                        k_backward<<<c.count, kSolveThreads, small_solve_smem(c.maxF, nr), s>>>(
+                            D.level_nodes + D.small_begin[L] + c.begin, pv, D.vbuf, b, ldb, nr);
+                        ++nl;
+                    }
                 }
                 if (lp.large_nodes.empty()) continue;
                 const Launch& ga = lp.assemble;

@@ -212,6 +212,17 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 P.upd_off[js] = P.buf_off[js] + (int64_t)s * ld + s;
             }
         }
+        // small_nodes are in decreasing F: cut them into size classes
+        {
+            auto cls = [](int32_t f) { return f <= 64 ? 0 : f <= 96 ? 1 : f <= 128 ? 2 : 3; };
+            for (int32_t k = 0; k < (int32_t)lp.small_nodes.size();) {
+                const int32_t c = cls(P.F[lp.small_nodes[k]]);
+                int32_t e = k;
+                while (e < (int32_t)lp.small_nodes.size() && cls(P.F[lp.small_nodes[e]]) == c) ++e;
+                lp.small_classes.push_back(LevelPlan::SmallClass{k, e - k, P.F[lp.small_nodes[k]]});
+                k = e;
+            }
+        }
         // after this level is assembled, its children are no longer needed
         for (int32_t js : nodes)
             for (int32_t k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k) {

@@ -68,6 +68,13 @@ struct LevelPlan {
     std::vector<int32_t> small_nodes;        // fronts done by the fused one-CTA kernel
     std::vector<int32_t> large_nodes;        // fronts done by the blocked path
     int32_t small_maxF = 0;
+    // small fronts in size classes (F <= 64, 96, 128, 176), one launch each so
+    // that the smaller fronts get the shared memory (and occupancy) they need:
+    // {first index into small_nodes, count, largest F}
+    struct SmallClass {
+        int32_t begin, count, maxF;
+    };
+    std::vector<SmallClass> small_classes;
     Launch assemble;                          // large fronts: extend-add into dense fronts
     std::vector<Launch> panel;                // per panel step: diagonal block + TRSM
     std::vector<std::vector<Launch>> update;  // per panel step: Schur updates (one launch per tile size)
