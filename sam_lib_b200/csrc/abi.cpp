@@ -573,7 +573,7 @@ int SPR_API(spr_b200_plan_check)(const I* mspar, const I* mtrees, const I* msifa
     std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
     sprb::Plan p;
     const int rc = sprb::build_plan(ms.data(), mt.data(), mf.data(), p);
-    for (int i = 0; i < 11; ++i) out[i] = 0.0;
+    for (int i = 0; i < 13; ++i) out[i] = 0.0;
     out[0] = rc;
     if (rc != 0) return rc;
     int64_t oob = 0, ov = 0;
@@ -593,6 +593,10 @@ int SPR_API(spr_b200_plan_check)(const I* mspar, const I* mtrees, const I* msifa
     out[8] = (double)nsmall;
     out[9] = (double)nlarge;
     out[10] = (double)p.jobs.size();
+    int64_t cf = 0, ct = 0;
+    sprb::check_coverage(p, cf, ct);
+    out[11] = (double)cf;
+    out[12] = (double)ct;
     return 0;
 }
 

@@ -554,4 +554,57 @@ void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps) {
     }
 }
 
+void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
+    fp64 = tc = 0;
+    const int64_t ns = P.nsuper;
+    for (int which = 0; which < 2; ++which) {
+        // per front: per column, the K intervals it receives
+        std::vector<std::vector<std::vector<std::pair<int32_t, int32_t>>>> cov(ns);
+        auto add = [&](const Launch& l) {
+            for (int64_t j = 0; j < l.job_count; ++j) {
+                const Job& jb = P.jobs[l.job_begin + j];
+                auto& c = cov[jb.node];
+                if (c.empty()) c.resize(P.F[jb.node]);
+                for (int32_t col = jb.c0; col < jb.c_end; ++col) c[col].emplace_back(jb.k_lo, jb.k_hi);
+            }
+        };
+        for (const LevelPlan& lp : P.levels) {
+            for (const auto& v : lp.update)
+                for (const Launch& l : v) add(l);
+            if (which == 0) {
+                for (const auto& v : lp.far)
+                    for (const Launch& l : v) add(l);
+                for (const Launch& l : lp.outer) add(l);
+            } else {
+                for (const auto& v : lp.far_tc)
+                    for (const TcLaunch& t : v) add(t.gemm);
+                for (const TcLaunch& t : lp.outer_tc) add(t.gemm);
+            }
+        }
+        int64_t bad = 0;
+        for (int64_t js = 0; js < ns; ++js) {
+            if (P.F[js] <= kSmallMaxF) continue;
+            const int32_t F = P.F[js], S = P.S[js];
+            auto& c = cov[js];
+            if (c.empty()) c.resize(F);
+            for (int32_t col = 0; col < F; ++col) {
+                const int32_t want = col < S ? (col / kNB) * kNB : S;
+                auto& v = c[col];
+                std::sort(v.begin(), v.end());
+                int32_t at = 0;
+                bool ok = true;
+                for (const auto& iv : v) {
+                    if (iv.first != at || iv.second <= iv.first) {
+                        ok = false;
+                        break;
+                    }
+                    at = iv.second;
+                }
+                if (!ok || at != want) ++bad;
+            }
+        }
+        (which == 0 ? fp64 : tc) = bad;
+    }
+}
+
 }  // namespace sprb

@@ -165,5 +165,13 @@ int64_t buffer_doubles(const Plan& P, int64_t js);
 // Self-check of the arena layout: counts buffers outside the arena and
 // overlaps between buffers that are live at the same level.
 void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps);
+// Schur-update coverage: every column c of every large front must receive
+// exactly the K ranges that tile [0, 64 floor(c / 64)) for c < S (earlier
+// panels; a column's own panel is eliminated by the diagonal block and TRSM)
+// and [0, S) for c >= S,
+// once, across the update, far and K = S launches.  Counts the columns that
+// do not, for the FP64 launch lists (fp64) and the tensor-core lists in the
+// mixed mode's use (tc: FP64 panel-chain updates + tensor-core far and K = S).
+void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc);
 
 }  // namespace sprb
