@@ -33,7 +33,7 @@ def _rank_main(rank, world, port, outdir):
     dist.init_process_group('gloo', rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         st = load_structure(6)
-        out = np.zeros(11)
+        out = np.zeros(13)
         rc = spr.load(8).spr_b200_plan_check(spr._ptr(st['mspar']), spr._ptr(st['mtrees']),
                                              spr._ptr(st['msifa']), spr._ptr(out))
         plans = [None] * world
