@@ -149,3 +149,50 @@ def test_partial_factorisation_mode_is_reported():
     msp[56] = 1
     g = gpu_sprsol(rs, sm, rhs(rs.neq, 1, 7), iop=1, mspar=msp)
     assert g['ierr'] == -4
+
+
+def test_pivot_failure_inside_a_dense_front():
+    """A pivot driven to zero inside the largest (dense-path) front: IERR -3,
+    the failing equation (MSPAR(27)), NUMNEG of the columns before it and
+    TOL(2:3) as the oracle reports them (SPRF17's test, sprfc1.f:1272-1294)."""
+    from sam_lib_b200.system import diag_positions
+    rs, sm = ref_system(8)
+    sp = rs.mspar
+    ns = int(sp[10])
+    xs = rs.mtrees[sp[44] - 1: sp[44] + ns]
+    xl = rs.mtrees[sp[45] - 1: sp[45] + ns]
+    F = np.diff(xl)
+    js = int(np.argmax(F))
+    assert F[js] > 176                       # a dense-path front
+    j = int(xs[js] - 1 + (xs[js + 1] - xs[js]) // 2)
+    pos = diag_positions(rs.mspar, rs.mtrees, rs.msifa)
+    o1 = run_sprsol('orc', rs, sm, rhs(rs.neq, 1, 8), iop=1)
+    z = sm.copy()
+    z[pos[j]] -= o1['sm'][pos[j]]            # the pivot of column j becomes (nearly) zero
+    b = rhs(rs.neq, 1, 8)
+    o = run_sprsol('orc', rs, z, b, iop=1, tol1=1e-8)
+    g = gpu_sprsol(rs, z, b, iop=1, tol1=1e-8)
+    assert o['ierr'] == g['ierr'] == -3
+    assert g['mspar'][26] == o['mspar'][26] == j + 1
+    assert g['mspar'][25] == o['mspar'][25]
+    # TOL(3) is the column's original diagonal; TOL(2) the failing pivot, a
+    # rounding-level remainder whose value depends on the summation order
+    assert abs(g['tol'][2] - o['tol'][2]) <= 1e-12 * abs(o['tol'][2])
+    assert abs(g['tol'][1]) <= 1e-8 * abs(o['tol'][2])
+
+
+def test_integer4_abi_matches_oracle():
+    """libspr_b200_i4.so (INTEGER*4 build) through sprsol_ gives the INTEGER*8 results."""
+    rs, sm = ref_system(6, 'loguniform')
+    b = rhs(rs.neq, 2, 9)
+    o = run_sprsol('orc', rs, sm, b)
+    sm4 = sm.copy()
+    B = np.asfortranarray(b.copy())
+    msp4 = rs.mspar.astype(np.int32)
+    tol = np.array([1e-12, 0.0, 0.0])
+    ierr = spr.sprsol(3, msp4, rs.mtrees.astype(np.int32), rs.msifa.astype(np.int32), sm4, B, rs.neq, 2, tol,
+                      int_kind=4)
+    assert ierr == o['ierr'] == 0
+    assert np.array_equal(msp4.astype(np.int64), o['mspar'])
+    assert close_factor(sm4, o['sm'])
+    assert relerr(B, o['b']) <= 1e-6
