@@ -37,6 +37,17 @@ void sprfc1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double
              SPR_INT* iwork, double* rwork, const SPR_INT* lpu, SPR_INT* ierr,
              void (*mvmult)(), void (*mmmult)());
 
+/* Replaces SPRFC3, src/SPR/sprfc3.f:5-277 (LDL' factorisation that does not
+ * stop on singularity; it is what SPRLAN calls, sprlan.f:814).  TOL(4): on entry
+ * TOL(1) is the zero threshold and TOL(4) scales the replacement pivot
+ * sign(TOL(1) max(1, |TOL(4) a_jj|), d) (sprfc3.f:1083-1099); a zero diagonal
+ * becomes 1 (sprfc3.f:561-572).  DCOR(2,NEQ) receives, per equation, the
+ * original pivot (or a negative pivot) and the inserted value.  IERR = -3 with
+ * MSPAR(27) = -(number replaced) leaves a complete factor (MSPAR(1) = 5). */
+void sprfc3_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* tol,
+             SPR_INT* iwork, double* rwork, double* dcor, const SPR_INT* lpu, SPR_INT* ierr,
+             void (*mvmult)(), void (*mmmult)());
+
 /* Replaces SPRFS1, src/SPR/sprfs1.f:5-263 (forward reduction + D^-1). */
 void sprfs1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
              const SPR_INT* ldb, const SPR_INT* nrhs, SPR_INT* iwork, double* rwork,
@@ -61,6 +72,11 @@ int spr_b200_set_stream(void* handle, void* stream);
  * out[0]=TOL(2) out[1]=TOL(3) out[2]=NUMNEG out[3]=SUPEQT out[4]=LIERR
  * (0, -30 pivot below TOL(1), -35 exact zero diagonal). */
 int spr_b200_factor_dev(void* handle, double* d_sm, double tol1, double* out);
+/* The same with SPRFC3 semantics (SPRF31, sprfc3.f:372-806): tol = {TOL(1),
+ * TOL(4)}, d_dcor = device DCOR(2,NEQ).  out as above; LIERR = -31 and
+ * SUPEQT = the number of replaced pivots when any was replaced. */
+int spr_b200_factor3_dev(void* handle, double* d_sm, const double* tol, double* d_dcor,
+                         double* out);
 /* Forward (which=1, SPRFS3 sprfs1.f:266), back (which=2, SPRBS4 sprbs1.f:251)
  * or both (3) on device B (ldb x nrhs, column-major) with device SM. */
 int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ldb,

@@ -10,6 +10,9 @@
  *   SPRF11  src/SPR/sprfc1.f:286-713   (multifrontal loop, TOL(2)/TOL(3))
  *   SPRF12/13/14 sprfc1.f:716-982      (relative indices, extend-add)
  *   SPRF15/17 sprfc1.f:985-1299        (LDL' of the S fully-summed columns)
+ *   SPRFC3/SPRF31/SPRF37 src/SPR/sprfc3.f:5-277, 372-806, 1011-1104
+ *                                      (the variant that replaces singular
+ *                                       pivots and records them in DCOR)
  *   LMVY18  src/SPR/lmvy18.f:5-173     (column update inside SPRF17)
  *   LMMY18  src/SPR/lmmy18.f:5-192     (Schur update of the update matrix)
  *   SPRFS1/3/5/6, SPRFB1/2 src/SPR/sprfs1.f  (forward + diagonal solve)
@@ -66,12 +69,16 @@ typedef struct {
     I n;             /* its order                                          */
 } update_t;
 
-/* Returns the SPRF11 ERROR code (0, -30 or -35) and fills numneg/supeqt. */
+/* Returns the SPRF11 ERROR code (0, -30 or -35) and fills numneg/supeqt.
+ * With dcor != NULL it follows SPRF31 instead (sprfc3.f:372-806): zero
+ * diagonals become 1, pivots at or below TOL(1)|a_jj| are replaced
+ * (SPRF37, sprfc3.f:1083-1099), and the code is -31 with supeqt = the number
+ * replaced, or 0. */
 static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
-                       I *numneg_out, I *supeqt_out)
+                       I *numneg_out, I *supeqt_out, double *dcor)
 {
     const I ns = s->nsuper;
-    I numneg = 0, supeqt = 0, error = 0;
+    I numneg = 0, supeqt = 0, error = 0, nsing = 0;
     tol[1] = 0.0;
     tol[2] = 0.0;
     /* pre-pass: original diagonal, zero check, trace (sprfc1.f:465-488) */
@@ -80,7 +87,15 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
         I p = s->xlnz[js] - 1;
         for (I j = s->xsuper[js]; j < s->xsuper[js + 1]; j++) {
             diag[j - 1] = lnz[p];
-            if (diag[j - 1] == 0.0) {
+            if (dcor) {                  /* sprfc3.f:561-573 */
+                dcor[2 * (j - 1)] = 0.0;
+                dcor[2 * (j - 1) + 1] = 0.0;
+                if (diag[j - 1] == 0.0) {
+                    diag[j - 1] = 1.0;
+                    dcor[2 * (j - 1) + 1] = 1.0;
+                    lnz[p] = 1.0;
+                }
+            } else if (diag[j - 1] == 0.0) {
                 numneg++;
                 if (numneg == 1) {
                     supeqt = j;
@@ -139,7 +154,18 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
             }
             const double adiag = diag[fst - 1 + j];
             double d = X[j + j * F];
-            if (fabs(d) <= tol[0] * fabs(adiag)) {
+            if (dcor) {                  /* SPRF37, sprfc3.f:1083-1099 */
+                double *dc = dcor + 2 * (fst - 1 + j);
+                if (fabs(d) <= tol[0] * fabs(adiag)) {
+                    nsing++;
+                    dc[0] = d;
+                    const double m = fabs(tol[3] * adiag);
+                    d = copysign(fabs(tol[0] * (m > 1.0 ? m : 1.0)), d);
+                    X[j + j * F] = d;
+                    dc[1] = d;
+                }
+                if (d < 0.0 && dc[0] == 0.0) dc[0] = d;
+            } else if (fabs(d) <= tol[0] * fabs(adiag)) {
                 error = -(j + 1);
                 tol[1] = d;
                 tol[2] = adiag;
@@ -189,6 +215,10 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
             if (diag[i] > 0.0 && (mdiag == 0.0 || mdiag > diag[i])) mdiag = diag[i];
         tol[1] = (tol[1] != 0.0) ? 1.0 / tol[1] : 0.0;
         tol[2] = (mdiag != 0.0) ? tol[2] / mdiag : 0.0;
+    }
+    if (dcor && nsing > 0) {             /* sprfc3.f:796-799 */
+        supeqt = nsing;
+        error = -31;
     }
     *numneg_out = numneg;
     *supeqt_out = supeqt;
@@ -280,10 +310,38 @@ void orc_sprfc1_(I *mspar, I *mtrees, I *msifa, double *sm, double *tol,
     sym_t s;
     sym_from_mspar(&s, mspar, mtrees, msifa);
     I numneg = 0, supeqt = 0;
-    I lierr = oracle_factor(&s, sm, sm + s.neq, tol, &numneg, &supeqt);
+    I lierr = oracle_factor(&s, sm, sm + s.neq, tol, &numneg, &supeqt, NULL);
     if (lierr != 0) {                    /* sprfc1.f:251-265 */
         *ierr = (lierr / 10 == -3) ? -3 : -4;
         mspar[26] = supeqt;
+    } else if (numneg > 0) {
+        *ierr = 3;
+    }
+    mspar[25] = numneg;
+}
+
+/* SPRFC3 (sprfc3.f:5-277): TOL(4), DCOR(2,NEQ); IERR -3 with MSPAR(27) =
+ * -(number of replaced pivots) leaves a complete factor. */
+void orc_sprfc3_(I *mspar, I *mtrees, I *msifa, double *sm, double *tol,
+                 I *iwork, double *rwork, double *dcor, const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {                  /* sprfc3.f:139-143 */
+        mspar[0] = -5;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 5;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    I numneg = 0, supeqt = 0;
+    I lierr = oracle_factor(&s, sm, sm + s.neq, tol, &numneg, &supeqt, dcor);
+    if (lierr != 0) {                    /* sprfc3.f:249-258 */
+        *ierr = (lierr / 10 == -3) ? -3 : -4;
+        mspar[26] = (lierr == -31) ? -supeqt : supeqt;
     } else if (numneg > 0) {
         *ierr = 3;
     }

@@ -2,11 +2,12 @@
 
 The product is the C-ABI library ``libspr_b200.so`` (built in-tree by
 ``sam_lib_b200.build``): it exports the reference's Fortran entry points
-``sprsol_``, ``sprfc1_``, ``sprfs1_`` and ``sprbs1_`` (INTEGER*8 ABI;
+``sprsol_``, ``sprfc1_``, ``sprfc3_``, ``sprfs1_`` and ``sprbs1_`` (INTEGER*8 ABI;
 ``libspr_b200_i4.so`` has the INTEGER*4 ABI) plus a device-level API.  This
 module is the Python mirror of that interface: the same routine names,
 argument meaning and IERR conventions as src/SPR/sprsol.f, sprfc1.f,
-sprfs1.f and sprbs1.f, with numpy arrays standing in for the Fortran arrays.
+sprfc3.f, sprfs1.f and sprbs1.f, with numpy arrays standing in for the
+Fortran arrays.
 
 There is no CPU fallback: if the library is missing, importing the
 interface raises.
@@ -39,6 +40,8 @@ def load(int_kind=8):
         lib.spr_b200_set_stream.argtypes = [vp, vp]
         lib.spr_b200_factor_dev.argtypes = [vp, vp, C.c_double, vp]
         lib.spr_b200_factor_dev.restype = C.c_int
+        lib.spr_b200_factor3_dev.argtypes = [vp, vp, vp, vp, vp]
+        lib.spr_b200_factor3_dev.restype = C.c_int
         lib.spr_b200_solve_dev.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, C.c_int]
         lib.spr_b200_solve_dev.restype = C.c_int
         lib.spr_b200_info.argtypes = [vp, vp]
@@ -112,6 +115,28 @@ def sprfc1(mspar, mtrees, msifa, sm, tol, iwork=None, rwork=None, lpu=-1, int_ki
     return ierr.value
 
 
+def sprfc3(mspar, mtrees, msifa, sm, tol, dcor, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFC3 (src/SPR/sprfc3.f:5): LDL' factorisation that replaces singular pivots.
+
+    TOL has 4 entries (TOL(1) zero threshold, TOL(4) replacement scale on
+    entry; TOL(2), TOL(3) on exit); DCOR is a float64 array of 2*NEQ entries
+    (DCOR(2,NEQ) column-major).  Returns IERR: -3 with MSPAR(27) = -(number of
+    replaced pivots) still leaves a complete factor in SM.
+    """
+    np_t, c_t = _ints(int_kind)
+    if tol.dtype != np.float64 or tol.size < 4:
+        raise TypeError('TOL must be a float64 array of 4 entries')
+    if dcor.dtype != np.float64 or dcor.size < 2 * int(mspar[7]):
+        raise TypeError('DCOR must be a float64 array of 2*NEQ entries')
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfc3_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
+                           _ptr(iwork), _ptr(rwork), _ptr(dcor), _ref(lpu, c_t), C.byref(ierr),
+                           None, None)
+    return ierr.value
+
+
 def sprfs1(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork=None, rwork=None, lpu=-1, int_kind=8):
     """SPRFS1 (src/SPR/sprfs1.f:5): forward reduction + diagonal scaling; returns IERR."""
     np_t, c_t = _ints(int_kind)
@@ -170,6 +195,19 @@ class DeviceSolver:
         rc = self.lib.spr_b200_factor_dev(self.h, C.c_void_p(self._dev(d_sm)), tol1, _ptr(out))
         if rc != 0:
             raise RuntimeError('spr_b200_factor_dev failed with %d' % rc)
+        return dict(tol2=out[0], tol3=out[1], numneg=int(out[2]), supeqt=int(out[3]),
+                    lierr=int(out[4]))
+
+    def factor3(self, d_sm, d_dcor, tol1=1.0e-12, tol4=1.0):
+        """SPRFC3 semantics (SPRF31, sprfc3.f:372): singular pivots are replaced
+        and recorded in the device DCOR(2,NEQ) (2*NEQ doubles); returns the dict
+        of factor(), with lierr = -31 and supeqt = the number replaced if any."""
+        out = np.zeros(5)
+        tol = np.array([tol1, tol4])
+        rc = self.lib.spr_b200_factor3_dev(self.h, C.c_void_p(self._dev(d_sm)), _ptr(tol),
+                                           C.c_void_p(self._dev(d_dcor)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError('spr_b200_factor3_dev failed with %d' % rc)
         return dict(tol2=out[0], tol3=out[1], numneg=int(out[2]), supeqt=int(out[3]),
                     lierr=int(out[4]))
 

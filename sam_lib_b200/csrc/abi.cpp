@@ -51,6 +51,7 @@ struct Ctx {
     double* d_sm = nullptr;
     double* d_b = nullptr;
     int64_t b_cap = 0;
+    double* d_dcor = nullptr;          // SPRFC3's DCOR(2,NEQ) on the device
     cudaStream_t stream = nullptr;
     // device factor residency
     const double* sm_host = nullptr;
@@ -59,6 +60,7 @@ struct Ctx {
     ~Ctx() {
         if (d_sm) cudaFree(d_sm);
         if (d_b) cudaFree(d_b);
+        if (d_dcor) cudaFree(d_dcor);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -189,23 +191,46 @@ int ensure_b(Ctx* c, int64_t n) {
     return 0;
 }
 
-// H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR.
-I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu) {
+// H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR, or
+// with dcor (host DCOR(2,NEQ)) the SPRFC3 one.
+I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nullptr) {
     const int64_t neq = mspar[7], nzerol = mspar[15];
     const int64_t nsm = neq + nzerol;
+    const char* who = dcor ? "SPRFC3" : "SPRFC1";
     cudaStream_t s = c->stream;
     if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return -4;
+    Engine::Singular fc3{0.0, nullptr};
+    if (dcor) {
+        if (!c->d_dcor && cudaMalloc((void**)&c->d_dcor, 2 * std::max<int64_t>(neq, 1) * sizeof(double)) != cudaSuccess)
+            return -4;
+        fc3.tol4 = tol[3];
+        fc3.d_dcor = c->d_dcor;
+    }
     FactorResult r;
-    if (c->eng.factor(c->d_sm, tol[0], r) != 0) {
-        msg(lpu, "SPRFC1", "CUDA failure in the factorisation");
+    if (c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr) != 0) {
+        msg(lpu, who, "CUDA failure in the factorisation");
         return -4;
     }
     if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -4;
+    if (dcor && cudaMemcpyAsync(dcor, c->d_dcor, 2 * neq * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return -4;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
     I ierr = 0;
     tol[1] = r.tol2;
     tol[2] = r.tol3;
-    if (r.lierr != 0) {                               // sprfc1.f:251-265
+    if (r.lierr == -31) {                             // sprfc3.f:249-258
+        ierr = -3;
+        mspar[26] = -(I)r.supeqt;
+        if (lpu >= 0) {
+            char buf[256];
+            snprintf(buf, sizeof buf, "SINGULAR EQUATION SYSTEM: %" PRId64 " PIVOT(S) REPLACED (TOL(1) = %g)",
+                     r.supeqt, tol[0]);
+            msg(lpu, who, buf);
+        }
+        c->sm_host = sm;
+        c->sm_fp = sm_fingerprint(sm, nsm);
+        c->resident = true;
+    } else if (r.lierr != 0) {                        // sprfc1.f:251-265
         ierr = (r.lierr / 10 == -3) ? -3 : -4;
         mspar[26] = (I)r.supeqt;
         if (lpu >= 0) {
@@ -216,15 +241,15 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu) {
             else
                 snprintf(buf, sizeof buf, "PIVOT BELOW THE TOL(1) THRESHOLD IN EQUATION %" PRId64
                          " (%" PRId64 " NEGATIVE PIVOTS BEFORE IT)", r.supeqt, r.numneg);
-            msg(lpu, "SPRFC1", buf);
+            msg(lpu, who, buf);
         }
         c->resident = false;
     } else {
         if (r.numneg > 0) {
             ierr = 3;
             if (lpu >= 0)
-                fprintf(stderr, " *** WARNING from SPR routine SPRFC1 (GPU)\n     THE STIFFNESS MATRIX IS NOT POSITIVE "
-                        "DEFINITE: %" PRId64 " NEGATIVE PIVOT(S)\n", r.numneg);
+                fprintf(stderr, " *** WARNING from SPR routine %s (GPU)\n     THE STIFFNESS MATRIX IS NOT POSITIVE "
+                        "DEFINITE: %" PRId64 " NEGATIVE PIVOT(S)\n", who, r.numneg);
         }
         c->sm_host = sm;
         c->sm_fp = sm_fingerprint(sm, nsm);
@@ -348,6 +373,49 @@ void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
     if (*ierr < 0 && *ierr != -3) mspar[0] = -5;
 }
 
+// SPRFC3 (src/SPR/sprfc3.f:5): LDL' factorisation that replaces singular
+// pivots instead of stopping (TOL(4) scales the replacement) and reports them
+// in DCOR(2,NEQ); IERR = -3 with MSPAR(27) = -(number replaced) still leaves a
+// complete factor, MSPAR(1) = 5.
+void SPR_API(sprfc3_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I* iwork, double* rwork, double* dcor,
+                      const I* lpu, I* ierr, void (*mvmult)(), void (*mmmult)()) {
+    (void)iwork;
+    (void)rwork;
+    (void)mvmult;
+    (void)mmmult;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfc3.f:139-143
+        mspar[0] = -5;
+        *ierr = -1;
+        msg(*lpu, "SPRFC3", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 5;
+    *ierr = 0;
+    if (!fc1_lengths_ok(mspar)) {                       // sprfc3.f:209-234 (same checks as SPRFC1)
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFC3", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (unsupported_mode(mspar)) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRFC3", "PARTIAL FACTORISATION (MSPAR(57)>0) IS NOT HANDLED BY THE GPU PATH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c) {
+        mspar[0] = -5;
+        *ierr = (err == -2) ? -2 : -4;
+        msg(*lpu, "SPRFC3", "COULD NOT SET UP THE GPU CONTEXT");
+        return;
+    }
+    *ierr = do_factor(c, mspar, sm, tol, *lpu, dcor);
+    if (*ierr == -4) mspar[0] = -5;
+}
+
 // SPRFS1 (src/SPR/sprfs1.f:5): forward reduction and diagonal scaling of B.
 void SPR_API(sprfs1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb, const I* nrhs, I* iwork,
                       double* rwork, const I* lpu, I* ierr) {
@@ -468,6 +536,22 @@ int SPR_API(spr_b200_set_stream)(void* handle, void* stream) {
 int SPR_API(spr_b200_factor_dev)(void* handle, double* d_sm, double tol1, double* out) {
     FactorResult r;
     int rc = static_cast<Engine*>(handle)->factor(d_sm, tol1, r);
+    if (rc != 0) return rc;
+    out[0] = r.tol2;
+    out[1] = r.tol3;
+    out[2] = (double)r.numneg;
+    out[3] = (double)r.supeqt;
+    out[4] = (double)r.lierr;
+    return 0;
+}
+
+// SPRFC3 semantics on device buffers: tol = {TOL(1), TOL(4)}, d_dcor = the
+// device DCOR(2,NEQ); out as spr_b200_factor_dev, LIERR = -31 with
+// SUPEQT = the number of replaced pivots when any was replaced.
+int SPR_API(spr_b200_factor3_dev)(void* handle, double* d_sm, const double* tol, double* d_dcor, double* out) {
+    FactorResult r;
+    Engine::Singular fc3{tol[1], d_dcor};
+    int rc = static_cast<Engine*>(handle)->factor(d_sm, tol[0], r, &fc3);
     if (rc != 0) return rc;
     out[0] = r.tol2;
     out[1] = r.tol3;

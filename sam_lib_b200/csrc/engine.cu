@@ -54,6 +54,7 @@ struct Stats {
     double trace;            // sum a_jj, sprfc1.f:483
     double mindpos;          // smallest positive pivot, sprfc1.f:690-697
     int tc_timeout;          // a tensor-core update CTA gave up waiting (see tc_gemm.cuh)
+    unsigned long long nsing;    // SPRFC3: pivots replaced by the TOL(1)/TOL(4) rule
 };
 
 struct PV {
@@ -76,6 +77,12 @@ struct PV {
     const int64_t* rect_off;
     const int64_t* fwd_off;
     double tol1;
+    // SPRFC3 semantics (sprfc3.f:549-572, 1083-1099): a zero diagonal becomes
+    // 1 and a pivot at or below TOL(1)|a_jj| is replaced instead of stopping;
+    // both are recorded in DCOR(2,NEQ) (dcor[2j], dcor[2j+1])
+    int fc3;
+    double tol4;
+    double* dcor;
 };
 
 struct Engine::Dev {
@@ -177,6 +184,27 @@ __device__ void record_fail(const PV& P, int js, int col, double d, double ad) {
     atomicExch(&P.st->pivot_fail, 1);
 }
 
+// SPRF37 (sprfc3.f:1083-1099): the pivot d of a column with original
+// diagonal ad becomes sign(TOL(1) max(1, |TOL(4) ad|), d) when |d| <= TOL(1)|ad|.
+__device__ __forceinline__ double fc3_pivot(const PV& P, double d, double ad) {
+    return fabs(d) <= P.tol1 * fabs(ad) ? copysign(fabs(P.tol1 * fmax(1.0, fabs(P.tol4 * ad))), d) : d;
+}
+
+// DCOR entries of column col (0-based) for the pivot d0 before and dn after
+// the replacement: DCOR(1) = d0 on a replacement, else (or if d0 == 0) dn when
+// dn < 0; DCOR(2) = dn on a replacement.  One thread per column.
+__device__ __forceinline__ void fc3_record(const PV& P, int col, double d0, double dn) {
+    const bool sing = fabs(d0) <= P.tol1 * fabs(P.adiag[col]);
+    double* dc = P.dcor + 2 * (int64_t)col;
+    double c1 = sing ? d0 : 0.0;
+    if (dn < 0.0 && c1 == 0.0) c1 = dn;
+    if (sing || dn < 0.0) dc[0] = c1;
+    if (sing) {
+        dc[1] = dn;
+        atomicAdd(&P.st->nsing, 1ull);
+    }
+}
+
 __device__ __forceinline__ bool children_bad(const PV& P, int js) {
     for (int k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k)
         if (P.sn_bad[P.child[k]]) return true;
@@ -191,9 +219,21 @@ __global__ void k_prepass(PV P, int64_t nsuper) {
     for (int64_t js = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; js < nsuper;
          js += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int s = P.S[js], f = P.F[js], fst = P.fst[js];
-        const double* col = P.lnz + P.lnz_off[js];
+        double* col = P.lnz + P.lnz_off[js];
         for (int j = lane; j < s; j += 32) {
-            const double a = col[lnz_col(j, f)];
+            double a = col[lnz_col(j, f)];
+            if (P.fc3) {                                  // sprfc3.f:561-572
+                double* dc = P.dcor + 2 * (int64_t)(fst + j);
+                dc[0] = 0.0;
+                dc[1] = 0.0;
+                if (a == 0.0) {
+                    a = 1.0;
+                    dc[1] = 1.0;
+                    col[lnz_col(j, f)] = 1.0;
+                }
+                P.adiag[fst + j] = a;
+                continue;
+            }
             P.adiag[fst + j] = a;
             if (a == 0.0) {
                 atomicAdd(&P.st->zero_count, 1);
@@ -237,6 +277,7 @@ __global__ void k_reduce(const double* v, int64_t n, double* out) {
 // Small fronts: fused extend-add + LDL' + Schur update, one CTA per front.
 // Shared memory holds the packed lower front F(F+1)/2 plus one column.
 // ---------------------------------------------------------------------------
+template <bool FC3>
 __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P) {
     extern __shared__ double sh[];
     if (P.st->any_fail) return;
@@ -283,9 +324,13 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
     double tmax = 0.0;
     bool failed = false;
     for (int k = 0; k < S; ++k) {
-        const double d = A[pk(k, k, F)];
+        double d = A[pk(k, k, F)];
         const double ad = P.adiag[fst + k];
-        if (fabs(d) <= P.tol1 * fabs(ad)) {            // sprfc1.f:1274
+        if (FC3) {
+            const double d0 = d;
+            d = fc3_pivot(P, d0, ad);
+            if (tid == 0) fc3_record(P, fst + k, d0, d);
+        } else if (fabs(d) <= P.tol1 * fabs(ad)) {     // sprfc1.f:1274
             if (tid == 0) record_fail(P, js, k, d, ad);
             failed = true;
             break;
@@ -299,6 +344,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             A[pk(i, k, F)] = a * rd;
         }
         __syncthreads();
+        if (FC3 && tid == 0) A[pk(k, k, F)] = d;     // every thread has read the old pivot
         for (int j = k + 1 + warp; j < F; j += nwarp) {
             const double ljk = A[pk(j, k, F)];
             double* cj = A + pk(j, j, F) - j;
@@ -410,6 +456,7 @@ __global__ void k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, 
 // rows i = tx + 16a and columns j = ty + 16b of the block; right-looking with
 // the unscaled column (a_ij -= a_ik * a_jk / d_k), scaled to L at the end.
 // Also forms X = L11^-1 (unit lower) for the panel TRSM and the solves.
+template <bool FC3>
 __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     // Register-resident: thread (tx, ty) keeps entries (tx + 16a, ty + 16b) of
     // the block in v[a][b] through the elimination and of X = L^-1 in x[a][b]
@@ -452,6 +499,11 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
 #pragma unroll
                 for (int b = 1; b < R; ++b)
                     if (b == kb) c = v[a][b];
+                if (FC3 && i == k) {
+                    const double c0 = c;
+                    c = fc3_pivot(P, c0, adv[k]);
+                    fc3_record(P, fst + k0 + k, c0, c);
+                }
                 if (i >= k && i < nb) vec[buf][i] = c;
                 if (i == k) {
                     dd[k] = c;
@@ -461,7 +513,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         }
         __syncthreads();
         const double d = vec[buf][k];
-        if (fabs(d) <= P.tol1 * fabs(adv[k])) {
+        if (!FC3 && fabs(d) <= P.tol1 * fabs(adv[k])) {
             failed = k;
             if (tid == 0) record_fail(P, js, k0 + k, d, adv[k]);
             break;
@@ -504,7 +556,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
 #pragma unroll
         for (int b = 0; b < R; ++b) {
             const int i = tx + 16 * a, j = ty + 16 * b;
-            if (i >= j && i < nb && j < nb) A[i][j] = (i > j) ? v[a][b] * rdv[j] : v[a][b];
+            if (i >= j && i < nb && j < nb) A[i][j] = (i > j) ? v[a][b] * rdv[j] : (FC3 ? dd[j] : v[a][b]);
         }
     __syncthreads();
     // X = L^-1 by a column sweep: X = I, then at step m every X[i][j] with
@@ -1931,7 +1983,8 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
     const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + kSmallMaxF) * sizeof(double);
     if ((size_t)smem_max < need) return -4;
-    CK(cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
@@ -2028,6 +2081,9 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.rect_off = D.rect_off;
     v.fwd_off = D.fwd_off;
     v.tol1 = tol1;
+    v.fc3 = 0;
+    v.tol4 = 0.0;
+    v.dcor = nullptr;
     return v;
 }
 
@@ -2094,7 +2150,10 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             for (const LevelPlan::SmallClass& c : lp.small_classes) {
                 const int F = c.maxF;
                 const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
-                k_small_front<<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
+                if (pv.fc3)
+                    k_small_front<true><<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
+                else
+                    k_small_front<false><<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
                 ++timing.launches;
             }
         }
@@ -2111,7 +2170,10 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         for (size_t st = 0; st < lp.panel.size(); ++st) {
             const Launch& pl = lp.panel[st];
             mark(3);
-            k_diag<<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+            if (pv.fc3)
+                k_diag<true><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+            else
+                k_diag<false><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             ++timing.launches;
             if (pl.ntasks > 0) {
                 mark(4);
@@ -2169,10 +2231,16 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
     ++timing.launches;
 }
 
-int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
+int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular* fc3) {
     Dev& D = *d_;
     cudaStream_t s = stream_;
     PV pv = make_view(D, P_, d_sm, tol1);
+    if (fc3) {
+        if (!fc3->d_dcor) return -2;
+        pv.fc3 = 1;
+        pv.tol4 = fc3->tol4;
+        pv.dcor = fc3->d_dcor;
+    }
     linv_valid_ = false;
     if (mixed_ == 1) {
         const int rc = ensure_slabs();
@@ -2193,7 +2261,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
     const bool graph = use_graphs_ && !profile_ && s != nullptr;
     if (graph) {
         const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_,
-                           (int64_t)std::min(tc_min_flops_, 9.0e18)};
+                           (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2275,6 +2343,10 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res) {
         return 0;
     }
     linv_valid_ = true;
+    if (fc3 && hs.nsing > 0) {                     // sprfc3.f:796-799
+        res.lierr = -31;
+        res.supeqt = (int64_t)hs.nsing;
+    }
     res.numneg = hs.numneg;
     res.tol2 = (hs.tol2 != 0.0) ? 1.0 / hs.tol2 : 0.0;          // sprfc1.f:699-703
     res.tol3 = (hs.mindpos != 0.0) ? hs.trace / hs.mindpos : 0.0;  // sprfc1.f:704-708
@@ -2589,7 +2661,7 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     pv.tol1 = tol1;
     for (int64_t stp = 0; stp < nblk; ++stp) {
         const StepJobs& sj = steps[stp];
-        k_diag<<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
+        k_diag<false><<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
         if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, nullptr, pv);
         if (sj.upd_tasks > 0)
             K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, nullptr,

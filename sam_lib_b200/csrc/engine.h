@@ -14,9 +14,10 @@ namespace sprb {
 // Outcome of a factorisation, in the reference's terms (SPRF11/SPRFC1,
 // src/SPR/sprfc1.f:240-283 and :690-708).
 struct FactorResult {
-    int64_t lierr = 0;       // 0, -30 (pivot below threshold) or -35 (zero diagonal)
+    int64_t lierr = 0;       // 0, -30 (pivot below threshold), -35 (zero diagonal) or,
+                             // SPRFC3 semantics, -31 (pivots replaced)
     int64_t numneg = 0;      // MSPAR(26)
-    int64_t supeqt = 0;      // MSPAR(27) on error
+    int64_t supeqt = 0;      // MSPAR(27) on error; SPRFC3: the number of replaced pivots
     double tol2 = 0.0;       // TOL(2)
     double tol3 = 0.0;       // TOL(3)
 };
@@ -46,7 +47,16 @@ public:
     void set_stream(cudaStream_t s) { stream_ = s; }
     cudaStream_t stream() const { return stream_; }
     // Device-resident factorisation of sm = [D(NEQ) | LNZ(NZEROL)] (device pointer).
-    int factor(double* d_sm, double tol1, FactorResult& res);
+    int factor(double* d_sm, double tol1, FactorResult& res) { return factor(d_sm, tol1, res, nullptr); }
+    // SPRFC3 semantics (src/SPR/sprfc3.f:372-806): zero diagonals become 1 and
+    // pivots at or below TOL(1)|a_jj| are replaced by
+    // sign(TOL(1) max(1, |TOL(4) a_jj|), d); the factorisation always completes
+    // and records both in d_dcor (device, DCOR(2,NEQ) column-major).
+    struct Singular {
+        double tol4;
+        double* d_dcor;
+    };
+    int factor(double* d_sm, double tol1, FactorResult& res, const Singular* fc3);
     // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
     int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
     // Iterative refinement (mixed precision): build_residual() compacts the
@@ -88,8 +98,10 @@ private:
         int64_t n;
         int w;
         int64_t v;
+        const void* c = nullptr;
+        double y = 0.0;
         bool operator==(const GraphKey& o) const {
-            return a == o.a && b == o.b && x == o.x && n == o.n && w == o.w && v == o.v;
+            return a == o.a && b == o.b && x == o.x && n == o.n && w == o.w && v == o.v && c == o.c && y == o.y;
         }
     };
     struct GraphEntry {

@@ -39,11 +39,14 @@ def pytest_collection_modifyitems(config, items):
 
 
 @functools.lru_cache(maxsize=None)
-def ref_system(n, emod='uniform', seed=2):
-    """(RefSystem, assembled SM) for an n^3 hex box, cached per process."""
+def ref_system(n, emod='uniform', seed=2, clamp=True):
+    """(RefSystem, assembled SM) for an n^3 hex box, cached per process.
+
+    clamp=False leaves the box free: K is singular with the six rigid-body
+    modes in its null space."""
     from oracle.refpipe import RefSystem
     from sam_lib_b200.fe import HexBox, hex8_stiffness, element_moduli
-    box = HexBox(n)
+    box = HexBox(n, clamp_face=clamp)
     rs = RefSystem(box)
     ke = hex8_stiffness()
     E = element_moduli(box.nel, emod, seed=seed)

@@ -116,3 +116,89 @@ def test_error_codes_match_reference():
     assert r['mspar'][26] == o['mspar'][26]
     assert r['mspar'][25] == o['mspar'][25]
     assert np.array_equal(r['tol'], o['tol'])
+
+
+# ---------------------------------------------------------------------------
+# SPRFC3 (src/SPR/sprfc3.f): singular pivots replaced and recorded in DCOR
+# ---------------------------------------------------------------------------
+
+def run_sprfc3(which, rs, sm, tol1, tol4, mspar=None):
+    from oracle.refpipe import lib as reflib, _p, _i
+    sm = sm.copy()
+    msp = rs.mspar.copy() if mspar is None else mspar.copy()
+    tol = np.array([tol1, 0.0, 0.0, tol4])
+    dcor = np.full(2 * rs.neq, 7.0)        # every entry is written (sprfc3.f:564-565)
+    iw = np.zeros(int(rs.mspar[13]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + 8)
+    ierr = C.c_int64(0)
+    if which == 'ref':
+        R = reflib()
+        R.sprfc3_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw), _p(rw),
+                  _p(dcor), _i(-1), C.byref(ierr), C.cast(R.lmvy18_, C.c_void_p),
+                  C.cast(R.lmmy18_, C.c_void_p))
+    else:
+        _lib().orc_sprfc3_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw),
+                           _p(rw), _p(dcor), _i(-1), C.byref(ierr))
+    return dict(sm=sm, tol=tol, dcor=dcor.reshape(-1, 2), ierr=ierr.value, mspar=msp)
+
+
+def _same(r, o):
+    assert r['ierr'] == o['ierr']
+    assert np.array_equal(r['sm'], o['sm'])
+    assert np.array_equal(r['tol'], o['tol'])
+    assert np.array_equal(r['dcor'], o['dcor'])
+    assert np.array_equal(r['mspar'], o['mspar'])
+
+
+def test_sprfc3_rigid_body_modes_match_reference():
+    """Free box: the six rigid-body modes give six pivots at rounding level,
+    each replaced by sign(TOL(1) max(1, |TOL(4) a_jj|), d)."""
+    rs, sm = ref_system(4, clamp=False)
+    r = run_sprfc3('ref', rs, sm, 1e-8, 1e-2)
+    o = run_sprfc3('orc', rs, sm, 1e-8, 1e-2)
+    _same(r, o)
+    assert o['ierr'] == -3 and o['mspar'][0] == 5
+    assert o['mspar'][26] == -6                   # MSPAR(27) = -(number replaced)
+    rep = np.nonzero(o['dcor'][:, 1])[0]
+    assert len(rep) == 6
+    from sam_lib_b200.system import diag_positions
+    adiag = sm[diag_positions(rs.mspar, rs.mtrees, rs.msifa)]
+    np.testing.assert_array_equal(np.abs(o['dcor'][rep, 1]),
+                                  1e-8 * np.maximum(1.0, np.abs(1e-2 * adiag[rep])))
+
+
+def test_sprfc3_zero_diagonal_indefinite_and_threshold_match_reference():
+    from sam_lib_b200.system import diag_positions
+    rs, sm = ref_system(5)
+    pos = diag_positions(rs.mspar, rs.mtrees, rs.msifa)
+    # an exact zero diagonal becomes 1 (DCOR(2,j) = 1, sprfc3.f:566-571)
+    z = sm.copy()
+    j = rs.neq // 2
+    z[pos[j]] = 0.0
+    r = run_sprfc3('ref', rs, z, 1e-12, 1.0)
+    o = run_sprfc3('orc', rs, z, 1e-12, 1.0)
+    _same(r, o)
+    assert o['dcor'][j, 1] == 1.0
+    # an indefinite shift: DCOR(1,j) holds the negative pivots, IERR = 3
+    from scipy.linalg import eigh
+    rs3, sm3 = ref_system(3)
+    K = dense_from_sm(rs3, sm3)
+    M = np.diag(K.diagonal() - dense_from_sm(rs3, shifted_sm(rs3, sm3, 1.0)).diagonal())
+    w = eigh(K, M, eigvals_only=True)
+    ssm = shifted_sm(rs3, sm3, 0.5 * (w[5] + w[6]))
+    r = run_sprfc3('ref', rs3, ssm, 1e-12, 1.0)
+    o = run_sprfc3('orc', rs3, ssm, 1e-12, 1.0)
+    _same(r, o)
+    assert o['ierr'] == 3 and o['mspar'][25] == 6
+    assert np.count_nonzero(o['dcor'][:, 0] < 0.0) == 6
+    # a large TOL(1): regular pivots replaced, the factor still completes
+    r = run_sprfc3('ref', rs, sm, 0.45, 0.5)
+    o = run_sprfc3('orc', rs, sm, 0.45, 0.5)
+    _same(r, o)
+    assert o['ierr'] == -3 and o['mspar'][26] < 0 and o['mspar'][0] == 5
+    # preceding error not cleared (sprfc3.f:139-143)
+    bad = rs.mspar.copy()
+    bad[0] = -2
+    r = run_sprfc3('ref', rs, sm, 1e-12, 1.0, mspar=bad)
+    o = run_sprfc3('orc', rs, sm, 1e-12, 1.0, mspar=bad)
+    assert r['ierr'] == o['ierr'] == -1 and r['mspar'][0] == o['mspar'][0] == -5
