@@ -17,8 +17,13 @@
  *   LMMY18  src/SPR/lmmy18.f:5-192     (Schur update of the update matrix)
  *   SPRFS1/3/5/6, SPRFB1/2 src/SPR/sprfs1.f  (forward + diagonal solve)
  *   SPRBS1/4/6 src/SPR/sprbs1.f        (back solve)
- * for the plain configuration the GPU path handles (MSPAR(57)<=0,
- * MSPAR(58)=0, no panels: numerically identical, panels only re-block).
+ * for the configurations the GPU path handles: MSPAR(58)=0, no panels
+ * (numerically identical, panels only re-block), and MSPAR(57) <= 0 or the
+ * partial factorisation of MSPAR(57) > 0: the retained supernodes
+ * (SUPSUP > 0) are assembled but not eliminated (sprfc1.f:463-470,
+ * 587-608) and skipped by the solves (sprfs1.f:371, sprbs1.f:347), which
+ * treat the equations beyond LDB < NEQ as absent (sprfs1.f:201,
+ * sprbs1.f:189).
  *
  * Every floating-point update is accumulated in the same order as the
  * reference (the 8-way unrolled groups of LMMY18/LMVY18/SPRFS6 add their
@@ -41,7 +46,15 @@ typedef int64_t I;
 typedef struct {
     I neq, nsuper, nofsub, nzerol, mfront;
     const I *xsuper, *xsibl, *sibl, *xlindx, *lindx, *xlnz;
+    const I *supsup;     /* SUPSUP(NSUPER), MTREES(XLINDX+NSUPER+1) (sprfc1.f:183) */
+    I lpar57;            /* MSPAR(57) */
 } sym_t;
+
+/* A retained supernode of a partial factorisation (sprfc1.f:587). */
+static int retained(const sym_t *s, I js)
+{
+    return s->lpar57 > 0 && s->supsup[js] > 0;
+}
 
 /* Pointers into MTREES/MSIFA exactly as SPRFC1 derives them (sprfc1.f:165-196). */
 static void sym_from_mspar(sym_t *s, const I *mspar, const I *mtrees, const I *msifa)
@@ -58,6 +71,8 @@ static void sym_from_mspar(sym_t *s, const I *mspar, const I *mtrees, const I *m
     s->xlindx = mtrees + (mspar[45] - 1);
     s->lindx = msifa + (mspar[46] - 1);
     s->xlnz = msifa + (mspar[47] - 1);
+    s->supsup = s->xlindx + (s->nsuper + 1);
+    s->lpar57 = mspar[56];
 }
 
 /* ---------------------------------------------------------------------- */
@@ -81,8 +96,14 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
     I numneg = 0, supeqt = 0, error = 0, nsing = 0;
     tol[1] = 0.0;
     tol[2] = 0.0;
+    if (s->lpar57 > 0) {                 /* sprfc1.f:463, sprfc3.f:551-554 */
+        for (I i = 0; i < s->neq; i++) diag[i] = 0.0;
+        if (dcor)
+            for (I i = 0; i < 2 * s->neq; i++) dcor[i] = 0.0;
+    }
     /* pre-pass: original diagonal, zero check, trace (sprfc1.f:465-488) */
     for (I js = 0; js < ns; js++) {
+        if (retained(s, js)) continue;   /* sprfc1.f:467 */
         I len = s->xlindx[js + 1] - s->xlindx[js];
         I p = s->xlnz[js] - 1;
         for (I j = s->xsuper[js]; j < s->xsuper[js + 1]; j++) {
@@ -145,8 +166,10 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
             free(U);
             pend[c].upd = NULL;
         }
-        /* SPRF17: left-looking LDL' of columns 0..S-1 over all F rows */
-        for (I j = 0; j < S && error == 0; j++) {
+        /* SPRF17: left-looking LDL' of columns 0..S-1 over all F rows; a
+         * retained supernode is only assembled (sprfc1.f:587) */
+        const I Se = retained(s, js) ? 0 : S;
+        for (I j = 0; j < Se && error == 0; j++) {
             for (I k = 0; k < j; k++) {
                 const double a = -(X[j + k * F] * diag[fst - 1 + k]);
                 for (I i = j; i < F; i++)
@@ -190,7 +213,7 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
             double *U = (double *)malloc(sizeof(double) * (size_t)(q * q));
             for (I b = 0; b < q; b++) {
                 for (I a = b; a < q; a++) U[a + b * q] = X[(S + a) + (S + b) * F];
-                for (I k = 0; k < S; k++) {
+                for (I k = 0; k < Se; k++) {
                     const double a1 = -(X[(S + b) + k * F] * diag[fst - 1 + k]);
                     for (I a = b; a < q; a++)
                         U[a + b * q] = U[a + b * q] + a1 * X[(S + a) + k * F];
@@ -237,6 +260,10 @@ static void oracle_forward(const sym_t *s, const double *lnz, double *b, double 
         const I F = s->xlindx[js + 1] - s->xlindx[js];
         const I *rows = s->lindx + (s->xlindx[js] - 1);
         const double *L = lnz + p0;
+        if (retained(s, js)) {           /* sprfs1.f:371 */
+            p0 += F * S - (S * (S - 1)) / 2;
+            continue;
+        }
         for (I i = 0; i < F; i++) loc[i] = rows[i] <= s->neq ? b[rows[i] - 1] : 0.0;
         /* column j of the packed trapezoid starts at j*F - j(j-1)/2 */
         for (I j = 0; j < S; j++) {
@@ -278,6 +305,7 @@ static void oracle_backward(const sym_t *s, const double *lnz, double *b, double
         const I *rows = s->lindx + (s->xlindx[js] - 1);
         p0 -= F * S - (S * (S - 1)) / 2;
         const double *L = lnz + p0;
+        if (retained(s, js)) continue;   /* sprbs1.f:347 */
         for (I i = 0; i < F; i++) loc[i] = rows[i] <= s->neq ? b[rows[i] - 1] : 0.0;
         for (I j = S - 1; j >= 0; j--) {
             const I cj = j * F - (j * (j - 1)) / 2;
@@ -364,13 +392,15 @@ void orc_sprfs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
     *ierr = 0;
     sym_t s;
     sym_from_mspar(&s, mspar, mtrees, msifa);
+    const double *lnz = sm + s.neq;      /* LNZ = DIAG + NEQ before the reset */
+    if (mspar[56] == 1 && *ldb < s.neq) s.neq = *ldb;   /* sprfs1.f:201 */
     if (*ldb < s.neq) {
         mspar[0] = -2;
         *ierr = -2;
         return;
     }
     double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
-    for (I r = 0; r < *nrhs; r++) oracle_forward(&s, sm + s.neq, b + r * (*ldb), loc);
+    for (I r = 0; r < *nrhs; r++) oracle_forward(&s, lnz, b + r * (*ldb), loc);
     free(loc);
 }
 
@@ -388,13 +418,15 @@ void orc_sprbs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
     *ierr = 0;
     sym_t s;
     sym_from_mspar(&s, mspar, mtrees, msifa);
+    const double *lnz = sm + s.neq;
+    if (mspar[56] == 1 && *ldb < s.neq) s.neq = *ldb;   /* sprbs1.f:189 */
     if (*ldb < s.neq) {
         mspar[0] = -2;
         *ierr = -2;
         return;
     }
     double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
-    for (I r = 0; r < *nrhs; r++) oracle_backward(&s, sm + s.neq, b + r * (*ldb), loc);
+    for (I r = 0; r < *nrhs; r++) oracle_backward(&s, lnz, b + r * (*ldb), loc);
     free(loc);
 }
 

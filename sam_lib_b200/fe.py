@@ -23,9 +23,13 @@ HEX8_CORNERS = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
 
 
 class HexBox:
-    """SAM control arrays of an n^3 hex8 box, face x=0 clamped."""
+    """SAM control arrays of an n^3 hex8 box, face x=0 clamped.
 
-    def __init__(self, n, ndof_per_node=3, clamp_face=True):
+    retain_face=True marks the DOFs of the face x=n as external (MSC = 2): the
+    reference pipeline then numbers them last and makes their supernodes the
+    retained (superelement) ones, SUPSUP > 0 (src/SPR/sprtrs.f:1142-1204)."""
+
+    def __init__(self, n, ndof_per_node=3, clamp_face=True, retain_face=False):
         self.n = int(n)
         n1 = self.n + 1
         self.nanod = n1 ** 3
@@ -54,6 +58,11 @@ class HexBox:
             fixed_nodes = np.nonzero(node_i == 0)[0]
             for d in range(ndof_per_node):
                 msc[fixed_nodes * ndof_per_node + d] = 0
+        if retain_face:
+            node_i = (np.arange(self.nanod) % n1)
+            ext_nodes = np.nonzero(node_i == self.n)[0]
+            for d in range(ndof_per_node):
+                msc[ext_nodes * ndof_per_node + d] = 2
         self.msc = msc
         self.mpar = np.zeros(50, dtype=np.int64)
         self.mpar[0] = self.nanod       # MPAR(1) NANOD

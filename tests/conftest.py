@@ -39,14 +39,16 @@ def pytest_collection_modifyitems(config, items):
 
 
 @functools.lru_cache(maxsize=None)
-def ref_system(n, emod='uniform', seed=2, clamp=True):
+def ref_system(n, emod='uniform', seed=2, clamp=True, retain=False):
     """(RefSystem, assembled SM) for an n^3 hex box, cached per process.
 
     clamp=False leaves the box free: K is singular with the six rigid-body
-    modes in its null space."""
+    modes in its null space.  retain=True makes the face x=n external (MSC=2):
+    its equations are numbered last and form the retained supernodes of a
+    partial factorisation (MSPAR(57) = 1)."""
     from oracle.refpipe import RefSystem
     from sam_lib_b200.fe import HexBox, hex8_stiffness, element_moduli
-    box = HexBox(n, clamp_face=clamp)
+    box = HexBox(n, clamp_face=clamp, retain_face=retain)
     rs = RefSystem(box)
     ke = hex8_stiffness()
     E = element_moduli(box.nel, emod, seed=seed)

@@ -202,3 +202,79 @@ def test_sprfc3_zero_diagonal_indefinite_and_threshold_match_reference():
     r = run_sprfc3('ref', rs, sm, 1e-12, 1.0, mspar=bad)
     o = run_sprfc3('orc', rs, sm, 1e-12, 1.0, mspar=bad)
     assert r['ierr'] == o['ierr'] == -1 and r['mspar'][0] == o['mspar'][0] == -5
+
+
+# ---------------------------------------------------------------------------
+# Partial factorisation (MSPAR(57) = 1): retained supernodes of external DOFs
+# ---------------------------------------------------------------------------
+
+def retained_info(rs):
+    """(first retained equation, 0-based; number of retained equations)."""
+    sp = rs.mspar
+    ns = int(sp[10])
+    xs = rs.mtrees[sp[44] - 1: sp[44] + ns]
+    supsup = rs.mtrees[sp[45] + ns: sp[45] + 2 * ns]
+    ret = np.nonzero(supsup > 0)[0]
+    first = int(xs[ret[0]] - 1)
+    return first, rs.neq - first
+
+
+@pytest.mark.parametrize('n', [3, 6])
+def test_partial_factorisation_matches_reference(n):
+    """SPRSOL with MSPAR(57) = 1 on a box whose face x=n is external (MSC=2):
+    the factor (retained supernodes assembled, not eliminated), the condensed
+    load (forward with LDB = NEQ), and the internal solution for zero
+    retained displacements (LDB < NEQ) are the reference's bit for bit."""
+    rs, sm = ref_system(n, retain=True)
+    msp = rs.mspar.copy()
+    msp[56] = 1
+    first, nret = retained_info(rs)
+    assert nret == 3 * (n + 1) ** 2
+    b = rhs(rs.neq, 2, 40 + n)
+    r = run_sprsol('ref', rs, sm, b, iop=1, mspar=msp)
+    o = run_sprsol('orc', rs, sm, b, iop=1, mspar=msp)
+    assert r['ierr'] == o['ierr'] == 0
+    assert np.array_equal(r['sm'], o['sm'])
+    assert np.array_equal(r['tol'], o['tol'])
+    assert np.array_equal(r['mspar'], o['mspar'])
+    assert not np.any(o['sm'][first:rs.neq])          # D of the retained equations stays 0
+    # forward reduction over all NEQ rows: the retained rows get the condensed load
+    fac = o['sm']
+    r = run_sprsol('ref', rs, fac, b, iop=5, mspar=r['mspar'])
+    o = run_sprsol('orc', rs, fac, b, iop=5, mspar=o['mspar'])
+    assert r['ierr'] == o['ierr'] == 0
+    assert np.array_equal(r['b'], o['b'])
+    # factor + forward + back with LDB = number of internal equations
+    bi = np.asfortranarray(b[:first].copy())
+    r = _sprsol_ldb('ref', rs, sm, bi, msp, first)
+    o = _sprsol_ldb('orc', rs, sm, bi, msp, first)
+    assert r['ierr'] == o['ierr'] == 0
+    assert np.array_equal(r['b'], o['b'])
+    # which is the internal solution with the retained DOFs held at zero
+    K = dense_from_sm(rs, sm)
+    xi = np.linalg.solve(K[:first, :first], b[:first])
+    assert np.max(np.abs(o['b'] - xi)) <= 1e-10 * np.max(np.abs(xi))
+    # and the retained supernodes of LNZ hold the Schur complement
+    S = K[first:, first:] - K[first:, :first] @ np.linalg.solve(K[:first, :first], K[:first, first:])
+    Kf = dense_from_sm(rs, fac)
+    assert np.max(np.abs(Kf[first:, first:] - S)) <= 1e-10 * np.max(np.abs(S))
+    # SPRFC3 with MSPAR(57) = 1: DCOR of the retained equations stays 0 (sprfc3.f:551-554)
+    r = run_sprfc3('ref', rs, sm, 1e-12, 1.0, mspar=msp)
+    o = run_sprfc3('orc', rs, sm, 1e-12, 1.0, mspar=msp)
+    _same(r, o)
+    assert not np.any(o['dcor'][first:])
+
+
+def _sprsol_ldb(which, rs, sm, b, mspar, ldb):
+    from oracle.refpipe import lib as reflib, _p, _i
+    sm = sm.copy()
+    b = np.asfortranarray(b.copy())
+    msp = mspar.copy()
+    tol = np.array([1e-12, 0.0, 0.0])
+    iw = np.zeros(int(rs.mspar[13]) + int(rs.mspar[12]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + int(rs.mspar[13]) + 8)
+    ierr = C.c_int64(0)
+    f = reflib().sprsol_ if which == 'ref' else _lib().orc_sprsol_
+    f(_i(3), _p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(b), _i(ldb), _i(b.shape[1]),
+      _p(tol), _p(iw), _p(rw), _i(-1), C.byref(ierr))
+    return dict(sm=sm, b=b, tol=tol, ierr=ierr.value, mspar=msp)
