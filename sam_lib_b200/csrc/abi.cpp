@@ -110,6 +110,7 @@ void structure_key(const I* mspar, const I* mtrees, const I* msifa, std::vector<
     snap.clear();
     for (int i = 2; i < 25; ++i) snap.push_back((int64_t)mspar[i]);
     for (int i = 40; i < 50; ++i) snap.push_back((int64_t)mspar[i]);
+    snap.push_back((int64_t)mspar[56]);              // MSPAR(57): partial factorisation
     h = 0;
     const int64_t nsuper = mspar[10];
     const I* xs = mtrees + (mspar[44] - 1);
@@ -300,7 +301,17 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
                               cudaMemcpyHostToDevice, s) != cudaSuccess)
             return -4;
     }
-    if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, which) != 0) return -4;
+    if (neq != nfull && which == 3) {
+        // the back sweep of the reference sees the equations beyond LDB as
+        // zero (sprbs1.f:189), not as the forward sweep left them
+        if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, 1) != 0) return -4;
+        if (cudaMemset2DAsync(c->d_b + neq, nfull * sizeof(double), 0, (nfull - neq) * sizeof(double), nrhs, s) !=
+            cudaSuccess)
+            return -4;
+        if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, 2) != 0) return -4;
+    } else if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, which) != 0) {
+        return -4;
+    }
     if (peri2e || neq != nfull) {
         if (cudaMemcpyAsync(tmp.data(), c->d_b, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
             return -4;
@@ -321,12 +332,6 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
     return 0;
-}
-
-bool unsupported_mode(const I* mspar) {
-    // partial factorisation with retained (superelement) DOFs stays on the
-    // reference's code path: the GPU path reports it instead of guessing.
-    return mspar[56] > 0;
 }
 
 }  // namespace
@@ -353,12 +358,6 @@ void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         mspar[0] = -2;
         *ierr = -2;
         msg(*lpu, "SPRFC1", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
-        return;
-    }
-    if (unsupported_mode(mspar)) {
-        mspar[0] = -5;
-        *ierr = -4;
-        msg(*lpu, "SPRFC1", "PARTIAL FACTORISATION (MSPAR(57)>0) IS NOT HANDLED BY THE GPU PATH");
         return;
     }
     int err = 0;
@@ -396,12 +395,6 @@ void SPR_API(sprfc3_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         mspar[0] = -2;
         *ierr = -2;
         msg(*lpu, "SPRFC3", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
-        return;
-    }
-    if (unsupported_mode(mspar)) {
-        mspar[0] = -5;
-        *ierr = -4;
-        msg(*lpu, "SPRFC3", "PARTIAL FACTORISATION (MSPAR(57)>0) IS NOT HANDLED BY THE GPU PATH");
         return;
     }
     int err = 0;

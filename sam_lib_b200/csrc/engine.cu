@@ -83,6 +83,8 @@ struct PV {
     int fc3;
     double tol4;
     double* dcor;
+    // partial factorisation: 1 for the retained supernodes (null if none)
+    const uint8_t* ret;
 };
 
 struct Engine::Dev {
@@ -110,6 +112,7 @@ struct Engine::Dev {
     int32_t* sn_neg = nullptr;
     int32_t* sn_fail = nullptr;
     int32_t* sn_bad = nullptr;
+    uint8_t* ret = nullptr;                      // retained supernodes (partial factorisation)
     double* sn_faild = nullptr;
     double* sn_faila = nullptr;
     Stats* st = nullptr;
@@ -184,6 +187,11 @@ __device__ void record_fail(const PV& P, int js, int col, double d, double ad) {
     atomicExch(&P.st->pivot_fail, 1);
 }
 
+// A retained supernode of a partial factorisation (MSPAR(57) > 0, SUPSUP > 0):
+// assembled but not eliminated (sprfc1.f:587), skipped by the solves
+// (sprfs1.f:371, sprbs1.f:347).
+__device__ __forceinline__ bool is_retained(const PV& P, int js) { return P.ret != nullptr && P.ret[js] != 0; }
+
 // SPRF37 (sprfc3.f:1083-1099): the pivot d of a column with original
 // diagonal ad becomes sign(TOL(1) max(1, |TOL(4) ad|), d) when |d| <= TOL(1)|ad|.
 __device__ __forceinline__ double fc3_pivot(const PV& P, double d, double ad) {
@@ -220,6 +228,17 @@ __global__ void k_prepass(PV P, int64_t nsuper) {
          js += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int s = P.S[js], f = P.F[js], fst = P.fst[js];
         double* col = P.lnz + P.lnz_off[js];
+        if (is_retained(P, js)) {                     // D stays 0 (sprfc1.f:463-467, sprfc3.f:551-554)
+            for (int j = lane; j < s; j += 32) {
+                P.adiag[fst + j] = 0.0;
+                P.dvec[fst + j] = 0.0;
+                if (P.fc3) {
+                    P.dcor[2 * (int64_t)(fst + j)] = 0.0;
+                    P.dcor[2 * (int64_t)(fst + j) + 1] = 0.0;
+                }
+            }
+            continue;
+        }
         for (int j = lane; j < s; j += 32) {
             double a = col[lnz_col(j, f)];
             if (P.fc3) {                                  // sprfc3.f:561-572
@@ -319,11 +338,13 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
         }
         __syncthreads();
     }
-    // LDL' of the S fully-summed columns with the trailing (Schur) update
+    // LDL' of the S fully-summed columns with the trailing (Schur) update;
+    // a retained front is only assembled
     int neg = 0;
     double tmax = 0.0;
     bool failed = false;
-    for (int k = 0; k < S; ++k) {
+    const bool ret = is_retained(P, js);
+    for (int k = 0; k < (ret ? 0 : S); ++k) {
         double d = A[pk(k, k, F)];
         const double ad = P.adiag[fst + k];
         if (FC3) {
@@ -372,7 +393,8 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
     // write back the S columns (LNZ layout == packed layout) and the pivots
     double* lnzw = P.lnz + P.lnz_off[js];
     for (int i = tid; i < supsze; i += blockDim.x) lnzw[i] = A[i];
-    for (int j = tid; j < S; j += blockDim.x) P.dvec[fst + j] = A[pk(j, j, F)];
+    if (!ret)
+        for (int j = tid; j < S; j += blockDim.x) P.dvec[fst + j] = A[pk(j, j, F)];
     const int q = F - S;
     if (q > 0) {
         double* U = P.arena + P.upd_off[js];
@@ -1144,7 +1166,9 @@ k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int 
         }
         wsm[i * nrhs + r] = v;
     }
-    for (int j0 = 0; j0 < S; j0 += kSmallBlk) {
+    // a retained front only passes its sums on (own rows to B, the rest to the parent)
+    const bool ret = is_retained(P, js);
+    for (int j0 = 0; j0 < (ret ? 0 : S); j0 += kSmallBlk) {
         const int nb = min(kSmallBlk, S - j0), m = F - j0;
         for (int e = tid; e < m * nb; e += blockDim.x) {
             const int i = e % m, c = e / m;
@@ -1171,7 +1195,7 @@ k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int 
     }
     for (int e = tid; e < F * nrhs; e += blockDim.x) {
         const int i = e % F, r = e / F;
-        if (i < S) b[(int64_t)(fst + i) + r * ldb] = wsm[i * nrhs + r] / Lb[lnz_col(i, F)];
+        if (i < S) b[(int64_t)(fst + i) + r * ldb] = ret ? wsm[i * nrhs + r] : wsm[i * nrhs + r] / Lb[lnz_col(i, F)];
         else wg[(int64_t)r * F + i] = wsm[i * nrhs + r];
     }
 }
@@ -1180,6 +1204,7 @@ __global__ void __launch_bounds__(kSolveThreads)
 k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
     extern __shared__ double wsm[];
     const int js = nodes[blockIdx.x];
+    if (is_retained(P, js)) return;
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* Ls = wsm + (size_t)F * nrhs;
     const double* Lb = P.lnz + P.lnz_off[js];
@@ -1703,7 +1728,7 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int F = P.F[js], S = P.S[js];
-    if (F <= S) return;
+    if (F <= S || is_retained(P, js)) return;
     const int c = (int)(task - jb.task0);
     const int nrc = (F - S + kRectRows - 1) / kRectRows;
     double* w = vbuf + P.rbase[js] * nrhs;
@@ -1716,14 +1741,20 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
 }
 
 // y_j /= d_j and scatter of the own rows (thread per column)
-__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, const double* ysol, double* b,
-                             int64_t ldb, int nrhs) {
+// (a retained front passes its gathered sums through: the rows keep them)
+__global__ void k_fwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, const double* ysol,
+                             const double* gathered, double* b, int64_t ldb, int nrhs) {
     const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
+    if (is_retained(P, js)) {
+        const double* g = gathered + P.rbase[js] * nrhs;
+        for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = g[(int64_t)r * F + j];
+        return;
+    }
     const double* y = ysol + P.rbase[js] * nrhs;
     const double d = lcol(P, js, F, j)[j];
     for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = y[(int64_t)r * F + j] / d;
@@ -1750,6 +1781,7 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (is_retained(P, js)) return;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
     const double* w = xsol + P.rbase[js] * nrhs;
@@ -1962,6 +1994,8 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         D.all_count.push_back((int64_t)(lp.small_nodes.size() + lp.large_nodes.size()));
     }
     if (dev_upload(o, &D.level_nodes, small) || dev_upload(o, &D.all_nodes, all)) return -4;
+    D.ret = nullptr;
+    if (P_.any_retained && dev_upload(o, &D.ret, P_.retained)) return -4;
     CK(cudaMalloc((void**)&D.arena, std::max<int64_t>(P_.arena_doubles, 32) * sizeof(double)));
     CK(cudaMalloc((void**)&D.adiag, P_.neq * sizeof(double)));
     o.push_back(D.adiag);
@@ -2084,6 +2118,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.fc3 = 0;
     v.tol4 = 0.0;
     v.dcor = nullptr;
+    v.ret = D.ret;
     return v;
 }
 
@@ -2432,7 +2467,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 const Launch& wb = lp.writeback;
                 mark(4);
                 k_fwd_finish<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
-                                                               D.vbuf2, b, ldb, nr);
+                                                               D.vbuf2, D.vbuf, b, ldb, nr);
                 ++nl;
             }
         }

@@ -85,7 +85,17 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     const int64_t* xlindx = mtrees + (mspar[45] - 1);
     const int64_t* lindx = msifa + (mspar[46] - 1);
     const int64_t* xlnz = msifa + (mspar[47] - 1);
+    const int64_t* supsup = xlindx + (ns + 1);          // sprfc1.f:183
+    const bool lpar57 = mspar[56] > 0;
 
+    P.retained.assign(ns, 0);
+    P.any_retained = false;
+    if (lpar57)
+        for (int64_t js = 0; js < ns; ++js)
+            if (supsup[js] > 0) {
+                P.retained[js] = 1;
+                P.any_retained = true;
+            }
     P.fst.resize(ns);
     P.S.resize(ns);
     P.F.resize(ns);
@@ -103,6 +113,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         P.lnz_off[js] = xlnz[js] - 1;
         P.lindx_off[js] = xlindx[js] - 1;
         if (P.S[js] <= 0 || P.F[js] < P.S[js]) return -2;
+        if (P.retained[js]) continue;                  // sprtrs.f:1956
         const double s = P.S[js], f = P.F[js];
         // RINFO(3) and RINFO(4) per supernode, src/SPR/sprtrs.f:1961-1980
         P.factor_flops += ((f * f) + 2.0 * f) * s - 2.0 * (1.0 + f) * (s * (s + 1.0) / 2.0) +
@@ -291,8 +302,13 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (int32_t js : lp.large_nodes)
             add_job(lp.assemble, Job{js, 0, P.F[js], P.F[js], 0, 0, 0}, P.F[js]);
         close_launch(lp.assemble);
+        // elimination, Schur updates and the solve steps: retained fronts excluded
+        lp.elim_nodes.clear();
+        for (int32_t js : lp.large_nodes)
+            if (!P.retained[js]) lp.elim_nodes.push_back(js);
+        const std::vector<int32_t>& elim = lp.elim_nodes;
         int32_t smax = 0;
-        for (int32_t js : lp.large_nodes) smax = std::max(smax, P.S[js]);
+        for (int32_t js : elim) smax = std::max(smax, P.S[js]);
         const int32_t nsteps = (smax + kNB - 1) / kNB;
         lp.panel.assign(nsteps, Launch());
         lp.update.assign(nsteps, std::vector<Launch>());
@@ -347,7 +363,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (int32_t st = 0; st < nsteps; ++st) {
             const int32_t k0 = st * kNB;
             open_launch(lp.panel[st]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
@@ -356,7 +372,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.panel[st]);
             std::vector<Job> jl, jfar;
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
@@ -385,7 +401,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             emit_updates(jfar, lp.far[st]);
             emit_tc(jfar, lp.far_tc[st], P.slab_rows_far);
             open_launch(lp.fsolve[st]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
@@ -394,7 +410,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.fsolve[st]);
             open_launch(lp.bsolve[st]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t nb = std::min(kNB, s - k0);
@@ -409,7 +425,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (int32_t sb = 0; sb < nsb; ++sb) {
             const int32_t k0 = sb * kSolveBlock;
             open_launch(lp.blk_mv[sb]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t k1 = std::min(k0 + kSolveBlock, s);
@@ -417,7 +433,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.blk_mv[sb]);
             open_launch(lp.fs_upd[sb]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t k1 = std::min(k0 + kSolveBlock, s);
@@ -426,7 +442,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             }
             close_launch(lp.fs_upd[sb]);
             open_launch(lp.bs_upd[sb]);
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
                 const int32_t k1 = std::min(k0 + kSolveBlock, s);
@@ -436,7 +452,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         }
         open_launch(lp.rect);
         int64_t roff = 0, foff = 0;
-        for (int32_t js : lp.large_nodes) {
+        for (int32_t js : elim) {
             const int32_t s = P.S[js], f = P.F[js];
             if (f <= s) continue;
             const int64_t nrc = (f - s + kRectRows - 1) / kRectRows;
@@ -451,14 +467,14 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         P.fwd_entries = std::max(P.fwd_entries, foff);
         close_launch(lp.rect);
         open_launch(lp.rect_rows);
-        for (int32_t js : lp.large_nodes) {
+        for (int32_t js : elim) {
             const int32_t s = P.S[js], f = P.F[js];
             if (f > s) add_job(lp.rect_rows, Job{js, s, f, f, 0, 0, 0}, f - s);
         }
         close_launch(lp.rect_rows);
         {
             std::vector<Job> jl;
-            for (int32_t js : lp.large_nodes) {
+            for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (f > s) {
                     jl.push_back(Job{js, s, f, f, 0, s, 0});
@@ -513,7 +529,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     }
     open_launch(P.inv_blocks);
     for (int64_t js = 0; js < ns; ++js) {
-        if (P.F[js] <= kSmallMaxF) continue;
+        if (P.F[js] <= kSmallMaxF || P.retained[js]) continue;
         for (int32_t k0 = 0; k0 < P.S[js]; k0 += kSolveBlock)
             add_job(P.inv_blocks, Job{(int32_t)js, k0, std::min(k0 + kSolveBlock, P.S[js]), P.F[js], k0,
                                       std::min(k0 + kSolveBlock, P.S[js]), 0}, 1);
@@ -588,7 +604,8 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
             auto& c = cov[js];
             if (c.empty()) c.resize(F);
             for (int32_t col = 0; col < F; ++col) {
-                const int32_t want = col < S ? (col / kNB) * kNB : S;
+                // a retained front receives no update at all
+                const int32_t want = P.retained[js] ? 0 : col < S ? (col / kNB) * kNB : S;
                 auto& v = c[col];
                 std::sort(v.begin(), v.end());
                 int32_t at = 0;

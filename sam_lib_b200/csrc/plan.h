@@ -66,7 +66,8 @@ struct TcLaunch {
 
 struct LevelPlan {
     std::vector<int32_t> small_nodes;        // fronts done by the fused one-CTA kernel
-    std::vector<int32_t> large_nodes;        // fronts done by the blocked path
+    std::vector<int32_t> large_nodes;        // fronts done by the blocked path (assembly, write-back)
+    std::vector<int32_t> elim_nodes;         // of those, the ones eliminated (not retained)
     int32_t small_maxF = 0;
     // small fronts in size classes (F <= 64, 96, 128, 176), one launch each so
     // that the smaller fronts get the shared memory (and occupancy) they need:
@@ -111,6 +112,11 @@ struct Plan {
     std::vector<int64_t> lnz_off, lindx_off;
     std::vector<int32_t> child_ptr, child;   // children in SIBL order
     std::vector<int32_t> rows;               // LINDX (0-based rows), concatenated like LINDX
+    // partial factorisation (MSPAR(57) > 0): the retained supernodes
+    // (SUPSUP > 0, src/SPR/sprtrs.f:1142-1204) are assembled but not
+    // eliminated (sprfc1.f:587) and skipped by the solves (sprfs1.f:371)
+    std::vector<uint8_t> retained;
+    bool any_retained = false;
     // update-row -> parent-row maps, one per non-root supernode with F > S
     std::vector<int64_t> rel_off;            // per node, offset into rel
     std::vector<int32_t> rel;
@@ -168,7 +174,7 @@ void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps);
 // Schur-update coverage: every column c of every large front must receive
 // exactly the K ranges that tile [0, 64 floor(c / 64)) for c < S (earlier
 // panels; a column's own panel is eliminated by the diagonal block and TRSM)
-// and [0, S) for c >= S,
+// and [0, S) for c >= S (nothing for a retained front),
 // once, across the update, far and K = S launches.  Counts the columns that
 // do not, for the FP64 launch lists (fp64) and the tensor-core lists in the
 // mixed mode's use (tc: FP64 panel-chain updates + tensor-core far and K = S).

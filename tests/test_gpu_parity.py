@@ -143,12 +143,19 @@ def test_error_codes_match_oracle():
         assert np.allclose(g['tol'], o['tol'], rtol=1e-10, atol=0)
 
 
-def test_partial_factorisation_mode_is_reported():
+def test_partial_factorisation_without_retained_dofs_is_a_full_factor():
+    """MSPAR(57) = 1 on a structure without external DOFs (no SUPSUP > 0):
+    nothing is retained, so factor and solution are the full ones."""
     rs, sm = ref_system(3)
     msp = rs.mspar.copy()
     msp[56] = 1
-    g = gpu_sprsol(rs, sm, rhs(rs.neq, 1, 7), iop=1, mspar=msp)
-    assert g['ierr'] == -4
+    b = rhs(rs.neq, 1, 7)
+    o = run_sprsol('orc', rs, sm, b, mspar=msp)
+    g = gpu_sprsol(rs, sm, b, mspar=msp)
+    assert g['ierr'] == o['ierr'] == 0
+    assert np.array_equal(g['mspar'], o['mspar'])
+    assert close_factor(g['sm'], o['sm'])
+    assert relerr(g['b'], o['b']) <= 1e-9
 
 
 def test_pivot_failure_inside_a_dense_front():

@@ -69,3 +69,20 @@ def test_plan_self_check_benchmark_structures(n):
     assert out[4] == 0 and out[5] == 0
     assert out[11] == 0 and out[12] == 0
     assert abs(out[6] - st['rinfo'][2]) <= 1e-12 * st['rinfo'][2]
+
+
+@pytest.mark.parametrize('n', [6, 8])
+def test_plan_self_check_partial_factorisation(n):
+    """MSPAR(57) = 1 on a box with an external face: the retained root front
+    (small at 6^3, dense at 8^3) gets no elimination or update launches, the
+    arena stays consistent, and RINFO(3) excludes it as the reference does
+    (src/SPR/sprtrs.f:1956)."""
+    rs, _ = ref_system(n, retain=True)
+    msp = rs.mspar.copy()
+    msp[56] = 1
+    out = np.zeros(13)
+    rc = spr.load(8).spr_b200_plan_check(spr._ptr(msp), spr._ptr(rs.mtrees), spr._ptr(rs.msifa), spr._ptr(out))
+    assert rc == 0 and out[0] == 0
+    assert out[4] == 0 and out[5] == 0
+    assert out[11] == 0 and out[12] == 0
+    assert abs(out[6] - rs.rinfo[2]) <= 1e-12 * rs.rinfo[2]
