@@ -13,6 +13,10 @@
  *   SPRFC3/SPRF31/SPRF37 src/SPR/sprfc3.f:5-277, 372-806, 1011-1104
  *                                      (the variant that replaces singular
  *                                       pivots and records them in DCOR)
+ *   SPRFC2/SPRF21/SPRF27, CMVY18, CMMY18 src/SPR/sprfc2.f, cmvy18.f,
+ *                                      cmmy18.f (Cholesky C C')
+ *   SPRFS2/SPRFS7/SPRFS9, SPRBS2/SPRBS7/SPRBS9 src/SPR/sprfs2.f, sprbs2.f
+ *                                      (its forward and back solves)
  *   LMVY18  src/SPR/lmvy18.f:5-173     (column update inside SPRF17)
  *   LMMY18  src/SPR/lmmy18.f:5-192     (Schur update of the update matrix)
  *   SPRFS1/3/5/6, SPRFB1/2 src/SPR/sprfs1.f  (forward + diagonal solve)
@@ -89,8 +93,8 @@ typedef struct {
  * diagonals become 1, pivots at or below TOL(1)|a_jj| are replaced
  * (SPRF37, sprfc3.f:1083-1099), and the code is -31 with supeqt = the number
  * replaced, or 0. */
-static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
-                       I *numneg_out, I *supeqt_out, double *dcor)
+static I oracle_factor_mode(const sym_t *s, double *diag, double *lnz, double *tol,
+                            I *numneg_out, I *supeqt_out, double *dcor, int chol)
 {
     const I ns = s->nsuper;
     I numneg = 0, supeqt = 0, error = 0, nsing = 0;
@@ -170,13 +174,29 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
          * retained supernode is only assembled (sprfc1.f:587) */
         const I Se = retained(s, js) ? 0 : S;
         for (I j = 0; j < Se && error == 0; j++) {
-            for (I k = 0; k < j; k++) {
-                const double a = -(X[j + k * F] * diag[fst - 1 + k]);
+            for (I k = 0; k < j; k++) {     /* LMVY18, or CMVY18 without D */
+                const double a = chol ? -X[j + k * F] : -(X[j + k * F] * diag[fst - 1 + k]);
                 for (I i = j; i < F; i++)
                     X[i + j * F] = X[i + j * F] + a * X[i + k * F];
             }
             const double adiag = diag[fst - 1 + j];
             double d = X[j + j * F];
+            if (chol) {                  /* SPRF27, sprfc2.f:1001-1032 */
+                if (d <= tol[0] * fabs(adiag)) {
+                    error = -(j + 1);
+                    tol[1] = d;
+                    tol[2] = adiag;
+                    break;
+                }
+                const double r0 = adiag / d;
+                tol[1] = (tol[1] > r0) ? tol[1] : r0;
+                d = sqrt(d);
+                diag[fst - 1 + j] = d;
+                X[j + j * F] = d;
+                d = 1.0 / d;
+                for (I i = j + 1; i < F; i++) X[i + j * F] = X[i + j * F] * d;
+                continue;
+            }
             if (dcor) {                  /* SPRF37, sprfc3.f:1083-1099 */
                 double *dc = dcor + 2 * (fst - 1 + j);
                 if (fabs(d) <= tol[0] * fabs(adiag)) {
@@ -213,8 +233,8 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
             double *U = (double *)malloc(sizeof(double) * (size_t)(q * q));
             for (I b = 0; b < q; b++) {
                 for (I a = b; a < q; a++) U[a + b * q] = X[(S + a) + (S + b) * F];
-                for (I k = 0; k < Se; k++) {
-                    const double a1 = -(X[(S + b) + k * F] * diag[fst - 1 + k]);
+                for (I k = 0; k < Se; k++) {   /* LMMY18, or CMMY18 without D */
+                    const double a1 = chol ? -X[(S + b) + k * F] : -(X[(S + b) + k * F] * diag[fst - 1 + k]);
                     for (I a = b; a < q; a++)
                         U[a + b * q] = U[a + b * q] + a1 * X[(S + a) + k * F];
                 }
@@ -237,7 +257,10 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
         for (I i = 0; i < s->neq; i++)
             if (diag[i] > 0.0 && (mdiag == 0.0 || mdiag > diag[i])) mdiag = diag[i];
         tol[1] = (tol[1] != 0.0) ? 1.0 / tol[1] : 0.0;
-        tol[2] = (mdiag != 0.0) ? tol[2] / mdiag : 0.0;
+        if (chol)                        /* sprfc2.f:712-716 */
+            tol[2] = (mdiag != 0.0) ? tol[2] / (mdiag * mdiag) : 0.0;
+        else
+            tol[2] = (mdiag != 0.0) ? tol[2] / mdiag : 0.0;
     }
     if (dcor && nsing > 0) {             /* sprfc3.f:796-799 */
         supeqt = nsing;
@@ -248,11 +271,19 @@ static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
     return error;
 }
 
+static I oracle_factor(const sym_t *s, double *diag, double *lnz, double *tol,
+                       I *numneg_out, I *supeqt_out, double *dcor)
+{
+    return oracle_factor_mode(s, diag, lnz, tol, numneg_out, supeqt_out, dcor, 0);
+}
+
 /* ---------------------------------------------------------------------- */
 /* Solves: SPRFS3/SPRFS5/SPRFS6 and SPRBS4/SPRBS6                          */
 /* ---------------------------------------------------------------------- */
 
-static void oracle_forward(const sym_t *s, const double *lnz, double *b, double *loc)
+/* chol: the Cholesky forward solve C y = b of SPRFS9 (sprfs2.f:575-610):
+ * each column is divided by its diagonal before it updates the others. */
+static void oracle_forward(const sym_t *s, const double *lnz, double *b, double *loc, int chol)
 {
     I p0 = 0;
     for (I js = 0; js < s->nsuper; js++) {
@@ -268,6 +299,7 @@ static void oracle_forward(const sym_t *s, const double *lnz, double *b, double 
         /* column j of the packed trapezoid starts at j*F - j(j-1)/2 */
         for (I j = 0; j < S; j++) {
             const I cj = j * F - (j * (j - 1)) / 2;
+            if (chol) loc[j] = loc[j] / L[cj];
             const double x = loc[j];
             for (I i = j + 1; i < S; i++) loc[i] = loc[i] - x * L[cj + (i - j)];
         }
@@ -289,14 +321,16 @@ static void oracle_forward(const sym_t *s, const double *lnz, double *b, double 
             }
             loc[i] = y;
         }
-        for (I j = 0; j < S; j++) loc[j] = loc[j] / L[j * F - (j * (j - 1)) / 2];
+        if (!chol)
+            for (I j = 0; j < S; j++) loc[j] = loc[j] / L[j * F - (j * (j - 1)) / 2];
         for (I i = 0; i < F; i++)
             if (rows[i] <= s->neq) b[rows[i] - 1] = loc[i];
         p0 += F * S - (S * (S - 1)) / 2;
     }
 }
 
-static void oracle_backward(const sym_t *s, const double *lnz, double *b, double *loc)
+/* chol: the Cholesky back solve C' x = y of SPRBS9 (sprbs2.f:500-540). */
+static void oracle_backward(const sym_t *s, const double *lnz, double *b, double *loc, int chol)
 {
     I p0 = s->nzerol;
     for (I js = s->nsuper - 1; js >= 0; js--) {
@@ -311,7 +345,7 @@ static void oracle_backward(const sym_t *s, const double *lnz, double *b, double
             const I cj = j * F - (j * (j - 1)) / 2;
             double r = 0.0;
             for (I i = j + 1; i < F; i++) r = r + loc[i] * L[cj + (i - j)];
-            loc[j] = loc[j] - r;
+            loc[j] = chol ? (loc[j] - r) / L[cj] : loc[j] - r;
         }
         for (I i = 0; i < F; i++)
             if (rows[i] <= s->neq) b[rows[i] - 1] = loc[i];
@@ -400,7 +434,7 @@ void orc_sprfs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
         return;
     }
     double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
-    for (I r = 0; r < *nrhs; r++) oracle_forward(&s, lnz, b + r * (*ldb), loc);
+    for (I r = 0; r < *nrhs; r++) oracle_forward(&s, lnz, b + r * (*ldb), loc, 0);
     free(loc);
 }
 
@@ -426,7 +460,7 @@ void orc_sprbs1_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
         return;
     }
     double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
-    for (I r = 0; r < *nrhs; r++) oracle_backward(&s, lnz, b + r * (*ldb), loc);
+    for (I r = 0; r < *nrhs; r++) oracle_backward(&s, lnz, b + r * (*ldb), loc, 0);
     free(loc);
 }
 
@@ -440,4 +474,81 @@ void orc_sprsol_(const I *iop, I *mspar, I *mtrees, I *msifa, double *sm, double
         orc_sprfs1_(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork, rwork, lpu, ierr);
     if (*iop >= 3 && *iop != 5 && *ierr >= 0)
         orc_sprbs1_(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork, lpu, ierr);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Cholesky C C': SPRFC2, SPRFS2, SPRBS2                                    */
+/* ---------------------------------------------------------------------- */
+
+/* SPRFC2 (sprfc2.f:5-270): MSPAR(1) = 6; on an error MSPAR(27) = SUPEQT. */
+void orc_sprfc2_(I *mspar, I *mtrees, I *msifa, double *sm, double *tol,
+                 I *iwork, double *rwork, const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {                  /* sprfc2.f:123-127 */
+        mspar[0] = -6;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 6;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    I numneg = 0, supeqt = 0;
+    I lierr = oracle_factor_mode(&s, sm, sm + s.neq, tol, &numneg, &supeqt, NULL, 1);
+    if (lierr != 0) {                    /* sprfc2.f:244-255 */
+        *ierr = (lierr / 10 == -3) ? -3 : -4;
+        mspar[26] = supeqt;
+    }
+    mspar[25] = numneg;
+}
+
+/* SPRFS2 / SPRBS2 (sprfs2.f:5-265, sprbs2.f:5-250): MSPAR(1) = 8. */
+static void orc_chol_solve(int back, I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                           const I *ldb, const I *nrhs, I *ierr)
+{
+    if (mspar[0] < 0) {
+        mspar[0] = -8;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 8;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    const double *lnz = sm + s.neq;
+    if (mspar[56] == 1 && *ldb < s.neq) s.neq = *ldb;
+    if (*ldb < s.neq) {
+        mspar[0] = -2;
+        *ierr = -2;
+        return;
+    }
+    double *loc = (double *)malloc(sizeof(double) * (size_t)(s.mfront + 1));
+    for (I r = 0; r < *nrhs; r++) {
+        if (back)
+            oracle_backward(&s, lnz, b + r * (*ldb), loc, 1);
+        else
+            oracle_forward(&s, lnz, b + r * (*ldb), loc, 1);
+    }
+    free(loc);
+}
+
+void orc_sprfs2_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                 const I *ldb, const I *nrhs, I *iwork, double *rwork,
+                 const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    orc_chol_solve(0, mspar, mtrees, msifa, sm, b, ldb, nrhs, ierr);
+}
+
+void orc_sprbs2_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
+                 const I *ldb, const I *nrhs, double *rwork, const I *lpu, I *ierr)
+{
+    (void)rwork;
+    (void)lpu;
+    orc_chol_solve(1, mspar, mtrees, msifa, sm, b, ldb, nrhs, ierr);
 }

@@ -278,3 +278,111 @@ def _sprsol_ldb(which, rs, sm, b, mspar, ldb):
     f(_i(3), _p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(b), _i(ldb), _i(b.shape[1]),
       _p(tol), _p(iw), _p(rw), _i(-1), C.byref(ierr))
     return dict(sm=sm, b=b, tol=tol, ierr=ierr.value, mspar=msp)
+
+
+# ---------------------------------------------------------------------------
+# Cholesky C C' (src/SPR/sprfc2.f, sprfs2.f, sprbs2.f, cmvy18.f, cmmy18.f)
+# ---------------------------------------------------------------------------
+
+def run_chol(which, rs, sm, b, tol1=1e-12, mspar=None, ldb=None, steps='fsb'):
+    """SPRFC2 (f), SPRFS2 (s: forward) and SPRBS2 (b: back), in that order,
+    as `steps` lists them."""
+    from oracle.refpipe import lib as reflib, _p, _i
+    sm = sm.copy()
+    ldb = rs.neq if ldb is None else ldb
+    b = np.asfortranarray(b.copy())
+    nrhs = b.shape[1]
+    msp = rs.mspar.copy() if mspar is None else mspar.copy()
+    tol = np.array([tol1, 0.0, 0.0])
+    iw = np.zeros(int(rs.mspar[13]) + int(rs.mspar[12]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + int(rs.mspar[13]) + 8)
+    ierr = C.c_int64(0)
+    ierrs = []
+    R = reflib()
+    for st in steps:
+        ierr.value = 0
+        if st == 'f':
+            if which == 'ref':
+                R.sprfc2_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw), _p(rw), _i(-1),
+                          C.byref(ierr), C.cast(R.cmvy18_, C.c_void_p), C.cast(R.cmmy18_, C.c_void_p))
+            else:
+                _lib().orc_sprfc2_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw), _p(rw),
+                                   _i(-1), C.byref(ierr))
+        elif st == 's':
+            f = R.sprfs2_ if which == 'ref' else _lib().orc_sprfs2_
+            f(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(b), _i(ldb), _i(nrhs), _p(iw), _p(rw), _i(-1),
+              C.byref(ierr))
+        else:
+            f = R.sprbs2_ if which == 'ref' else _lib().orc_sprbs2_
+            f(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(b), _i(ldb), _i(nrhs), _p(rw), _i(-1),
+              C.byref(ierr))
+        ierrs.append(ierr.value)
+        if ierr.value < 0:
+            break
+    return dict(sm=sm, b=b, tol=tol, ierr=ierrs, mspar=msp)
+
+
+def _same_chol(r, o):
+    assert r['ierr'] == o['ierr']
+    for k in ('sm', 'b', 'tol', 'mspar'):
+        assert np.array_equal(r[k], o[k]), k
+
+
+@pytest.mark.parametrize('n,emod', [(3, 'uniform'), (6, 'loguniform'), (8, 'uniform')])
+def test_cholesky_bitwise_equals_reference(n, emod):
+    rs, sm = ref_system(n, emod)
+    b = rhs(rs.neq, 2, 60 + n)
+    r = run_chol('ref', rs, sm, b)
+    o = run_chol('orc', rs, sm, b)
+    _same_chol(r, o)
+    assert o['ierr'] == [0, 0, 0] and o['mspar'][0] == 8
+    K = dense_from_sm(rs, sm)
+    assert np.linalg.norm(K @ o['b'] - b) <= 1e-12 * np.linalg.norm(b)
+
+
+def test_cholesky_error_paths_match_reference():
+    rs, sm = ref_system(3)
+    b = rhs(rs.neq, 1, 61)
+    # an indefinite shift: the first non-positive pivot stops it (sprfc2.f:1001-1008)
+    from scipy.linalg import eigh
+    K = dense_from_sm(rs, sm)
+    M = np.diag(K.diagonal() - dense_from_sm(rs, shifted_sm(rs, sm, 1.0)).diagonal())
+    w = eigh(K, M, eigvals_only=True)
+    ssm = shifted_sm(rs, sm, 0.5 * (w[3] + w[4]))
+    r = run_chol('ref', rs, ssm, b, steps='f')
+    o = run_chol('orc', rs, ssm, b, steps='f')
+    _same_chol(r, o)
+    assert o['ierr'] == [-3] and o['mspar'][26] > 0 and o['tol'][1] <= 0.0
+    # an exact zero diagonal (-35: MSPAR(26) counts them, MSPAR(27) the first)
+    from sam_lib_b200.system import diag_positions
+    z = sm.copy()
+    z[diag_positions(rs.mspar, rs.mtrees, rs.msifa)[7]] = 0.0
+    r = run_chol('ref', rs, z, b, steps='f')
+    o = run_chol('orc', rs, z, b, steps='f')
+    _same_chol(r, o)
+    assert o['ierr'] == [-3] and o['mspar'][26] == 8 and o['mspar'][25] == 1
+    # preceding error not cleared
+    bad = rs.mspar.copy()
+    bad[0] = -2
+    for st in 'fsb':
+        r = run_chol('ref', rs, sm, b, mspar=bad, steps=st)
+        o = run_chol('orc', rs, sm, b, mspar=bad, steps=st)
+        _same_chol(r, o)
+        assert o['ierr'] == [-1] and o['mspar'][0] == (-6 if st == 'f' else -8)
+
+
+def test_cholesky_partial_factorisation_matches_reference():
+    rs, sm = ref_system(6, retain=True)
+    msp = rs.mspar.copy()
+    msp[56] = 1
+    first, _ = retained_info(rs)
+    b = rhs(rs.neq, 2, 62)
+    r = run_chol('ref', rs, sm, b[:first], mspar=msp, ldb=first)
+    o = run_chol('orc', rs, sm, b[:first], mspar=msp, ldb=first)
+    _same_chol(r, o)
+    K = dense_from_sm(rs, sm)
+    xi = np.linalg.solve(K[:first, :first], b[:first])
+    assert np.max(np.abs(o['b'] - xi)) <= 1e-10 * np.max(np.abs(xi))
+    r = run_chol('ref', rs, sm, b, mspar=msp, steps='fs')
+    o = run_chol('orc', rs, sm, b, mspar=msp, steps='fs')
+    _same_chol(r, o)
