@@ -48,6 +48,25 @@ void sprfc3_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double
              SPR_INT* iwork, double* rwork, double* dcor, const SPR_INT* lpu, SPR_INT* ierr,
              void (*mvmult)(), void (*mmmult)());
 
+/* Replaces SPRFC2, src/SPR/sprfc2.f:5-270 (Cholesky C C' factorisation,
+ * MSPAR(1) = 6).  A pivot d <= TOL(1)|a_jj| stops it with IERR = -3,
+ * MSPAR(27) = the equation, TOL(2) = d and TOL(3) = a_jj (sprfc2.f:1001-1008).
+ * MVMULT/MMMULT are CMVY18/CMMY18 (cmvy18.f:5, cmmy18.f:5) and are not called. */
+void sprfc2_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* tol,
+             SPR_INT* iwork, double* rwork, const SPR_INT* lpu, SPR_INT* ierr,
+             void (*mvmult)(), void (*mmmult)());
+
+/* Replaces SPRFS2, src/SPR/sprfs2.f:5-265 (forward sweep C y = b on a C C'
+ * factor, MSPAR(1) = 8). */
+void sprfs2_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
+             const SPR_INT* ldb, const SPR_INT* nrhs, SPR_INT* iwork, double* rwork,
+             const SPR_INT* lpu, SPR_INT* ierr);
+
+/* Replaces SPRBS2, src/SPR/sprbs2.f:5-250 (back sweep C' x = y, MSPAR(1) = 8). */
+void sprbs2_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
+             const SPR_INT* ldb, const SPR_INT* nrhs, double* rwork, const SPR_INT* lpu,
+             SPR_INT* ierr);
+
 /* Replaces SPRFS1, src/SPR/sprfs1.f:5-263 (forward reduction + D^-1). */
 void sprfs1_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,
              const SPR_INT* ldb, const SPR_INT* nrhs, SPR_INT* iwork, double* rwork,

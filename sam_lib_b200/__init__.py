@@ -2,12 +2,13 @@
 
 The product is the C-ABI library ``libspr_b200.so`` (built in-tree by
 ``sam_lib_b200.build``): it exports the reference's Fortran entry points
-``sprsol_``, ``sprfc1_``, ``sprfc3_``, ``sprfs1_`` and ``sprbs1_`` (INTEGER*8 ABI;
+``sprsol_``, ``sprfc1_``, ``sprfc2_``, ``sprfc3_``, ``sprfs1_``, ``sprfs2_``,
+``sprbs1_`` and ``sprbs2_`` (INTEGER*8 ABI;
 ``libspr_b200_i4.so`` has the INTEGER*4 ABI) plus a device-level API.  This
 module is the Python mirror of that interface: the same routine names,
 argument meaning and IERR conventions as src/SPR/sprsol.f, sprfc1.f,
-sprfc3.f, sprfs1.f and sprbs1.f, with numpy arrays standing in for the
-Fortran arrays.
+sprfc2.f, sprfc3.f, sprfs1.f, sprfs2.f, sprbs1.f and sprbs2.f, with numpy
+arrays standing in for the Fortran arrays.
 
 There is no CPU fallback: if the library is missing, importing the
 interface raises.
@@ -134,6 +135,40 @@ def sprfc3(mspar, mtrees, msifa, sm, tol, dcor, iwork=None, rwork=None, lpu=-1, 
     load(int_kind).sprfc3_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
                            _ptr(iwork), _ptr(rwork), _ptr(dcor), _ref(lpu, c_t), C.byref(ierr),
                            None, None)
+    return ierr.value
+
+
+def sprfc2(mspar, mtrees, msifa, sm, tol, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFC2 (src/SPR/sprfc2.f:5): Cholesky factorisation C C' of SM; returns IERR."""
+    np_t, c_t = _ints(int_kind)
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfc2_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
+                           _ptr(iwork), _ptr(rwork), _ref(lpu, c_t), C.byref(ierr), None, None)
+    return ierr.value
+
+
+def sprfs2(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFS2 (src/SPR/sprfs2.f:5): forward sweep C y = b on a C C' factor; returns IERR."""
+    np_t, c_t = _ints(int_kind)
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfs2_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(b),
+                           _ref(ldb, c_t), _ref(nrhs, c_t), _ptr(iwork), _ptr(rwork),
+                           _ref(lpu, c_t), C.byref(ierr))
+    return ierr.value
+
+
+def sprbs2(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork=None, lpu=-1, int_kind=8):
+    """SPRBS2 (src/SPR/sprbs2.f:5): back sweep C' x = y; returns IERR."""
+    _, c_t = _ints(int_kind)
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprbs2_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(b),
+                           _ref(ldb, c_t), _ref(nrhs, c_t), _ptr(rwork), _ref(lpu, c_t),
+                           C.byref(ierr))
     return ierr.value
 
 

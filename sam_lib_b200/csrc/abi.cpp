@@ -52,6 +52,7 @@ struct Ctx {
     double* d_b = nullptr;
     int64_t b_cap = 0;
     double* d_dcor = nullptr;          // SPRFC3's DCOR(2,NEQ) on the device
+    bool dev_chol = false;             // the device holds the L D L' form of a host C C' factor
     cudaStream_t stream = nullptr;
     // device factor residency
     const double* sm_host = nullptr;
@@ -192,12 +193,13 @@ int ensure_b(Ctx* c, int64_t n) {
     return 0;
 }
 
-// H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR, or
-// with dcor (host DCOR(2,NEQ)) the SPRFC3 one.
-I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nullptr) {
+// H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR, with
+// dcor (host DCOR(2,NEQ)) the SPRFC3 one, with chol the SPRFC2 one (the host
+// receives C C', the device keeps its L D L' form for the solves).
+I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nullptr, bool chol = false) {
     const int64_t neq = mspar[7], nzerol = mspar[15];
     const int64_t nsm = neq + nzerol;
-    const char* who = dcor ? "SPRFC3" : "SPRFC1";
+    const char* who = chol ? "SPRFC2" : dcor ? "SPRFC3" : "SPRFC1";
     cudaStream_t s = c->stream;
     if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return -4;
     Engine::Singular fc3{0.0, nullptr};
@@ -208,11 +210,16 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
         fc3.d_dcor = c->d_dcor;
     }
     FactorResult r;
-    if (c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr) != 0) {
+    const int frc = chol ? c->eng.factor_chol(c->d_sm, tol[0], r) : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
+    if (frc != 0) {
         msg(lpu, who, "CUDA failure in the factorisation");
         return -4;
     }
+    const bool chol_ok = chol && r.lierr == 0;
+    if (chol_ok && c->eng.chol_convert(c->d_sm, true) != 0) return -4;
     if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -4;
+    if (chol_ok && c->eng.chol_convert(c->d_sm, false) != 0) return -4;
+    c->dev_chol = chol_ok;
     if (dcor && cudaMemcpyAsync(dcor, c->d_dcor, 2 * neq * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return -4;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -4;
@@ -261,23 +268,29 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
 }
 
 // Makes the device SM hold this host SM's factor (re-uploading if needed).
-int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm) {
+// With chol the host SM is a C C' factor (SPRFC2): the device keeps its
+// L D L' form, which the Cholesky solves use with a sqrt(D) scaling.
+int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm, bool chol = false) {
     const int64_t nsm = mspar[7] + mspar[15];
-    if (c->resident && c->sm_host == sm && c->sm_fp == sm_fingerprint(sm, nsm)) return 0;
+    if (c->resident && c->sm_host == sm && c->sm_fp == sm_fingerprint(sm, nsm) && c->dev_chol == chol) return 0;
     if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return -4;
     c->eng.invalidate_factor();
+    if (chol && c->eng.chol_convert(c->d_sm, false) != 0) return -4;
+    c->dev_chol = chol;
     c->sm_host = sm;
     c->sm_fp = sm_fingerprint(sm, nsm);
     c->resident = true;
     return 0;
 }
 
-// Forward (which=1), back (2) or both (3) for B(LDB,NRHS) on the host.
-int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I nrhs, int which) {
+// Forward (which=1), back (2) or both (3) for B(LDB,NRHS) on the host; with
+// chol the C C' sweeps of SPRFS2 (which=1) or SPRBS2 (which=2).
+int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I nrhs, int which,
+             bool chol = false) {
     const int64_t neq = (mspar[56] == 1 && ldb < mspar[7]) ? (int64_t)ldb : (int64_t)mspar[7];
     if (nrhs <= 0) return 0;
-    if (ensure_factor_on_device(c, mspar, sm) != 0) return -4;
+    if (ensure_factor_on_device(c, mspar, sm, chol) != 0) return -4;
     if (ensure_b(c, (int64_t)mspar[7] * nrhs) != 0) return -4;
     cudaStream_t s = c->stream;
     const bool peri2e = mspar[57] >= 1;                 // sprfs1.f:240-250, SPRFB3/SPRFB4
@@ -309,6 +322,11 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
             cudaSuccess)
             return -4;
         if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, 2) != 0) return -4;
+    } else if (chol) {
+        // C^-1 b = D^1/2 (D^-1 L^-1 b);  C^-T y = L^-T (D^-1/2 y)
+        if (which == 2 && c->eng.scale_sqrt_d(c->d_sm, c->d_b, nfull, nrhs, true) != 0) return -4;
+        if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, which) != 0) return -4;
+        if (which == 1 && c->eng.scale_sqrt_d(c->d_sm, c->d_b, nfull, nrhs, false) != 0) return -4;
     } else if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, which) != 0) {
         return -4;
     }
@@ -407,6 +425,83 @@ void SPR_API(sprfc3_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
     }
     *ierr = do_factor(c, mspar, sm, tol, *lpu, dcor);
     if (*ierr == -4) mspar[0] = -5;
+}
+
+// SPRFC2 (src/SPR/sprfc2.f:5): Cholesky factorisation C C' of SM in place
+// (MSPAR(1) = 6).  A non-positive pivot (d <= TOL(1)|a_jj|) stops it with
+// IERR = -3 and MSPAR(27) = the equation, TOL(2) = d, TOL(3) = a_jj.
+void SPR_API(sprfc2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I* iwork, double* rwork, const I* lpu,
+                      I* ierr, void (*mvmult)(), void (*mmmult)()) {
+    (void)iwork;
+    (void)rwork;
+    (void)mvmult;   // CMVY18/CMMY18 (cmvy18.f:5, cmmy18.f:5): the GPU applies the update they define
+    (void)mmmult;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfc2.f:123-127
+        mspar[0] = -6;
+        *ierr = -1;
+        msg(*lpu, "SPRFC2", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 6;
+    *ierr = 0;
+    if (!fc1_lengths_ok(mspar)) {                       // the checks of SPRFC1
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFC2", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c) {
+        mspar[0] = -6;
+        *ierr = (err == -2) ? -2 : -4;
+        msg(*lpu, "SPRFC2", "COULD NOT SET UP THE GPU CONTEXT");
+        return;
+    }
+    *ierr = do_factor(c, mspar, sm, tol, *lpu, nullptr, true);
+    if (*ierr == -4) mspar[0] = -6;
+}
+
+// SPRFS2 / SPRBS2 (src/SPR/sprfs2.f:5, sprbs2.f:5): the forward C y = b and
+// back C' x = y sweeps on a C C' factor (MSPAR(1) = 8).
+static void chol_sweep(const char* who, int which, I* mspar, I* mtrees, I* msifa, double* sm, double* b,
+                       const I* ldb, const I* nrhs, const I* lpu, I* ierr) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfs2.f:139-143, sprbs2.f:134-138
+        mspar[0] = -8;
+        *ierr = -1;
+        msg(*lpu, who, "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 8;
+    *ierr = 0;
+    if (!solve_lengths_ok(mspar, *ldb)) {
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, who, "MTREES/MSIFA/SM/B, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, which, true) != 0) {
+        mspar[0] = -8;
+        *ierr = -4;
+        msg(*lpu, who, "GPU CHOLESKY SOLVE FAILED");
+    }
+}
+
+void SPR_API(sprfs2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb, const I* nrhs, I* iwork,
+                      double* rwork, const I* lpu, I* ierr) {
+    (void)iwork;
+    (void)rwork;
+    chol_sweep("SPRFS2", 1, mspar, mtrees, msifa, sm, b, ldb, nrhs, lpu, ierr);
+}
+
+void SPR_API(sprbs2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, const I* ldb, const I* nrhs,
+                      double* rwork, const I* lpu, I* ierr) {
+    (void)rwork;
+    chol_sweep("SPRBS2", 2, mspar, mtrees, msifa, sm, b, ldb, nrhs, lpu, ierr);
 }
 
 // SPRFS1 (src/SPR/sprfs1.f:5): forward reduction and diagonal scaling of B.

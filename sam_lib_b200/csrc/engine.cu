@@ -296,7 +296,17 @@ __global__ void k_reduce(const double* v, int64_t n, double* out) {
 // Small fronts: fused extend-add + LDL' + Schur update, one CTA per front.
 // Shared memory holds the packed lower front F(F+1)/2 plus one column.
 // ---------------------------------------------------------------------------
-template <bool FC3>
+// Pivot rules of the factorisation kernels: SPRF17's |d| <= TOL(1)|a| stops
+// (sprfc1.f:1274), SPRF37 replaces the pivot (sprfc3.f:1083), SPRF27's
+// d <= TOL(1)|a| stops the Cholesky form (sprfc2.f:1001-1008; the C C'
+// factor is formed from L D L' afterwards, see k_chol_convert).
+enum PivotRule { kPivotLDL = 0, kPivotReplace = 1, kPivotChol = 2 };
+
+__device__ __forceinline__ bool pivot_fails(int rule, double d, double ad, double tol1) {
+    return rule == kPivotChol ? d <= tol1 * fabs(ad) : fabs(d) <= tol1 * fabs(ad);
+}
+
+template <int PR>
 __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P) {
     extern __shared__ double sh[];
     if (P.st->any_fail) return;
@@ -347,11 +357,11 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
     for (int k = 0; k < (ret ? 0 : S); ++k) {
         double d = A[pk(k, k, F)];
         const double ad = P.adiag[fst + k];
-        if (FC3) {
+        if (PR == kPivotReplace) {
             const double d0 = d;
             d = fc3_pivot(P, d0, ad);
             if (tid == 0) fc3_record(P, fst + k, d0, d);
-        } else if (fabs(d) <= P.tol1 * fabs(ad)) {     // sprfc1.f:1274
+        } else if (pivot_fails(PR, d, ad, P.tol1)) {   // sprfc1.f:1274, sprfc2.f:1004
             if (tid == 0) record_fail(P, js, k, d, ad);
             failed = true;
             break;
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             A[pk(i, k, F)] = a * rd;
         }
         __syncthreads();
-        if (FC3 && tid == 0) A[pk(k, k, F)] = d;     // every thread has read the old pivot
+        if (PR == kPivotReplace && tid == 0) A[pk(k, k, F)] = d;   // every thread has read the old pivot
         for (int j = k + 1 + warp; j < F; j += nwarp) {
             const double ljk = A[pk(j, k, F)];
             double* cj = A + pk(j, j, F) - j;
@@ -478,7 +488,7 @@ __global__ void k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, 
 // rows i = tx + 16a and columns j = ty + 16b of the block; right-looking with
 // the unscaled column (a_ij -= a_ik * a_jk / d_k), scaled to L at the end.
 // Also forms X = L11^-1 (unit lower) for the panel TRSM and the solves.
-template <bool FC3>
+template <int PR>
 __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     // Register-resident: thread (tx, ty) keeps entries (tx + 16a, ty + 16b) of
     // the block in v[a][b] through the elimination and of X = L^-1 in x[a][b]
@@ -521,7 +531,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
 #pragma unroll
                 for (int b = 1; b < R; ++b)
                     if (b == kb) c = v[a][b];
-                if (FC3 && i == k) {
+                if (PR == kPivotReplace && i == k) {
                     const double c0 = c;
                     c = fc3_pivot(P, c0, adv[k]);
                     fc3_record(P, fst + k0 + k, c0, c);
@@ -535,7 +545,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         }
         __syncthreads();
         const double d = vec[buf][k];
-        if (!FC3 && fabs(d) <= P.tol1 * fabs(adv[k])) {
+        if (PR != kPivotReplace && pivot_fails(PR, d, adv[k], P.tol1)) {
             failed = k;
             if (tid == 0) record_fail(P, js, k0 + k, d, adv[k]);
             break;
@@ -578,7 +588,8 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
 #pragma unroll
         for (int b = 0; b < R; ++b) {
             const int i = tx + 16 * a, j = ty + 16 * b;
-            if (i >= j && i < nb && j < nb) A[i][j] = (i > j) ? v[a][b] * rdv[j] : (FC3 ? dd[j] : v[a][b]);
+            if (i >= j && i < nb && j < nb)
+                A[i][j] = (i > j) ? v[a][b] * rdv[j] : (PR == kPivotReplace ? dd[j] : v[a][b]);
         }
     __syncthreads();
     // X = L^-1 by a column sweep: X = I, then at step m every X[i][j] with
@@ -1789,6 +1800,51 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
 }
 
 // ---------------------------------------------------------------------------
+// Cholesky form (SPRFC2, src/SPR/sprfc2.f:1013-1032): column j of C is
+// L(:, j) sqrt(d_j) with sqrt(d_j) on the diagonal and in D; back again, d_j =
+// c_jj^2 and L(:, j) = C(:, j) / c_jj.  Retained fronts are left as assembled.
+// One CTA per supernode, one warp per column of the packed trapezoid.
+// ---------------------------------------------------------------------------
+template <bool TO_CHOL>
+__global__ void k_chol_convert(PV P, int64_t nsuper) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int64_t js = blockIdx.x; js < nsuper; js += gridDim.x) {
+        if (is_retained(P, (int)js)) continue;
+        const int S = P.S[js], F = P.F[js], fst = P.fst[js];
+        double* base = P.lnz + P.lnz_off[js];
+        for (int j = warp; j < S; j += nwarp) {
+            double* col = base + lnz_col(j, F);          // col[0] is the diagonal
+            const double x = col[0];
+            const double diag = TO_CHOL ? sqrt(x) : x * x;
+            const double sc = TO_CHOL ? diag : 1.0 / x;
+            for (int i = 1 + lane; i < F - j; i += 32) col[i] *= sc;
+            __syncwarp();
+            if (lane == 0) {
+                col[0] = diag;
+                P.dvec[fst + j] = diag;
+            }
+        }
+    }
+}
+
+// b(i, r) times sqrt(d_i) (divide = 0) or divided by it, where d_i > 0:
+// C^-1 b = D^1/2 (D^-1 L^-1 b) after the L D L' forward sweep, and
+// C^-T y = L^-T (D^-1/2 y) before the back sweep (SPRFS9/SPRBS9,
+// sprfs2.f:575-610, sprbs2.f:500-540, with C = L D^1/2).
+__global__ void k_scale_sqrt_d(const double* dvec, double* b, int64_t ldb, int64_t n, int64_t nrhs, int divide) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * nrhs;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, r = e / n;
+        const double d = dvec[i];
+        if (d > 0.0) {
+            const double sq = sqrt(d);
+            double* x = b + i + r * ldb;
+            *x = divide ? *x / sq : *x * sq;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Residual of the FP64 matrix for iterative refinement (the product SPRPRQ
 // forms from the packed pattern, src/SPR/sprprm.f:243-325): the nonzeros of
 // the assembled LNZ are compacted once into a full symmetric CSR with rows
@@ -2017,8 +2073,9 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
     const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + kSmallMaxF) * sizeof(double);
     if ((size_t)smem_max < need) return -4;
-    CK(cudaFuncSetAttribute(k_small_front<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-    CK(cudaFuncSetAttribute(k_small_front<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<kPivotLDL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<kPivotReplace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<kPivotChol>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
@@ -2185,10 +2242,13 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             for (const LevelPlan::SmallClass& c : lp.small_classes) {
                 const int F = c.maxF;
                 const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
+                const int32_t* nodes = D.level_nodes + D.small_begin[L] + c.begin;
                 if (pv.fc3)
-                    k_small_front<true><<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
+                    k_small_front<kPivotReplace><<<c.count, 256, smem, s>>>(nodes, pv);
+                else if (chol_)
+                    k_small_front<kPivotChol><<<c.count, 256, smem, s>>>(nodes, pv);
                 else
-                    k_small_front<false><<<c.count, 256, smem, s>>>(D.level_nodes + D.small_begin[L] + c.begin, pv);
+                    k_small_front<kPivotLDL><<<c.count, 256, smem, s>>>(nodes, pv);
                 ++timing.launches;
             }
         }
@@ -2206,9 +2266,11 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             const Launch& pl = lp.panel[st];
             mark(3);
             if (pv.fc3)
-                k_diag<true><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+                k_diag<kPivotReplace><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+            else if (chol_)
+                k_diag<kPivotChol><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             else
-                k_diag<false><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+                k_diag<kPivotLDL><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             ++timing.launches;
             if (pl.ntasks > 0) {
                 mark(4);
@@ -2295,7 +2357,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     // the legacy default stream cannot be captured: graphs need a stream of our own
     const bool graph = use_graphs_ && !profile_ && s != nullptr;
     if (graph) {
-        const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_,
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_ | (chol_ ? 16 : 0),
                            (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
@@ -2385,6 +2447,39 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     res.numneg = hs.numneg;
     res.tol2 = (hs.tol2 != 0.0) ? 1.0 / hs.tol2 : 0.0;          // sprfc1.f:699-703
     res.tol3 = (hs.mindpos != 0.0) ? hs.trace / hs.mindpos : 0.0;  // sprfc1.f:704-708
+    if (chol_) {                                                   // sprfc2.f:699-716
+        const double m = std::sqrt(hs.mindpos);
+        res.tol3 = (m != 0.0) ? hs.trace / (m * m) : 0.0;
+    }
+    return 0;
+}
+
+int Engine::factor_chol(double* d_sm, double tol1, FactorResult& res) {
+    chol_ = true;
+    const int rc = factor(d_sm, tol1, res, nullptr);
+    chol_ = false;
+    return rc;
+}
+
+int Engine::chol_convert(double* d_sm, bool to_chol) {
+    Dev& D = *d_;
+    PV pv = make_view(D, P_, d_sm, 0.0);
+    const int grid = (int)std::min<int64_t>(P_.nsuper, 8 * (int64_t)std::max(sm_count_, 1));
+    if (to_chol)
+        k_chol_convert<true><<<grid, 256, 0, stream_>>>(pv, P_.nsuper);
+    else
+        k_chol_convert<false><<<grid, 256, 0, stream_>>>(pv, P_.nsuper);
+    CK(cudaGetLastError());
+    linv_valid_ = false;
+    return 0;
+}
+
+int Engine::scale_sqrt_d(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, bool divide) {
+    const int64_t n = P_.neq * nrhs;
+    if (n <= 0) return 0;
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 8 * (int64_t)std::max(sm_count_, 1));
+    k_scale_sqrt_d<<<grid, 256, 0, stream_>>>(d_sm, d_b, ldb, P_.neq, nrhs, divide ? 1 : 0);
+    CK(cudaGetLastError());
     return 0;
 }
 
@@ -2696,7 +2791,7 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     pv.tol1 = tol1;
     for (int64_t stp = 0; stp < nblk; ++stp) {
         const StepJobs& sj = steps[stp];
-        k_diag<false><<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
+        k_diag<kPivotLDL><<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
         if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, nullptr, pv);
         if (sj.upd_tasks > 0)
             K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, nullptr,

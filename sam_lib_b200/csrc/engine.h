@@ -57,6 +57,15 @@ public:
         double* d_dcor;
     };
     int factor(double* d_sm, double tol1, FactorResult& res, const Singular* fc3);
+    // SPRFC2 semantics (src/SPR/sprfc2.f:276-725): the pivot test is SPRF27's
+    // d <= TOL(1)|a_jj| (a non-positive pivot stops) and TOL(3) is
+    // trace / min(sqrt d)^2.  The device SM is left in L D L' form; chol_convert
+    // turns it into the C C' form (C = L D^1/2, sqrt d in D) and back.
+    int factor_chol(double* d_sm, double tol1, FactorResult& res);
+    int chol_convert(double* d_sm, bool to_chol);
+    // b (device, ldb x nrhs, the first NEQ rows) times sqrt(d), or divided by
+    // it, for every equation with d > 0 (d = the D part of an L D L' device SM)
+    int scale_sqrt_d(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, bool divide);
     // Device-resident forward (which=1), back (which=2) or both (3) on b (device, ldb x nrhs).
     int solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which);
     // Iterative refinement (mixed precision): build_residual() compacts the
@@ -118,6 +127,7 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     int mixed_ = 0;
+    bool chol_ = false;                      // factor with SPRF27's pivot rule
     double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
     int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
     std::vector<std::pair<int, cudaEvent_t>> marks_;
