@@ -177,10 +177,18 @@ bool fc1_lengths_ok(const I* mspar) {
     return !(iwused > niwork || mtused > ntrees || mlused > nmsifa || smused > nsm || rwused > nrwork);
 }
 
+// Reference length checks of the solves (src/SPR/sprfs1.f:147-226,
+// sprbs1.f:141-215; SPRFS2/SPRBS2 the same): MTREES and MSIFA must hold what
+// MSPAR says they hold, and LDB >= NEQ (NEQ = LDB when MSPAR(57) = 1).
 bool solve_lengths_ok(const I* mspar, I ldb) {
+    const int64_t nsuper = mspar[10], nb = mspar[11], nofsub = mspar[14], nelact = mspar[18];
+    const int64_t nmsifa = mspar[2], ntrees = mspar[3];
+    const int64_t supsup = mspar[45] + nsuper + 1, elseq = supsup + nsuper, xelseq = elseq + nelact;
+    const int64_t mtused = xelseq + nb + 1 + nb;
+    const int64_t mlused = mspar[46] + nofsub - 1;
     int64_t neq = mspar[7];
     if (mspar[56] == 1 && ldb < neq) neq = ldb;   // sprfs1.f:201
-    return ldb >= neq;
+    return !(mtused > ntrees || mlused > nmsifa || ldb < neq);
 }
 
 int ensure_b(Ctx* c, int64_t n) {

@@ -86,3 +86,58 @@ def test_plan_self_check_partial_factorisation(n):
     assert out[4] == 0 and out[5] == 0
     assert out[11] == 0 and out[12] == 0
     assert abs(out[6] - rs.rinfo[2]) <= 1e-12 * rs.rinfo[2]
+
+
+def test_length_checks_match_reference_without_a_gpu():
+    """MSPAR claiming a shorter MTREES or MSIFA than the structure needs, or
+    LDB < NEQ, gives IERR = -2 and MSPAR(1) = -2 from every entry point, as
+    from the reference (src/SPR/sprfc1.f:205-236, sprfs1.f:203-226,
+    sprbs1.f:191-215, sprfc2.f, sprfs2.f, sprbs2.f, sprfc3.f:209-234); the
+    checks come before any device work."""
+    from oracle.refpipe import lib as reflib, _p, _i
+    rs, sm = ref_system(3)
+    R = reflib()
+    b = np.asfortranarray(np.ones((rs.neq, 1)))
+    iw = np.zeros(int(rs.mspar[13]) + int(rs.mspar[12]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + int(rs.mspar[13]) + 8)
+    dcor = np.zeros(2 * rs.neq)
+    # MSPAR(4) = NTREES one short; MSPAR(3) = NMSIFA one short of what the
+    # factorisation uses (SPLIT + NBLOCK) or of what the solves use (LINDX + NOFSUB - 1)
+    mlused_solve = int(rs.mspar[46] + rs.mspar[14] - 1)
+    cases = [(3, lambda name: rs.mspar[3] - 1),
+             (2, lambda name: rs.mspar[2] - 1 if name.startswith('sprfc') else mlused_solve - 1)]
+    for slot, short in cases:
+        for name in ('sprfc1', 'sprfc2', 'sprfc3', 'sprfs1', 'sprbs1', 'sprfs2', 'sprbs2'):
+            msp = rs.mspar.copy()
+            msp[slot] = short(name)
+            mr, mg = msp.copy(), msp.copy()
+            er, eg = C.c_int64(0), None
+            tol = np.array([1e-12, 0.0, 0.0, 1.0])
+            if name in ('sprfc1', 'sprfc2'):
+                mv = R.cmvy18_ if name == 'sprfc2' else R.lmvy18_
+                mm = R.cmmy18_ if name == 'sprfc2' else R.lmmy18_
+                getattr(R, name + '_')(_p(mr), _p(rs.mtrees), _p(rs.msifa), _p(sm.copy()), _p(tol), _p(iw),
+                                       _p(rw), _i(-1), C.byref(er), C.cast(mv, C.c_void_p),
+                                       C.cast(mm, C.c_void_p))
+                eg = getattr(spr, name)(mg, rs.mtrees, rs.msifa, sm.copy(), tol.copy())
+            elif name == 'sprfc3':
+                R.sprfc3_(_p(mr), _p(rs.mtrees), _p(rs.msifa), _p(sm.copy()), _p(tol), _p(iw), _p(rw),
+                          _p(dcor), _i(-1), C.byref(er), C.cast(R.lmvy18_, C.c_void_p),
+                          C.cast(R.lmmy18_, C.c_void_p))
+                eg = spr.sprfc3(mg, rs.mtrees, rs.msifa, sm.copy(), tol.copy(), dcor.copy())
+            elif name in ('sprfs1', 'sprfs2'):
+                getattr(R, name + '_')(_p(mr), _p(rs.mtrees), _p(rs.msifa), _p(sm.copy()), _p(b.copy()),
+                                       _i(rs.neq), _i(1), _p(iw), _p(rw), _i(-1), C.byref(er))
+                eg = getattr(spr, name)(mg, rs.mtrees, rs.msifa, sm.copy(), b.copy(), rs.neq, 1)
+            else:
+                getattr(R, name + '_')(_p(mr), _p(rs.mtrees), _p(rs.msifa), _p(sm.copy()), _p(b.copy()),
+                                       _i(rs.neq), _i(1), _p(rw), _i(-1), C.byref(er))
+                eg = getattr(spr, name)(mg, rs.mtrees, rs.msifa, sm.copy(), b.copy(), rs.neq, 1)
+            assert er.value == eg == -2, (name, slot, er.value, eg)
+            assert mr[0] == mg[0] == -2, (name, slot)
+    # LDB < NEQ without a partial factorisation
+    for name in ('sprfs1', 'sprbs1', 'sprfs2', 'sprbs2'):
+        mg = rs.mspar.copy()
+        bs = np.asfortranarray(np.ones((rs.neq - 1, 1)))
+        eg = getattr(spr, name)(mg, rs.mtrees, rs.msifa, sm.copy(), bs, rs.neq - 1, 1)
+        assert eg == -2 and mg[0] == -2, name
