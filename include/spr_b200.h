@@ -151,7 +151,9 @@ int spr_b200_tc_stats(void* handle, double* out);
 int spr_b200_set_profile(void* handle, int on);
 /* Host-only plan build + self-check (no GPU needed).  out (13 doubles):
  * [0] build status [1] NSUPER [2] tree levels [3] front arena doubles
- * [4] buffers outside the arena [5] overlapping live buffers [6] RINFO(3)
+ * [4] buffers outside the arena plus relative-index (SPRF12 LINDEX) and
+ * contribution-list entries out of range or not used exactly once
+ * [5] overlapping live buffers [6] RINFO(3)
  * [7] solve flops per RHS [8] small fronts [9] large fronts [10] jobs
  * [11] columns whose FP64 Schur-update K ranges do not tile the earlier
  * panels (all S columns, for update columns) exactly once [12] the same for

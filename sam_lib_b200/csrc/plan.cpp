@@ -551,6 +551,36 @@ void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps) {
     const int64_t ns = P.nsuper;
     for (int64_t js = 0; js < ns; ++js)
         if (P.buf_off[js] < 0 || P.buf_off[js] + buffer_doubles(P, js) > P.arena_doubles) ++oob;
+    // index maps: a child's relative rows (SPRF12's LINDEX) lie in [0, F_p)
+    // of its parent's rows, strictly increasing, and its column t lands in
+    // parent column rel[t] exactly once in the contribution lists
+    std::vector<int64_t> seen(P.rel.size(), 0);
+    for (int64_t c = 0; c < ns; ++c) {
+        const int32_t q = P.F[c] - P.S[c];
+        if (q <= 0) continue;
+        const int32_t p = P.parent[c];
+        if (p < 0 || P.rel_off[c] < 0 || P.rel_off[c] + q > (int64_t)P.rel.size()) {
+            ++oob;
+            continue;
+        }
+        for (int32_t t = 0; t < q; ++t) {
+            const int32_t r = P.rel[P.rel_off[c] + t];
+            if (r < 0 || r >= P.F[p] || (t > 0 && r <= P.rel[P.rel_off[c] + t - 1])) ++oob;
+        }
+    }
+    for (int64_t p = 0; p < ns; ++p)
+        for (int32_t j = 0; j < P.F[p]; ++j)
+            for (int64_t e = P.cptr[P.rbase[p] + j]; e < P.cptr[P.rbase[p] + j + 1]; ++e) {
+                const int32_t c = P.cchild[e], t = P.ct[e];
+                if (c < 0 || c >= ns || P.parent[c] != p || t < 0 || t >= P.F[c] - P.S[c] ||
+                    P.rel[P.rel_off[c] + t] != j) {
+                    ++oob;
+                    continue;
+                }
+                ++seen[P.rel_off[c] + t];
+            }
+    for (int64_t k = 0; k < (int64_t)seen.size(); ++k)
+        if (seen[k] != 1) ++oob;
     const int32_t nlev = (int32_t)P.levels.size();
     std::vector<std::vector<int32_t>> live(nlev);
     for (int64_t js = 0; js < ns; ++js) {

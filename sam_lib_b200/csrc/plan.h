@@ -168,8 +168,10 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
 
 // Size in doubles of a node's device buffer (update matrix or dense front).
 int64_t buffer_doubles(const Plan& P, int64_t js);
-// Self-check of the arena layout: counts buffers outside the arena and
-// overlaps between buffers that are live at the same level.
+// Self-check of the arena layout and the index maps: counts buffers outside
+// the arena plus relative-index / contribution-list entries out of range or
+// not used exactly once (oob), and overlaps between buffers that are live at
+// the same level.
 void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps);
 // Schur-update coverage: every column c of every large front must receive
 // exactly the K ranges that tile [0, 64 floor(c / 64)) for c < S (earlier

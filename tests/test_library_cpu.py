@@ -38,7 +38,7 @@ def test_plan_self_check(n):
                                          out.ctypes.data_as(C.c_void_p))
     assert rc == 0 and out[0] == 0
     assert out[1] == rs.mspar[10]                 # NSUPER
-    assert out[4] == 0, 'buffers outside the arena'
+    assert out[4] == 0, 'buffers outside the arena or index-map entries out of range'
     assert out[5] == 0, 'live buffers overlap'
     assert abs(out[6] - rs.rinfo[2]) <= 1e-12 * rs.rinfo[2]   # RINFO(3)
     assert out[11] == 0 and out[12] == 0, 'Schur-update K ranges do not tile every column exactly once'
