@@ -654,4 +654,150 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Stream-schedule check of the factorisation (a race detector on the host).
+//
+// Replays the launch order of the factorisation of every level: per panel
+// step the diagonal block + TRSM and the panel-chain updates on the main
+// stream; at the end of a super-panel the far columns' update on the side
+// stream, forked by an event after the step's TRSM and joined before the
+// next trailing update (every kSuperPanel / kNB steps) and before the K = S
+// update.  Vector clocks give the happens-before order of the two streams.
+// Per large front it counts
+//   * a panel whose columns have not received exactly the K ranges [0, k0)
+//     from updates ordered before it, or that an unordered update writes;
+//   * an update whose K panel columns are not final (diagonal block + TRSM
+//     ordered before it);
+//   * two updates on different streams that write a common element unordered;
+//   * an update of the S columns not ordered before the write-back.
+// tc: the far and K = S updates take the tensor-core path (split + product on
+// the same stream as the FP64 launch they replace).  skip_join drops the
+// joins, which must make the check fail wherever far launches exist.
+// ---------------------------------------------------------------------------
+namespace {
+struct SchedOp {
+    int stream;                      // 0 main, 1 side
+    int64_t vc[2];                   // vector clock after the op
+    int32_t c0, c_end, r0, r_end;    // written block (columns, rows)
+    int32_t k_lo, k_hi;              // K range applied (updates)
+    int kind;                        // 0 panel, 1 update, 2 write-back
+};
+bool hb(const SchedOp& a, const SchedOp& b) { return a.vc[a.stream] <= b.vc[a.stream]; }
+}  // namespace
+
+int64_t check_schedule(const Plan& P, bool tc, bool skip_join) {
+    int64_t bad = 0;
+    for (const LevelPlan& lp : P.levels) {
+        if (lp.elim_nodes.empty()) continue;
+        std::map<int32_t, std::vector<SchedOp>> ops;     // per front, in issue order
+        int64_t vc_main[2] = {0, 0}, vc_side[2] = {0, 0};
+        int64_t far_done[2] = {-1, -1};
+        auto issue = [&](int stream, const Job& j, int kind) {
+            int64_t* vc = stream == 0 ? vc_main : vc_side;
+            ++vc[stream];
+            SchedOp o;
+            o.stream = stream;
+            o.vc[0] = vc[0];
+            o.vc[1] = vc[1];
+            o.kind = kind;
+            o.k_lo = j.k_lo;
+            o.k_hi = j.k_hi;
+            if (kind == 0) {                              // panel: columns [k_lo, k_hi), rows to F
+                o.c0 = j.k_lo;
+                o.c_end = j.k_hi;
+                o.r0 = j.k_lo;
+                o.r_end = j.r_end;
+            } else if (kind == 1) {
+                o.c0 = j.c0;
+                o.c_end = j.c_end;
+                o.r0 = j.c0;
+                o.r_end = j.r_end;
+            } else {
+                o.c0 = 0;
+                o.c_end = j.c_end;
+                o.r0 = 0;
+                o.r_end = j.r_end;
+            }
+            ops[j.node].push_back(o);
+        };
+        auto issue_launch = [&](int stream, const Launch& l, int kind) {
+            for (int64_t k = 0; k < l.job_count; ++k) issue(stream, P.jobs[l.job_begin + k], kind);
+        };
+        auto wait = [&](int64_t* dst, const int64_t* ev) {
+            dst[0] = std::max(dst[0], ev[0]);
+            dst[1] = std::max(dst[1], ev[1]);
+        };
+        auto join = [&]() {
+            if (far_done[0] >= 0 && !skip_join) wait(vc_main, far_done);
+            far_done[0] = far_done[1] = -1;
+        };
+        for (size_t st = 0; st < lp.panel.size(); ++st) {
+            issue_launch(0, lp.panel[st], 0);
+            const bool has_far = tc ? !lp.far_tc[st].empty() : !lp.far[st].empty();
+            if (has_far) wait(vc_side, vc_main);         // fork after the step's TRSM
+            if ((st + 1) % (kSuperPanel / kNB) == 0) join();
+            for (const Launch& ul : lp.update[st]) issue_launch(0, ul, 1);
+            if (has_far) {
+                if (tc)
+                    for (const TcLaunch& t : lp.far_tc[st]) issue_launch(1, t.gemm, 1);
+                else
+                    for (const Launch& fl : lp.far[st]) issue_launch(1, fl, 1);
+                far_done[0] = vc_side[0];
+                far_done[1] = vc_side[1];
+            }
+        }
+        join();
+        if (tc)
+            for (const TcLaunch& t : lp.outer_tc) issue_launch(0, t.gemm, 1);
+        else
+            for (const Launch& ol : lp.outer) issue_launch(0, ol, 1);
+        for (int32_t js : lp.elim_nodes) issue(0, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, 2);
+        for (auto& kv : ops) {
+            const std::vector<SchedOp>& v = kv.second;
+            for (size_t a = 0; a < v.size(); ++a) {
+                const SchedOp& A = v[a];
+                if (A.kind == 0) {
+                    // columns [k0, k0 + nb): K coverage [0, k0) from updates ordered before
+                    for (int32_t c = A.c0; c < A.c_end; ++c) {
+                        std::vector<std::pair<int32_t, int32_t>> iv;
+                        for (const SchedOp& U : v) {
+                            if (U.kind != 1 || c < U.c0 || c >= U.c_end) continue;
+                            if (!hb(U, A)) {
+                                ++bad;
+                                continue;
+                            }
+                            iv.emplace_back(U.k_lo, U.k_hi);
+                        }
+                        std::sort(iv.begin(), iv.end());
+                        int32_t at = 0;
+                        bool ok = true;
+                        for (const auto& x : iv) {
+                            if (x.first != at) ok = false;
+                            at = x.second;
+                        }
+                        if (!ok || at != A.c0) ++bad;
+                    }
+                } else if (A.kind == 1) {
+                    // its K panel columns are final before it
+                    for (const SchedOp& Q : v)
+                        if (Q.kind == 0 && Q.c0 < A.k_hi && A.k_lo < Q.c_end && !hb(Q, A)) ++bad;
+                    // no unordered writer of a common element on the other stream
+                    for (size_t b = a + 1; b < v.size(); ++b) {
+                        const SchedOp& B = v[b];
+                        if (B.kind != 1 || B.stream == A.stream) continue;
+                        const bool cols = A.c0 < B.c_end && B.c0 < A.c_end;
+                        const bool rows = A.r0 < B.r_end && B.r0 < A.r_end;
+                        if (cols && rows && !hb(A, B) && !hb(B, A)) ++bad;
+                    }
+                } else {
+                    for (const SchedOp& U : v)
+                        if (U.kind == 1 && U.c0 < A.c_end && !hb(U, A)) ++bad;
+                }
+            }
+        }
+    }
+    return bad;
+}
+
 }  // namespace sprb

@@ -181,5 +181,11 @@ void check_plan(const Plan& P, int64_t& oob, int64_t& overlaps);
 // do not, for the FP64 launch lists (fp64) and the tensor-core lists in the
 // mixed mode's use (tc: FP64 panel-chain updates + tensor-core far and K = S).
 void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc);
+// Happens-before check of the factorisation's two-stream launch schedule
+// (panels, panel-chain and far updates, K = S update, write-back): the number
+// of ordering violations, 0 for a race-free schedule.  tc: the far and K = S
+// updates on the tensor-core path; skip_join: the schedule without its
+// side-stream joins (a self-test: must report violations where far launches exist).
+int64_t check_schedule(const Plan& P, bool tc, bool skip_join);
 
 }  // namespace sprb

@@ -141,3 +141,32 @@ def test_length_checks_match_reference_without_a_gpu():
         bs = np.asfortranarray(np.ones((rs.neq - 1, 1)))
         eg = getattr(spr, name)(mg, rs.mtrees, rs.msifa, sm.copy(), bs, rs.neq - 1, 1)
         assert eg == -2 and mg[0] == -2, name
+
+
+@pytest.mark.parametrize('which', ['box12', 'gold24', 'gold48', 'retained8'])
+def test_factor_stream_schedule_is_race_free(which):
+    """Happens-before replay of the factorisation's two-stream schedule (the
+    far trailing updates on a side stream, forked and joined by events): no
+    panel starts before its columns have all their earlier updates, no update
+    reads a panel that is not final, no two unordered launches write a common
+    element, in the FP64 and the tensor-core form.  Without the joins the same
+    check must fail wherever far launches exist (a self-test of the check)."""
+    from sam_lib_b200.system import load_structure
+    if which == 'box12':
+        rs, _ = ref_system(12)
+        ms, mt, mf = rs.mspar, rs.mtrees, rs.msifa
+    elif which == 'retained8':
+        rs, _ = ref_system(8, retain=True)
+        ms, mt, mf = rs.mspar.copy(), rs.mtrees, rs.msifa
+        ms[56] = 1
+    else:
+        st = load_structure(int(which[4:]))
+        ms, mt, mf = st['mspar'], st['mtrees'], st['msifa']
+    out = np.zeros(4)
+    rc = spr.load(8).spr_b200_schedule_check(spr._ptr(ms), spr._ptr(mt), spr._ptr(mf), spr._ptr(out))
+    assert rc == 0
+    assert out[0] == 0 and out[1] == 0, 'ordering violations in the factor schedule'
+    if out[3] > 0:
+        assert out[2] > 0, 'the check does not see the missing joins'
+    if which.startswith('gold'):
+        assert out[3] > 0
