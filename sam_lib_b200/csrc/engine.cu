@@ -19,6 +19,7 @@
 // update), all fronts of the level batched into each launch.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -40,6 +41,12 @@ namespace sprb {
     } while (0)
 
 constexpr int kMaxRHS = 16;          // right-hand sides per solve pass
+
+// NVTX range for the host timeline of a profiler (no-op without one).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 // ---------------------------------------------------------------------------
 // Device views
@@ -2235,8 +2242,11 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
     k_prepass<<<(int)std::min<int64_t>((P_.nsuper * 32 + 255) / 256, 4736), 256, 0, s>>>(pv, P_.nsuper);
     k_reduce<false><<<1, 1024, 0, s>>>(D.adiag, P_.neq, &D.st->trace);
     timing.launches += 2;
+    char lname[48];
     for (size_t L = 0; L < P_.levels.size(); ++L) {
         const LevelPlan& lp = P_.levels[L];
+        snprintf(lname, sizeof lname, "factor level %zu", L);
+        NvtxRange level_range(lname);
         if (!lp.small_nodes.empty()) {
             mark(1);
             for (const LevelPlan::SmallClass& c : lp.small_classes) {
@@ -2329,6 +2339,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
 }
 
 int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular* fc3) {
+    NvtxRange range("spr_b200 factor");
     Dev& D = *d_;
     cudaStream_t s = stream_;
     PV pv = make_view(D, P_, d_sm, tol1);
@@ -2621,6 +2632,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
 }
 
 int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, int which) {
+    NvtxRange range("spr_b200 solve");
     Dev& D = *d_;
     cudaStream_t s = stream_;
     PV pv = make_view(D, P_, const_cast<double*>(d_sm), 0.0);
