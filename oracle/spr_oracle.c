@@ -17,6 +17,7 @@
  *                                      cmmy18.f (Cholesky C C')
  *   SPRFS2/SPRFS7/SPRFS9, SPRBS2/SPRBS7/SPRBS9 src/SPR/sprfs2.f, sprbs2.f
  *                                      (its forward and back solves)
+ *   SPRFC4/SPRF41/SPRF47 src/SPR/sprfc4.f (the Cholesky form of SPRFC3)
  *   LMVY18  src/SPR/lmvy18.f:5-173     (column update inside SPRF17)
  *   LMMY18  src/SPR/lmmy18.f:5-192     (Schur update of the update matrix)
  *   SPRFS1/3/5/6, SPRFB1/2 src/SPR/sprfs1.f  (forward + diagonal solve)
@@ -181,13 +182,32 @@ static I oracle_factor_mode(const sym_t *s, double *diag, double *lnz, double *t
             }
             const double adiag = diag[fst - 1 + j];
             double d = X[j + j * F];
-            if (chol) {                  /* SPRF27, sprfc2.f:1001-1032 */
+            if (chol && dcor) {          /* SPRF47, sprfc4.f:978-996 */
+                double *dc = dcor + 2 * (fst - 1 + j);
+                if (d < -tol[0] * fabs(adiag)) {
+                    error = -(j + 1);
+                    tol[1] = d;
+                    tol[2] = adiag;
+                    dc[0] = d;
+                    dc[1] = d;
+                    break;
+                } else if (d <= tol[0] * fabs(adiag)) {
+                    nsing++;
+                    dc[0] = d;
+                    const double m = fabs(tol[3] * adiag);
+                    d = tol[0] * (m > 1.0 ? m : 1.0);
+                    X[j + j * F] = d;
+                    dc[1] = d;
+                }
+            } else if (chol) {           /* SPRF27, sprfc2.f:1001-1032 */
                 if (d <= tol[0] * fabs(adiag)) {
                     error = -(j + 1);
                     tol[1] = d;
                     tol[2] = adiag;
                     break;
                 }
+            }
+            if (chol) {
                 const double r0 = adiag / d;
                 tol[1] = (tol[1] > r0) ? tol[1] : r0;
                 d = sqrt(d);
@@ -223,7 +243,7 @@ static I oracle_factor_mode(const sym_t *s, double *diag, double *lnz, double *t
         }
         if (error != 0) {
             supeqt = fst - error - 1;
-            error = -30;
+            error = (chol && dcor) ? -32 : -30;   /* sprfc4.f:612-616 */
             free(X);
             break;
         }
@@ -262,9 +282,9 @@ static I oracle_factor_mode(const sym_t *s, double *diag, double *lnz, double *t
         else
             tol[2] = (mdiag != 0.0) ? tol[2] / mdiag : 0.0;
     }
-    if (dcor && nsing > 0) {             /* sprfc3.f:796-799 */
+    if (dcor && nsing > 0) {             /* sprfc3.f:796-799, sprfc4.f:719-722 */
         supeqt = nsing;
-        error = -31;
+        error = chol ? -33 : -31;
     }
     *numneg_out = numneg;
     *supeqt_out = supeqt;
@@ -551,4 +571,31 @@ void orc_sprbs2_(I *mspar, I *mtrees, I *msifa, double *sm, double *b,
     (void)rwork;
     (void)lpu;
     orc_chol_solve(1, mspar, mtrees, msifa, sm, b, ldb, nrhs, ierr);
+}
+
+/* SPRFC4 (sprfc4.f:5-262): the Cholesky form of SPRFC3.  IERR -3 with
+ * MSPAR(27) = -(number replaced) leaves a complete factor; a pivot below
+ * -TOL(1)|a_jj| stops it with MSPAR(27) = the equation. */
+void orc_sprfc4_(I *mspar, I *mtrees, I *msifa, double *sm, double *tol,
+                 I *iwork, double *rwork, double *dcor, const I *lpu, I *ierr)
+{
+    (void)iwork;
+    (void)rwork;
+    (void)lpu;
+    if (mspar[0] < 0) {                  /* sprfc4.f:133-137 */
+        mspar[0] = -6;
+        *ierr = -1;
+        return;
+    }
+    mspar[0] = 6;
+    *ierr = 0;
+    sym_t s;
+    sym_from_mspar(&s, mspar, mtrees, msifa);
+    I numneg = 0, supeqt = 0;
+    I lierr = oracle_factor_mode(&s, sm, sm + s.neq, tol, &numneg, &supeqt, dcor, 1);
+    if (lierr != 0) {                    /* sprfc4.f:244-256 */
+        *ierr = (lierr / 10 == -3) ? -3 : -4;
+        mspar[26] = (lierr == -33) ? -supeqt : supeqt;
+    }
+    mspar[25] = numneg;
 }

@@ -386,3 +386,57 @@ def test_cholesky_partial_factorisation_matches_reference():
     r = run_chol('ref', rs, sm, b, mspar=msp, steps='fs')
     o = run_chol('orc', rs, sm, b, mspar=msp, steps='fs')
     _same_chol(r, o)
+
+
+def run_sprfc4(which, rs, sm, tol1, tol4, mspar=None):
+    from oracle.refpipe import lib as reflib, _p, _i
+    sm = sm.copy()
+    msp = rs.mspar.copy() if mspar is None else mspar.copy()
+    tol = np.array([tol1, 0.0, 0.0, tol4])
+    dcor = np.full(2 * rs.neq, 7.0)
+    iw = np.zeros(int(rs.mspar[13]) + 8, dtype=np.int64)
+    rw = np.zeros(int(rs.mspar[16]) + 8)
+    ierr = C.c_int64(0)
+    if which == 'ref':
+        R = reflib()
+        R.sprfc4_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw), _p(rw),
+                  _p(dcor), _i(-1), C.byref(ierr), C.cast(R.cmvy18_, C.c_void_p),
+                  C.cast(R.cmmy18_, C.c_void_p))
+    else:
+        _lib().orc_sprfc4_(_p(msp), _p(rs.mtrees), _p(rs.msifa), _p(sm), _p(tol), _p(iw),
+                           _p(rw), _p(dcor), _i(-1), C.byref(ierr))
+    return dict(sm=sm, tol=tol, dcor=dcor.reshape(-1, 2), ierr=ierr.value, mspar=msp)
+
+
+def test_sprfc4_matches_reference():
+    """SPRFC4 (sprfc4.f), the Cholesky form of SPRFC3: rigid-body pivots of a
+    free box replaced by +TOL(1) max(1, |TOL(4) a_jj|) (IERR -3, MSPAR(27) = -6,
+    a complete factor); an indefinite shift stopped at its first pivot below
+    -TOL(1)|a_jj| (MSPAR(27) = that equation); an SPD box; a zero diagonal."""
+    rs, sm = ref_system(4, clamp=False)
+    r = run_sprfc4('ref', rs, sm, 1e-8, 1e-2)
+    o = run_sprfc4('orc', rs, sm, 1e-8, 1e-2)
+    _same(r, o)
+    assert o['ierr'] == -3 and o['mspar'][26] == -6 and o['mspar'][0] == 6
+    assert np.count_nonzero(o['dcor'][:, 1]) == 6 and np.all(o['dcor'][:, 1] >= 0.0)
+    rs3, sm3 = ref_system(3)
+    from scipy.linalg import eigh
+    K = dense_from_sm(rs3, sm3)
+    M = np.diag(K.diagonal() - dense_from_sm(rs3, shifted_sm(rs3, sm3, 1.0)).diagonal())
+    w = eigh(K, M, eigvals_only=True)
+    ssm = shifted_sm(rs3, sm3, 0.5 * (w[3] + w[4]))
+    r = run_sprfc4('ref', rs3, ssm, 1e-12, 1.0)
+    o = run_sprfc4('orc', rs3, ssm, 1e-12, 1.0)
+    _same(r, o)
+    assert o['ierr'] == -3 and o['mspar'][26] > 0 and o['tol'][1] < 0.0
+    r = run_sprfc4('ref', rs3, sm3, 1e-12, 1.0)
+    o = run_sprfc4('orc', rs3, sm3, 1e-12, 1.0)
+    _same(r, o)
+    assert o['ierr'] == 0 and not np.any(o['dcor'])
+    from sam_lib_b200.system import diag_positions
+    z = sm3.copy()
+    z[diag_positions(rs3.mspar, rs3.mtrees, rs3.msifa)[20]] = 0.0
+    r = run_sprfc4('ref', rs3, z, 1e-12, 1.0)
+    o = run_sprfc4('orc', rs3, z, 1e-12, 1.0)
+    _same(r, o)
+    assert o['dcor'][20, 1] == 1.0
