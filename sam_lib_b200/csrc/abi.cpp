@@ -326,9 +326,21 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
         // the back sweep of the reference sees the equations beyond LDB as
         // zero (sprbs1.f:189), not as the forward sweep left them
         if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, 1) != 0) return -4;
-        if (cudaMemset2DAsync(c->d_b + neq, nfull * sizeof(double), 0, (nfull - neq) * sizeof(double), nrhs, s) !=
-            cudaSuccess)
+        if (peri2e) {                                   // beyond LDB in the external numbering
+            if (cudaMemcpyAsync(tmp.data(), c->d_b, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                return -4;
+            for (int64_t r = 0; r < nrhs; ++r)
+                for (int64_t k = 0; k < nfull; ++k)
+                    if ((int64_t)msifa[k] - 1 >= neq) tmp[r * nfull + k] = 0.0;
+            if (cudaMemcpyAsync(c->d_b, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess)
+                return -4;
+        } else if (cudaMemset2DAsync(c->d_b + neq, nfull * sizeof(double), 0, (nfull - neq) * sizeof(double), nrhs,
+                                     s) != cudaSuccess) {
             return -4;
+        }
         if (c->eng.solve(c->d_sm, c->d_b, nfull, nrhs, 2) != 0) return -4;
     } else if (chol) {
         // C^-1 b = D^1/2 (D^-1 L^-1 b);  C^-T y = L^-T (D^-1/2 y)
