@@ -6,7 +6,7 @@ Workload (one step): the numeric phase of SPR on the 48^3 hex8 elasticity box
 factorisation of SM plus forward/diagonal/back solves of 4 right-hand sides
 U[-1,1] (seed 1).  The symbolic structure is the reference's own (its MMD
 ordering, supernodes and symbolic factorisation, committed as
-tests/golden/structures/hex48.npz); SM is assembled by the library's SPRADM
+sam_lib_b200/structures/hex48.npz); SM is assembled by the library's SPRADM
 main add.  Synthetic, seeded data; no dataset is involved.
 
   value  : GFLOP/s of factor+solve = (RINFO(3) + NRHS*RINFO(4)) / t, with SM
@@ -78,7 +78,8 @@ def _cpu_worker(args):
     ke = hex8_stiffness()
     sm0 = rs.assemble(lambda e: ke)
     b0 = np.asfortranarray(np.random.default_rng(1).uniform(-1.0, 1.0, size=(rs.neq, NRHS)))
-    flops = float(rs.rinfo[2] + NRHS * (2.0 * rs.rinfo[3] + rs.neq))
+    # RINFO(3) + NRHS * RINFO(4); RINFO(4) is already 2*sum + NEQ (sprtrs.f:2019)
+    flops = float(rs.rinfo[2] + NRHS * rs.rinfo[3])
     times = []
     for _ in range(reps):
         sm = sm0.copy()
@@ -103,9 +104,32 @@ def cpu_sample(nproc, reps):
 
 
 def sample_desc(cores):
-    return ('reference SPRSOL IOP=3 (factor + %d-RHS solve) on the %d^3 hex8 box (26,460 eq) of the '
-            'same family, machine-translated Fortran SPR built with gcc -O2, %d process%s' %
-            (NRHS, SAMPLE_N, cores, '' if cores == 1 else 'es'))
+    return ('reference SPRSOL IOP=3 (factor + %d-RHS solve) on the %d^3 hex8 box (26,460 eq, RINFO(3) '
+            '4.37e10) of the same family, machine-translated Fortran SPR built with gcc -O2, %d process%s%s' %
+            (NRHS, SAMPLE_N, cores, '' if cores == 1 else 'es',
+             ' (the reference is single-threaded: one system runs on one core)' if cores == 1 else
+             ', one independent system each'))
+
+
+def sample_config():
+    return {'workload': 'bounded sample of the %d^3 workload: the %d^3 box of the same hex8 family, LDL\' '
+                        'factor + %d RHS solve' % (N_MESH, SAMPLE_N, NRHS),
+            'mesh': '%dx%dx%d' % (SAMPLE_N, SAMPLE_N, SAMPLE_N), 'neq': 26460, 'nrhs': NRHS}
+
+
+def _ladder_worker(n):
+    """One SPRSOL IOP=1 factorisation of the n^3 box: (n, NEQ, RINFO(3), seconds)."""
+    from oracle.refpipe import RefSystem
+    from sam_lib_b200.fe import HexBox, hex8_stiffness
+    rs = RefSystem(HexBox(n))
+    ke = hex8_stiffness()
+    sm = rs.assemble(lambda e: ke)
+    b = np.zeros((rs.neq, 1), order='F')
+    t = time.perf_counter()
+    ierr, _, _ = rs.sprsol(1, sm, b)
+    dt = time.perf_counter() - t
+    assert ierr == 0
+    return n, rs.neq, float(rs.rinfo[2]), dt
 
 
 # ---------------------------------------------------------------------------
@@ -368,21 +392,55 @@ def form_adjoint(torch, reps=3):
 
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path (the machine-translated
+    SPR Fortran) on this host.  The reference is single-threaded and has no way
+    to spread one system over cores, so `value` is its rate on one core; each
+    step is one SPRSOL(IOP=3) of the bounded 20^3 sample (about 5-7 s).  Also
+    reported: a size ladder (one factorisation each of 12^3..24^3, so that the
+    rate's size dependence is visible before anyone extrapolates it to 48^3),
+    the RINFO(3)-based extrapolation to the 48^3 factorisation, and the
+    all-core aggregate of independent sample systems (one process per core)."""
     if rank != 0:
         return
-    nproc = os.cpu_count() or 1
-    flops, times = cpu_sample(nproc, args.warmup + args.steps)
-    per_step = [max(t[s] for t in times) for s in range(args.warmup, args.warmup + args.steps)]
+    ladder = []
+    for n in (12, 16, 20, 24):
+        nn, neq, r3, dt = _ladder_worker(n)
+        ladder.append({'mesh': '%d^3' % nn, 'neq': neq, 'rinfo3': r3, 'factor_s': dt,
+                       'gflops': r3 / dt / 1e9})
+    flops, times = cpu_sample(1, args.warmup + args.steps)
+    per_step = times[0][args.warmup:]
     t = float(np.mean(per_step))
-    value = nproc * flops / t / 1e9
+    value = flops / t / 1e9
+    nproc = os.cpu_count() or 1
+    agg_flops, agg_times = cpu_sample(nproc, 1)
+    agg = nproc * agg_flops / max(tt[0] for tt in agg_times) / 1e9
+    rinfo3_48 = 1.419e13
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t * 1e3, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded hex8 meshes)',
-            'config': config(args.n),
-            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': nproc, 'kind': 'reference',
-                             'sample': sample_desc(nproc)},
-            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+            'config': config(args.n), 'sample_config': sample_config(),
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': 1, 'kind': 'reference',
+                             'sample': sample_desc(1)},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+            'ladder': ladder,
+            'extrapolated_48_factor_s': rinfo3_48 / (value * 1e9),
+            'extrapolation_note': '48^3 RINFO(3) 1.419e13 at the 1-core sample rate; the ladder shows the '
+                                  'rate at 12^3..24^3, the 48^3 top fronts are larger still',
+            'aggregate_all_cores': {'value': agg, 'unit': UNIT, 'cores': nproc,
+                                    'sample': sample_desc(nproc),
+                                    'note': 'independent systems only; not a rate for one system'},
+            'host_cpu': _cpu_model()}
     print(json.dumps(line), flush=True)
+
+
+def _cpu_model():
+    try:
+        for line in open('/proc/cpuinfo'):
+            if line.startswith('model name'):
+                return line.split(':', 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def run_ours(args, rank, world, local_rank):

@@ -104,7 +104,9 @@ int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ld
  * [3]=tree levels [4]=last factor ms [5]=last solve ms [6]=launches of the
  * last factorisation [7]=Schur-update launches [8]=Schur-update ms (profile
  * mode) [9]=Schur-update algorithmic flops [10]=launches of the last solve
- * [11]=NZEROL.  info must hold 12 doubles. */
+ * [11]=NZEROL [12]=pivots with |d| < tau |a_jj| that the mixed-mode inertia
+ * guard counted in the last factorisation [13]=1 if the guard redid that
+ * factorisation in FP64.  info must hold 14 doubles. */
 int spr_b200_info(void* handle, double* info);
 /* Per-supernode negative-pivot counts and first failing column (-1 if none)
  * of the last spr_b200_factor_dev (NSUPER entries each): per-system inertia
@@ -118,6 +120,22 @@ int spr_b200_sn_stats(void* handle, int32_t* neg, int32_t* fail);
  * 1 and 2 with spr_b200_refine against the FP64 matrix
  * (spr_b200_build_residual).  Returns -2 for an unknown mode. */
 int spr_b200_set_mode(void* handle, int mode);
+/* No reference counterpart (the reference has no mixed precision).  Inertia
+ * guard of modes 1 and 2: each mixed factorisation first keeps a copy of the
+ * assembled device SM (one extra SM-sized buffer, allocated once); when it
+ * meets a pivot with |d| < tau |a_jj| (a_jj the original diagonal) or a
+ * failed pivot test, its sign or the test may depend on the TF32 rounding,
+ * so the factorisation is redone in FP64 from that copy and NUMNEG, IERR and
+ * TOL are the FP64 ones (the pivot rule of SPRF17, sprfc1.f:1272-1283).
+ * Default tau = 1e-3; tau = 0 switches the guard and the copy off. */
+int spr_b200_set_inertia_guard(void* handle, double tau);
+/* No reference counterpart.  Watchdog of the tensor-core update kernel:
+ * every mbarrier wait gives up after wait_ns nanoseconds (default 2e9; 1e6 ..
+ * 6e10 accepted), the kernel then frees its tensor memory and returns, and
+ * the factorisation returns -4.  drop != 0 is a test switch: the first CTA of
+ * each tensor-core launch skips its first operand load, so that its waits run
+ * out.  Returns -2 for a limit outside the range. */
+int spr_b200_set_watchdog(void* handle, double wait_ns, int drop);
 /* Residual operator for refinement: compacts the FP64 matrix held in an
  * assembled (not yet factored) device SM into a CSR (the product SPRPRQ forms
  * from the packed pattern, sprprm.f:243-325). */

@@ -55,6 +55,10 @@ def load(int_kind=8):
         lib.spr_b200_refine.restype = C.c_int
         lib.spr_b200_set_mode.argtypes = [vp, C.c_int]
         lib.spr_b200_set_mode.restype = C.c_int
+        lib.spr_b200_set_inertia_guard.argtypes = [vp, C.c_double]
+        lib.spr_b200_set_inertia_guard.restype = C.c_int
+        lib.spr_b200_set_watchdog.argtypes = [vp, C.c_double, C.c_int]
+        lib.spr_b200_set_watchdog.restype = C.c_int
         lib.spr_b200_autotune.argtypes = [vp, vp, vp]
         lib.spr_b200_autotune.restype = C.c_int
         lib.spr_b200_tc_stats.argtypes = [vp, vp]
@@ -254,10 +258,11 @@ class DeviceSolver:
             raise RuntimeError('spr_b200_solve_dev failed with %d' % rc)
 
     def info(self):
-        out = np.zeros(12)
+        out = np.zeros(14)
         self.lib.spr_b200_info(self.h, _ptr(out))
         keys = ('factor_flops', 'solve_flops', 'arena_bytes', 'levels', 'factor_ms', 'solve_ms',
-                'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops', 'solve_launches', 'nzerol')
+                'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops', 'solve_launches', 'nzerol',
+                'near_pivots', 'fp64_redo')
         return dict(zip(keys, out.tolist()))
 
     def sn_stats(self, nsuper):
@@ -286,6 +291,18 @@ class DeviceSolver:
         rc = self.lib.spr_b200_set_mode(self.h, int(mixed))
         if rc != 0:
             raise ValueError('unknown factorisation mode %r' % (mixed,))
+
+    def set_inertia_guard(self, tau):
+        """Mixed modes: redo the factorisation in FP64 when a pivot has
+        |d| < tau |a_jj| or fails the pivot test (default 1e-3, 0 = off)."""
+        if self.lib.spr_b200_set_inertia_guard(self.h, float(tau)) != 0:
+            raise ValueError('bad inertia-guard tolerance %r' % (tau,))
+
+    def set_watchdog(self, wait_s=2.0, drop=False):
+        """Wait limit of the tensor-core kernel's barriers; drop=True is the
+        test switch that makes one CTA's waits run out."""
+        if self.lib.spr_b200_set_watchdog(self.h, float(wait_s) * 1e9, 1 if drop else 0) != 0:
+            raise ValueError('bad watchdog limit %r' % (wait_s,))
 
     def autotune(self, d_sm_assembled):
         """Mixed-mode autotuner on a copy of the assembled SM; returns the choice and times."""

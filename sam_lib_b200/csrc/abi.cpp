@@ -16,16 +16,20 @@
 
 #include <algorithm>
 #include <cinttypes>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
 #include "elements.h"
 #include "engine.h"
+#include "smhash.h"
 
 #ifndef SPR_INT
 #define SPR_INT int64_t
@@ -74,23 +78,24 @@ uint64_t mix(uint64_t h, uint64_t v) {
     return h;
 }
 
-// Sampled fingerprint of SM: detects a re-assembled or different matrix
-// between a factorisation and later solves without reading all of SM.
-uint64_t sm_fingerprint(const double* sm, int64_t n) {
-    uint64_t h = mix(0, (uint64_t)n);
-    const int64_t samples = 4096;
-    const int64_t step = n > samples ? n / samples : 1;
-    for (int64_t i = 0; i < n; i += step) {
-        uint64_t v;
-        std::memcpy(&v, sm + i, 8);
-        h = mix(h, v);
-    }
-    for (int64_t i = n > 64 ? n - 64 : 0; i < n; ++i) {
-        uint64_t v;
-        std::memcpy(&v, sm + i, 8);
-        h = mix(h, v);
-    }
-    return h;
+// Residency of the device factor across calls: a solve call reuses the
+// device factor only if the host SM still holds exactly what the
+// factorisation wrote back.  The check hashes all of the host SM (smhash.h;
+// the factorisation hashed the same bytes on the device before the copy), so
+// an edit of a single entry between SPRFC1 and SPRFS1 makes the solve
+// re-upload SM.  SPR_B200_TRUST_SM=1 skips the host hash: the caller then
+// promises not to modify SM between a factorisation and its solves.
+bool trust_sm() {
+    static const bool t = [] {
+        const char* v = std::getenv("SPR_B200_TRUST_SM");
+        return v != nullptr && v[0] == '1';
+    }();
+    return t;
+}
+
+int host_threads() {
+    const unsigned n = std::thread::hardware_concurrency();
+    return (int)std::min(16u, std::max(1u, n));
 }
 
 std::vector<int64_t> widen(const I* a, int64_t n) {
@@ -156,6 +161,76 @@ Ctx* get_ctx(I* mspar, I* mtrees, I* msifa, int& err) {
     Ctx* raw = c.get();
     g_ctx[key] = std::move(c);
     return raw;
+}
+
+// MVMULT/MMMULT callbacks.  SPRFC1 and SPRFC3 take the LDL' kernels LMVY18
+// (y += sum_j (-a_j(1) d_j) a_j, lmvy18.f:5-173) and LMMY18 (packed lower
+// Y -= X D X', lmmy18.f:5-192); SPRFC2 takes the C C' kernels CMVY18 and
+// CMMY18 (the same without D, cmvy18.f:5, cmmy18.f:5).  The GPU applies the
+// update those kernels define and never calls the routine it is given, so a
+// routine that computes something else would be ignored silently.  Instead,
+// a non-null routine is run once on a small probe (3x3 / 3x2 operands, the
+// reference's argument conventions) and the call is refused (IERR = -4)
+// unless it reproduces that update.  The verdict is cached per routine.
+typedef void (*LmvFn)(I*, I*, double*, double*, I*, double*);
+typedef void (*LmmFn)(I*, I*, I*, I*, double*, double*, double*, I*);
+typedef void (*CmvFn)(I*, I*, double*, I*, double*);
+typedef void (*CmmFn)(I*, I*, I*, I*, double*, double*, I*);
+
+bool close_vec(const double* a, const double* b, int n) {
+    for (int i = 0; i < n; ++i)
+        if (!(std::fabs(a[i] - b[i]) <= 1e-12 * (1.0 + std::fabs(b[i])))) return false;
+    return true;
+}
+
+bool probe_mv(void (*f)(), bool with_d) {
+    I m = 3, n = 3;
+    double A[9] = {0.5, -1.25, 0.75, 1.5, 0.25, -0.5, -0.625, 2.0, 1.125};
+    double D[3] = {2.0, -3.0, 0.5};
+    I apnt[4] = {1, 4, 7, 10};        // APNT(J+1) - (M+1) = (J-1) M, lmvy18.f:148-150
+    double Y[3] = {1.0, -2.0, 0.25}, E[3] = {1.0, -2.0, 0.25};
+    for (int j = 0; j < 3; ++j) {
+        const double a = -A[3 * j] * (with_d ? D[j] : 1.0);
+        for (int i = 0; i < 3; ++i) E[i] += a * A[3 * j + i];
+    }
+    if (with_d)
+        reinterpret_cast<LmvFn>(f)(&m, &n, Y, D, apnt, A);
+    else
+        reinterpret_cast<CmvFn>(f)(&m, &n, Y, apnt, A);
+    return close_vec(Y, E, 3);
+}
+
+bool probe_mm(void (*f)(), bool with_d) {
+    I m = 3, n = 2, q = 2, ldy = 3;
+    double X[6] = {0.5, -1.25, 0.75, 1.5, 0.25, -0.5};
+    double D[2] = {2.0, -3.0};
+    I xpnt[3] = {1, 4, 7};            // XPNT(J+1) = one past column J, lmmy18.f:18-19
+    double Y[5] = {1.0, -2.0, 0.25, 0.5, 3.0}, E[5];
+    std::memcpy(E, Y, sizeof(E));
+    for (int c = 0, base = 0; c < 2; base += 3 - c, ++c)
+        for (int r = c; r < 3; ++r)
+            for (int j = 0; j < 2; ++j) E[base + r - c] += -X[3 * j + c] * (with_d ? D[j] : 1.0) * X[3 * j + r];
+    if (with_d)
+        reinterpret_cast<LmmFn>(f)(&m, &n, &q, xpnt, X, D, Y, &ldy);
+    else
+        reinterpret_cast<CmmFn>(f)(&m, &n, &q, xpnt, X, Y, &ldy);
+    return close_vec(Y, E, 5);
+}
+
+// true when both callbacks are null or compute the kernels' update
+bool callbacks_ok(void (*mv)(), void (*mm)(), bool ldlt) {
+    static std::map<std::pair<const void*, int>, bool> seen;   // under g_mu
+    auto check = [&](void (*f)(), int kind) {
+        if (!f) return true;
+        const auto key = std::make_pair((const void*)f, kind);
+        auto it = seen.find(key);
+        if (it != seen.end()) return it->second;
+        const bool ok = (kind & 1) ? probe_mm(f, (kind & 2) != 0) : probe_mv(f, (kind & 2) != 0);
+        seen[key] = ok;
+        return ok;
+    };
+    const int d = ldlt ? 2 : 0;
+    return check(mv, d) && check(mm, d | 1);
 }
 
 // Reference length checks of SPRFC1 (src/SPR/sprfc1.f:150-236).
@@ -225,6 +300,8 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     }
     const bool chol_ok = chol && r.lierr == 0;
     if (chol_ok && c->eng.chol_convert(c->d_sm, true) != 0) return -4;
+    uint64_t fp = 0;                                  // hash of exactly what the host receives
+    if (c->eng.hash(c->d_sm, nsm, fp) != 0) return -4;
     if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -4;
     if (chol_ok && c->eng.chol_convert(c->d_sm, false) != 0) return -4;
     c->dev_chol = chol_ok;
@@ -244,7 +321,7 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
             msg(lpu, who, buf);
         }
         c->sm_host = sm;
-        c->sm_fp = sm_fingerprint(sm, nsm);
+        c->sm_fp = fp;
         c->resident = true;
     } else if (r.lierr != 0) {                        // sprfc1.f:251-265
         ierr = (r.lierr / 10 == -3) ? -3 : -4;
@@ -268,7 +345,7 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
                         "DEFINITE: %" PRId64 " NEGATIVE PIVOT(S)\n", who, r.numneg);
         }
         c->sm_host = sm;
-        c->sm_fp = sm_fingerprint(sm, nsm);
+        c->sm_fp = fp;
         c->resident = true;
     }
     mspar[25] = (I)r.numneg;
@@ -278,16 +355,22 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
 // Makes the device SM hold this host SM's factor (re-uploading if needed).
 // With chol the host SM is a C C' factor (SPRFC2): the device keeps its
 // L D L' form, which the Cholesky solves use with a sqrt(D) scaling.
-int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm, bool chol = false) {
+// fresh: the factorisation ran in the same call (SPRSOL with IOP <= 3), so the
+// host SM cannot have changed since.
+int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm, bool chol = false, bool fresh = false) {
     const int64_t nsm = mspar[7] + mspar[15];
-    if (c->resident && c->sm_host == sm && c->sm_fp == sm_fingerprint(sm, nsm) && c->dev_chol == chol) return 0;
+    if (c->resident && c->sm_host == sm && c->dev_chol == chol &&
+        (fresh || trust_sm() || c->sm_fp == sprb::sm_hash_host(sm, nsm, host_threads())))
+        return 0;
     if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return -4;
+    uint64_t fp = 0;
+    if (c->eng.hash(c->d_sm, nsm, fp) != 0) return -4;
     c->eng.invalidate_factor();
     if (chol && c->eng.chol_convert(c->d_sm, false) != 0) return -4;
     c->dev_chol = chol;
     c->sm_host = sm;
-    c->sm_fp = sm_fingerprint(sm, nsm);
+    c->sm_fp = fp;
     c->resident = true;
     return 0;
 }
@@ -295,10 +378,10 @@ int ensure_factor_on_device(Ctx* c, const I* mspar, const double* sm, bool chol 
 // Forward (which=1), back (2) or both (3) for B(LDB,NRHS) on the host; with
 // chol the C C' sweeps of SPRFS2 (which=1) or SPRBS2 (which=2).
 int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I nrhs, int which,
-             bool chol = false) {
+             bool chol = false, bool fresh = false) {
     const int64_t neq = (mspar[56] == 1 && ldb < mspar[7]) ? (int64_t)ldb : (int64_t)mspar[7];
     if (nrhs <= 0) return 0;
-    if (ensure_factor_on_device(c, mspar, sm, chol) != 0) return -4;
+    if (ensure_factor_on_device(c, mspar, sm, chol, fresh) != 0) return -4;
     if (ensure_b(c, (int64_t)mspar[7] * nrhs) != 0) return -4;
     cudaStream_t s = c->stream;
     const bool peri2e = mspar[57] >= 1;                 // sprfs1.f:240-250, SPRFB3/SPRFB4
@@ -381,8 +464,6 @@ void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
                       I* ierr, void (*mvmult)(), void (*mmmult)()) {
     (void)iwork;
     (void)rwork;
-    (void)mvmult;   // the GPU path always applies the LDL' kernels (LMVY18/LMMY18)
-    (void)mmmult;
     std::lock_guard<std::mutex> lk(g_mu);
     if (mspar[0] < 0) {                                 // sprfc1.f:140-148
         mspar[0] = -5;
@@ -396,6 +477,12 @@ void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         mspar[0] = -2;
         *ierr = -2;
         msg(*lpu, "SPRFC1", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (!callbacks_ok(mvmult, mmmult, true)) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRFC1", "MVMULT/MMMULT DO NOT COMPUTE THE LDL' UPDATES OF LMVY18/LMMY18");
         return;
     }
     int err = 0;
@@ -418,8 +505,6 @@ void SPR_API(sprfc3_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
                       const I* lpu, I* ierr, void (*mvmult)(), void (*mmmult)()) {
     (void)iwork;
     (void)rwork;
-    (void)mvmult;
-    (void)mmmult;
     std::lock_guard<std::mutex> lk(g_mu);
     if (mspar[0] < 0) {                                 // sprfc3.f:139-143
         mspar[0] = -5;
@@ -433,6 +518,12 @@ void SPR_API(sprfc3_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         mspar[0] = -2;
         *ierr = -2;
         msg(*lpu, "SPRFC3", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (!callbacks_ok(mvmult, mmmult, true)) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRFC3", "MVMULT/MMMULT DO NOT COMPUTE THE LDL' UPDATES OF LMVY18/LMMY18");
         return;
     }
     int err = 0;
@@ -454,8 +545,6 @@ void SPR_API(sprfc2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
                       I* ierr, void (*mvmult)(), void (*mmmult)()) {
     (void)iwork;
     (void)rwork;
-    (void)mvmult;   // CMVY18/CMMY18 (cmvy18.f:5, cmmy18.f:5): the GPU applies the update they define
-    (void)mmmult;
     std::lock_guard<std::mutex> lk(g_mu);
     if (mspar[0] < 0) {                                 // sprfc2.f:123-127
         mspar[0] = -6;
@@ -469,6 +558,12 @@ void SPR_API(sprfc2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         mspar[0] = -2;
         *ierr = -2;
         msg(*lpu, "SPRFC2", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (!callbacks_ok(mvmult, mmmult, false)) {
+        mspar[0] = -6;
+        *ierr = -4;
+        msg(*lpu, "SPRFC2", "MVMULT/MMMULT DO NOT COMPUTE THE C C' UPDATES OF CMVY18/CMMY18");
         return;
     }
     int err = 0;
@@ -608,7 +703,7 @@ void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, d
         }
         int err = 0;
         Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-        if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3) != 0) {
+        if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3, false, op <= 3) != 0) {
             mspar[0] = -7;
             *ierr = -4;
             msg(*lpu, "SPRSOL", "GPU SOLVE FAILED");
@@ -677,7 +772,9 @@ int SPR_API(spr_b200_solve_dev)(void* handle, const double* d_sm, double* d_b, i
 // [2]=front arena bytes, [3]=levels, [4]=last factor ms, [5]=last solve ms,
 // [6]=kernel launches of the last factorisation, [7]=Schur-update launches,
 // [8]=Schur-update ms (profile mode), [9]=Schur-update algorithmic flops,
-// [10]=kernel launches of the last solve, [11]=NZEROL.
+// [10]=kernel launches of the last solve, [11]=NZEROL, [12]=pivots the
+// mixed-mode inertia guard counted in the last factorisation, [13]=1 if that
+// factorisation was redone in FP64 by the guard.
 int SPR_API(spr_b200_info)(void* handle, double* info) {
     Engine* e = static_cast<Engine*>(handle);
     const sprb::Plan& p = e->plan();
@@ -693,6 +790,8 @@ int SPR_API(spr_b200_info)(void* handle, double* info) {
     info[9] = p.gemm_flops;
     info[10] = (double)e->timing.solve_launches;
     info[11] = (double)p.nzerol;
+    info[12] = (double)e->last_near_pivots();
+    info[13] = e->last_refactored() ? 1.0 : 0.0;
     return 0;
 }
 
@@ -720,6 +819,21 @@ int SPR_API(spr_b200_refine)(void* handle, const double* d_sm, const double* d_b
 int SPR_API(spr_b200_set_mode)(void* handle, int mode) {
     if (mode < 0 || mode > 2) return -2;
     static_cast<Engine*>(handle)->set_mixed(mode);
+    return 0;
+}
+
+// Inertia guard of the mixed mode (default tau = 1e-3; 0 = off).
+int SPR_API(spr_b200_set_inertia_guard)(void* handle, double tau) {
+    if (!(tau >= 0.0)) return -2;
+    static_cast<Engine*>(handle)->set_inertia_guard(tau);
+    return 0;
+}
+
+// Watchdog of the tensor-core update: wait limit (ns, > 0) and the test
+// switch that makes one CTA's waits run out.
+int SPR_API(spr_b200_set_watchdog)(void* handle, double wait_ns, int drop) {
+    if (!(wait_ns >= 1.0e6 && wait_ns <= 6.0e10)) return -2;
+    static_cast<Engine*>(handle)->set_watchdog((unsigned long long)wait_ns, drop != 0);
     return 0;
 }
 

@@ -27,6 +27,7 @@
 #include <cstring>
 
 #include "engine.h"
+#include "smhash.h"
 
 namespace sprb {
 
@@ -62,6 +63,7 @@ struct Stats {
     double mindpos;          // smallest positive pivot, sprfc1.f:690-697
     int tc_timeout;          // a tensor-core update CTA gave up waiting (see tc_gemm.cuh)
     unsigned long long nsing;    // SPRFC3: pivots replaced by the TOL(1)/TOL(4) rule
+    unsigned long long near_piv; // pivots with |d| < near_tol |a_jj| (mixed-mode inertia guard)
 };
 
 struct PV {
@@ -92,6 +94,14 @@ struct PV {
     double* dcor;
     // partial factorisation: 1 for the retained supernodes (null if none)
     const uint8_t* ret;
+    // inertia guard of the mixed mode: pivots with |d| < near_tol |a_jj| are
+    // counted (their sign may depend on the TF32 rounding); 0 = off
+    double near_tol;
+    // time limit of every mbarrier wait of the tensor-core update (ns), and a
+    // test switch: when set, CTA 0 of each tensor-core launch skips its first
+    // operand load, so that its waits run out and the launch reports a timeout
+    unsigned long long wait_ns;
+    int tc_drop;
 };
 
 struct Engine::Dev {
@@ -130,6 +140,7 @@ struct Engine::Dev {
     int64_t bbuf_rhs = 0;
     std::vector<void*> owned;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    unsigned long long* hbuf = nullptr;          // result of k_sm_hash
     // tensor-core (mixed) updates: operand slabs and the TMA map over them
     float* slab = nullptr;
     alignas(64) CUtensorMap slab_map;
@@ -270,6 +281,17 @@ __global__ void k_prepass(PV P, int64_t nsuper) {
     }
 }
 
+// Content hash of a device array (see smhash.h): each thread sums its words'
+// mixes, the partial sums meet in one 64-bit atomic add (order-free).
+__global__ void k_sm_hash(const double* a, int64_t n, unsigned long long* out) {
+    unsigned long long acc = 0ull;
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += sm_mix(__ldcs(reinterpret_cast<const unsigned long long*>(w + i)), (uint64_t)i);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
 // Deterministic single-CTA reductions over a vector: sum, or min over positives.
 template <bool kMinPos>
 __global__ void k_reduce(const double* v, int64_t n, double* out) {
@@ -309,8 +331,19 @@ __global__ void k_reduce(const double* v, int64_t n, double* out) {
 // factor is formed from L D L' afterwards, see k_chol_convert).
 enum PivotRule { kPivotLDL = 0, kPivotReplace = 1, kPivotChol = 2 };
 
+// A NaN or infinite pivot (a NaN or Inf anywhere in SM reaches some pivot
+// through the Schur updates) fails the test as well, so that the call reports
+// an error instead of a factor full of NaN.
 __device__ __forceinline__ bool pivot_fails(int rule, double d, double ad, double tol1) {
+    if (!isfinite(d)) return true;
     return rule == kPivotChol ? d <= tol1 * fabs(ad) : fabs(d) <= tol1 * fabs(ad);
+}
+
+// Mixed-mode inertia guard: a pivot this close to zero relative to its
+// original diagonal may have its sign decided by the TF32 rounding of the
+// updates that formed it.
+__device__ __forceinline__ bool near_zero_pivot(const PV& P, double d, double ad) {
+    return P.near_tol > 0.0 && fabs(d) < P.near_tol * fabs(ad);
 }
 
 template <int PR>
@@ -374,6 +407,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             break;
         }
         if (d < 0.0) ++neg;
+        if (tid == 0 && near_zero_pivot(P, d, ad)) atomicAdd(&P.st->near_piv, 1ull);
         tmax = fmax(tmax, ad / d);
         const double rd = 1.0 / d;
         for (int i = k + 1 + tid; i < F; i += blockDim.x) {
@@ -572,19 +606,22 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     // inertia and TOL(2) of the processed columns (sprfc1.f:1280-1290)
     if (tid < 32) {
         const int kend = failed < 0 ? nb : failed;
-        int neg = 0;
+        int neg = 0, near = 0;
         double tmax = 0.0;
         for (int k = tid; k < kend; k += 32) {
             if (dd[k] < 0.0) ++neg;
+            if (near_zero_pivot(P, dd[k], adv[k])) ++near;
             tmax = fmax(tmax, adv[k] / dd[k]);
         }
         for (int o = 16; o > 0; o >>= 1) {
             neg += __shfl_xor_sync(0xffffffffu, neg, o);
+            near += __shfl_xor_sync(0xffffffffu, near, o);
             tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
         }
         if (tid == 0) {
             P.sn_neg[js] += neg;
             atomicAdd(&P.st->numneg, (unsigned long long)neg);
+            if (near) atomicAdd(&P.st->near_piv, (unsigned long long)near);
             if (failed < 0) atomic_max_double(&P.st->tol2, tmax);
         }
     }
@@ -1994,6 +2031,7 @@ Engine::~Engine() {
     if (csr_.cv) cudaFree(csr_.cv);
     if (csr_.rowabs) cudaFree(csr_.rowabs);
     if (rbuf_) cudaFree(rbuf_);
+    if (guard_copy_) cudaFree(guard_copy_);
     if (!d_) return;
     for (void* p : d_->owned) cudaFree(p);
     if (d_->arena) cudaFree(d_->arena);
@@ -2009,11 +2047,9 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     if (rc != 0) return rc;
     Dev& D = *d_;
     auto& o = D.owned;
-    {
-        int dev = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
-    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
     {
         // side stream and the fork/join events of one factorisation (two per
         // step that forks a far update)
@@ -2074,10 +2110,12 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     o.push_back(D.sn_faila);
     CK(cudaMalloc((void**)&D.st, sizeof(Stats)));
     o.push_back(D.st);
+    CK(cudaMalloc((void**)&D.hbuf, sizeof(unsigned long long)));
+    o.push_back(D.hbuf);
     CK(cudaEventCreate(&D.ev0));
     CK(cudaEventCreate(&D.ev1));
     int smem_max = 0;
-    CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
+    CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + kSmallMaxF) * sizeof(double);
     if ((size_t)smem_max < need) return -4;
     CK(cudaFuncSetAttribute(k_small_front<kPivotLDL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
@@ -2183,6 +2221,9 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.tol4 = 0.0;
     v.dcor = nullptr;
     v.ret = D.ret;
+    v.near_tol = 0.0;
+    v.wait_ns = 2000000000ull;
+    v.tc_drop = 0;
     return v;
 }
 
@@ -2349,10 +2390,29 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
         pv.tol4 = fc3->tol4;
         pv.dcor = fc3->d_dcor;
     }
+    pv.wait_ns = wait_ns_;
+    pv.tc_drop = tc_drop_ ? 1 : 0;
     linv_valid_ = false;
+    last_near_ = 0;
+    last_refactor_ = false;
     if (mixed_ == 1) {
         const int rc = ensure_slabs();
         if (rc != 0) return rc;
+    }
+    // inertia guard: keep the assembled SM, so that the factorisation can be
+    // redone in FP64 when a pivot's sign may depend on the TF32 rounding
+    const bool guard = mixed_ != 0 && guard_tol_ > 0.0;
+    const int64_t nsm = P_.neq + P_.nzerol;
+    if (guard) {
+        if (guard_cap_ < nsm) {
+            if (guard_copy_) cudaFree(guard_copy_);
+            guard_copy_ = nullptr;
+            guard_cap_ = 0;
+            CK(cudaMalloc((void**)&guard_copy_, nsm * sizeof(double)));
+            guard_cap_ = nsm;
+        }
+        CK(cudaMemcpyAsync(guard_copy_, d_sm, nsm * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        pv.near_tol = guard_tol_;
     }
     Stats init{};
     init.first_zero = 0x7fffffff;
@@ -2365,11 +2425,13 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     tc_pairs_.clear();
     CK(cudaEventRecord(D.ev0, s));
     std::vector<cudaEvent_t> gev;
-    // the legacy default stream cannot be captured: graphs need a stream of our own
-    const bool graph = use_graphs_ && !profile_ && s != nullptr;
+    // the legacy default stream cannot be captured: graphs need a stream of our own;
+    // the watchdog test launches kernel by kernel (its settings are not in the key)
+    const bool graph = use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull;
     if (graph) {
         const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_ | (chol_ ? 16 : 0),
-                           (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4};
+                           (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4,
+                           pv.near_tol};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2418,6 +2480,22 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
         fprintf(stderr, "spr_b200: a tensor-core update gave up waiting for its operands\n");
         return -4;
     }
+    if (guard && (hs.near_piv > 0 || (hs.pivot_fail && hs.zero_count == 0))) {
+        // a pivot within guard_tol_ |a_jj| of zero, or a failed pivot test,
+        // after TF32 updates: decide inertia and the pivot test in FP64
+        const float first_ms = timing.factor_ms;
+        const int64_t near = (int64_t)hs.near_piv;
+        CK(cudaMemcpyAsync(d_sm, guard_copy_, nsm * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        const int mode = mixed_;
+        mixed_ = 0;
+        const int rc = factor(d_sm, tol1, res, fc3);
+        mixed_ = mode;
+        timing.factor_ms += first_ms;
+        last_near_ = near;
+        last_refactor_ = true;
+        return rc;
+    }
+    last_near_ = (int64_t)hs.near_piv;
     if (hs.zero_count > 0) {                       // sprfc1.f:474-488
         // the reference's pre-pass has already replaced D by the original diagonal
         CK(cudaMemcpy(pv.dvec, D.adiag, P_.neq * sizeof(double), cudaMemcpyDeviceToDevice));
@@ -2462,6 +2540,21 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
         const double m = std::sqrt(hs.mindpos);
         res.tol3 = (m != 0.0) ? hs.trace / (m * m) : 0.0;
     }
+    return 0;
+}
+
+int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
+    Dev& D = *d_;
+    unsigned long long hv = 0ull;
+    CK(cudaMemsetAsync(D.hbuf, 0, sizeof(unsigned long long), stream_));
+    if (n > 0) {
+        const int grid = (int)std::min<int64_t>((n + 255) / 256, 8 * (int64_t)std::max(sm_count_, 1));
+        k_sm_hash<<<grid, 256, 0, stream_>>>(d_a, n, D.hbuf);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(&hv, D.hbuf, sizeof(hv), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    h = (uint64_t)hv;
     return 0;
 }
 
@@ -2710,6 +2803,14 @@ size_t dense_scratch_bytes(int64_t n) {
     add(sizeof(int64_t) * 8);
     add(sizeof(double) * 4);
     return b;
+}
+
+int dense_factor_setup() {
+    // k_trsm and the small-tile update use more than the default 48 KB of
+    // dynamic shared memory; the opt-in is per function and per device.
+    CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+    CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
+    return 0;
 }
 
 int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, double* d, void* scratch,

@@ -80,6 +80,8 @@ public:
     // Mixed mode autotuner (see engine.cu): times candidate engine choices on a
     // copy of the assembled SM and keeps the fastest.  out: 5 doubles.
     int autotune(const double* d_sm_assembled, double* out);
+    // Content hash (smhash.h) of n doubles of device memory, on the engine's stream.
+    int hash(const double* d_a, int64_t n, uint64_t& h);
     // Per-supernode negative-pivot counts and failing column of the last factor().
     int sn_stats(int32_t* neg, int32_t* fail);
     // The solves use the inverses of the diagonal blocks that factor() stores;
@@ -96,6 +98,21 @@ public:
     // 0 = FP64, 1 = tcgen05 tensor cores (k_gemm_tc), 2 = mma.sync (k_gemm_x3).
     void set_mixed(int mode) { mixed_ = mode; }
     int mixed() const { return mixed_; }
+    // Inertia guard of the mixed mode: when a pivot with |d| < tau |a_jj|
+    // (or a pivot failure) is met, the factorisation is redone in FP64 from
+    // a copy of the assembled SM taken before it, so NUMNEG and the pivot
+    // test are decided in FP64.  tau = 0 switches the guard (and the copy) off.
+    void set_inertia_guard(double tau) { guard_tol_ = tau; }
+    double inertia_guard() const { return guard_tol_; }
+    int64_t last_near_pivots() const { return last_near_; }
+    bool last_refactored() const { return last_refactor_; }
+    // Watchdog of the tensor-core update: time limit of each mbarrier wait
+    // (ns), and a test switch that makes one CTA's waits run out (the
+    // factorisation then returns -4 and the engine stays usable).
+    void set_watchdog(unsigned long long wait_ns, bool drop) {
+        wait_ns_ = wait_ns;
+        tc_drop_ = drop;
+    }
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
 
@@ -109,8 +126,10 @@ private:
         int64_t v;
         const void* c = nullptr;
         double y = 0.0;
+        double z = 0.0;
         bool operator==(const GraphKey& o) const {
-            return a == o.a && b == o.b && x == o.x && n == o.n && w == o.w && v == o.v && c == o.c && y == o.y;
+            return a == o.a && b == o.b && x == o.x && n == o.n && w == o.w && v == o.v && c == o.c && y == o.y &&
+                   z == o.z;
         }
     };
     struct GraphEntry {
@@ -127,6 +146,13 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     int mixed_ = 0;
+    double guard_tol_ = 1.0e-3;
+    int64_t last_near_ = 0;
+    bool last_refactor_ = false;
+    double* guard_copy_ = nullptr;           // assembled SM kept for the FP64 redo of the guard
+    int64_t guard_cap_ = 0;
+    unsigned long long wait_ns_ = 2000000000ull;
+    bool tc_drop_ = false;
     bool chol_ = false;                      // factor with SPRF27's pivot rule
     double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
     int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
@@ -164,6 +190,9 @@ private:
 // errors.  out[0]=NUMNEG out[1]=first failing column (1-based, 0 if none)
 // out[2]=that pivot out[3]=its original a_jj out[4]=max(a_jj/d_j).
 size_t dense_scratch_bytes(int64_t n);
+// Per-device set-up of dense_factor_with_scratch's kernels (their shared-memory
+// opt-in) on the current device; allocates nothing.  0 or -4.
+int dense_factor_setup();
 int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, double* d, void* scratch,
                               size_t scratch_bytes, cudaStream_t s, double* out);
 

@@ -52,6 +52,12 @@ void* scratch_address(int& err) {
             err = -4;
             return nullptr;
         }
+        // the kernels' shared-memory opt-in, so that the first call in a
+        // process (before any other entry point of this library) runs too
+        if (sprb::dense_factor_setup() != 0) {
+            err = -4;
+            return nullptr;
+        }
         g_scratch_ptr[dev] = p;
     }
     return g_scratch_ptr[dev];

@@ -1,5 +1,8 @@
 // Execution plan of the GPU numeric phase (see plan.h).
 #include "plan.h"
+#include "smhash.h"
+
+#include <thread>
 
 #include <algorithm>
 #include <cmath>
@@ -798,6 +801,26 @@ int64_t check_schedule(const Plan& P, bool tc, bool skip_join) {
         }
     }
     return bad;
+}
+
+uint64_t sm_hash_host(const double* a, int64_t n, int threads) {
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
+    auto part = [w](int64_t i0, int64_t i1) {
+        uint64_t acc = 0;
+        for (int64_t i = i0; i < i1; ++i) acc += sm_mix(w[i], (uint64_t)i);
+        return acc;
+    };
+    const int64_t per = int64_t(1) << 22;             // below 32 MB one thread is enough
+    int nt = (int)std::min<int64_t>(std::max(threads, 1), (n + per - 1) / per);
+    if (nt <= 1) return part(0, n);
+    std::vector<uint64_t> sums(nt, 0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t]() { sums[t] = part(n * t / nt, n * (t + 1) / nt); });
+    for (auto& th : pool) th.join();
+    uint64_t h = 0;
+    for (uint64_t v : sums) h += v;
+    return h;
 }
 
 }  // namespace sprb

@@ -40,7 +40,6 @@ constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024 + 256;
 constexpr int kThreads = 192;               // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2-5 epilogue
 constexpr uint32_t kTmemCols = 512;       // FP32 accumulator pair [0,256) + FP64 sums [256,512)
 constexpr int kChunk = 8;                   // K blocks (256 columns) per FP32 accumulation
-constexpr unsigned long long kWaitNs = 2000000000ull;    // 2 s per wait
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTM >> 3) << 17) |
@@ -74,14 +73,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase of the given parity; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait for the phase of the given parity; false when it gave up
+// after limit_ns (PV::wait_ns, 2 s by default).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
     for (;;) {
         for (int i = 0; i < 64; ++i)
             if (mbar_try(bar, parity)) return true;
-        if (now_ns() - t0 > kWaitNs) return false;
+        if (now_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
               const __grid_constant__ CUtensorMap tm) {
     using namespace tc;
     extern __shared__ uint8_t tc_raw[];
-    __shared__ uint64_t bars[2 * kStages + 4];
+    __shared__ uint64_t bars[2 * kStages + 5];
     __shared__ uint32_t tmem_slot;
     __shared__ int failed;
     if (P.st->any_fail) return;
@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             mbar_init(accf0 + 8 * b, 1);
             mbar_init(acce0 + 8 * b, 4);                  // one arrival per epilogue warp
         }
+        mbar_init(smem_u32(&bars[2 * kStages + 4]), 1);   // MMA drain before the TMEM is freed
         failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -302,12 +303,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             for (int kb = 0; kb < nkb; ++kb, ++g) {
                 const int s = (int)(g % kStages);
                 const uint32_t ph = (uint32_t)(g / kStages) & 1u;
-                if (g >= kStages && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                if (g >= kStages && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.wait_ns)) {
                     failed = 1;
                     break;
                 }
                 const uint32_t st = base + (uint32_t)s * kStageBytes;
                 const uint32_t fb = full0 + 8 * s;
+                if (P.tc_drop && blockIdx.x == 0 && g == 0) continue;     // watchdog test: never loaded
                 mbar_expect_tx(fb, kStageBytes);
                 const int64_t off = (int64_t)kb * np, arr = (int64_t)nkb * np;
                 tma_load_2d(st, &tm, fb, 0, (int)(ya + off));                                  // W_hi
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         }
         // drain: the last kStages issued stages must have landed before exit
         for (int64_t q = (g > kStages ? g - kStages : 0); q < g; ++q)
-            mbar_wait(full0 + 8 * (int)(q % kStages), (uint32_t)(q / kStages) & 1u);
+            mbar_wait(full0 + 8 * (int)(q % kStages), (uint32_t)(q / kStages) & 1u, P.wait_ns);
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer: chunks of kChunk K blocks into alternating accumulators
         int64_t g = 0, h = 0;
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             for (int c0 = 0; c0 < nkb && !stop; c0 += kChunk, ++h) {
                 const int b = (int)(h & 1);
                 const int64_t use = h >> 1;
-                if (use >= 1 && !mbar_wait(acce0 + 8 * b, (uint32_t)((use - 1) & 1))) {
+                if (use >= 1 && !mbar_wait(acce0 + 8 * b, (uint32_t)((use - 1) & 1), P.wait_ns)) {
                     failed = 1;
                     stop = true;
                     break;
@@ -340,7 +342,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 const int c1 = min(nkb, c0 + kChunk);
                 for (int kb = c0; kb < c1; ++kb, ++g) {
                     const int s = (int)(g % kStages);
-                    if (!mbar_wait(full0 + 8 * s, (uint32_t)(g / kStages) & 1u) || *(volatile int*)&failed) {
+                    if (!mbar_wait(full0 + 8 * s, (uint32_t)(g / kStages) & 1u, P.wait_ns) ||
+                        *(volatile int*)&failed) {
                         failed = 1;
                         stop = true;
                         break;
@@ -362,6 +365,10 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
             if (stop) break;
         }
+        // every MMA this thread issued has completed before the TMEM is freed
+        // (after a timeout some may still be in flight without a commit)
+        mma_commit(smem_u32(&bars[2 * kStages + 4]));
+        if (!mbar_wait(smem_u32(&bars[2 * kStages + 4]), 0u, P.wait_ns)) failed = 1;
     } else if (warp >= 2) {
         // ---- epilogue: warp w owns TMEM lanes 32 (w % 4) .. + 31 (tile rows)
         const int q = warp & 3;
@@ -382,7 +389,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             bool stop = false;
             for (int c = 0; c < nch; ++c, ++h) {
                 const int b = (int)(h & 1);
-                if (!mbar_wait(accf0 + 8 * b, (uint32_t)((h >> 1) & 1)) || *(volatile int*)&failed) {
+                if (!mbar_wait(accf0 + 8 * b, (uint32_t)((h >> 1) & 1), P.wait_ns) || *(volatile int*)&failed) {
                     failed = 1;
                     stop = true;
                     break;

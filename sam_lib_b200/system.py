@@ -4,8 +4,8 @@ The symbolic structure (MSPAR, MTREES, MSIFA, MEQN) is the reference's own:
 SPR's minimum-degree ordering, supernode partition and symbolic factorisation
 run on the host in the reference library (src/SPR/sprrnm.f, sprtrs.f,
 sprsmb.f).  For the seeded benchmark meshes their outputs are stored as
-compressed fixtures (tests/golden/structures/hex<n>.npz, produced by
-tests/golden/make_structures.py).  Assembly into SM is done here by the
+compressed package data (sam_lib_b200/structures/hex<n>.npz, produced by
+tests/golden/make_structures.py from the reference pipeline).  Assembly into SM is done here by the
 library's own bit-exact SPRADM main add (spr_b200_assemble).
 """
 import ctypes as C
@@ -16,8 +16,7 @@ import numpy as np
 from . import load
 from .fe import HexBox, hex8_stiffness
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-STRUCT_DIR = os.path.join(ROOT, 'tests', 'golden', 'structures')
+STRUCT_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'structures')
 
 
 def _p(a):

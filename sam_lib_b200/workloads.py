@@ -40,10 +40,25 @@ def lambda1(n):
     return float(w[0])
 
 
-def config4(count=512, seed=3, nrhs=16):
+def config4_draws(count=512, seed=3):
+    """(rng, box sizes n, shift factors) of the first two draws of config4."""
     rng = np.random.default_rng(seed)
     ns = rng.integers(3, 13, size=count)
     fac = rng.uniform(0.5, 2.0, size=count)
+    return rng, ns, fac
+
+
+def config4_system_sm(i, count=512, seed=3):
+    """(n, sigma, shifted SM) of system i of config4, without the right-hand sides."""
+    _, ns, fac = config4_draws(count, seed)
+    n = int(ns[i])
+    hs, sm, pos, mass = hex_system(n)
+    sigma = float(fac[i] * lambda1(n))
+    return n, sigma, shift_diagonal(sm, pos, mass, sigma), hs
+
+
+def config4(count=512, seed=3, nrhs=16):
+    rng, ns, fac = config4_draws(count, seed)
     systems = []
     for i in range(count):
         n = int(ns[i])

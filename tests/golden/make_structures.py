@@ -4,9 +4,10 @@ Runs the reference host pipeline (SPRPRP -> SPRSAS -> SPRRNM -> SPRTRS ->
 SPRSMB -> SPRPMP, from the oracle build oracle/_ref/libsprref.so, i.e. the
 reference's own minimum-degree ordering, supernode partition and symbolic
 factorisation) on n^3 hex8 boxes with the face x=0 clamped, and stores its
-outputs -- MSPAR, MTREES, MSIFA, MEQN, RINFO -- as compressed fixtures:
+outputs -- MSPAR, MTREES, MSIFA, MEQN, RINFO -- as compressed package data
+(the benchmark and the tests read them as a Fortran host's structure arrays):
 
-    tests/golden/structures/hex<n>.npz
+    sam_lib_b200/structures/hex<n>.npz
 
 The GPU product consumes these exactly as it would consume the arrays a
 Fortran host passes after calling those reference routines.
@@ -33,7 +34,7 @@ def delta(a):
 def make(n):
     rs = RefSystem(HexBox(n))
     sp = rs.mspar
-    out = os.path.join(HERE, 'structures', 'hex%d.npz' % n)
+    out = os.path.join(ROOT, 'sam_lib_b200', 'structures', 'hex%d.npz' % n)
     np.savez_compressed(out, n=n, mspar=sp, rinfo=rs.rinfo,
                         mtrees_d=delta(rs.mtrees[:sp[3]]), msifa_d=delta(rs.msifa[:sp[2]]),
                         meqn_d=delta(rs.meqn))

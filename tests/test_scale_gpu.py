@@ -1,0 +1,139 @@
+"""Parity at benchmark scale (GPU): the C ABI and the mixed mode against the
+oracle on 24^3 and 32^3 boxes, and per-system inertia of all 512 systems of
+the batched workload.
+
+The oracle (oracle/spr_oracle.c, pinned bitwise to the reference) runs in
+spawned worker processes, all cases at once, while the GPU cases run here.
+Cases (hex8 boxes, reference structure, SPRADM assembly):
+  24^3, E = 1                      (45,000 eq.)   FP64 through sprsol_
+  24^3, E = 1, K - 2.5 lambda1 M   (indefinite)   FP64 through sprsol_
+  32^3, E = 1, K - 2.5 lambda1 M   (104,544 eq.)  FP64 through sprsol_; mixed + refinement
+  32^3, E log-uniform [1, 1e4]     (cond ~1e9)    FP64 through sprsol_; mixed + refinement
+Tolerances (the GPU sums in another order than the reference):
+  factor   max|SM_gpu - SM_oracle| <= 1e-10 max|SM_oracle|
+  solution ||x - x_oracle|| / ||x_oracle|| <= 1e-9 (E = 1), 1e-6 (log-uniform)
+  inertia  NUMNEG, IERR, MSPAR exact; TOL(2), TOL(3) to 1e-10
+  mixed    NUMNEG exact, backward error <= 1e-12 after refinement, and the
+           refined solution against the oracle's FP64 solution to the same
+           solution tolerances
+The shifted cases also check that the oracle's smallest |d_j| / |a_jj| is
+far from zero (> 1e-8), so that their inertia is decided by FP64 rounding
+in any order.
+"""
+import concurrent.futures as cf
+import multiprocessing as mp
+import os
+
+import numpy as np
+import pytest
+
+import scale_oracle as so
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    'hex24': (24, 'uniform', 0.0, 2, 31),
+    'hex24_shift': (24, 'uniform', 2.5, 1, 32),
+    'hex32_shift': (32, 'uniform', 2.5, 2, 33),
+    'hex32_log': (32, 'loguniform', 0.0, 2, 34),
+}
+XTOL = {'uniform': 1e-9, 'loguniform': 1e-6}
+
+
+@pytest.fixture(scope='module')
+def oracle_runs(tmp_path_factory):
+    d = tmp_path_factory.mktemp('scale_oracle')
+    ex = cf.ProcessPoolExecutor(max_workers=min(12, os.cpu_count() or 1),
+                                mp_context=mp.get_context('spawn'))
+    futs = {k: ex.submit(so.run_case, v + (str(d / k),)) for k, v in CASES.items()}
+    chunks = [(i, min(512, i + 32)) for i in range(0, 512, 32)]
+    futs['batch'] = [ex.submit(so.batch_numneg, c) for c in chunks]
+    yield futs
+    ex.shutdown(wait=True, cancel_futures=True)
+
+
+def _oracle(futs, key):
+    out = futs[key].result(timeout=1800)
+    meta = np.load(out + '.meta.npz')
+    return dict(sm=np.load(out + '.sm.npy'), b=np.load(out + '.b.npy'), tol=meta['tol'],
+                mspar=meta['mspar'], ierr=int(meta['ierr']), min_ratio=float(meta['min_ratio']))
+
+
+def _relerr(x, y):
+    return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+
+@pytest.mark.parametrize('key', list(CASES))
+def test_fp64_abi_matches_oracle_at_scale(key, oracle_runs):
+    import sam_lib_b200 as spr
+    n, emod, sf, nrhs, seed = CASES[key]
+    hs, sm = so.case_system(n, emod, sf)
+    b = so.case_rhs(hs.neq, nrhs, seed)
+    o = _oracle(oracle_runs, key)
+    g_sm = sm.copy()
+    g_b = b.copy(order='F')
+    msp = hs.mspar.copy()
+    tol = np.array([1e-12, 0.0, 0.0])
+    ierr = spr.sprsol(3, msp, hs.mtrees, hs.msifa, g_sm, g_b, hs.neq, nrhs, tol)
+    spr.release_all()
+    assert ierr == o['ierr'] == 0, (ierr, o['ierr'])      # the solves reset SPRFC1's +3 (sprfs1.f:143)
+    assert np.array_equal(msp, o['mspar'])
+    if sf:
+        assert msp[25] > 0 and o['min_ratio'] > 1e-8, (msp[25], o['min_ratio'])
+    dsm = np.max(np.abs(g_sm - o['sm'])) / np.max(np.abs(o['sm']))
+    assert dsm <= 1e-10, dsm
+    ex = _relerr(g_b, o['b'])
+    assert ex <= XTOL[emod], ex
+    for k in (1, 2):
+        assert abs(tol[k] - o['tol'][k]) <= 1e-10 * abs(o['tol'][k]), (k, tol[k], o['tol'][k])
+    print('%s: NUMNEG %d  max|dSM|/max|SM| %.2e  solution rel. diff %.2e' % (key, msp[25], dsm, ex))
+
+
+@pytest.mark.parametrize('key', ['hex32_shift', 'hex32_log'])
+def test_mixed_refined_matches_oracle_at_scale(key, oracle_runs):
+    import torch
+    import sam_lib_b200 as spr
+    n, emod, sf, nrhs, seed = CASES[key]
+    hs, sm = so.case_system(n, emod, sf)
+    b = so.case_rhs(hs.neq, nrhs, seed)
+    o = _oracle(oracle_runs, key)
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    d_sm0 = torch.from_numpy(sm).cuda()
+    ds.build_residual(d_sm0)
+    d_b = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    d_x = torch.empty_like(d_b)
+    ds.set_mode(1)
+    d_mx = d_sm0.clone()
+    r = ds.factor(d_mx)
+    inf = ds.info()
+    ds.set_mode(0)
+    assert r['lierr'] == 0
+    assert r['numneg'] == o['mspar'][25], (r['numneg'], o['mspar'][25])
+    assert inf['fp64_redo'] == 0, inf              # away from an eigenvalue: the mixed factor is kept
+    it, berr, _ = ds.refine(d_mx, d_b, d_x, nrhs, tol=1e-12, maxit=20)
+    assert berr <= 1e-12 and it >= 1, (it, berr)
+    x = d_x.cpu().numpy().T
+    ex = _relerr(x, o['b'])
+    assert ex <= XTOL[emod], ex
+    print('%s mixed: NUMNEG %d  corrections %d  backward error %.2e  rel. diff from the oracle %.2e' %
+          (key, r['numneg'], it, berr, ex))
+    ds.close()
+
+
+@pytest.mark.parametrize('mode', [0, 1])
+def test_batched_inertia_of_all_512_systems_matches_oracle(mode, oracle_runs):
+    from sam_lib_b200.batch import BatchSolver
+    from sam_lib_b200.workloads import config4
+    want = [x for f in oracle_runs['batch'] for x in f.result(timeout=1800)]
+    assert len(want) == 512 and all(e in (0, 3) for e, _ in want)
+    bs = BatchSolver(config4())
+    bs.ds.set_mode(mode)
+    r = bs.run(solve=False)
+    bs.ds.set_mode(0)
+    assert r['lierr'] == 0
+    neg = bs.numneg()
+    wn = np.array([nn for _, nn in want])
+    bad = np.nonzero(neg != wn)[0]
+    assert bad.size == 0, [(int(i), int(neg[i]), int(wn[i])) for i in bad[:10]]
+    assert r['numneg'] == int(wn.sum())
+    assert (wn > 0).sum() > 100
