@@ -58,6 +58,7 @@ struct Ctx {
     double* d_dcor = nullptr;          // SPRFC3's DCOR(2,NEQ) on the device
     bool dev_chol = false;             // the device holds the L D L' form of a host C C' factor
     cudaStream_t stream = nullptr;
+    cudaStream_t copy = nullptr;       // host <-> device copies of a streamed factorisation
     // device factor residency
     const double* sm_host = nullptr;
     uint64_t sm_fp = 0;
@@ -67,6 +68,7 @@ struct Ctx {
         if (d_b) cudaFree(d_b);
         if (d_dcor) cudaFree(d_dcor);
         if (stream) cudaStreamDestroy(stream);
+        if (copy) cudaStreamDestroy(copy);
     }
 };
 
@@ -107,6 +109,13 @@ std::vector<int64_t> widen(const I* a, int64_t n) {
 void msg(I lpu, const char* routine, const char* text) {
     if (lpu < 0) return;
     fprintf(stderr, " *** ERROR return from SPR routine %s (GPU)\n     %s\n", routine, text);
+}
+
+// Message of a failed solve: rc -5 is the refused LDB < NEQ layout (see
+// reduced_rows_retained), anything else a CUDA failure.
+void solve_msg(I lpu, const char* routine, int rc, const char* text) {
+    msg(lpu, routine, rc == -5 ? "LDB < NEQ, BUT AN EQUATION OUTSIDE THE RETAINED SUPERNODES IS NUMBERED BEYOND LDB"
+                               : text);
 }
 
 // Structure fingerprint: MSPAR slots that describe the symbolic structure
@@ -276,15 +285,61 @@ int ensure_b(Ctx* c, int64_t n) {
     return 0;
 }
 
+// A solve with LDB < NEQ (MSPAR(57) = 1) handles only the equations whose
+// external number is at most LDB: the reference's gather reads the others as
+// zero and its scatter drops them, in every supernode it visits (SPRFB1/
+// SPRFB2, SPRFB3/SPRFB4 with PERI2E, sprfs1.f:704-900; SPRBS1 likewise).
+// The GPU sweeps run over all equations and zero those rows between the
+// forward and the back sweep, which is the same only when every such row
+// belongs to a retained supernode (never eliminated, skipped by both
+// sweeps), the layout the superelement partition produces.  Anything else
+// is refused rather than solved differently.
+bool reduced_rows_retained(Ctx* c, const I* msifa, int64_t ldb, bool peri2e) {
+    const sprb::Plan& P = c->eng.plan();
+    for (int64_t js = 0; js < P.nsuper; ++js) {
+        if (P.retained[js]) continue;
+        for (int64_t r = P.fst[js]; r < P.fst[js] + P.S[js]; ++r) {
+            const int64_t ext = peri2e ? (int64_t)msifa[r] - 1 : r;
+            if (ext >= ldb) return false;
+        }
+    }
+    return true;
+}
+
 // H2D of SM, device factorisation, D2H of SM.  Returns the SPRFC1 IERR, with
 // dcor (host DCOR(2,NEQ)) the SPRFC3 one, with chol the SPRFC2 one (the host
 // receives C C', the device keeps its L D L' form for the solves).
-I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nullptr, bool chol = false) {
+// True when the host array lies in page-locked memory (cudaMallocHost,
+// cudaHostRegister or a pinned torch tensor): copies from and to it are
+// asynchronous DMA, so they can overlap the factorisation.
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// The copy stream's downloads of a streamed factorisation must be complete
+// before the caller reads SM.
+int finish_copies(Ctx* c) {
+    return (c && c->copy && cudaStreamSynchronize(c->copy) != cudaSuccess) ? -4 : 0;
+}
+
+// defer: leave the streamed factorisation's last downloads running (the
+// caller queues a solve behind them and then calls finish_copies).
+I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nullptr, bool chol = false,
+            bool defer = false) {
     const int64_t neq = mspar[7], nzerol = mspar[15];
     const int64_t nsm = neq + nzerol;
     const char* who = chol ? "SPRFC2" : dcor ? "SPRFC3" : "SPRFC1";
     cudaStream_t s = c->stream;
-    if (cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return -4;
+    // SPRFC1 on a pinned SM: upload, factorisation and download overlap, level by level
+    const bool streamed = !chol && !dcor && is_pinned(sm);
+    if (streamed && !c->copy && cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) return -4;
+    if (!streamed && cudaMemcpyAsync(c->d_sm, sm, nsm * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return -4;
     Engine::Singular fc3{0.0, nullptr};
     if (dcor) {
         if (!c->d_dcor && cudaMalloc((void**)&c->d_dcor, 2 * std::max<int64_t>(neq, 1) * sizeof(double)) != cudaSuccess)
@@ -293,8 +348,11 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
         fc3.d_dcor = c->d_dcor;
     }
     FactorResult r;
-    const int frc = chol ? c->eng.factor_chol(c->d_sm, tol[0], r) : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
+    const int frc = streamed ? c->eng.factor_streamed(sm, c->d_sm, tol[0], r, c->copy)
+                    : chol   ? c->eng.factor_chol(c->d_sm, tol[0], r)
+                             : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
     if (frc != 0) {
+        finish_copies(c);
         msg(lpu, who, "CUDA failure in the factorisation");
         return -4;
     }
@@ -302,7 +360,11 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     if (chol_ok && c->eng.chol_convert(c->d_sm, true) != 0) return -4;
     uint64_t fp = 0;                                  // hash of exactly what the host receives
     if (c->eng.hash(c->d_sm, nsm, fp) != 0) return -4;
-    if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -4;
+    if (streamed) {
+        if (!defer && finish_copies(c) != 0) return -4;
+    } else if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+        return -4;
+    }
     if (chol_ok && c->eng.chol_convert(c->d_sm, false) != 0) return -4;
     c->dev_chol = chol_ok;
     if (dcor && cudaMemcpyAsync(dcor, c->d_dcor, 2 * neq * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -387,6 +449,7 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
     const bool peri2e = mspar[57] >= 1;                 // sprfs1.f:240-250, SPRFB3/SPRFB4
     std::vector<double> tmp;
     const int64_t nfull = mspar[7];
+    if (neq != nfull && !reduced_rows_retained(c, msifa, neq, peri2e)) return -5;
     if (peri2e || neq != nfull) {
         tmp.assign(nfull * nrhs, 0.0);
         const I* p2e = msifa;                           // PERI2E = MSIFA(1..NEQ)
@@ -455,6 +518,43 @@ int do_solve(Ctx* c, I* mspar, I* msifa, const double* sm, double* b, I ldb, I n
     return 0;
 }
 
+// SPRFC1 (src/SPR/sprfc1.f:5) under g_mu; returns the context (null on an
+// early error).  defer: see do_factor.
+Ctx* fc1_locked(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, const I* lpu, I* ierr, void (*mvmult)(),
+                void (*mmmult)(), bool defer) {
+    if (mspar[0] < 0) {                                 // sprfc1.f:140-148
+        mspar[0] = -5;
+        *ierr = -1;
+        msg(*lpu, "SPRFC1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return nullptr;
+    }
+    mspar[0] = 5;
+    *ierr = 0;
+    if (!fc1_lengths_ok(mspar)) {
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFC1", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return nullptr;
+    }
+    if (!callbacks_ok(mvmult, mmmult, true)) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRFC1", "MVMULT/MMMULT DO NOT COMPUTE THE LDL' UPDATES OF LMVY18/LMMY18");
+        return nullptr;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c) {
+        mspar[0] = -5;
+        *ierr = (err == -2) ? -2 : -4;
+        msg(*lpu, "SPRFC1", "COULD NOT SET UP THE GPU CONTEXT");
+        return nullptr;
+    }
+    *ierr = do_factor(c, mspar, sm, tol, *lpu, nullptr, false, defer);
+    if (*ierr < 0 && *ierr != -3) mspar[0] = -5;
+    return c;
+}
+
 }  // namespace
 
 extern "C" {
@@ -465,36 +565,7 @@ void SPR_API(sprfc1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
     (void)iwork;
     (void)rwork;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (mspar[0] < 0) {                                 // sprfc1.f:140-148
-        mspar[0] = -5;
-        *ierr = -1;
-        msg(*lpu, "SPRFC1", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
-        return;
-    }
-    mspar[0] = 5;
-    *ierr = 0;
-    if (!fc1_lengths_ok(mspar)) {
-        mspar[0] = -2;
-        *ierr = -2;
-        msg(*lpu, "SPRFC1", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
-        return;
-    }
-    if (!callbacks_ok(mvmult, mmmult, true)) {
-        mspar[0] = -5;
-        *ierr = -4;
-        msg(*lpu, "SPRFC1", "MVMULT/MMMULT DO NOT COMPUTE THE LDL' UPDATES OF LMVY18/LMMY18");
-        return;
-    }
-    int err = 0;
-    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-    if (!c) {
-        mspar[0] = -5;
-        *ierr = (err == -2) ? -2 : -4;
-        msg(*lpu, "SPRFC1", "COULD NOT SET UP THE GPU CONTEXT");
-        return;
-    }
-    *ierr = do_factor(c, mspar, sm, tol, *lpu);
-    if (*ierr < 0 && *ierr != -3) mspar[0] = -5;
+    fc1_locked(mspar, mtrees, msifa, sm, tol, lpu, ierr, mvmult, mmmult, false);
 }
 
 // SPRFC3 (src/SPR/sprfc3.f:5): LDL' factorisation that replaces singular
@@ -599,10 +670,11 @@ static void chol_sweep(const char* who, int which, I* mspar, I* mtrees, I* msifa
     }
     int err = 0;
     Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, which, true) != 0) {
+    const int rc = c ? do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, which, true) : -4;
+    if (rc != 0) {
         mspar[0] = -8;
         *ierr = -4;
-        msg(*lpu, who, "GPU CHOLESKY SOLVE FAILED");
+        solve_msg(*lpu, who, rc, "GPU CHOLESKY SOLVE FAILED");
     }
 }
 
@@ -641,10 +713,11 @@ void SPR_API(sprfs1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, cons
     }
     int err = 0;
     Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 1) != 0) {
+    const int rc = c ? do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 1) : -4;
+    if (rc != 0) {
         mspar[0] = -7;
         *ierr = -4;
-        msg(*lpu, "SPRFS1", "GPU FORWARD SOLVE FAILED");
+        solve_msg(*lpu, "SPRFS1", rc, "GPU FORWARD SOLVE FAILED");
     }
 }
 
@@ -669,10 +742,11 @@ void SPR_API(sprbs1_)(I* mspar, I* mtrees, I* msifa, double* sm, double* b, cons
     }
     int err = 0;
     Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-    if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 2) != 0) {
+    const int rc = c ? do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 2) : -4;
+    if (rc != 0) {
         mspar[0] = -7;
         *ierr = -4;
-        msg(*lpu, "SPRBS1", "GPU BACK SUBSTITUTION FAILED");
+        solve_msg(*lpu, "SPRBS1", rc, "GPU BACK SUBSTITUTION FAILED");
     }
 }
 
@@ -682,11 +756,17 @@ void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, d
                       const I* nrhs, double* tol, I* iwork, double* rwork, const I* lpu, I* ierr) {
     *ierr = 0;
     const I op = *iop;
-    if (op <= 3) SPR_API(sprfc1_)(mspar, mtrees, msifa, sm, tol, iwork, rwork, lpu, ierr, nullptr, nullptr);
-    const bool fwd = op >= 2 && op <= 5 && *ierr >= 0;
     const bool bwd = op >= 3 && op != 5;
+    std::unique_lock<std::mutex> lk(g_mu);
+    // IOP = 3: the factorisation's last downloads (pinned SM) overlap the solves
+    Ctx* fc = nullptr;
+    if (op <= 3) fc = fc1_locked(mspar, mtrees, msifa, sm, tol, lpu, ierr, nullptr, nullptr, op == 3);
+    const bool fwd = op >= 2 && op <= 5 && *ierr >= 0;
     if (fwd && bwd) {
-        std::lock_guard<std::mutex> lk(g_mu);
+        struct Finish {                                  // at every return below
+            Ctx* c;
+            ~Finish() { finish_copies(c); }
+        } finish{fc};
         if (mspar[0] < 0) {
             mspar[0] = -7;
             *ierr = -1;
@@ -703,13 +783,21 @@ void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, d
         }
         int err = 0;
         Ctx* c = get_ctx(mspar, mtrees, msifa, err);
-        if (!c || do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3, false, op <= 3) != 0) {
+        const int rc = c ? do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3, false, op <= 3) : -4;
+        if (rc != 0 || finish_copies(fc) != 0) {
             mspar[0] = -7;
             *ierr = -4;
-            msg(*lpu, "SPRSOL", "GPU SOLVE FAILED");
+            solve_msg(*lpu, "SPRSOL", rc, "GPU SOLVE FAILED");
         }
         return;
     }
+    if (finish_copies(fc) != 0 && *ierr >= 0) {
+        mspar[0] = -5;
+        *ierr = -4;
+        msg(*lpu, "SPRSOL", "GPU COPY OF THE FACTOR FAILED");
+        return;
+    }
+    lk.unlock();
     if (fwd) SPR_API(sprfs1_)(mspar, mtrees, msifa, sm, b, ldb, nrhs, iwork, rwork, lpu, ierr);
     if (bwd && !fwd && *ierr >= 0) SPR_API(sprbs1_)(mspar, mtrees, msifa, sm, b, ldb, nrhs, rwork, lpu, ierr);
 }

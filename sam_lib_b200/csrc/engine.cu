@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 
 #include "engine.h"
 #include "smhash.h"
@@ -102,6 +103,9 @@ struct PV {
     // operand load, so that its waits run out and the launch reports a timeout
     unsigned long long wait_ns;
     int tc_drop;
+    // streamed factorisation: the original diagonal gathered on the host
+    // (the pre-pass then reads it instead of LNZ, which is still uploading)
+    const double* adiag_in;
 };
 
 struct Engine::Dev {
@@ -191,7 +195,7 @@ __device__ __forceinline__ const Job& job_of(const Job* jobs, int64_t njobs, con
 // packed lower, column-major, order F: column j holds rows j..F-1
 __device__ __forceinline__ int pk(int i, int j, int F) { return j * F - ((j * (j - 1)) >> 1) + (i - j); }
 
-__device__ __forceinline__ int64_t lnz_col(int64_t j, int64_t F) { return j * F - (j * (j - 1)) / 2; }
+__host__ __device__ __forceinline__ int64_t lnz_col(int64_t j, int64_t F) { return j * F - (j * (j - 1)) / 2; }
 
 // record a failed pivot (sprfc1.f:1274-1279): first failure per supernode wins
 // A failed front poisons its ancestors only: fronts earlier in postorder than
@@ -258,7 +262,7 @@ __global__ void k_prepass(PV P, int64_t nsuper) {
             continue;
         }
         for (int j = lane; j < s; j += 32) {
-            double a = col[lnz_col(j, f)];
+            double a = P.adiag_in ? P.adiag_in[fst + j] : col[lnz_col(j, f)];
             if (P.fc3) {                                  // sprfc3.f:561-572
                 double* dc = P.dcor + 2 * (int64_t)(fst + j);
                 dc[0] = 0.0;
@@ -542,6 +546,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     __shared__ double rdv[kNB];
     __shared__ double dd[kNB];
     __shared__ double adv[kNB];
+    __shared__ double Tb[kNB * kNB / 4];    // T = L21 X11 of the inverse's doubling passes
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -636,48 +641,43 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
                 A[i][j] = (i > j) ? v[a][b] * rdv[j] : (PR == kPivotReplace ? dd[j] : v[a][b]);
         }
     __syncthreads();
-    // X = L^-1 by a column sweep: X = I, then at step m every X[i][j] with
-    // i > m >= j loses L[i][m] X[m][j]; row m of X is final at step m
-    double x[R][R];
-#pragma unroll
-    for (int a = 0; a < R; ++a)
-#pragma unroll
-        for (int b = 0; b < R; ++b) x[a][b] = (tx + 16 * a == ty + 16 * b) ? 1.0 : 0.0;
-    for (int m = 0; m < nb - 1; ++m) {
-        const int buf = m & 1, mb = m >> 4;
-        if (tx == (m & 15)) {
-#pragma unroll
-            for (int b = 0; b < R; ++b) {
-                const int j = ty + 16 * b;
-                double c = x[0][b];
-#pragma unroll
-                for (int a = 1; a < R; ++a)
-                    if (a == mb) c = x[a][b];
-                if (j <= m) vec[buf][j] = c;
+    // X = L^-1 by recursive doubling: after the pass of order b, each aligned
+    // diagonal block of X of order 2b is final, its lower-left quarter being
+    // X21 = -X22 (L21 X11) (X11, X22 from the pass before; unit diagonals).
+    // X is kept transposed in the free upper triangle of A (X[i][j] at A[j][i]),
+    // T = L21 X11 in Tb; 12 barriers instead of one per column.
+    for (int b = 1; b < kNB; b <<= 1) {
+        const int bb = b * b, tot = (kNB / (2 * b)) * bb;
+        for (int e = tid; e < tot; e += blockDim.x) {
+            const int k = e / bb, r = e - k * bb, i = r / b, j = r - i * b;
+            const int base = 2 * k * b, gi = base + b + i, gj = base + j;
+            double t = 0.0;
+            if (gi < nb) {
+                t = A[gi][gj];                                   // X11[j][j] = 1
+                for (int m = j + 1; m < b; ++m) t += A[gi][base + m] * A[gj][base + m];   // L21[i][m] X11[m][j]
             }
+            Tb[e] = t;
         }
         __syncthreads();
-        double xm[R];
-#pragma unroll
-        for (int b = 0; b < R; ++b) xm[b] = vec[buf][ty + 16 * b];
-#pragma unroll
-        for (int a = 0; a < R; ++a) {
-            const int i = tx + 16 * a;
-            if (i > m && i < nb) {
-                const double lim = A[i][m];
-#pragma unroll
-                for (int b = 0; b < R; ++b)
-                    if (ty + 16 * b <= m) x[a][b] -= lim * xm[b];
-            }
+        for (int e = tid; e < tot; e += blockDim.x) {
+            const int k = e / bb, r = e - k * bb, i = r / b, j = r - i * b;
+            const int base = 2 * k * b, gi = base + b + i;
+            double x = Tb[e];                                    // X22[i][i] = 1
+            for (int m = 0; m < i; ++m) x += A[base + b + m][gi] * Tb[k * bb + m * b + j];   // X22[i][m] T[m][j]
+            A[base + j][gi] = -x;
         }
+        __syncthreads();
     }
     double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int i = e % kNB, j = e / kNB;
+        lv[e] = (i < nb && j < nb) ? (i > j ? A[j][i] : (i == j ? 1.0 : 0.0)) : 0.0;
+    }
 #pragma unroll
     for (int a = 0; a < R; ++a)
 #pragma unroll
         for (int b = 0; b < R; ++b) {
             const int i = tx + 16 * a, j = ty + 16 * b;
-            lv[i + j * kNB] = (i < nb && j < nb) ? (i > j ? x[a][b] : (i == j ? 1.0 : 0.0)) : 0.0;
             if (i >= j && i < nb && j < nb) front[(int64_t)(k0 + i) + (int64_t)(k0 + j) * ld] = A[i][j];
         }
     if (tid < nb) P.dvec[fst + k0 + tid] = A[tid][tid];
@@ -1995,6 +1995,31 @@ __global__ void k_axpy(double* x, const double* d, int64_t n) {
 // Engine
 // ---------------------------------------------------------------------------
 #define TMAP(l) ((l).map_begin >= 0 ? d_->task_map + (l).map_begin : nullptr)
+// Copy plan of the streamed factorisation.  Levels below L1 form group 0; each
+// level L >= L1 is group L - L1 + 1 (L1 is the lowest level with at most
+// kMaxTopNodes supernodes at or above it, so the copies stay few).  A group's
+// LNZ ranges are its supernodes' blocks, adjacent blocks merged; group 0 is
+// the gaps between the others.
+struct Engine::Transfer {
+    static constexpr int64_t kMaxTopNodes = 1024;
+    int L1 = 0;
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges;   // per group: (LNZ offset, doubles)
+    std::vector<cudaEvent_t> up, done;                             // per group
+    cudaEvent_t start = nullptr, fin = nullptr;
+    std::vector<int64_t> diag_pos;                                 // LNZ offset of each equation's diagonal
+    double* h_diag = nullptr;                                      // pinned
+    double* d_diag = nullptr;
+    ~Transfer() {
+        for (cudaEvent_t e : up) cudaEventDestroy(e);
+        for (cudaEvent_t e : done) cudaEventDestroy(e);
+        if (start) cudaEventDestroy(start);
+        if (fin) cudaEventDestroy(fin);
+        if (h_diag) cudaFreeHost(h_diag);
+        if (d_diag) cudaFree(d_diag);
+    }
+    int group(int32_t level) const { return level < L1 ? 0 : level - L1 + 1; }
+};
+
 Engine::Engine() : d_(new Dev()) {
     const char* e = getenv("SPR_B200_GRAPHS");
     use_graphs_ = !(e && e[0] == '0');
@@ -2032,6 +2057,7 @@ Engine::~Engine() {
     if (csr_.rowabs) cudaFree(csr_.rowabs);
     if (rbuf_) cudaFree(rbuf_);
     if (guard_copy_) cudaFree(guard_copy_);
+    xfer_.reset();
     if (!d_) return;
     for (void* p : d_->owned) cudaFree(p);
     if (d_->arena) cudaFree(d_->arena);
@@ -2224,6 +2250,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.near_tol = 0.0;
     v.wait_ns = 2000000000ull;
     v.tc_drop = 0;
+    v.adiag_in = nullptr;
     return v;
 }
 
@@ -2288,6 +2315,15 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         const LevelPlan& lp = P_.levels[L];
         snprintf(lname, sizeof lname, "factor level %zu", L);
         NvtxRange level_range(lname);
+        if (hooks_) hooks_->before(L, s);
+        struct AfterLevel {                      // runs at every exit of this iteration
+            const LevelHooks* h;
+            size_t L;
+            cudaStream_t s;
+            ~AfterLevel() {
+                if (h) h->after(L, s);
+            }
+        } after_level{hooks_, L, s};
         if (!lp.small_nodes.empty()) {
             mark(1);
             for (const LevelPlan::SmallClass& c : lp.small_classes) {
@@ -2392,6 +2428,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     }
     pv.wait_ns = wait_ns_;
     pv.tc_drop = tc_drop_ ? 1 : 0;
+    pv.adiag_in = streamed_diag_;
     linv_valid_ = false;
     last_near_ = 0;
     last_refactor_ = false;
@@ -2427,7 +2464,8 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     std::vector<cudaEvent_t> gev;
     // the legacy default stream cannot be captured: graphs need a stream of our own;
     // the watchdog test launches kernel by kernel (its settings are not in the key)
-    const bool graph = use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull;
+    // a streamed factorisation enqueues its copies' waits between the levels
+    const bool graph = use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull && !hooks_;
     if (graph) {
         const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_ | (chol_ ? 16 : 0),
                            (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4,
@@ -2555,6 +2593,122 @@ int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
     CK(cudaMemcpyAsync(&hv, D.hbuf, sizeof(hv), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     h = (uint64_t)hv;
+    return 0;
+}
+
+namespace {
+// Waits for each group's upload before its first level; after a group's last
+// level, queues the download of its finished LNZ ranges on the copy stream.
+struct StreamHooks : LevelHooks {
+    const Engine::Transfer* t = nullptr;
+    size_t nlev = 0;
+    cudaStream_t cs = nullptr;
+    double* h_lnz = nullptr;
+    const double* d_lnz = nullptr;
+    void before(size_t L, cudaStream_t s) const override {
+        const int g = t->group((int32_t)L);
+        if (L == 0 || (g > 0)) cudaStreamWaitEvent(s, t->up[g], 0);
+    }
+    void after(size_t L, cudaStream_t s) const override {
+        const int g = t->group((int32_t)L);
+        const bool last_of_group = (L + 1 == nlev) || t->group((int32_t)(L + 1)) != g;
+        if (!last_of_group) return;
+        cudaEventRecord(t->done[g], s);
+        cudaStreamWaitEvent(cs, t->done[g], 0);
+        for (const auto& r : t->ranges[g])
+            cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double), cudaMemcpyDeviceToHost, cs);
+    }
+};
+}  // namespace
+
+int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResult& res, cudaStream_t cs) {
+    NvtxRange range("spr_b200 factor (streamed copies)");
+    const int64_t neq = P_.neq;
+    if (!xfer_) {
+        std::unique_ptr<Transfer> t(new Transfer());
+        const int32_t nlev = (int32_t)P_.levels.size();
+        std::vector<int64_t> at_level(nlev + 1, 0);
+        for (int64_t js = 0; js < P_.nsuper; ++js) ++at_level[P_.level[js]];
+        int64_t above = 0;
+        t->L1 = nlev;
+        for (int32_t L = nlev - 1; L >= 1; --L) {
+            above += at_level[L];
+            if (above > Transfer::kMaxTopNodes) break;
+            t->L1 = L;
+        }
+        const int ng = 1 + (nlev - t->L1);
+        t->ranges.assign(ng, {});
+        for (int64_t js = 0; js < P_.nsuper; ++js) {
+            const int64_t f = P_.F[js], sw = P_.S[js];
+            const int64_t off = P_.lnz_off[js], len = f * sw - sw * (sw - 1) / 2;
+            auto& rg = t->ranges[t->group(P_.level[js])];
+            if (!rg.empty() && rg.back().first + rg.back().second == off)
+                rg.back().second += len;
+            else
+                rg.emplace_back(off, len);
+        }
+        t->up.resize(ng);
+        t->done.resize(ng);
+        for (int g = 0; g < ng; ++g) {
+            CK(cudaEventCreateWithFlags(&t->up[g], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&t->done[g], cudaEventDisableTiming));
+        }
+        CK(cudaEventCreateWithFlags(&t->start, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&t->fin, cudaEventDisableTiming));
+        t->diag_pos.resize(neq);
+        for (int64_t js = 0; js < P_.nsuper; ++js)
+            for (int64_t j = 0; j < P_.S[js]; ++j) t->diag_pos[P_.fst[js] + j] = P_.lnz_off[js] + lnz_col(j, P_.F[js]);
+        CK(cudaMallocHost((void**)&t->h_diag, std::max<int64_t>(neq, 1) * sizeof(double)));
+        CK(cudaMalloc((void**)&t->d_diag, std::max<int64_t>(neq, 1) * sizeof(double)));
+        xfer_ = std::move(t);
+    }
+    Transfer& t = *xfer_;
+    cudaStream_t s = stream_;
+    double* h_lnz = h_sm + neq;
+    double* d_lnz = d_sm + neq;
+    // the copy stream starts after the compute stream's earlier work
+    CK(cudaEventRecord(t.start, s));
+    CK(cudaStreamWaitEvent(cs, t.start, 0));
+    // D on the compute stream (the pre-pass writes D of retained supernodes),
+    // LNZ on the copy stream group by group, lowest levels first
+    CK(cudaMemcpyAsync(d_sm, h_sm, neq * sizeof(double), cudaMemcpyHostToDevice, s));
+    for (size_t g = 0; g < t.ranges.size(); ++g) {
+        for (const auto& r : t.ranges[g])
+            CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double), cudaMemcpyHostToDevice,
+                               cs));
+        CK(cudaEventRecord(t.up[g], cs));
+    }
+    // the pre-pass needs every original diagonal before anything is factored
+    // (the zero test of sprfc1.f:465-488): gather them here while LNZ uploads
+    {
+        const int nt = (int)std::min<int64_t>(8, std::max<int64_t>(1, neq / 65536));
+        std::vector<std::thread> pool;
+        for (int k = 0; k < nt; ++k)
+            pool.emplace_back([&, k]() {
+                for (int64_t j = neq * k / nt; j < neq * (k + 1) / nt; ++j) t.h_diag[j] = h_lnz[t.diag_pos[j]];
+            });
+        for (auto& th : pool) th.join();
+    }
+    CK(cudaMemcpyAsync(t.d_diag, t.h_diag, neq * sizeof(double), cudaMemcpyHostToDevice, s));
+    StreamHooks hk;
+    hk.t = &t;
+    hk.nlev = P_.levels.size();
+    hk.cs = cs;
+    hk.h_lnz = h_lnz;
+    hk.d_lnz = d_lnz;
+    hooks_ = &hk;
+    streamed_diag_ = t.d_diag;
+    const int rc = factor(d_sm, tol1, res, nullptr);
+    hooks_ = nullptr;
+    streamed_diag_ = nullptr;
+    if (rc != 0) {
+        cudaStreamSynchronize(cs);
+        return rc;
+    }
+    // D is final only now (and on a zero diagonal it holds the original diagonal)
+    CK(cudaEventRecord(t.fin, s));
+    CK(cudaStreamWaitEvent(cs, t.fin, 0));
+    CK(cudaMemcpyAsync(h_sm, d_sm, neq * sizeof(double), cudaMemcpyDeviceToHost, cs));
     return 0;
 }
 

@@ -37,6 +37,15 @@ struct Timing {              // CUDA-event times of the last calls (ms)
     float phase_ms[20] = {};
 };
 
+// Callbacks around each elimination-tree level of a factorisation's launch
+// sequence (streamed factorisation: waits for a level's upload before it,
+// downloads of its finished columns after it).
+struct LevelHooks {
+    virtual ~LevelHooks() = default;
+    virtual void before(size_t level, cudaStream_t s) const = 0;
+    virtual void after(size_t level, cudaStream_t s) const = 0;
+};
+
 class Engine {
 public:
     Engine();
@@ -62,6 +71,13 @@ public:
     // trace / min(sqrt d)^2.  The device SM is left in L D L' form; chol_convert
     // turns it into the C C' form (C = L D^1/2, sqrt d in D) and back.
     int factor_chol(double* d_sm, double tol1, FactorResult& res);
+    // SPRFC1 semantics with the host copies overlapped: h_sm (pinned host
+    // memory, NEQ + NZEROL doubles) is uploaded level by level on the copy
+    // stream cs while the lower levels factor, and each level's finished
+    // columns go back into h_sm while the higher levels factor.  On return the
+    // factorisation is complete on the device (res as factor()); the last
+    // downloads may still run on cs: synchronise cs before reading h_sm.
+    int factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResult& res, cudaStream_t cs);
     int chol_convert(double* d_sm, bool to_chol);
     // b (device, ldb x nrhs, the first NEQ rows) times sqrt(d), or divided by
     // it, for every equation with d > 0 (d = the D part of an L D L' device SM)
@@ -115,6 +131,7 @@ public:
     }
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
+    struct Transfer;         // copy ranges and events of the streamed factorisation
 
 private:
     struct GraphKey {
@@ -145,6 +162,9 @@ private:
                        int64_t& nl);
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
+    const LevelHooks* hooks_ = nullptr;      // set during a streamed factorisation
+    const double* streamed_diag_ = nullptr;  // its host-gathered original diagonal (device)
+    std::unique_ptr<Transfer> xfer_;
     int mixed_ = 0;
     double guard_tol_ = 1.0e-3;
     int64_t last_near_ = 0;
