@@ -310,7 +310,7 @@ def form_mixed_ir(torch, spr, n, emod, reps=2):
             'rel_diff_vs_fp64_gpu_solution': rel}
 
 
-def form_batched(torch, reps=3):
+def form_batched(torch, reps=3, cpu_procs=0):
     """512 uneven shifted (indefinite) systems, 16 RHS each, as one forest."""
     from sam_lib_b200.batch import BatchSolver
     from sam_lib_b200.workloads import config4
@@ -353,7 +353,57 @@ def form_batched(torch, reps=3):
     torch.cuda.empty_cache()
     out['workload'] = ('512 boxes n~U{3..12} (seed 3), K - sigma M, sigma = U[0.5,2] x lambda1, '
                        '16 RHS each, merged forest (%s)' % 'one launch per kernel per tree level')
+    out['fp32_ir_note'] = ('the mixed form: 3xTF32 Schur updates in the fronts larger than 176 (FP32 '
+                           'accumulation), everything else FP64, then FP64 refinement to 1e-12; most fronts '
+                           'of these systems are small, so it gains little and the refinement sweeps cost more')
+    if cpu_procs:
+        out['cpu_reference'] = batched_cpu_sample(cpu_procs)
     return out
+
+
+def _batched_cpu_worker(idx):
+    """Reference SPRSOL(IOP=3), 16 RHS, on systems idx of the 512-system workload (CPU)."""
+    import time as _t
+    from oracle.refpipe import lib as reflib, _p, _i
+    import ctypes as _C
+    from sam_lib_b200.workloads import config4_system_sm
+    R = reflib()
+    done, t = 0, 0.0
+    for i in idx:
+        _, _, sm, hs = config4_system_sm(i)
+        sm = sm.copy()
+        b = np.asfortranarray(np.random.default_rng(i).uniform(-1.0, 1.0, size=(hs.neq, 16)))
+        msp = hs.mspar.copy()
+        tol = np.array([1e-12, 0.0, 0.0])
+        iw = np.zeros(int(hs.mspar[13]) + int(hs.mspar[12]) + 8, dtype=np.int64)
+        rw = np.zeros(int(hs.mspar[16]) + int(hs.mspar[13]) + 8)
+        ierr = _C.c_int64(0)
+        t0 = _t.perf_counter()
+        R.sprsol_(_i(3), _p(msp), _p(hs.mtrees), _p(hs.msifa), _p(sm), _p(b), _i(hs.neq), _i(16), _p(tol),
+                  _p(iw), _p(rw), _i(-1), _C.byref(ierr))
+        t += _t.perf_counter() - t0
+        done += 1
+    return done, t
+
+
+def batched_cpu_sample(nproc, per_proc=8):
+    """Systems/s of the reference on the 512-system workload, one process per
+    host core, each factoring and solving its own share of a bounded sample
+    (the first nproc*per_proc systems; sizes are drawn i.i.d., so the sample
+    has the workload's size mix)."""
+    import multiprocessing as mp
+    n = min(512, nproc * per_proc)
+    shares = [list(range(k, n, nproc)) for k in range(nproc)]
+    ctx = mp.get_context('spawn')
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_batched_cpu_worker, shares)
+    wall = time.perf_counter() - t0
+    busy = max(r[1] for r in res)
+    return {'systems_per_s': n / busy, 'unit': 'systems/s', 'cores': nproc, 'kind': 'reference',
+            'sample': 'reference SPRSOL IOP=3 (16 RHS) on the first %d of the 512 systems, %d processes '
+                      '(one per core, each timing its own systems; rate = systems / the slowest process time)' % (n, nproc),
+            'wall_s_incl_setup': wall}
 
 
 def form_adjoint(torch, reps=3):
@@ -568,7 +618,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_forms and args.n == N_MESH:
         forms = {'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
                  'mixed_ir_uniform': form_mixed_ir(torch, spr, N_MESH, 'uniform'),
-                 'batched': form_batched(torch), 'adjoint': form_adjoint(torch)}
+                 'batched': form_batched(torch, cpu_procs=os.cpu_count() or 1), 'adjoint': form_adjoint(torch)}
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',

@@ -56,6 +56,16 @@ void sprfc2_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double
              SPR_INT* iwork, double* rwork, const SPR_INT* lpu, SPR_INT* ierr,
              void (*mvmult)(), void (*mmmult)());
 
+/* Replaces SPRFC4, src/SPR/sprfc4.f:5-262 (Cholesky C C' with SPRF47's pivot
+ * replacement, sprfc4.f:978-1000): TOL(4) and DCOR(2,NEQ) as SPRFC3; a pivot
+ * below -TOL(1)|a_jj| stops with IERR = -3, MSPAR(27) = its equation; replaced
+ * pivots give IERR = -3, MSPAR(27) = -(number replaced) and a complete factor.
+ * MSPAR(1) = 6; MSPAR(26) = 0 as the reference reports it.  MVMULT/MMMULT as
+ * SPRFC2 (CMVY18/CMMY18, or null). */
+void sprfc4_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* tol,
+             SPR_INT* iwork, double* rwork, double* dcor, const SPR_INT* lpu, SPR_INT* ierr,
+             void (*mvmult)(), void (*mmmult)());
+
 /* Replaces SPRFS2, src/SPR/sprfs2.f:5-265 (forward sweep C y = b on a C C'
  * factor, MSPAR(1) = 8). */
 void sprfs2_(SPR_INT* mspar, SPR_INT* mtrees, SPR_INT* msifa, double* sm, double* b,

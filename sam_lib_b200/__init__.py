@@ -2,7 +2,7 @@
 
 The product is the C-ABI library ``libspr_b200.so`` (built in-tree by
 ``sam_lib_b200.build``): it exports the reference's Fortran entry points
-``sprsol_``, ``sprfc1_``, ``sprfc2_``, ``sprfc3_``, ``sprfs1_``, ``sprfs2_``,
+``sprsol_``, ``sprfc1_``, ``sprfc2_``, ``sprfc3_``, ``sprfc4_``, ``sprfs1_``, ``sprfs2_``,
 ``sprbs1_`` and ``sprbs2_`` (INTEGER*8 ABI;
 ``libspr_b200_i4.so`` has the INTEGER*4 ABI) plus a device-level API.  This
 module is the Python mirror of that interface: the same routine names,
@@ -137,6 +137,25 @@ def sprfc3(mspar, mtrees, msifa, sm, tol, dcor, iwork=None, rwork=None, lpu=-1, 
     rwork = np.zeros(1) if rwork is None else rwork
     ierr = c_t(0)
     load(int_kind).sprfc3_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
+                           _ptr(iwork), _ptr(rwork), _ptr(dcor), _ref(lpu, c_t), C.byref(ierr),
+                           None, None)
+    return ierr.value
+
+
+def sprfc4(mspar, mtrees, msifa, sm, tol, dcor, iwork=None, rwork=None, lpu=-1, int_kind=8):
+    """SPRFC4 (src/SPR/sprfc4.f:5): Cholesky factorisation C C' that replaces
+    small pivots (TOL(1), TOL(4); 4 TOL entries) and records them in DCOR
+    (2*NEQ); returns IERR (-3 with MSPAR(27) = -(number replaced) still leaves
+    a complete factor)."""
+    np_t, c_t = _ints(int_kind)
+    if tol.dtype != np.float64 or tol.size < 4:
+        raise TypeError('TOL must be a float64 array of 4 entries')
+    if dcor.dtype != np.float64 or dcor.size < 2 * int(mspar[7]):
+        raise TypeError('DCOR must be a float64 array of 2*NEQ entries')
+    iwork = np.zeros(1, dtype=np_t) if iwork is None else iwork
+    rwork = np.zeros(1) if rwork is None else rwork
+    ierr = c_t(0)
+    load(int_kind).sprfc4_(_ptr(mspar), _ptr(mtrees), _ptr(msifa), _ptr(sm), _ptr(tol),
                            _ptr(iwork), _ptr(rwork), _ptr(dcor), _ref(lpu, c_t), C.byref(ierr),
                            None, None)
     return ierr.value

@@ -333,7 +333,8 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
             bool defer = false) {
     const int64_t neq = mspar[7], nzerol = mspar[15];
     const int64_t nsm = neq + nzerol;
-    const char* who = chol ? "SPRFC2" : dcor ? "SPRFC3" : "SPRFC1";
+    const bool fc4 = chol && dcor;                    // SPRFC4: Cholesky with pivot replacement
+    const char* who = fc4 ? "SPRFC4" : chol ? "SPRFC2" : dcor ? "SPRFC3" : "SPRFC1";
     cudaStream_t s = c->stream;
     // SPRFC1 on a pinned SM: upload, factorisation and download overlap, level by level
     const bool streamed = !chol && !dcor && is_pinned(sm);
@@ -349,14 +350,14 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     }
     FactorResult r;
     const int frc = streamed ? c->eng.factor_streamed(sm, c->d_sm, tol[0], r, c->copy)
-                    : chol   ? c->eng.factor_chol(c->d_sm, tol[0], r)
+                    : chol   ? c->eng.factor_chol(c->d_sm, tol[0], r, fc4 ? &fc3 : nullptr)
                              : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
     if (frc != 0) {
         finish_copies(c);
         msg(lpu, who, "CUDA failure in the factorisation");
         return -4;
     }
-    const bool chol_ok = chol && r.lierr == 0;
+    const bool chol_ok = chol && (r.lierr == 0 || (fc4 && r.lierr == -33));
     if (chol_ok && c->eng.chol_convert(c->d_sm, true) != 0) return -4;
     uint64_t fp = 0;                                  // hash of exactly what the host receives
     if (c->eng.hash(c->d_sm, nsm, fp) != 0) return -4;
@@ -373,7 +374,7 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     I ierr = 0;
     tol[1] = r.tol2;
     tol[2] = r.tol3;
-    if (r.lierr == -31) {                             // sprfc3.f:249-258
+    if (r.lierr == -31 || r.lierr == -33) {           // sprfc3.f:249-258, sprfc4.f:244-256
         ierr = -3;
         mspar[26] = -(I)r.supeqt;
         if (lpu >= 0) {
@@ -410,7 +411,8 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
         c->sm_fp = fp;
         c->resident = true;
     }
-    mspar[25] = (I)r.numneg;
+    // SPRFC4 reports SPRF41's NUMZRO there, which it never counts (sprfc4.f:258)
+    mspar[25] = fc4 ? 0 : (I)r.numneg;
     return ierr;
 }
 
@@ -646,6 +648,48 @@ void SPR_API(sprfc2_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I*
         return;
     }
     *ierr = do_factor(c, mspar, sm, tol, *lpu, nullptr, true);
+    if (*ierr == -4) mspar[0] = -6;
+}
+
+// SPRFC4 (src/SPR/sprfc4.f:5): Cholesky factorisation C C' of SM in place that
+// replaces small pivots instead of stopping (SPRF47's rule, TOL(4) scales the
+// replacement) and records them in DCOR(2,NEQ); a pivot below -TOL(1)|a_jj|
+// stops it.  IERR = -3 with MSPAR(27) = -(number replaced) still leaves a
+// complete C C' factor; MSPAR(1) = 6, MSPAR(26) = 0.
+void SPR_API(sprfc4_)(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, I* iwork, double* rwork, double* dcor,
+                      const I* lpu, I* ierr, void (*mvmult)(), void (*mmmult)()) {
+    (void)iwork;
+    (void)rwork;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (mspar[0] < 0) {                                 // sprfc4.f:133-141
+        mspar[0] = -6;
+        *ierr = -1;
+        msg(*lpu, "SPRFC4", "ERROR FROM PRECEDING SAM/SPR ROUTINE IS NOT CLEARED");
+        return;
+    }
+    mspar[0] = 6;
+    *ierr = 0;
+    if (!fc1_lengths_ok(mspar)) {                       // sprfc4.f:203-228 (the checks of SPRFC1)
+        mspar[0] = -2;
+        *ierr = -2;
+        msg(*lpu, "SPRFC4", "MTREES/MSIFA/SM, AND/OR IWORK/RWORK: NOT GREAT ENOUGH");
+        return;
+    }
+    if (!callbacks_ok(mvmult, mmmult, false)) {
+        mspar[0] = -6;
+        *ierr = -4;
+        msg(*lpu, "SPRFC4", "MVMULT/MMMULT DO NOT COMPUTE THE C C' UPDATES OF CMVY18/CMMY18");
+        return;
+    }
+    int err = 0;
+    Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    if (!c) {
+        mspar[0] = -6;
+        *ierr = (err == -2) ? -2 : -4;
+        msg(*lpu, "SPRFC4", "COULD NOT SET UP THE GPU CONTEXT");
+        return;
+    }
+    *ierr = do_factor(c, mspar, sm, tol, *lpu, dcor, true);
     if (*ierr == -4) mspar[0] = -6;
 }
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -65,6 +66,7 @@ struct Stats {
     int tc_timeout;          // a tensor-core update CTA gave up waiting (see tc_gemm.cuh)
     unsigned long long nsing;    // SPRFC3: pivots replaced by the TOL(1)/TOL(4) rule
     unsigned long long near_piv; // pivots with |d| < near_tol |a_jj| (mixed-mode inertia guard)
+    int solve_timeout;       // a triangle task of the solves gave up waiting for a block (k_*_tri)
 };
 
 struct PV {
@@ -86,6 +88,7 @@ struct PV {
     double* xinv;            // inverses of the kSolveBlock-wide diagonal blocks
     const int64_t* rect_off;
     const int64_t* fwd_off;
+    const int64_t* tri_off;  // first block-ready flag of each large front (solves)
     double tol1;
     // SPRFC3 semantics (sprfc3.f:549-572, 1083-1099): a zero diagonal becomes
     // 1 and a pivot at or below TOL(1)|a_jj| is replaced instead of stopping;
@@ -122,6 +125,7 @@ struct Engine::Dev {
     int32_t* task_map = nullptr;
     int64_t* rect_off = nullptr;
     int64_t* fwd_off = nullptr;
+    int64_t* tri_off = nullptr;
     double* pbuf = nullptr;                      // back-solve rectangle partial sums
     int32_t* level_nodes = nullptr;              // small nodes of every level, concatenated
     std::vector<int64_t> small_begin;            // per level offset into level_nodes
@@ -142,6 +146,8 @@ struct Engine::Dev {
     int64_t vbuf_rhs = 0;
     double* bbuf = nullptr;                      // contiguous copy of B (ldb = NEQ)
     int64_t bbuf_rhs = 0;
+    int32_t* tri_tasks = nullptr;                // the solves' triangle tasks (node, block)
+    int32_t* tri_sync = nullptr;                 // block-ready flags, then one task counter per level
     std::vector<void*> owned;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     unsigned long long* hbuf = nullptr;          // result of k_sm_hash
@@ -333,14 +339,37 @@ __global__ void k_reduce(const double* v, int64_t n, double* out) {
 // (sprfc1.f:1274), SPRF37 replaces the pivot (sprfc3.f:1083), SPRF27's
 // d <= TOL(1)|a| stops the Cholesky form (sprfc2.f:1001-1008; the C C'
 // factor is formed from L D L' afterwards, see k_chol_convert).
-enum PivotRule { kPivotLDL = 0, kPivotReplace = 1, kPivotChol = 2 };
+// SPRF47 (sprfc4.f:978-1000) is the Cholesky form of SPRF37: a pivot below
+// -TOL(1)|a_jj| stops, one in [-TOL(1)|a_jj|, TOL(1)|a_jj|] is replaced by
+// TOL(1) max(1, |TOL(4) a_jj|) and recorded in DCOR(1:2, j).
+enum PivotRule { kPivotLDL = 0, kPivotReplace = 1, kPivotChol = 2, kPivotChol4 = 3 };
 
 // A NaN or infinite pivot (a NaN or Inf anywhere in SM reaches some pivot
 // through the Schur updates) fails the test as well, so that the call reports
 // an error instead of a factor full of NaN.
 __device__ __forceinline__ bool pivot_fails(int rule, double d, double ad, double tol1) {
     if (!isfinite(d)) return true;
+    if (rule == kPivotChol4) return d < -tol1 * fabs(ad);
     return rule == kPivotChol ? d <= tol1 * fabs(ad) : fabs(d) <= tol1 * fabs(ad);
+}
+
+// SPRF47's replacement of a small pivot (not a failing one): returns the
+// pivot to use and records DCOR(1,j) = d, DCOR(2,j) = the replacement.
+__device__ __forceinline__ double chol4_pivot(const PV& P, int col, double d, double ad, bool record) {
+    if (!(d <= P.tol1 * fabs(ad)) || d < -P.tol1 * fabs(ad)) return d;
+    const double dn = P.tol1 * fmax(1.0, fabs(P.tol4 * ad));
+    if (record) {
+        P.dcor[2 * (int64_t)col] = d;
+        P.dcor[2 * (int64_t)col + 1] = dn;
+        atomicAdd(&P.st->nsing, 1ull);
+    }
+    return dn;
+}
+
+// SPRF47 on a failing (negative) pivot: DCOR(1,j) = DCOR(2,j) = d.
+__device__ __forceinline__ void chol4_fail_record(const PV& P, int col, double d) {
+    P.dcor[2 * (int64_t)col] = d;
+    P.dcor[2 * (int64_t)col + 1] = d;
 }
 
 // Mixed-mode inertia guard: a pivot this close to zero relative to its
@@ -405,10 +434,15 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             const double d0 = d;
             d = fc3_pivot(P, d0, ad);
             if (tid == 0) fc3_record(P, fst + k, d0, d);
-        } else if (pivot_fails(PR, d, ad, P.tol1)) {   // sprfc1.f:1274, sprfc2.f:1004
-            if (tid == 0) record_fail(P, js, k, d, ad);
+        } else if (pivot_fails(PR, d, ad, P.tol1)) {   // sprfc1.f:1274, sprfc2.f:1004, sprfc4.f:980
+            if (tid == 0) {
+                record_fail(P, js, k, d, ad);
+                if (PR == kPivotChol4) chol4_fail_record(P, fst + k, d);
+            }
             failed = true;
             break;
+        } else if (PR == kPivotChol4) {
+            d = chol4_pivot(P, fst + k, d, ad, tid == 0);
         }
         if (d < 0.0) ++neg;
         if (tid == 0 && near_zero_pivot(P, d, ad)) atomicAdd(&P.st->near_piv, 1ull);
@@ -420,7 +454,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             A[pk(i, k, F)] = a * rd;
         }
         __syncthreads();
-        if (PR == kPivotReplace && tid == 0) A[pk(k, k, F)] = d;   // every thread has read the old pivot
+        if ((PR == kPivotReplace || PR == kPivotChol4) && tid == 0) A[pk(k, k, F)] = d;   // every thread has read the old pivot
         for (int j = k + 1 + warp; j < F; j += nwarp) {
             const double ljk = A[pk(j, k, F)];
             double* cj = A + pk(j, j, F) - j;
@@ -582,6 +616,8 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
                     c = fc3_pivot(P, c0, adv[k]);
                     fc3_record(P, fst + k0 + k, c0, c);
                 }
+                if (PR == kPivotChol4 && i == k && !pivot_fails(PR, c, adv[k], P.tol1))
+                    c = chol4_pivot(P, fst + k0 + k, c, adv[k], true);
                 if (i >= k && i < nb) vec[buf][i] = c;
                 if (i == k) {
                     dd[k] = c;
@@ -593,7 +629,10 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         const double d = vec[buf][k];
         if (PR != kPivotReplace && pivot_fails(PR, d, adv[k], P.tol1)) {
             failed = k;
-            if (tid == 0) record_fail(P, js, k0 + k, d, adv[k]);
+            if (tid == 0) {
+                record_fail(P, js, k0 + k, d, adv[k]);
+                if (PR == kPivotChol4) chol4_fail_record(P, fst + k0 + k, d);
+            }
             break;
         }
         const double rd = rdv[k];
@@ -638,7 +677,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         for (int b = 0; b < R; ++b) {
             const int i = tx + 16 * a, j = ty + 16 * b;
             if (i >= j && i < nb && j < nb)
-                A[i][j] = (i > j) ? v[a][b] * rdv[j] : (PR == kPivotReplace ? dd[j] : v[a][b]);
+                A[i][j] = (i > j) ? v[a][b] * rdv[j] : ((PR == kPivotReplace || PR == kPivotChol4) ? dd[j] : v[a][b]);
         }
     __syncthreads();
     // X = L^-1 by recursive doubling: after the pass of order b, each aligned
@@ -1815,6 +1854,225 @@ __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
     for (int r = 0; r < nrhs; ++r) b[(int64_t)(fst + j) + r * ldb] = y[(int64_t)r * F + j] / d;
 }
 
+// ---------------------------------------------------------------------------
+// Triangles of the solves as one dataflow launch per level.  Task (js, rb) is
+// the 64-row block rb of front js (rows [64 rb, 64 rb + 64) of [0, S)).
+// Forward: y_rb = X_rb (w_rb - sum_{b < rb} L[rb, b] y_b), X_rb = L_rb,rb^-1
+// (the stored 64x64 inverse); backward: x_cb = X_cb' (w_cb - sum_{r > cb}
+// L[r, cb]' x_r).  Persistent CTAs take tasks in order from a counter (forward
+// block-major ascending, backward descending), so a task only waits for
+// tasks taken before it, by CTAs that are running: the waits always end.
+// Each wait is bounded (PV::wait_ns); one that gives up sets
+// Stats::solve_timeout and an abort word every CTA checks, and the host
+// turns it into an error.  Per tile, a thread owns one row (forward) or one
+// column (backward) and a quarter of the 64 columns (rows).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long tri_now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// thread 0 waits (bounded) for flag; returns false when the launch aborts
+__device__ __forceinline__ bool tri_wait(const int* flag, int* abort_word, const PV& P) {
+    if (ld_acquire(flag)) return true;
+    const unsigned long long t0 = tri_now();
+    for (int spin = 0;; ++spin) {
+        if (ld_acquire(flag)) return true;
+        if (ld_acquire(abort_word)) return false;
+        if ((spin & 63) == 63 && tri_now() - t0 > P.wait_ns) {
+            atomicExch(&P.st->solve_timeout, 1);
+            st_release(abort_word, 1);
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+constexpr int kTriLd = kMaxRHS + 1;
+
+template <int NR>
+__global__ void __launch_bounds__(256) k_fwd_tri(const int32_t* tasks, int ntasks, int32_t* flags, int32_t* counter,
+                                                 PV P, const double* vbuf, double* ysol, int nrhs) {
+    __shared__ double ys[kNB][kTriLd];
+    __shared__ double part[4][kNB][kTriLd];
+    __shared__ int task_sh, ok_sh;
+    int* abort_word = counter + 1;
+    const int tid = threadIdx.x, row = tid & (kNB - 1), q = tid >> 6;
+    for (;;) {
+        if (tid == 0) task_sh = atomicAdd(counter, 1);
+        __syncthreads();
+        const int t = task_sh;
+        if (t >= ntasks) break;
+        const int js = tasks[2 * t], rb = tasks[2 * t + 1];
+        const int F = P.F[js], S = P.S[js];
+        const int r0 = rb * kNB, nrow = min(kNB, S - r0);
+        const double* base = P.lnz + P.lnz_off[js];
+        const int64_t vb = P.rbase[js] * nrhs;
+        int32_t* fl = flags + P.tri_off[js];
+        double acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+        bool ok = true;
+        for (int b = 0; b < rb; ++b) {
+            if (tid == 0) ok_sh = tri_wait(fl + b, abort_word, P);
+            __syncthreads();
+            if (!ok_sh) {
+                ok = false;
+                break;
+            }
+            for (int e = tid; e < kNB * nrhs; e += blockDim.x) {
+                const int i = e & (kNB - 1), r = e >> 6;
+                ys[i][r] = __ldcg(ysol + vb + (int64_t)r * F + kNB * b + i);
+            }
+            __syncthreads();
+            if (row < nrow) {
+                const int c0 = kNB * b + 16 * q;
+                int64_t p = lnz_col(c0, F) - c0 + r0 + row;           // L[r0 + row][c0]
+#pragma unroll 4
+                for (int k = 0; k < 16; ++k) {
+                    const double l = __ldg(base + p);
+                    p += F - (c0 + k) - 1;                            // next column, same row
+#pragma unroll
+                    for (int r = 0; r < NR; ++r)
+                        if (r < nrhs) acc[r] += l * ys[16 * q + k][r];
+                }
+            }
+            __syncthreads();
+        }
+        if (!ok) break;
+        // v = w - sum of the four quarters, then y = X v
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) part[q][row][r] = acc[r];
+        __syncthreads();
+        if (tid < kNB)
+            for (int r = 0; r < nrhs; ++r)
+                ys[row][r] = (row < nrow) ? __ldcg(vbuf + vb + (int64_t)r * F + r0 + row) -
+                                                ((part[0][row][r] + part[1][row][r]) + (part[2][row][r] + part[3][row][r]))
+                                          : 0.0;
+        __syncthreads();
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)rb * kNB * kNB;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+            const int m = 16 * q + k;
+            const double x = (m <= row) ? __ldg(lv + row + m * kNB) : 0.0;    // X[row][m], unit lower
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) acc[r] += x * ys[m][r];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) part[q][row][r] = acc[r];
+        __syncthreads();
+        if (tid < kNB && row < nrow)
+            for (int r = 0; r < nrhs; ++r)
+                ysol[vb + (int64_t)r * F + r0 + row] =
+                    (part[0][row][r] + part[1][row][r]) + (part[2][row][r] + part[3][row][r]);
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(fl + rb, 1);
+    }
+}
+
+template <int NR>
+__global__ void __launch_bounds__(256) k_bwd_tri(const int32_t* tasks, int ntasks, int32_t* flags, int32_t* counter,
+                                                 PV P, const double* vbuf, double* xsol, int nrhs) {
+    __shared__ double xs[kNB][kTriLd];
+    __shared__ double part[4][kNB][kTriLd];
+    __shared__ int task_sh, ok_sh;
+    int* abort_word = counter + 1;
+    const int tid = threadIdx.x, col = tid & (kNB - 1), q = tid >> 6;
+    for (;;) {
+        if (tid == 0) task_sh = atomicAdd(counter, 1);
+        __syncthreads();
+        if (task_sh >= ntasks) break;
+        const int t = ntasks - 1 - task_sh;                          // descending blocks
+        const int js = tasks[2 * t], cb = tasks[2 * t + 1];
+        const int F = P.F[js], S = P.S[js];
+        const int c0 = cb * kNB, ncol = min(kNB, S - c0);
+        const int nblk = (S + kNB - 1) / kNB;
+        const double* base = P.lnz + P.lnz_off[js];
+        const int64_t vb = P.rbase[js] * nrhs;
+        int32_t* fl = flags + P.tri_off[js];
+        double acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+        bool ok = true;
+        const int64_t pc = (col < ncol) ? lnz_col(c0 + col, F) - (c0 + col) : 0;   // column c0 + col, row 0
+        for (int rb = cb + 1; rb < nblk; ++rb) {
+            if (tid == 0) ok_sh = tri_wait(fl + rb, abort_word, P);
+            __syncthreads();
+            if (!ok_sh) {
+                ok = false;
+                break;
+            }
+            const int nr = min(kNB, S - rb * kNB);
+            for (int e = tid; e < kNB * nrhs; e += blockDim.x) {
+                const int i = e & (kNB - 1), r = e >> 6;
+                xs[i][r] = (i < nr) ? __ldcg(xsol + vb + (int64_t)r * F + kNB * rb + i) : 0.0;
+            }
+            __syncthreads();
+            if (col < ncol) {
+                const int i0 = kNB * rb + 16 * q;
+#pragma unroll 4
+                for (int k = 0; k < 16; ++k) {
+                    const int i = 16 * q + k;
+                    const double l = (i < nr) ? __ldg(base + pc + i0 + k) : 0.0;     // L[64 rb + i][c0 + col]
+#pragma unroll
+                    for (int r = 0; r < NR; ++r)
+                        if (r < nrhs) acc[r] += l * xs[i][r];
+                }
+            }
+            __syncthreads();
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) part[q][col][r] = acc[r];
+        __syncthreads();
+        if (tid < kNB)
+            for (int r = 0; r < nrhs; ++r)
+                xs[col][r] = (col < ncol) ? __ldcg(vbuf + vb + (int64_t)r * F + c0 + col) -
+                                                ((part[0][col][r] + part[1][col][r]) + (part[2][col][r] + part[3][col][r]))
+                                          : 0.0;
+        __syncthreads();
+        // x = X' v: x[col] = sum_{m >= col} X[m][col] v[m]
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)cb * kNB * kNB;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+            const int m = 16 * q + k;
+            const double x = (m >= col) ? __ldg(lv + m + col * kNB) : 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) acc[r] += x * xs[m][r];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) part[q][col][r] = acc[r];
+        __syncthreads();
+        if (tid < kNB && col < ncol)
+            for (int r = 0; r < nrhs; ++r)
+                xsol[vb + (int64_t)r * F + c0 + col] =
+                    (part[0][col][r] + part[1][col][r]) + (part[2][col][r] + part[3][col][r]);
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(fl + cb, 1);
+    }
+}
+
 // gather of the back sweep: own rows (forward result) and ancestors' solution
 __global__ void k_bwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
                              const double* b, int64_t ldb, int nrhs) {
@@ -2138,6 +2396,14 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     o.push_back(D.st);
     CK(cudaMalloc((void**)&D.hbuf, sizeof(unsigned long long)));
     o.push_back(D.hbuf);
+    if (dev_upload(o, &D.tri_tasks, P_.tri_tasks)) return -4;
+    if (dev_upload(o, &D.tri_off, P_.tri_off)) return -4;
+    CK(cudaMalloc((void**)&D.tri_sync, sizeof(int32_t) * (size_t)(P_.tri_flags + 2 * (int64_t)P_.levels.size() + 2)));
+    o.push_back(D.tri_sync);
+    {
+        const char* v = std::getenv("SPR_B200_SOLVE_BLOCKS");
+        tri_solve_ = !(v && v[0] == '1');
+    }
     CK(cudaEventCreate(&D.ev0));
     CK(cudaEventCreate(&D.ev1));
     int smem_max = 0;
@@ -2147,6 +2413,7 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(k_small_front<kPivotLDL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_small_front<kPivotReplace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_small_front<kPivotChol>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    CK(cudaFuncSetAttribute(k_small_front<kPivotChol4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_mv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem));
     CK(cudaFuncSetAttribute(k_fwd_blk_upd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
@@ -2242,6 +2509,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.xinv = D.xinv;
     v.rect_off = D.rect_off;
     v.fwd_off = D.fwd_off;
+    v.tri_off = D.tri_off;
     v.tol1 = tol1;
     v.fc3 = 0;
     v.tol4 = 0.0;
@@ -2330,7 +2598,9 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 const int F = c.maxF;
                 const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
                 const int32_t* nodes = D.level_nodes + D.small_begin[L] + c.begin;
-                if (pv.fc3)
+                if (pv.fc3 == 2)
+                    k_small_front<kPivotChol4><<<c.count, 256, smem, s>>>(nodes, pv);
+                else if (pv.fc3)
                     k_small_front<kPivotReplace><<<c.count, 256, smem, s>>>(nodes, pv);
                 else if (chol_)
                     k_small_front<kPivotChol><<<c.count, 256, smem, s>>>(nodes, pv);
@@ -2352,7 +2622,9 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         for (size_t st = 0; st < lp.panel.size(); ++st) {
             const Launch& pl = lp.panel[st];
             mark(3);
-            if (pv.fc3)
+            if (pv.fc3 == 2)
+                k_diag<kPivotChol4><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
+            else if (pv.fc3)
                 k_diag<kPivotReplace><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
             else if (chol_)
                 k_diag<kPivotChol><<<(int)pl.job_count, 256, 0, s>>>(jobs + pl.job_begin, pv);
@@ -2407,7 +2679,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         }
     }
     mark(8);
-    if (P_.inv_blocks.job_count > 0) {
+    if (!tri_solve_ && P_.inv_blocks.job_count > 0) {
         k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pv);
         ++timing.launches;
     }
@@ -2422,7 +2694,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     PV pv = make_view(D, P_, d_sm, tol1);
     if (fc3) {
         if (!fc3->d_dcor) return -2;
-        pv.fc3 = 1;
+        pv.fc3 = chol_ ? 2 : 1;               // SPRF47 (SPRFC4) or SPRF37 (SPRFC3)
         pv.tol4 = fc3->tol4;
         pv.dcor = fc3->d_dcor;
     }
@@ -2567,8 +2839,8 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
         return 0;
     }
     linv_valid_ = true;
-    if (fc3 && hs.nsing > 0) {                     // sprfc3.f:796-799
-        res.lierr = -31;
+    if (fc3 && hs.nsing > 0) {                     // sprfc3.f:796-799, sprfc4.f:719-722
+        res.lierr = chol_ ? -33 : -31;
         res.supeqt = (int64_t)hs.nsing;
     }
     res.numneg = hs.numneg;
@@ -2712,9 +2984,9 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     return 0;
 }
 
-int Engine::factor_chol(double* d_sm, double tol1, FactorResult& res) {
+int Engine::factor_chol(double* d_sm, double tol1, FactorResult& res, const Singular* fc4) {
     chol_ = true;
-    const int rc = factor(d_sm, tol1, res, nullptr);
+    const int rc = factor(d_sm, tol1, res, fc4);
     chol_ = false;
     return rc;
 }
@@ -2773,7 +3045,9 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
         double* b = d_b + r0 * ldb;
         const Job* jobs = D.jobs;
         auto blocks = [](int64_t threads) { return (int)((threads + 255) / 256); };
+        const size_t tri_bytes = sizeof(int32_t) * (size_t)(P_.tri_flags + 2 * (int64_t)P_.levels.size());
         if (which & 1) {
+            if (tri_solve_) cudaMemsetAsync(D.tri_sync, 0, tri_bytes, s);
             for (size_t L = 0; L < P_.levels.size(); ++L) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
@@ -2791,16 +3065,29 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                                                                D.vbuf, b, ldb, nr);
                 ++nl;
                 mark(2);
-                for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
-                    const Launch& ml = lp.blk_mv[sb];
-                    k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
-                                                                 D.vbuf2, nr);
+                if (tri_solve_ && lp.tri_count > 0) {
+                    const int nt = (int)lp.tri_count;
+                    const int grid = std::min(nt, 4 * std::max(sm_count_, 1));
+                    int32_t* ctr = D.tri_sync + P_.tri_flags + 2 * L;
+                    if (nr <= 4)
+                        k_fwd_tri<4><<<grid, 256, 0, s>>>(D.tri_tasks + 2 * lp.tri_begin, nt, D.tri_sync, ctr, pv,
+                                                          D.vbuf, D.vbuf2, nr);
+                    else
+                        k_fwd_tri<kMaxRHS><<<grid, 256, 0, s>>>(D.tri_tasks + 2 * lp.tri_begin, nt, D.tri_sync, ctr, pv,
+                                                                D.vbuf, D.vbuf2, nr);
                     ++nl;
-                    const Launch& fl = lp.fs_upd[sb];
-                    if (fl.ntasks > 0) {
-                        k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kUpdSmem, s>>>(jobs + fl.job_begin, fl.job_count, TMAP(fl), pv,
-                                                                       D.vbuf, D.vbuf2, nr);
+                } else {
+                    for (size_t sb = 0; sb < lp.fs_upd.size(); ++sb) {
+                        const Launch& ml = lp.blk_mv[sb];
+                        k_fwd_blk_mv<<<(int)ml.ntasks, 256, kMvSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv,
+                                                                     D.vbuf, D.vbuf2, nr);
                         ++nl;
+                        const Launch& fl = lp.fs_upd[sb];
+                        if (fl.ntasks > 0) {
+                            k_fwd_blk_upd2<<<(int)fl.ntasks, 256, kUpdSmem, s>>>(jobs + fl.job_begin, fl.job_count,
+                                                                           TMAP(fl), pv, D.vbuf, D.vbuf2, nr);
+                            ++nl;
+                        }
                     }
                 }
                 const Launch& rl = lp.rect;
@@ -2825,6 +3112,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
             }
         }
         if (which & 2) {
+            if (tri_solve_) cudaMemsetAsync(D.tri_sync, 0, tri_bytes, s);
             for (size_t L = P_.levels.size(); L-- > 0;) {
                 const LevelPlan& lp = P_.levels[L];
                 if (!lp.small_nodes.empty()) {
@@ -2857,16 +3145,29 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                     ++nl;
                 }
                 mark(8);
-                for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
-                    const Launch& ml = lp.blk_mv[sb];
-                    k_bwd_blk_mv<<<(int)ml.ntasks, 256, kBwdSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv, D.vbuf,
-                                                                 D.vbuf2, nr);
+                if (tri_solve_ && lp.tri_count > 0) {
+                    const int nt = (int)lp.tri_count;
+                    const int grid = std::min(nt, 4 * std::max(sm_count_, 1));
+                    int32_t* ctr = D.tri_sync + P_.tri_flags + 2 * L;
+                    if (nr <= 4)
+                        k_bwd_tri<4><<<grid, 256, 0, s>>>(D.tri_tasks + 2 * lp.tri_begin, nt, D.tri_sync, ctr, pv,
+                                                          D.vbuf, D.vbuf2, nr);
+                    else
+                        k_bwd_tri<kMaxRHS><<<grid, 256, 0, s>>>(D.tri_tasks + 2 * lp.tri_begin, nt, D.tri_sync, ctr, pv,
+                                                                D.vbuf, D.vbuf2, nr);
                     ++nl;
-                    const Launch& bl = lp.bs_upd[sb];
-                    if (bl.ntasks > 0) {
-                        k_bwd_blk_upd<<<(int)bl.ntasks, 256, kBwdSmem, s>>>(jobs + bl.job_begin, bl.job_count, TMAP(bl), pv, D.vbuf,
-                                                                     D.vbuf2, nr);
+                } else {
+                    for (size_t sb = lp.bs_upd.size(); sb-- > 0;) {
+                        const Launch& ml = lp.blk_mv[sb];
+                        k_bwd_blk_mv<<<(int)ml.ntasks, 256, kBwdSmem, s>>>(jobs + ml.job_begin, ml.job_count, TMAP(ml), pv,
+                                                                     D.vbuf, D.vbuf2, nr);
                         ++nl;
+                        const Launch& bl = lp.bs_upd[sb];
+                        if (bl.ntasks > 0) {
+                            k_bwd_blk_upd<<<(int)bl.ntasks, 256, kBwdSmem, s>>>(jobs + bl.job_begin, bl.job_count,
+                                                                         TMAP(bl), pv, D.vbuf, D.vbuf2, nr);
+                            ++nl;
+                        }
                     }
                 }
                 mark(10);
@@ -2888,6 +3189,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     if (!D.vbuf || !D.vbuf2) return -4;
     CK(cudaEventRecord(D.ev0, s));
     int64_t nl = 0;
+    CK(cudaMemsetAsync(&D.st->solve_timeout, 0, sizeof(int), s));
     if (!linv_valid_) {
         for (const LevelPlan& lp : P_.levels)
             for (const Launch& pl : lp.panel)
@@ -2895,7 +3197,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
                     k_linv<<<(int)pl.job_count, 64, 0, s>>>(D.jobs + pl.job_begin, pv);
                     ++nl;
                 }
-        if (P_.inv_blocks.job_count > 0) {
+        if (!tri_solve_ && P_.inv_blocks.job_count > 0) {
             PV pvi = pv;
             pvi.sn_bad = nullptr;
             k_inv_block<<<(int)P_.inv_blocks.job_count, 256, kInvSmem, s>>>(D.jobs + P_.inv_blocks.job_begin, pvi);
@@ -2923,9 +3225,15 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     }
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());
+    int tri_timeout = 0;
+    CK(cudaMemcpyAsync(&tri_timeout, &D.st->solve_timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     CK(cudaEventElapsedTime(&timing.solve_ms, D.ev0, D.ev1));
     timing.solve_launches = nl;
+    if (tri_timeout) {
+        fprintf(stderr, "spr_b200: a triangle task of the solve gave up waiting for a block\n");
+        return -4;
+    }
     if (profile_) {
         for (int k = 9; k < 20; ++k) timing.phase_ms[k] = 0.f;
         for (size_t k = 0; k < marks_.size(); ++k) {

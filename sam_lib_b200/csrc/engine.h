@@ -68,9 +68,12 @@ public:
     int factor(double* d_sm, double tol1, FactorResult& res, const Singular* fc3);
     // SPRFC2 semantics (src/SPR/sprfc2.f:276-725): the pivot test is SPRF27's
     // d <= TOL(1)|a_jj| (a non-positive pivot stops) and TOL(3) is
-    // trace / min(sqrt d)^2.  The device SM is left in L D L' form; chol_convert
+    // trace / min(sqrt d)^2.  With fc4, SPRFC4 semantics (sprfc4.f:265-725):
+    // zero diagonals become 1, a pivot below -TOL(1)|a_jj| stops, one up to
+    // TOL(1)|a_jj| is replaced by TOL(1) max(1, |TOL(4) a_jj|), both recorded in
+    // DCOR; LIERR -33 with SUPEQT = the number replaced.  The device SM is left in L D L' form; chol_convert
     // turns it into the C C' form (C = L D^1/2, sqrt d in D) and back.
-    int factor_chol(double* d_sm, double tol1, FactorResult& res);
+    int factor_chol(double* d_sm, double tol1, FactorResult& res, const Singular* fc4 = nullptr);
     // SPRFC1 semantics with the host copies overlapped: h_sm (pinned host
     // memory, NEQ + NZEROL doubles) is uploaded level by level on the copy
     // stream cs while the lower levels factor, and each level's finished
@@ -162,6 +165,7 @@ private:
                        int64_t& nl);
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
+    bool tri_solve_ = true;                  // solve triangles as one dataflow launch per level
     const LevelHooks* hooks_ = nullptr;      // set during a streamed factorisation
     const double* streamed_diag_ = nullptr;  // its host-gathered original diagonal (device)
     std::unique_ptr<Transfer> xfer_;

@@ -530,6 +530,31 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (Launch& l : lp.bs_upd) build_map(l);
         for (Launch& l : lp.blk_mv) build_map(l);
     }
+    // triangle tasks of the solves: per level, block-major (every task's
+    // dependencies, the lower blocks of its own front, come earlier)
+    P.tri_off.assign(ns, -1);
+    P.tri_flags = 0;
+    P.tri_tasks.clear();
+    for (LevelPlan& lp : P.levels) {
+        std::vector<int32_t> fr;
+        int32_t nbmax = 0;
+        for (int32_t js : lp.elim_nodes) {
+            if (P.F[js] <= kSmallMaxF) continue;
+            fr.push_back(js);
+            P.tri_off[js] = P.tri_flags;
+            const int32_t nb = (P.S[js] + kNB - 1) / kNB;
+            P.tri_flags += nb;
+            nbmax = std::max(nbmax, nb);
+        }
+        lp.tri_begin = (int64_t)P.tri_tasks.size() / 2;
+        for (int32_t b = 0; b < nbmax; ++b)
+            for (int32_t js : fr)
+                if (b * kNB < P.S[js]) {
+                    P.tri_tasks.push_back(js);
+                    P.tri_tasks.push_back(b);
+                }
+        lp.tri_count = (int64_t)P.tri_tasks.size() / 2 - lp.tri_begin;
+    }
     open_launch(P.inv_blocks);
     for (int64_t js = 0; js < ns; ++js) {
         if (P.F[js] <= kSmallMaxF || P.retained[js]) continue;

@@ -90,6 +90,10 @@ struct LevelPlan {
     std::vector<Launch> blk_mv;               // product with the block inverse, 32 rows/columns per task
     Launch rect;                              // rectangle rows [S, F): one task per 256 x 256 tile
     Launch rect_rows;                         // forward solve, rows [S, F): one task per row
+    // triangle of the solves as one dataflow launch: tasks (node, 64-row
+    // block) of the level's eliminated large fronts, block-major, in
+    // Plan::tri_tasks[tri_begin .. tri_begin + tri_count)
+    int64_t tri_begin = 0, tri_count = 0;
     // trailing update columns beyond the next super-panel (side stream)
     std::vector<std::vector<Launch>> far;
     std::vector<std::vector<TcLaunch>> far_tc;
@@ -145,6 +149,11 @@ struct Plan {
     int64_t rect_entries = 0;
     std::vector<int64_t> fwd_off;            // forward-sweep rectangle partials, per level
     int64_t fwd_entries = 0;
+    // the solves' triangle tasks (pairs node, 64-row block) of every level
+    // and, per large front, the first of its blocks' ready flags
+    std::vector<int32_t> tri_tasks;
+    std::vector<int64_t> tri_off;
+    int64_t tri_flags = 0;
     bool any_large = false;
     // levels and tasks
     std::vector<LevelPlan> levels;
