@@ -511,22 +511,19 @@ __global__ void k_poison(const Job* jobs, int64_t njobs, const int32_t* tmap, PV
 }
 
 // Extend-add into a dense column-major front: one warp per front column.
-__global__ void k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P) {
-    if (P.st->any_fail) return;
-    const int lane = threadIdx.x & 31;
-    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (task >= ntasks) return;
-    const Job& jb = job_of(jobs, njobs, tmap, task);
-    const int js = jb.node;
-    if (P.sn_bad[js]) return;
-    const int j = jb.c0 + (int)(task - jb.task0);
-    const int F = P.F[js], S = P.S[js];
-    const int ld = P.buf_ld[js];
-    double* col = P.arena + P.buf_off[js] + (int64_t)j * ld;
-    // loops unrolled by four with the loads of a group ahead of its stores,
-    // so that each lane keeps four memory requests in flight
+// The column is built in chunks of kAsmRows rows in shared memory: the chunk
+// starts as the LNZ column (fully-summed columns) or zero, receives the
+// children's update entries whose parent rows fall into it (each child's rows
+// are increasing in the parent, so a per-child cursor, kept in one lane,
+// advances chunk by chunk), and is written once.  Each front entry is written
+// once and each child entry read once, in the same order of additions as a
+// column-at-a-time scatter (deterministic, no atomics).  A column with more
+// than 32 contributions (one cursor per lane) scatters into HBM instead.
+constexpr int kAsmRows = 256;
+
+__device__ __forceinline__ void asm_scatter_column(const PV& P, double* col, int j, int F, int S, const double* src,
+                                                   int64_t e0, int64_t e1, int lane) {
     if (j < S) {
-        const double* src = P.lnz + P.lnz_off[js] + lnz_col(j, F) - j;
         int i = j + lane;
         for (; i + 96 < F; i += 128) {
             const double a0 = __ldcg(src + i), a1 = __ldcg(src + i + 32), a2 = __ldcg(src + i + 64),
@@ -541,23 +538,84 @@ __global__ void k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, 
         for (int i = j + lane; i < F; i += 32) col[i] = 0.0;
     }
     __syncwarp();
-    const int64_t e0 = P.cptr[P.rbase[js] + j], e1 = P.cptr[P.rbase[js] + j + 1];
     for (int64_t e = e0; e < e1; ++e) {
         const int c = P.cchild[e], t = P.ct[e];
         const int q = P.F[c] - P.S[c];
         const int32_t* rel = P.rel + P.rel_off[c];
         const double* U = P.arena + P.upd_off[c] + (int64_t)t * P.buf_ld[c];
-        int r = t + lane;
-        for (; r + 96 < q; r += 128) {
-            const int i0 = __ldg(rel + r), i1 = __ldg(rel + r + 32), i2 = __ldg(rel + r + 64), i3 = __ldg(rel + r + 96);
-            const double u0 = __ldcg(U + r), u1 = __ldcg(U + r + 32), u2 = __ldcg(U + r + 64), u3 = __ldcg(U + r + 96);
-            const double c0 = __ldcg(col + i0), c1 = __ldcg(col + i1), c2 = __ldcg(col + i2), c3 = __ldcg(col + i3);
-            col[i0] = c0 + u0;
-            col[i1] = c1 + u1;
-            col[i2] = c2 + u2;
-            col[i3] = c3 + u3;
+        for (int r = t + lane; r < q; r += 32) col[rel[r]] += U[r];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_assemble(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks,
+                                                  PV P) {
+    __shared__ double chunk[8][kAsmRows];
+    if (P.st->any_fail) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t task = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (task >= ntasks) return;
+    const Job& jb = job_of(jobs, njobs, tmap, task);
+    const int js = jb.node;
+    if (P.sn_bad[js]) return;
+    const int j = jb.c0 + (int)(task - jb.task0);
+    const int F = P.F[js], S = P.S[js];
+    const int ld = P.buf_ld[js];
+    double* col = P.arena + P.buf_off[js] + (int64_t)j * ld;
+    const double* src = (j < S) ? P.lnz + P.lnz_off[js] + lnz_col(j, F) - j : nullptr;
+    const int64_t e0 = P.cptr[P.rbase[js] + j], e1 = P.cptr[P.rbase[js] + j + 1];
+    const int ne = (int)(e1 - e0);
+    if (ne > 32) {
+        asm_scatter_column(P, col, j, F, S, src, e0, e1, lane);
+        return;
+    }
+    // lane k holds contribution k: child, its update column, rows, cursor
+    int my_c = 0, my_t = 0, my_q = 0, cur = 0;
+    if (lane < ne) {
+        my_c = P.cchild[e0 + lane];
+        my_t = P.ct[e0 + lane];
+        my_q = P.F[my_c] - P.S[my_c];
+        cur = my_t;
+    }
+    double* acc = chunk[threadIdx.x >> 5];
+    for (int lo = j; lo < F; lo += kAsmRows) {
+        const int n = min(kAsmRows, F - lo), hi = lo + n;
+        for (int i = lane; i < n; i += 32) acc[i] = src ? __ldcg(src + lo + i) : 0.0;
+        __syncwarp();
+        for (int k = 0; k < ne; ++k) {
+            const int c = __shfl_sync(0xffffffffu, my_c, k);
+            const int t = __shfl_sync(0xffffffffu, my_t, k);
+            const int q = __shfl_sync(0xffffffffu, my_q, k);
+            int r = __shfl_sync(0xffffffffu, cur, k);
+            const int32_t* rel = P.rel + P.rel_off[c];
+            const double* U = P.arena + P.upd_off[c] + (int64_t)t * P.buf_ld[c];
+            for (;;) {
+                // four 32-row steps with their loads first; the rows inside
+                // [lo, hi) form a prefix (the parent rows increase)
+                int ri[4];
+                double u[4];
+#pragma unroll
+                for (int st = 0; st < 4; ++st) {
+                    const int rr = r + 32 * st + lane;
+                    ri[st] = rr < q ? __ldg(rel + rr) : 0x7fffffff;
+                    u[st] = rr < q ? __ldcg(U + rr) : 0.0;
+                }
+                bool more = true;
+#pragma unroll
+                for (int st = 0; st < 4; ++st) {
+                    if (!more) break;
+                    const bool in = ri[st] < hi;
+                    if (in) acc[ri[st] - lo] += u[st];
+                    const unsigned m = __ballot_sync(0xffffffffu, in);
+                    r += __popc(m);
+                    more = (m == 0xffffffffu);
+                }
+                if (!more) break;
+            }
+            if (lane == k) cur = r;
+            __syncwarp();
         }
-        for (; r < q; r += 32) col[rel[r]] += U[r];
+        for (int i = lane; i < n; i += 32) col[lo + i] = acc[i];
         __syncwarp();
     }
 }
