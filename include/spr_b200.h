@@ -139,12 +139,15 @@ int spr_b200_set_mode(void* handle, int mode);
  * TOL are the FP64 ones (the pivot rule of SPRF17, sprfc1.f:1272-1283).
  * Default tau = 1e-3; tau = 0 switches the guard and the copy off. */
 int spr_b200_set_inertia_guard(void* handle, double tau);
-/* No reference counterpart.  Watchdog of the tensor-core update kernel:
- * every mbarrier wait gives up after wait_ns nanoseconds (default 2e9; 1e6 ..
- * 6e10 accepted), the kernel then frees its tensor memory and returns, and
- * the factorisation returns -4.  drop != 0 is a test switch: the first CTA of
- * each tensor-core launch skips its first operand load, so that its waits run
- * out.  Returns -2 for a limit outside the range. */
+/* No reference counterpart.  Watchdog of the kernels that wait on device
+ * flags: the tensor-core update kernel's mbarrier waits and the solves'
+ * block-ready flags each give up after wait_ns nanoseconds (default 2e9;
+ * 1e6 .. 6e10 accepted); the kernel then returns (the tensor-core one after
+ * freeing its tensor memory) and the factorisation or solve returns -4.
+ * drop != 0 is a test switch: the first CTA of each tensor-core launch skips
+ * its first operand load and one task of each solve triangle launch never
+ * reports its block, so that waits run out.  Returns -2 for a limit outside
+ * the range. */
 int spr_b200_set_watchdog(void* handle, double wait_ns, int drop);
 /* Residual operator for refinement: compacts the FP64 matrix held in an
  * assembled (not yet factored) device SM into a CSR (the product SPRPRQ forms

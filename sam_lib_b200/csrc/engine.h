@@ -125,9 +125,11 @@ public:
     double inertia_guard() const { return guard_tol_; }
     int64_t last_near_pivots() const { return last_near_; }
     bool last_refactored() const { return last_refactor_; }
-    // Watchdog of the tensor-core update: time limit of each mbarrier wait
-    // (ns), and a test switch that makes one CTA's waits run out (the
-    // factorisation then returns -4 and the engine stays usable).
+    // Watchdog of the kernels that wait on device flags (the tensor-core
+    // update's mbarriers, the solves' block-ready flags): time limit of each
+    // wait (ns), and a test switch that makes some waits run out (one CTA's
+    // operand load, one solve task's report is skipped); the factorisation or
+    // solve then returns -4 and the engine stays usable.
     void set_watchdog(unsigned long long wait_ns, bool drop) {
         wait_ns_ = wait_ns;
         tc_drop_ = drop;

@@ -67,6 +67,29 @@ def test_watchdog_timeout_is_reported_and_engine_stays_usable():
     ds.close()
 
 
+def test_solve_watchdog_timeout_is_reported_and_engine_stays_usable():
+    """One task of each solve triangle launch never reports its block: the
+    tasks waiting for it give up after the short limit, the solve returns -4,
+    and the next solve on the same engine is correct."""
+    import torch
+    rs, sm = ref_system(12)
+    ds = spr.DeviceSolver(rs.mspar, rs.mtrees, rs.msifa)
+    d = torch.from_numpy(sm).cuda()
+    ds.factor(d)
+    b = rhs(rs.neq, 2, 6)
+    d_b0 = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    ds.set_watchdog(0.05, drop=True)
+    d_b = d_b0.clone()
+    with pytest.raises(RuntimeError, match='-4'):
+        ds.solve(d, d_b, 2)
+    ds.set_watchdog(2.0, drop=False)
+    d_b = d_b0.clone()
+    ds.solve(d, d_b, 2)
+    o = run_sprsol('orc', rs, sm, b)
+    assert relerr(d_b.cpu().numpy().T, o['b']) <= 1e-9
+    ds.close()
+
+
 def test_edit_of_the_factor_between_calls_is_seen():
     rs, sm = ref_system(6, 'loguniform')
     b = rhs(rs.neq, 2, 9)
