@@ -244,6 +244,9 @@ int spr_b200_elem_assemble(void* handle, double* d_sm, const double* d_em, const
  * skipped).  With lam solving K lam = dL/du this is dL/dtheta_e. */
 int spr_b200_elem_grad(void* handle, const double* d_u, const double* d_lam, int64_t ld, int64_t nrhs,
                        const double* d_em, const double* d_dscale, double* d_grad, void* stream);
+/* No reference counterpart.  The number of device contexts the Fortran entry
+ * points hold (one per MSPAR/MTREES/MSIFA triple they were called with). */
+int spr_b200_contexts(void);
 /* Frees every device context cached by the Fortran entry points. */
 void spr_b200_release_all(void);
 

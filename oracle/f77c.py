@@ -59,13 +59,36 @@ def _pp_eval(expr, defines):
     return bool(eval(expr))
 
 
-def read_statements(path, defines=None):
-    """Return [(label, text, 'file:line')] with continuations joined."""
+_UNIT_HDR = re.compile(r'^ {6}\s*(?:(?:INTEGER|DOUBLE\s*PRECISION|REAL|LOGICAL)(?:\*\d+|\(\s*kind\s*=\s*\w+\s*\))?\s+)?'
+                       r'(?:SUBROUTINE|FUNCTION)\s+(\w+)', re.I)
+_UNIT_END = re.compile(r'^ {6}\s*END\s*$', re.I)
+
+
+def _pick_units(raw_lines, keep):
+    """Blank out every line outside the program units named in `keep` (a
+    source file of many routines of which only a few are needed; line numbers
+    are kept for the messages)."""
+    out, inside = [], False
+    for raw in raw_lines:
+        m = _UNIT_HDR.match(raw)
+        if m and not inside:
+            inside = m.group(1).upper() in keep
+        out.append(raw if inside else '')
+        if inside and _UNIT_END.match(raw):
+            inside = False
+    return out
+
+
+def read_statements(path, defines=None, keep=None):
+    """Return [(label, text, 'file:line')] with continuations joined; with
+    `keep`, only the named program units of the file."""
     defines = defines or {}
     out = []
     active = []                      # stack of (parent_active, this_active)
     with open(path, encoding='latin-1') as fh:
         raw_lines = fh.read().split('\n')
+    if keep:
+        raw_lines = _pick_units(raw_lines, keep)
     for ln, raw in enumerate(raw_lines, 1):
         raw = raw.rstrip('\r')
         if raw.startswith('#'):
@@ -195,6 +218,16 @@ def tokenize(s):
             text = s[i:j]
             if is_real:
                 toks.append(('real', text, kind))
+            elif j + 1 < n and s[j] == '_' and s[j + 1].isalpha():
+                # integer literal with a kind parameter (0_I4, 1_I8)
+                k = j + 1
+                while k < n and (s[k].isalnum() or s[k] == '_'):
+                    k += 1
+                kname = s[j + 1:k]
+                if kname not in ('I4', 'I8'):
+                    raise F77Error('unsupported literal kind ' + kname)
+                toks.append(('int', text, kname.lower()))
+                j = k
             else:
                 toks.append(('int', text))
             i = j
@@ -327,7 +360,7 @@ class Parser:
     def p_prim(self):
         tok = self.take()
         if tok[0] == 'int':
-            return ('int', tok[1])
+            return ('int', tok[1]) if len(tok) == 2 else ('ikind', tok[1], tok[2])
         if tok[0] == 'real':
             return ('real', tok[1], tok[2])
         if tok[0] == 'str':
@@ -476,7 +509,12 @@ class Translator:
 
     # ---------------- front end ----------------
     def load(self, path):
-        stmts = read_statements(path, self.defines)
+        # "file.f:NAME1,NAME2" translates only those routines of the file
+        keep = None
+        if ':' in os.path.basename(path):
+            path, names = path.rsplit(':', 1)
+            keep = set(n.strip().upper() for n in names.split(',') if n.strip())
+        stmts = read_statements(path, self.defines, keep)
         unit = None
         for label, text, where in stmts:
             norm, strings = normalise(text)
@@ -612,7 +650,7 @@ class Translator:
     # ---------------- helpers ----------------
     def const_eval(self, unit, e):
         k = e[0]
-        if k == 'int':
+        if k in ('int', 'ikind'):
             return int(e[1])
         if k == 'paren':
             return self.const_eval(unit, e[1])
@@ -655,6 +693,8 @@ class Translator:
         k = e[0]
         if k == 'int':
             return 'i'
+        if k == 'ikind':
+            return e[2]
         if k == 'real':
             return 'd' if e[2] == 'd' else 'f'
         if k == 'log':
@@ -738,6 +778,8 @@ class Translator:
         k = e[0]
         if k == 'int':
             return '((fint)%s)' % e[1]
+        if k == 'ikind':
+            return '((%s)%s)' % ('int32_t' if e[2] == 'i4' else 'int64_t', e[1])
         if k == 'real':
             txt = e[1].replace('D', 'e').replace('E', 'e')
             if '.' not in txt and 'e' not in txt:
@@ -1135,6 +1177,16 @@ class Translator:
             if u.kind == 'fun':
                 rt = CTYPE[u.rettype or 'f']
             parts.append('%s %s_();' % (rt, u.name.lower()))
+        # typed EXTERNAL functions defined outside this translation (BLAS,
+        # other libraries): their return type must be declared
+        ext = {}
+        for u in self.units:
+            for sym in u.syms.values():
+                nm = sym.name.lower() + '_'
+                if sym.external and sym.type is not None and not sym.dummy and nm not in self.routines:
+                    ext[nm] = CTYPE[sym.type]
+        for nm in sorted(ext):
+            parts.append('%s %s();' % (ext[nm], nm))
         parts.append('')
         for u in self.units:
             parts.append(self.emit_unit(u))

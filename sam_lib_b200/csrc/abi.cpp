@@ -1160,6 +1160,13 @@ int SPR_API(spr_b200_elem_grad)(void* handle, const double* d_u, const double* d
 }
 
 // Releases every cached context (device memory of the Fortran entry points).
+// Number of device contexts the Fortran entry points hold (one per
+// structure triple they were called with); 0 before any call.
+int SPR_API(spr_b200_contexts)(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return (int)g_ctx.size();
+}
+
 void SPR_API(spr_b200_release_all)(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_ctx.clear();
