@@ -310,6 +310,46 @@ def form_mixed_ir(torch, spr, n, emod, reps=2):
             'rel_diff_vs_fp64_gpu_solution': rel}
 
 
+def form_mixed_vs_reference(torch, spr, n=20, emod='loguniform'):
+    """Mixed + refinement against the reference's own FP64 CPU solve (the
+    translated SPR SPRSOL) on a size the CPU affords: the n^3 box with the
+    config-3 moduli, 4 RHS.  Reports the relative difference of the refined
+    solution from the reference's, NUMNEG of both and the refinement."""
+    from oracle.refpipe import RefSystem
+    from sam_lib_b200.fe import HexBox, hex8_stiffness, element_moduli
+    from sam_lib_b200.system import HexSystem
+    moduli = element_moduli(n ** 3, emod, seed=2)
+    hs = HexSystem(n, moduli=moduli)
+    sm = hs.assemble()
+    f = np.random.default_rng(1).uniform(-1.0, 1.0, size=(NRHS, hs.neq))
+    rs = RefSystem(HexBox(n))
+    ke = hex8_stiffness()
+    rsm = rs.assemble(lambda e: ke * moduli[e])
+    same = bool(np.array_equal(rsm, sm))                 # SPRADM and the library's assembly agree
+    rb = np.asfortranarray(f.T.copy())
+    t0 = time.perf_counter()
+    ierr, _, rneg = rs.sprsol(3, rsm, rb)
+    t_ref = time.perf_counter() - t0
+    ds = spr.DeviceSolver(hs.mspar, hs.mtrees, hs.msifa)
+    d_sm0 = torch.from_numpy(sm).cuda()
+    ds.build_residual(d_sm0)
+    ds.set_mode(1)
+    d_sm = d_sm0.clone()
+    fr = ds.factor(d_sm)
+    d_b = torch.from_numpy(f).cuda()
+    d_x = torch.empty_like(d_b)
+    it, berr, _ = ds.refine(d_sm, d_b, d_x, NRHS, tol=1e-12, maxit=30)
+    x = d_x.cpu().numpy().T
+    ds.close()
+    del d_sm0, d_sm, d_b, d_x
+    torch.cuda.empty_cache()
+    return {'system': '%d^3 hex8, E %s (seed 2), %d RHS U[-1,1] seed 1' % (n, emod, NRHS),
+            'reference': 'translated SPR SPRSOL IOP=3 (FP64, 1 core, %.1f s)' % t_ref,
+            'rel_diff_vs_reference_solution': float(np.linalg.norm(x - rb) / np.linalg.norm(rb)),
+            'numneg': fr['numneg'], 'numneg_reference': int(rneg), 'ir_corrections': it, 'backward_error': berr,
+            'same_assembled_matrix': same}
+
+
 def form_batched(torch, reps=3, cpu_procs=0):
     """512 uneven shifted (indefinite) systems, 16 RHS each, as one forest."""
     from sam_lib_b200.batch import BatchSolver
@@ -616,7 +656,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.empty_cache()
     forms = None
     if rank == 0 and world == 1 and not args.no_forms and args.n == N_MESH:
-        forms = {'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
+        forms = {'mixed_ir_vs_reference_cpu': form_mixed_vs_reference(torch, spr),
+                 'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
                  'mixed_ir_uniform': form_mixed_ir(torch, spr, N_MESH, 'uniform'),
                  'batched': form_batched(torch, cpu_procs=os.cpu_count() or 1), 'adjoint': form_adjoint(torch)}
     if rank == 0:
