@@ -446,6 +446,45 @@ def batched_cpu_sample(nproc, per_proc=8):
             'wall_s_incl_setup': wall}
 
 
+def form_batched_sharded(torch, rank, world, dist, reps=3):
+    """The 512-system workload sharded over the ranks (round robin by system,
+    no exchange on the data path): each rank factors and solves its share as
+    one forest; the batch time is the maximum over ranks (CUDA events on each
+    rank's stream)."""
+    from sam_lib_b200.batch import BatchSolver
+    from sam_lib_b200.replicas import max_over_ranks, shard
+    from sam_lib_b200.workloads import config4
+    systems = config4()
+    mine = [systems[i] for i in shard(len(systems), rank, world)]
+    bs = BatchSolver(mine)
+    st = torch.cuda.Stream()
+    bs.ds.set_stream(st.cuda_stream)
+    ts = []
+    for r in range(reps + 1):
+        with torch.cuda.stream(st):
+            bs.sm.copy_(bs.sm0)
+            bs.b.copy_(bs.b0)
+        st.synchronize()
+        dist.barrier()
+        e0, e1 = _ev(torch), _ev(torch)
+        e0.record(st)
+        fr = bs.ds.factor(bs.sm)
+        bs.ds.solve(bs.sm, bs.b, bs.nrhs)
+        e1.record(st)
+        e1.synchronize()
+        if r > 0:
+            ts.append(e0.elapsed_time(e1))
+    t = max_over_ranks(float(np.mean(ts)) / 1e3, dist, 'cuda')
+    neg = bs.numneg()
+    total_neg = max_over_ranks(float(neg.sum()), None)
+    del bs
+    torch.cuda.empty_cache()
+    return {'systems_per_s': len(systems) / t, 's_per_batch': t, 'ranks': world,
+            'systems_this_rank': len(mine), 'numneg_rank0': int(total_neg), 'lierr_rank0': fr['lierr'],
+            'workload': '512 boxes n~U{3..12} (seed 3), K - sigma M, 16 RHS each, sharded round robin '
+                        '(strong scaling: the same 512 systems for any number of ranks), FP64'}
+
+
 def form_adjoint(torch, reps=3):
     """32^3 SIMP compliance: forward (assemble + factor + solve) vs forward + backward."""
     from sam_lib_b200.adjoint import SimpModel, simp_solve, simp_workload
@@ -655,6 +694,11 @@ def run_ours(args, rank, world, local_rank):
     del ds, d_sm0, d_sm, d_b0, d_b
     torch.cuda.empty_cache()
     forms = None
+    if world > 1 and not args.no_forms:
+        # every rank takes part (the same collective steps on all ranks)
+        bs = form_batched_sharded(torch, rank, world, dist)
+        if rank == 0:
+            forms = {'batched_sharded': bs}
     if rank == 0 and world == 1 and not args.no_forms and args.n == N_MESH:
         forms = {'mixed_ir_vs_reference_cpu': form_mixed_vs_reference(torch, spr),
                  'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
