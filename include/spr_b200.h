@@ -116,7 +116,8 @@ int spr_b200_solve_dev(void* handle, const double* d_sm, double* d_b, int64_t ld
  * mode) [9]=Schur-update algorithmic flops [10]=launches of the last solve
  * [11]=NZEROL [12]=pivots with |d| < tau |a_jj| that the mixed-mode inertia
  * guard counted in the last factorisation [13]=1 if the guard redid that
- * factorisation in FP64.  info must hold 14 doubles. */
+ * factorisation in FP64 [14]=trace of the original diagonal (sprfc1.f:483).
+ * info must hold 15 doubles. */
 int spr_b200_info(void* handle, double* info);
 /* Per-supernode negative-pivot counts and first failing column (-1 if none)
  * of the last spr_b200_factor_dev (NSUPER entries each): per-system inertia
@@ -149,6 +150,23 @@ int spr_b200_set_inertia_guard(void* handle, double tau);
  * reports its block, so that waits run out.  Returns -2 for a limit outside
  * the range. */
 int spr_b200_set_watchdog(void* handle, double wait_ns, int drop);
+/* No reference counterpart.  One system split across GPUs (one process and
+ * one handle per GPU, the same structure on all; orchestrated by
+ * sam_lib_b200/split.py).  spr_b200_set_skip: supernodes with mask[js] != 0
+ * (NSUPER bytes) are left alone by spr_b200_factor_dev and spr_b200_solve_dev;
+ * NULL clears the mask.  spr_b200_set_exchange: for the following
+ * factorisations, node fo_node[k]'s update block ((F-S) x (F-S) doubles,
+ * column-major, leading dimension F-S) is copied to the device buffer
+ * fo_buf[k] right after that node's tree level, and fi_buf[k] is copied into
+ * node fi_node[k]'s block right before its parent's level; for the following
+ * forward sweeps the same with the update vectors ((F-S) x nrhs doubles, nrhs
+ * <= 16), vo_* and vi_*.  Copies run on the handle's stream.  -2 for a bad
+ * node or buffer. */
+int spr_b200_set_skip(void* handle, const uint8_t* mask);
+int spr_b200_set_exchange(void* handle, int64_t nfo, const int32_t* fo_node, double* const* fo_buf,
+                          int64_t nfi, const int32_t* fi_node, double* const* fi_buf, int64_t nvo,
+                          const int32_t* vo_node, double* const* vo_buf, int64_t nvi,
+                          const int32_t* vi_node, double* const* vi_buf);
 /* Residual operator for refinement: compacts the FP64 matrix held in an
  * assembled (not yet factored) device SM into a CSR (the product SPRPRQ forms
  * from the packed pattern, sprprm.f:243-325). */

@@ -59,6 +59,11 @@ def load(int_kind=8):
         lib.spr_b200_set_inertia_guard.restype = C.c_int
         lib.spr_b200_set_watchdog.argtypes = [vp, C.c_double, C.c_int]
         lib.spr_b200_set_watchdog.restype = C.c_int
+        lib.spr_b200_set_skip.argtypes = [vp, vp]
+        lib.spr_b200_set_skip.restype = C.c_int
+        lib.spr_b200_set_exchange.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp,
+                                              C.c_int64, vp, vp]
+        lib.spr_b200_set_exchange.restype = C.c_int
         lib.spr_b200_autotune.argtypes = [vp, vp, vp]
         lib.spr_b200_autotune.restype = C.c_int
         lib.spr_b200_tc_stats.argtypes = [vp, vp]
@@ -277,11 +282,11 @@ class DeviceSolver:
             raise RuntimeError('spr_b200_solve_dev failed with %d' % rc)
 
     def info(self):
-        out = np.zeros(14)
+        out = np.zeros(15)
         self.lib.spr_b200_info(self.h, _ptr(out))
         keys = ('factor_flops', 'solve_flops', 'arena_bytes', 'levels', 'factor_ms', 'solve_ms',
                 'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops', 'solve_launches', 'nzerol',
-                'near_pivots', 'fp64_redo')
+                'near_pivots', 'fp64_redo', 'trace')
         return dict(zip(keys, out.tolist()))
 
     def sn_stats(self, nsuper):
@@ -322,6 +327,32 @@ class DeviceSolver:
         test switch that makes one CTA's waits run out."""
         if self.lib.spr_b200_set_watchdog(self.h, float(wait_s) * 1e9, 1 if drop else 0) != 0:
             raise ValueError('bad watchdog limit %r' % (wait_s,))
+
+    def set_skip(self, mask):
+        """Split runs: supernodes with mask[js] (NSUPER bools) are left alone; None clears."""
+        if mask is None:
+            rc = self.lib.spr_b200_set_skip(self.h, None)
+        else:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            rc = self.lib.spr_b200_set_skip(self.h, _ptr(m))
+        if rc != 0:
+            raise RuntimeError('spr_b200_set_skip failed with %d' % rc)
+
+    def set_exchange(self, factor_out=(), factor_in=(), vec_out=(), vec_in=()):
+        """Split runs: lists of (node, device buffer) for the update blocks of
+        the following factorisations and the update vectors of the following
+        forward sweeps (see include/spr_b200.h)."""
+        def arr(lst):
+            nodes = np.array([int(n) for n, _ in lst], dtype=np.int32)
+            bufs = (C.c_void_p * max(1, len(lst)))(*[C.c_void_p(self._dev(b)) for _, b in lst])
+            return len(lst), nodes, bufs
+        parts = [arr(l) for l in (factor_out, factor_in, vec_out, vec_in)]
+        args = []
+        for n, nodes, bufs in parts:
+            args += [n, _ptr(nodes), C.cast(bufs, C.c_void_p)]
+        rc = self.lib.spr_b200_set_exchange(self.h, *args)
+        if rc != 0:
+            raise RuntimeError('spr_b200_set_exchange failed with %d' % rc)
 
     def autotune(self, d_sm_assembled):
         """Mixed-mode autotuner on a copy of the assembled SM; returns the choice and times."""

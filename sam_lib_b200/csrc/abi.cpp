@@ -906,7 +906,8 @@ int SPR_API(spr_b200_solve_dev)(void* handle, const double* d_sm, double* d_b, i
 // [8]=Schur-update ms (profile mode), [9]=Schur-update algorithmic flops,
 // [10]=kernel launches of the last solve, [11]=NZEROL, [12]=pivots the
 // mixed-mode inertia guard counted in the last factorisation, [13]=1 if that
-// factorisation was redone in FP64 by the guard.
+// factorisation was redone in FP64 by the guard, [14]=trace of the original
+// diagonal (sprfc1.f:483) of the last factorisation.
 int SPR_API(spr_b200_info)(void* handle, double* info) {
     Engine* e = static_cast<Engine*>(handle);
     const sprb::Plan& p = e->plan();
@@ -924,6 +925,7 @@ int SPR_API(spr_b200_info)(void* handle, double* info) {
     info[11] = (double)p.nzerol;
     info[12] = (double)e->last_near_pivots();
     info[13] = e->last_refactored() ? 1.0 : 0.0;
+    info[14] = e->last_trace();
     return 0;
 }
 
@@ -951,6 +953,35 @@ int SPR_API(spr_b200_refine)(void* handle, const double* d_sm, const double* d_b
 int SPR_API(spr_b200_set_mode)(void* handle, int mode) {
     if (mode < 0 || mode > 2) return -2;
     static_cast<Engine*>(handle)->set_mixed(mode);
+    return 0;
+}
+
+// Split across GPUs: node mask (NSUPER bytes, nonzero = another rank's; null
+// clears it) and the exchange lists of the following factorisations
+// (update blocks) and forward sweeps (update vectors).
+int SPR_API(spr_b200_set_skip)(void* handle, const uint8_t* mask) {
+    return static_cast<Engine*>(handle)->set_skip(mask);
+}
+
+int SPR_API(spr_b200_set_exchange)(void* handle, int64_t nfo, const int32_t* fo_node, double* const* fo_buf,
+                                   int64_t nfi, const int32_t* fi_node, double* const* fi_buf, int64_t nvo,
+                                   const int32_t* vo_node, double* const* vo_buf, int64_t nvi, const int32_t* vi_node,
+                                   double* const* vi_buf) {
+    Engine* e = static_cast<Engine*>(handle);
+    const int64_t ns = e->plan().nsuper;
+    auto list = [ns](int64_t n, const int32_t* node, double* const* buf, std::vector<Engine::Xfer>& out) {
+        out.clear();
+        for (int64_t k = 0; k < n; ++k) {
+            if (node[k] < 0 || node[k] >= ns || !buf[k]) return false;
+            out.push_back(Engine::Xfer{node[k], buf[k]});
+        }
+        return true;
+    };
+    std::vector<Engine::Xfer> fo, fi, vo, vi;
+    if (!list(nfo, fo_node, fo_buf, fo) || !list(nfi, fi_node, fi_buf, fi) || !list(nvo, vo_node, vo_buf, vo) ||
+        !list(nvi, vi_node, vi_buf, vi))
+        return -2;
+    e->set_exchange(std::move(fo), std::move(fi), std::move(vo), std::move(vi));
     return 0;
 }
 

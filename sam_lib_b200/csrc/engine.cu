@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <thread>
 
 #include "engine.h"
@@ -109,6 +110,9 @@ struct PV {
     // streamed factorisation: the original diagonal gathered on the host
     // (the pre-pass then reads it instead of LNZ, which is still uploading)
     const double* adiag_in;
+    // node mask of a run split across GPUs: supernodes with skip[js] != 0 are
+    // left alone (null: none)
+    const uint8_t* skip;
 };
 
 struct Engine::Dev {
@@ -146,6 +150,8 @@ struct Engine::Dev {
     int64_t vbuf_rhs = 0;
     double* bbuf = nullptr;                      // contiguous copy of B (ldb = NEQ)
     int64_t bbuf_rhs = 0;
+    uint8_t* skip = nullptr;                     // node mask of a split run
+    bool skip_on = false;
     int32_t* tri_tasks = nullptr;                // the solves' triangle tasks (node, block)
     int32_t* tri_sync = nullptr;                 // block-ready flags, then one task counter per level
     std::vector<void*> owned;
@@ -240,6 +246,9 @@ __device__ __forceinline__ void fc3_record(const PV& P, int col, double d0, doub
         atomicAdd(&P.st->nsing, 1ull);
     }
 }
+
+// a supernode another GPU handles (split runs)
+__device__ __forceinline__ bool node_off(const PV& P, int js) { return P.skip != nullptr && P.skip[js] != 0; }
 
 __device__ __forceinline__ bool children_bad(const PV& P, int js) {
     for (int k = P.child_ptr[js]; k < P.child_ptr[js + 1]; ++k)
@@ -384,6 +393,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
     extern __shared__ double sh[];
     if (P.st->any_fail) return;
     const int js = nodes[blockIdx.x];
+    if (node_off(P, js)) return;
     if (children_bad(P, js)) {
         if (threadIdx.x == 0) P.sn_bad[js] = 1;
         return;
@@ -507,7 +517,7 @@ __global__ void k_poison(const Job* jobs, int64_t njobs, const int32_t* tmap, PV
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     const int js = jobs[j].node;
-    if (children_bad(P, js)) P.sn_bad[js] = 1;
+    if (!node_off(P, js) && children_bad(P, js)) P.sn_bad[js] = 1;
 }
 
 // Extend-add into a dense column-major front: one warp per front column.
@@ -557,7 +567,7 @@ __global__ void __launch_bounds__(256) k_assemble(const Job* jobs, int64_t njobs
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int j = jb.c0 + (int)(task - jb.task0);
     const int F = P.F[js], S = P.S[js];
     const int ld = P.buf_ld[js];
@@ -642,7 +652,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int ld = P.buf_ld[js], fst = P.fst[js];
     double* front = P.arena + P.buf_off[js];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
@@ -804,7 +814,7 @@ __global__ void __launch_bounds__(128) k_trsm(const Job* jobs, int64_t njobs, co
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int F = P.F[js], ld = P.buf_ld[js];
     const int r0 = jb.c0 + (int)(task - jb.task0) * kTRSMRows;
     double* front = P.arena + P.buf_off[js];
@@ -936,7 +946,7 @@ k_gemm(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int ld = P.buf_ld[js];
     // decode the lower-triangle tile (column tile jt, row tile it >= jt)
     const int64_t u = task - jb.task0;
@@ -1118,7 +1128,7 @@ __global__ void __launch_bounds__(128) k_gemm_x3(const Job* jobs, int64_t njobs,
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int ld = P.buf_ld[js];
     const int64_t u = task - jb.task0;
     const int nct = (jb.c_end - jb.c0 + T - 1) / T;
@@ -1263,7 +1273,7 @@ __global__ void k_writeback(const Job* jobs, int64_t njobs, const int32_t* tmap,
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int j = jb.c0 + (int)(task - jb.task0);
     const int F = P.F[js], ld = P.buf_ld[js];
     const double* col = P.arena + P.buf_off[js] + (int64_t)j * ld;
@@ -1303,6 +1313,7 @@ __global__ void __launch_bounds__(kSolveThreads)
 k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
     extern __shared__ double wsm[];           // w[i * nrhs + r], then Ls[(i - j0) * (kSmallBlk + 1) + c]
     const int js = nodes[blockIdx.x];
+    if (node_off(P, js)) return;
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* Ls = wsm + (size_t)F * nrhs;
     double* wg = vbuf + P.rbase[js] * nrhs;   // update rows for the parent (r*F + i)
@@ -1356,6 +1367,7 @@ __global__ void __launch_bounds__(kSolveThreads)
 k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int nrhs) {
     extern __shared__ double wsm[];
     const int js = nodes[blockIdx.x];
+    if (node_off(P, js)) return;
     if (is_retained(P, js)) return;
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* Ls = wsm + (size_t)F * nrhs;
@@ -1418,6 +1430,7 @@ __global__ void k_fwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int i = (int)(task - jb.task0);
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* w = vbuf + P.rbase[js] * nrhs;
@@ -1539,7 +1552,7 @@ __global__ void __launch_bounds__(256) k_inv_block(const Job* jobs, PV P) {
     double(*Ts)[kNB + 1] = Bs + kNB;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
-    if (P.sn_bad && P.sn_bad[js]) return;
+    if ((P.sn_bad && P.sn_bad[js]) || node_off(P, js)) return;
     const int F = P.F[js];
     const double* base = P.lnz + P.lnz_off[js];
     const double* lv0 = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
@@ -1753,6 +1766,7 @@ __global__ void __launch_bounds__(256) k_fwd_rect_part(const Job* jobs, int64_t 
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int F = P.F[js], S = P.S[js];
     const int ncc = jb.k_hi;
     const int64_t u = task - jb.task0;
@@ -1792,6 +1806,7 @@ __global__ void k_fwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int F = P.F[js], S = P.S[js];
     const int row = S + (int)(task - jb.task0);
     const int ncc = (S + kRectCols - 1) / kRectCols;
@@ -1817,6 +1832,7 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int F = P.F[js], S = P.S[js];
     const int ncc = jb.k_hi;
     const int64_t u = task - jb.task0;
@@ -1879,6 +1895,7 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int F = P.F[js], S = P.S[js];
     if (F <= S || is_retained(P, js)) return;
     const int c = (int)(task - jb.task0);
@@ -1900,6 +1917,7 @@ __global__ void k_fwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
     if (is_retained(P, js)) {
@@ -1971,6 +1989,10 @@ __global__ void __launch_bounds__(256) k_fwd_tri(const int32_t* tasks, int ntask
         const int t = task_sh;
         if (t >= ntasks) break;
         const int js = tasks[2 * t], rb = tasks[2 * t + 1];
+        if (node_off(P, js)) {
+            __syncthreads();                                          // all have read task_sh
+            continue;
+        }
         const int F = P.F[js], S = P.S[js];
         const int r0 = rb * kNB, nrow = min(kNB, S - r0);
         const double* base = P.lnz + P.lnz_off[js];
@@ -2058,6 +2080,10 @@ __global__ void __launch_bounds__(256) k_bwd_tri(const int32_t* tasks, int ntask
         if (task_sh >= ntasks) break;
         const int t = ntasks - 1 - task_sh;                          // descending blocks
         const int js = tasks[2 * t], cb = tasks[2 * t + 1];
+        if (node_off(P, js)) {
+            __syncthreads();
+            continue;
+        }
         const int F = P.F[js], S = P.S[js];
         const int c0 = cb * kNB, ncol = min(kNB, S - c0);
         const int nblk = (S + kNB - 1) / kNB;
@@ -2139,6 +2165,7 @@ __global__ void k_bwd_gather(const Job* jobs, int64_t njobs, const int32_t* tmap
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     const int i = (int)(task - jb.task0);
     const int F = P.F[js], S = P.S[js], fst = P.fst[js];
     double* w = vbuf + P.rbase[js] * nrhs;
@@ -2153,6 +2180,7 @@ __global__ void k_bwd_finish(const Job* jobs, int64_t njobs, const int32_t* tmap
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
+    if (node_off(P, js)) return;
     if (is_retained(P, js)) return;
     const int j = (int)(task - jb.task0);
     const int F = P.F[js], fst = P.fst[js];
@@ -2578,6 +2606,7 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
     v.wait_ns = 2000000000ull;
     v.tc_drop = 0;
     v.adiag_in = nullptr;
+    v.skip = D.skip_on ? D.skip : nullptr;
     return v;
 }
 
@@ -2615,6 +2644,80 @@ void Engine::launch_tc(const TcLaunch& t, cudaStream_t s, const PV& pv, std::vec
     timing.launches += 2;
     ++timing.gemm_launches;
 }
+
+// ---------------------------------------------------------------------------
+// Split across GPUs: node mask and the exchange of subtree roots' update
+// blocks (factor) and update vectors (forward solve).
+// ---------------------------------------------------------------------------
+int Engine::set_skip(const uint8_t* host_mask) {
+    Dev& D = *d_;
+    if (!host_mask) {
+        D.skip_on = false;
+        split_ = !fout_.empty() || !fin_.empty() || !vout_.empty() || !vin_.empty();
+        return 0;
+    }
+    if (!D.skip) {
+        CK(cudaMalloc((void**)&D.skip, std::max<int64_t>(P_.nsuper, 1)));
+        D.owned.push_back(D.skip);
+    }
+    CK(cudaMemcpy(D.skip, host_mask, P_.nsuper, cudaMemcpyHostToDevice));
+    D.skip_on = true;
+    split_ = true;
+    return 0;
+}
+
+void Engine::set_exchange(std::vector<Xfer> fo, std::vector<Xfer> fi, std::vector<Xfer> vo, std::vector<Xfer> vi) {
+    fout_ = std::move(fo);
+    fin_ = std::move(fi);
+    vout_ = std::move(vo);
+    vin_ = std::move(vi);
+    split_ = d_->skip_on || !fout_.empty() || !fin_.empty() || !vout_.empty() || !vin_.empty();
+}
+
+// node js's update block <-> buf ((F-S) x (F-S), leading dimension F-S)
+void Engine::block_copy(int32_t js, double* buf, bool out, cudaStream_t s) {
+    const int64_t q = P_.F[js] - P_.S[js];
+    if (q <= 0) return;
+    double* blk = d_->arena + P_.upd_off[js];
+    const size_t ld = (size_t)P_.buf_ld[js] * sizeof(double), w = (size_t)q * sizeof(double);
+    if (out)
+        cudaMemcpy2DAsync(buf, w, blk, ld, w, q, cudaMemcpyDeviceToDevice, s);
+    else
+        cudaMemcpy2DAsync(blk, ld, buf, w, w, q, cudaMemcpyDeviceToDevice, s);
+}
+
+// node js's forward update vector (rows [S, F) of its front vector, per RHS) <-> buf ((F-S) x nrhs)
+void Engine::vec_copy(int32_t js, double* buf, bool out, int64_t nrhs, cudaStream_t s) {
+    const int64_t f = P_.F[js], q = f - P_.S[js];
+    if (q <= 0) return;
+    double* v = d_->vbuf + P_.rbase[js] * nrhs + P_.S[js];
+    const size_t ld = (size_t)f * sizeof(double), w = (size_t)q * sizeof(double);
+    if (out)
+        cudaMemcpy2DAsync(buf, w, v, ld, w, nrhs, cudaMemcpyDeviceToDevice, s);
+    else
+        cudaMemcpy2DAsync(v, ld, buf, w, w, nrhs, cudaMemcpyDeviceToDevice, s);
+}
+
+namespace {
+// The exchange lists as level hooks: "in" entries before their parent's
+// level, "out" entries after their node's level.
+struct ExchangeHooks : LevelHooks {
+    const Plan* P = nullptr;
+    const std::vector<Engine::Xfer>* out = nullptr;
+    const std::vector<Engine::Xfer>* in = nullptr;
+    std::function<void(int32_t, double*, bool, cudaStream_t)> copy;
+    void before(size_t L, cudaStream_t s) const override {
+        for (const Engine::Xfer& x : *in) {
+            const int32_t p = P->parent[x.node];
+            if (p >= 0 && (size_t)P->level[p] == L) copy(x.node, x.buf, false, s);
+        }
+    }
+    void after(size_t L, cudaStream_t s) const override {
+        for (const Engine::Xfer& x : *out)
+            if ((size_t)P->level[x.node] == L) copy(x.node, x.buf, true, s);
+    }
+};
+}  // namespace
 
 void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_t>& gev) {
     Dev& D = *d_;
@@ -2795,7 +2898,22 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     std::vector<cudaEvent_t> gev;
     // the legacy default stream cannot be captured: graphs need a stream of our own;
     // the watchdog test launches kernel by kernel (its settings are not in the key)
-    // a streamed factorisation enqueues its copies' waits between the levels
+    // a streamed factorisation enqueues its copies' waits between the levels;
+    // a split run its exchanges
+    ExchangeHooks xh;
+    const LevelHooks* saved_hooks = hooks_;
+    if (split_ && !hooks_) {
+        xh.P = &P_;
+        xh.out = &fout_;
+        xh.in = &fin_;
+        xh.copy = [this](int32_t js, double* b, bool o, cudaStream_t st) { block_copy(js, b, o, st); };
+        hooks_ = &xh;
+    }
+    struct RestoreHooks {
+        const LevelHooks** h;
+        const LevelHooks* v;
+        ~RestoreHooks() { *h = v; }
+    } restore{&hooks_, saved_hooks};
     const bool graph = use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull && !hooks_;
     if (graph) {
         const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_ | (chol_ ? 16 : 0),
@@ -2845,6 +2963,7 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     }
     marks_.clear();
     res = FactorResult();
+    last_trace_ = hs.trace;
     if (hs.tc_timeout) {
         fprintf(stderr, "spr_b200: a tensor-core update gave up waiting for its operands\n");
         return -4;
@@ -3107,8 +3226,25 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
         const size_t tri_bytes = sizeof(int32_t) * (size_t)(P_.tri_flags + 2 * (int64_t)P_.levels.size());
         if (which & 1) {
             if (tri_solve_) cudaMemsetAsync(D.tri_sync, 0, tri_bytes, s);
+            // split run: the other ranks' subtree roots' update vectors come in
+            // before their parent's level, this rank's go out after their level
+            ExchangeHooks vx;
+            vx.P = &P_;
+            vx.out = &vout_;
+            vx.in = &vin_;
+            vx.copy = [this, nr](int32_t js, double* buf, bool o, cudaStream_t st) { vec_copy(js, buf, o, nr, st); };
+            const bool vexch = !vout_.empty() || !vin_.empty();
             for (size_t L = 0; L < P_.levels.size(); ++L) {
                 const LevelPlan& lp = P_.levels[L];
+                if (vexch) vx.before(L, s);
+                struct AfterLevel {
+                    const ExchangeHooks* h;
+                    size_t L;
+                    cudaStream_t s;
+                    ~AfterLevel() {
+                        if (h) h->after(L, s);
+                    }
+                } after_level{vexch ? &vx : nullptr, L, s};
                 if (!lp.small_nodes.empty()) {
                     mark(0);
                     for (const LevelPlan::SmallClass& c : lp.small_classes) {
@@ -3266,7 +3402,7 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
         }
         linv_valid_ = true;
     }
-    if (use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull) {
+    if (use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull && !split_) {
         const GraphKey key{(const void*)d_sm, (const void*)d_b, (double)ldb, nrhs, which, (int64_t)(uintptr_t)D.vbuf};
         cudaGraphExec_t exec = find_graph(key);
         if (!exec) {

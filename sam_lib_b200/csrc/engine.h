@@ -124,6 +124,7 @@ public:
     void set_inertia_guard(double tau) { guard_tol_ = tau; }
     double inertia_guard() const { return guard_tol_; }
     int64_t last_near_pivots() const { return last_near_; }
+    double last_trace() const { return last_trace_; }
     bool last_refactored() const { return last_refactor_; }
     // Watchdog of the kernels that wait on device flags (the tensor-core
     // update's mbarriers, the solves' block-ready flags): time limit of each
@@ -134,6 +135,22 @@ public:
         wait_ns_ = wait_ns;
         tc_drop_ = drop;
     }
+    // A system split across GPUs (one engine per rank, the same plan on all):
+    // supernodes with mask[js] != 0 are left alone by factor() and solve()
+    // (another rank factors them); null clears the mask.  The exchange lists
+    // of the following factor() move update blocks ((F-S) x (F-S) doubles,
+    // column-major, leading dimension F-S), those of the forward sweep of the
+    // following solve() update vectors ((F-S) x nrhs): an "out" entry is
+    // copied from the node's block/vector into buf right after the node's
+    // level, an "in" entry from buf into it right before its parent's level,
+    // both on the engine's stream.  The lists stay until replaced.
+    struct Xfer {
+        int32_t node;
+        double* buf;
+    };
+    int set_skip(const uint8_t* host_mask);
+    void set_exchange(std::vector<Xfer> factor_out, std::vector<Xfer> factor_in, std::vector<Xfer> vec_out,
+                      std::vector<Xfer> vec_in);
     Timing timing;
     struct Dev;              // device copies of the plan and work buffers
     struct Transfer;         // copy ranges and events of the streamed factorisation
@@ -168,12 +185,17 @@ private:
     std::vector<GraphEntry> graphs_;
     bool use_graphs_ = true;
     bool tri_solve_ = true;                  // solve triangles as one dataflow launch per level
+    std::vector<Xfer> fout_, fin_, vout_, vin_;   // exchange lists of a split run
+    bool split_ = false;                     // a mask or exchange lists are set (no graphs)
+    void block_copy(int32_t js, double* buf, bool out, cudaStream_t s);
+    void vec_copy(int32_t js, double* buf, bool out, int64_t nrhs, cudaStream_t s);
     const LevelHooks* hooks_ = nullptr;      // set during a streamed factorisation
     const double* streamed_diag_ = nullptr;  // its host-gathered original diagonal (device)
     std::unique_ptr<Transfer> xfer_;
     int mixed_ = 0;
     double guard_tol_ = 1.0e-3;
     int64_t last_near_ = 0;
+    double last_trace_ = 0.0;
     bool last_refactor_ = false;
     double* guard_copy_ = nullptr;           // assembled SM kept for the FP64 redo of the guard
     int64_t guard_cap_ = 0;

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256) k_split_tc(const Job* jobs, int64_t njobs
     const int64_t task = blockIdx.x;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
-    if (P.sn_bad[js]) return;
+    if (P.sn_bad[js] || node_off(P, js)) return;
     const int64_t np = tc::padded_rows(jb);
     const int nkb = tc::k_blocks(jb);
     const int64_t u = task - jb.task0;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         int64_t g = 0;
         for (int64_t task = blockIdx.x; task < ntasks && !*(volatile int*)&failed; task += gridDim.x) {
             const Job& jb = job_of(jobs, njobs, tmap, task);
-            if (P.sn_bad[jb.node]) continue;
+            if (P.sn_bad[jb.node] || node_off(P, jb.node)) continue;
             int it, jt;
             tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
             const int64_t np = padded_rows(jb);
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         int64_t g = 0, h = 0;
         for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
             const Job& jb = job_of(jobs, njobs, tmap, task);
-            if (P.sn_bad[jb.node]) continue;
+            if (P.sn_bad[jb.node] || node_off(P, jb.node)) continue;
             const int nkb = k_blocks(jb);
             bool stop = false;
             for (int c0 = 0; c0 < nkb && !stop; c0 += kChunk, ++h) {
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
             const Job& jb = job_of(jobs, njobs, tmap, task);
             const int js = jb.node;
-            if (P.sn_bad[js]) continue;
+            if (P.sn_bad[js] || node_off(P, js)) continue;
             int it, jt;
             tile_of(task - jb.task0, (jb.c_end - jb.c0 + kTM - 1) / kTM, (jb.r_end - jb.c0 + kTM - 1) / kTM, it, jt);
             const int i0 = jb.c0 + it * kTM, j0 = jb.c0 + jt * kTM;
