@@ -2095,7 +2095,9 @@ __global__ void __launch_bounds__(256) k_bwd_tri(const int32_t* tasks, int ntask
         for (int r = 0; r < NR; ++r) acc[r] = 0.0;
         bool ok = true;
         const int64_t pc = (col < ncol) ? lnz_col(c0 + col, F) - (c0 + col) : 0;   // column c0 + col, row 0
-        for (int rb = cb + 1; rb < nblk; ++rb) {
+        // the blocks below finish from the bottom up: take them in that order,
+        // so that only the nearest one (cb + 1, the last to finish) is waited for
+        for (int rb = nblk - 1; rb > cb; --rb) {
             if (tid == 0) ok_sh = tri_wait(fl + rb, abort_word, P);
             __syncthreads();
             if (!ok_sh) {
