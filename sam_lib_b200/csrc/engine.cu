@@ -1998,11 +1998,39 @@ __global__ void __launch_bounds__(256) k_fwd_tri(const int32_t* tasks, int ntask
         const double* base = P.lnz + P.lnz_off[js];
         const int64_t vb = P.rbase[js] * nrhs;
         int32_t* fl = flags + P.tri_off[js];
+        // loads that need no other task: this row's X entries (the product
+        // with the block inverse at the end) and the right-hand side
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)rb * kNB * kNB;
+        constexpr bool kPreX = NR <= 4;                                      // registers allow it
+        double xr[kPreX ? 16 : 1];
+        if constexpr (kPreX) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int m = 16 * q + k;
+                xr[k] = (m <= row) ? __ldg(lv + row + m * kNB) : 0.0;       // X[row][m], unit lower
+            }
+        }
+        double wv[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            wv[r] = (tid < kNB && row < nrow && r < nrhs) ? __ldcg(vbuf + vb + (int64_t)r * F + r0 + row) : 0.0;
         double acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[r] = 0.0;
         bool ok = true;
         for (int b = 0; b < rb; ++b) {
+            // this thread's 16 entries of the tile L[rb, b] first: they do not
+            // depend on block b, so their latency overlaps the wait for it
+            double lr[16];
+            {
+                const int c0 = kNB * b + 16 * q;
+                int64_t p = lnz_col(c0, F) - c0 + r0 + row;           // L[r0 + row][c0]
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    lr[k] = (row < nrow) ? __ldg(base + p) : 0.0;
+                    p += F - (c0 + k) - 1;                            // next column, same row
+                }
+            }
             if (tid == 0) ok_sh = tri_wait(fl + b, abort_word, P);
             __syncthreads();
             if (!ok_sh) {
@@ -2014,18 +2042,11 @@ __global__ void __launch_bounds__(256) k_fwd_tri(const int32_t* tasks, int ntask
                 ys[i][r] = __ldcg(ysol + vb + (int64_t)r * F + kNB * b + i);
             }
             __syncthreads();
-            if (row < nrow) {
-                const int c0 = kNB * b + 16 * q;
-                int64_t p = lnz_col(c0, F) - c0 + r0 + row;           // L[r0 + row][c0]
-#pragma unroll 4
-                for (int k = 0; k < 16; ++k) {
-                    const double l = __ldg(base + p);
-                    p += F - (c0 + k) - 1;                            // next column, same row
 #pragma unroll
-                    for (int r = 0; r < NR; ++r)
-                        if (r < nrhs) acc[r] += l * ys[16 * q + k][r];
-                }
-            }
+            for (int k = 0; k < 16; ++k)
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if (r < nrhs) acc[r] += lr[k] * ys[16 * q + k][r];
             __syncthreads();
         }
         if (!ok) break;
@@ -2035,21 +2056,27 @@ __global__ void __launch_bounds__(256) k_fwd_tri(const int32_t* tasks, int ntask
             if (r < nrhs) part[q][row][r] = acc[r];
         __syncthreads();
         if (tid < kNB)
-            for (int r = 0; r < nrhs; ++r)
-                ys[row][r] = (row < nrow) ? __ldcg(vbuf + vb + (int64_t)r * F + r0 + row) -
-                                                ((part[0][row][r] + part[1][row][r]) + (part[2][row][r] + part[3][row][r]))
-                                          : 0.0;
-        __syncthreads();
-        const double* lv = P.linv + P.linv_off[js] + (int64_t)rb * kNB * kNB;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-#pragma unroll 4
-        for (int k = 0; k < 16; ++k) {
-            const int m = 16 * q + k;
-            const double x = (m <= row) ? __ldg(lv + row + m * kNB) : 0.0;    // X[row][m], unit lower
 #pragma unroll
             for (int r = 0; r < NR; ++r)
-                if (r < nrhs) acc[r] += x * ys[m][r];
+                if (r < nrhs)
+                    ys[row][r] = (row < nrow) ? wv[r] - ((part[0][row][r] + part[1][row][r]) +
+                                                         (part[2][row][r] + part[3][row][r]))
+                                              : 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            double x;
+            if constexpr (kPreX) {
+                x = xr[k];
+            } else {
+                const int m = 16 * q + k;
+                x = (m <= row) ? __ldg(lv + row + m * kNB) : 0.0;
+            }
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) acc[r] += x * ys[16 * q + k][r];
         }
 #pragma unroll
         for (int r = 0; r < NR; ++r)
@@ -2095,32 +2122,46 @@ __global__ void __launch_bounds__(256) k_bwd_tri(const int32_t* tasks, int ntask
         for (int r = 0; r < NR; ++r) acc[r] = 0.0;
         bool ok = true;
         const int64_t pc = (col < ncol) ? lnz_col(c0 + col, F) - (c0 + col) : 0;   // column c0 + col, row 0
+        const double* lv = P.linv + P.linv_off[js] + (int64_t)cb * kNB * kNB;
+        constexpr bool kPreX = NR <= 4;
+        double xr[kPreX ? 16 : 1];
+        if constexpr (kPreX) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int m = 16 * q + k;
+                xr[k] = (m >= col) ? __ldg(lv + m + col * kNB) : 0.0;       // X[m][col]
+            }
+        }
+        double wv[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            wv[r] = (tid < kNB && col < ncol && r < nrhs) ? __ldcg(vbuf + vb + (int64_t)r * F + c0 + col) : 0.0;
         // the blocks below finish from the bottom up: take them in that order,
         // so that only the nearest one (cb + 1, the last to finish) is waited for
         for (int rb = nblk - 1; rb > cb; --rb) {
+            const int nr = min(kNB, S - rb * kNB);
+            double lr[16];                                   // L[64 rb + 16 q + k][c0 + col], ahead of the wait
+            {
+                const int i0 = kNB * rb + 16 * q;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) lr[k] = (col < ncol && 16 * q + k < nr) ? __ldg(base + pc + i0 + k) : 0.0;
+            }
             if (tid == 0) ok_sh = tri_wait(fl + rb, abort_word, P);
             __syncthreads();
             if (!ok_sh) {
                 ok = false;
                 break;
             }
-            const int nr = min(kNB, S - rb * kNB);
             for (int e = tid; e < kNB * nrhs; e += blockDim.x) {
                 const int i = e & (kNB - 1), r = e >> 6;
                 xs[i][r] = (i < nr) ? __ldcg(xsol + vb + (int64_t)r * F + kNB * rb + i) : 0.0;
             }
             __syncthreads();
-            if (col < ncol) {
-                const int i0 = kNB * rb + 16 * q;
-#pragma unroll 4
-                for (int k = 0; k < 16; ++k) {
-                    const int i = 16 * q + k;
-                    const double l = (i < nr) ? __ldg(base + pc + i0 + k) : 0.0;     // L[64 rb + i][c0 + col]
 #pragma unroll
-                    for (int r = 0; r < NR; ++r)
-                        if (r < nrhs) acc[r] += l * xs[i][r];
-                }
-            }
+            for (int k = 0; k < 16; ++k)
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if (r < nrhs) acc[r] += lr[k] * xs[16 * q + k][r];
             __syncthreads();
         }
         if (!ok) break;
@@ -2129,19 +2170,25 @@ __global__ void __launch_bounds__(256) k_bwd_tri(const int32_t* tasks, int ntask
             if (r < nrhs) part[q][col][r] = acc[r];
         __syncthreads();
         if (tid < kNB)
-            for (int r = 0; r < nrhs; ++r)
-                xs[col][r] = (col < ncol) ? __ldcg(vbuf + vb + (int64_t)r * F + c0 + col) -
-                                                ((part[0][col][r] + part[1][col][r]) + (part[2][col][r] + part[3][col][r]))
-                                          : 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs)
+                    xs[col][r] = (col < ncol) ? wv[r] - ((part[0][col][r] + part[1][col][r]) +
+                                                         (part[2][col][r] + part[3][col][r]))
+                                              : 0.0;
         __syncthreads();
         // x = X' v: x[col] = sum_{m >= col} X[m][col] v[m]
-        const double* lv = P.linv + P.linv_off[js] + (int64_t)cb * kNB * kNB;
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-#pragma unroll 4
+#pragma unroll
         for (int k = 0; k < 16; ++k) {
             const int m = 16 * q + k;
-            const double x = (m >= col) ? __ldg(lv + m + col * kNB) : 0.0;
+            double x;
+            if constexpr (kPreX) {
+                x = xr[k];
+            } else {
+                x = (m >= col) ? __ldg(lv + m + col * kNB) : 0.0;
+            }
 #pragma unroll
             for (int r = 0; r < NR; ++r)
                 if (r < nrhs) acc[r] += x * xs[m][r];
