@@ -262,6 +262,11 @@ int spr_b200_elem_assemble(void* handle, double* d_sm, const double* d_em, const
  * skipped).  With lam solving K lam = dL/du this is dL/dtheta_e. */
 int spr_b200_elem_grad(void* handle, const double* d_u, const double* d_lam, int64_t ld, int64_t nrhs,
                        const double* d_em, const double* d_dscale, double* d_grad, void* stream);
+/* No reference counterpart.  Timing of the last factorisation through the
+ * Fortran entry points on a page-locked SM (copies overlapped with the
+ * factorisation): out[0] = ms of upload before the first level could start,
+ * out[1] = factorisation ms, out[2] = ms of download after its end (3 doubles). */
+int spr_b200_copy_stats(double* out);
 /* No reference counterpart.  The number of device contexts the Fortran entry
  * points hold (one per MSPAR/MTREES/MSIFA triple they were called with). */
 int spr_b200_contexts(void);

@@ -59,6 +59,7 @@ struct Ctx {
     bool dev_chol = false;             // the device holds the L D L' form of a host C C' factor
     cudaStream_t stream = nullptr;
     cudaStream_t copy = nullptr;       // host <-> device copies of a streamed factorisation
+    bool streamed_pending = false;     // its timing is read once the copies are done
     // device factor residency
     const double* sm_host = nullptr;
     uint64_t sm_fp = 0;
@@ -323,8 +324,16 @@ bool is_pinned(const void* p) {
 
 // The copy stream's downloads of a streamed factorisation must be complete
 // before the caller reads SM.
+double g_copy_ms[3] = {0.0, 0.0, 0.0};            // of the last streamed factorisation
+
 int finish_copies(Ctx* c) {
-    return (c && c->copy && cudaStreamSynchronize(c->copy) != cudaSuccess) ? -4 : 0;
+    if (!c || !c->copy) return 0;
+    if (cudaStreamSynchronize(c->copy) != cudaSuccess) return -4;
+    if (c->streamed_pending) {
+        c->eng.streamed_times(g_copy_ms);
+        c->streamed_pending = false;
+    }
+    return 0;
 }
 
 // defer: leave the streamed factorisation's last downloads running (the
@@ -349,6 +358,7 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
         fc3.d_dcor = c->d_dcor;
     }
     FactorResult r;
+    if (streamed) c->streamed_pending = true;
     const int frc = streamed ? c->eng.factor_streamed(sm, c->d_sm, tol[0], r, c->copy)
                     : chol   ? c->eng.factor_chol(c->d_sm, tol[0], r, fc4 ? &fc3 : nullptr)
                              : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
@@ -1191,6 +1201,15 @@ int SPR_API(spr_b200_elem_grad)(void* handle, const double* d_u, const double* d
 }
 
 // Releases every cached context (device memory of the Fortran entry points).
+// Timing of the last factorisation through the Fortran entry points with a
+// pinned SM: out[0] = ms of upload before the factorisation could start,
+// out[1] = factorisation ms, out[2] = ms of download after it.
+int SPR_API(spr_b200_copy_stats)(double* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int k = 0; k < 3; ++k) out[k] = g_copy_ms[k];
+    return 0;
+}
+
 // Number of device contexts the Fortran entry points hold (one per
 // structure triple they were called with); 0 before any call.
 int SPR_API(spr_b200_contexts)(void) {

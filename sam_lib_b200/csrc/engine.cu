@@ -2400,6 +2400,7 @@ struct Engine::Transfer {
     std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges;   // per group: (LNZ offset, doubles)
     std::vector<cudaEvent_t> up, done;                             // per group
     cudaEvent_t start = nullptr, fin = nullptr;
+    cudaEvent_t ts = nullptr, tu = nullptr, tf = nullptr, te = nullptr;   // timing: start, group 0 up, factor end, last download
     std::vector<int64_t> diag_pos;                                 // LNZ offset of each equation's diagonal
     double* h_diag = nullptr;                                      // pinned
     double* d_diag = nullptr;
@@ -2408,6 +2409,10 @@ struct Engine::Transfer {
         for (cudaEvent_t e : done) cudaEventDestroy(e);
         if (start) cudaEventDestroy(start);
         if (fin) cudaEventDestroy(fin);
+        if (ts) cudaEventDestroy(ts);
+        if (tu) cudaEventDestroy(tu);
+        if (te) cudaEventDestroy(te);
+        if (tf) cudaEventDestroy(tf);
         if (h_diag) cudaFreeHost(h_diag);
         if (d_diag) cudaFree(d_diag);
     }
@@ -3154,6 +3159,10 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
         }
         CK(cudaEventCreateWithFlags(&t->start, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&t->fin, cudaEventDisableTiming));
+        CK(cudaEventCreate(&t->ts));
+        CK(cudaEventCreate(&t->tu));
+        CK(cudaEventCreate(&t->te));
+        CK(cudaEventCreate(&t->tf));
         t->diag_pos.resize(neq);
         for (int64_t js = 0; js < P_.nsuper; ++js)
             for (int64_t j = 0; j < P_.S[js]; ++j) t->diag_pos[P_.fst[js] + j] = P_.lnz_off[js] + lnz_col(j, P_.F[js]);
@@ -3167,6 +3176,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     double* d_lnz = d_sm + neq;
     // the copy stream starts after the compute stream's earlier work
     CK(cudaEventRecord(t.start, s));
+    CK(cudaEventRecord(t.ts, s));
     CK(cudaStreamWaitEvent(cs, t.start, 0));
     // D on the compute stream (the pre-pass writes D of retained supernodes),
     // LNZ on the copy stream group by group, lowest levels first
@@ -3176,6 +3186,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double), cudaMemcpyHostToDevice,
                                cs));
         CK(cudaEventRecord(t.up[g], cs));
+        if (g == 0) CK(cudaEventRecord(t.tu, cs));
     }
     // the pre-pass needs every original diagonal before anything is factored
     // (the zero test of sprfc1.f:465-488): gather them here while LNZ uploads
@@ -3206,8 +3217,23 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     }
     // D is final only now (and on a zero diagonal it holds the original diagonal)
     CK(cudaEventRecord(t.fin, s));
+    CK(cudaEventRecord(t.tf, s));
     CK(cudaStreamWaitEvent(cs, t.fin, 0));
     CK(cudaMemcpyAsync(h_sm, d_sm, neq * sizeof(double), cudaMemcpyDeviceToHost, cs));
+    CK(cudaEventRecord(t.te, cs));
+    return 0;
+}
+
+int Engine::streamed_times(double* out) {
+    out[0] = out[1] = out[2] = 0.0;
+    if (!xfer_) return 0;
+    float a = 0.f, c = 0.f;
+    if (cudaEventElapsedTime(&a, xfer_->ts, xfer_->tu) != cudaSuccess ||
+        cudaEventElapsedTime(&c, xfer_->tf, xfer_->te) != cudaSuccess)
+        return -4;
+    out[0] = a;
+    out[1] = timing.factor_ms;
+    out[2] = c;
     return 0;
 }
 

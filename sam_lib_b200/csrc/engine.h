@@ -81,6 +81,11 @@ public:
     // factorisation is complete on the device (res as factor()); the last
     // downloads may still run on cs: synchronise cs before reading h_sm.
     int factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResult& res, cudaStream_t cs);
+    // After the copy stream of the last streamed factorisation has finished:
+    // out[0] = ms from its start until the lowest level group was up (the
+    // upload not overlapped), out[1] = factorisation ms, out[2] = ms from the
+    // end of the factorisation to the end of the last download.
+    int streamed_times(double* out);
     int chol_convert(double* d_sm, bool to_chol);
     // b (device, ldb x nrhs, the first NEQ rows) times sqrt(d), or divided by
     // it, for every equation with d > 0 (d = the D part of an L D L' device SM)
