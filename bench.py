@@ -519,6 +519,93 @@ def form_adjoint(torch, reps=3):
     return res
 
 
+def form_assembly(torch, n=N_MESH, reps=3, ref_elements=1024):
+    """Element stiffness + SPRADM on the device at n^3 (distorted mesh, seed 5;
+    log-uniform moduli, seed 2), against the library's host SPRADM
+    restatement (one core) and the translated reference SPRADM on a sample of
+    elements (per-call ctypes overhead included).  Device SM must equal the
+    host SM bit for bit."""
+    import ctypes
+    import sam_lib_b200 as spr
+    from sam_lib_b200.adjoint import ElementOps
+    from sam_lib_b200.fe import element_moduli
+    from sam_lib_b200.system import HexSystem
+    hs = HexSystem(n)
+    box = hs.box
+    ops = ElementOps(hs)
+    d_xyz = torch.from_numpy(box.distorted_coords(5)).cuda()
+    d_E = torch.from_numpy(element_moduli(box.nel, 'loguniform', seed=2)).cuda()
+    d_em = torch.empty((box.nel, 24, 24), dtype=torch.float64, device='cuda')
+    d_sm = torch.empty(hs.neq + hs.nzerol, dtype=torch.float64, device='cuda')
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    tk, ta = [], []
+    for r in range(reps + 1):
+        flush.zero_()
+        e0, e1, e2 = _ev(torch), _ev(torch), _ev(torch)
+        e0.record()
+        ops.hex8(d_xyz, d_E, 0.3, out=d_em)
+        e1.record()
+        ops.assemble(d_sm, d_em)
+        e2.record()
+        e2.synchronize()
+        if r > 0:
+            tk.append(e0.elapsed_time(e1))
+            ta.append(e1.elapsed_time(e2))
+    em = d_em.cpu().numpy().reshape(-1)
+    sm = np.zeros(hs.neq + hs.nzerol)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)     # noqa: E731
+    i8 = ctypes.c_int64
+    t0 = time.perf_counter()
+    rc = spr.load(8).spr_b200_assemble(p(hs.mspar), p(hs.mtrees), p(hs.msifa), p(hs.meqn), p(box.madof),
+                                       p(box.mpmnpc), p(box.mmnpc), i8(box.nel), i8(24), p(em), None, p(sm))
+    t_host = time.perf_counter() - t0
+    assert rc == 0
+    same = bool(np.array_equal(d_sm.cpu().numpy(), sm))
+    try:
+        ref = _reference_spradm_sample(ref_elements, box.nel)
+    except Exception as exc:       # the reference library is test infrastructure; report its absence
+        ref = {'unavailable': str(exc)[:200]}
+    t_k, t_a = float(np.mean(tk)) / 1e3, float(np.mean(ta)) / 1e3
+    em_bytes = 576 * 8 * box.nel
+    del d_em, d_sm, d_xyz, d_E, flush, ops
+    torch.cuda.empty_cache()
+    return {'workload': '%d^3 hex8 box, nodes moved U[-0.15,0.15] (seed 5), E log-uniform (seed 2), nu 0.3' % n,
+            'elements': box.nel, 'hex8_s': t_k, 'assemble_s': t_a, 'device_s': t_k + t_a,
+            'hex8_write_gbs': em_bytes / t_k / 1e9, 'host_restatement_s': t_host,
+            'host_over_device': t_host / (t_k + t_a), 'device_sm_equals_host_sm': same,
+            'reference_spradm': ref}
+
+
+def _reference_spradm_sample(count, nel_full, n=12):
+    """The translated reference SPRADM, one call per element for the first
+    `count` elements of the n^3 box (its symbolic inputs from the reference
+    pipeline; the per-element work does not depend on the mesh size):
+    seconds per element, and that rate times nel_full."""
+    import ctypes
+    from oracle.refpipe import RefSystem, lib, _p, _i
+    from sam_lib_b200.fe import HexBox, hex8_stiffness
+    L = lib()
+    b = HexBox(n)
+    rs = RefSystem(b)
+    sm = np.zeros(rs.neq + rs.nzerol)
+    sv = np.zeros(1)
+    tt = np.zeros(1)
+    iw = np.zeros(int(rs.mspar[38]) + 64, dtype=np.int64)
+    ierr = ctypes.c_int64(0)
+    ke = np.asfortranarray(hex8_stiffness())
+    count = min(count, b.nel)
+    t0 = time.perf_counter()
+    for e in range(count):
+        L.spradm_(_p(ke), _p(tt), _p(rs.mpar), _p(rs.mspar), _p(b.madof), _p(rs.meqn), _p(b.mpmnpc),
+                  _p(b.mmnpc), _p(b.mpmceq), _p(b.mmceq), _p(rs.msica), _p(rs.mtrees), _p(rs.msifa),
+                  _p(rs.mdofnc), _p(sm), _p(sv), _p(iw), _i(e + 1), _i(24), _i(-1), _i(0), ctypes.byref(ierr))
+    dt = time.perf_counter() - t0
+    return {'elements_timed': count, 'mesh': '%d^3' % n, 's_per_element': dt / count,
+            'extrapolated_s': dt / count * nel_full,
+            'note': 'one SPRADM call per element through ctypes (call overhead included), 1 core; '
+                    'element matrices formed beforehand (not timed)'}
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the path (the machine-translated
@@ -708,7 +795,8 @@ def run_ours(args, rank, world, local_rank):
         forms = {'mixed_ir_vs_reference_cpu': form_mixed_vs_reference(torch, spr),
                  'mixed_ir_loguniform': form_mixed_ir(torch, spr, N_MESH, 'loguniform'),
                  'mixed_ir_uniform': form_mixed_ir(torch, spr, N_MESH, 'uniform'),
-                 'batched': form_batched(torch, cpu_procs=os.cpu_count() or 1), 'adjoint': form_adjoint(torch)}
+                 'batched': form_batched(torch, cpu_procs=os.cpu_count() or 1), 'adjoint': form_adjoint(torch),
+                 'assembly': form_assembly(torch)}
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',

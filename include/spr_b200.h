@@ -221,11 +221,25 @@ int spr_b200_schedule_check(const SPR_INT* mspar, const SPR_INT* mtrees, const S
  * (src/SPR/spradm.f:818-859) for systems without constraint equations:
  * SM(NEQ+K) += EM(I,J), J=1..NEDOF, I<=J, elements in order (bit-exact with
  * SPRADM).  EM of element e = em_scale[e]*em, or the e-th matrix of em when
- * em_scale is NULL.  MEQN as renumbered by SPRTRS/SPREQN (sprtrs.f:3762). */
+ * em_scale is NULL.  MEQN as renumbered by SPRTRS/SPREQN (sprtrs.f:3762).
+ * Returns 0, or -3 on a DOF count or pattern mismatch. */
 int spr_b200_assemble(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                       const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
                       const SPR_INT* mmnpc, SPR_INT nel, SPR_INT nedof, const double* em,
                       const double* em_scale, double* sm);
+/* Replaces SPRADM (src/SPR/spradm.f:5) called once per element in order,
+ * constraint equations included: SPRAD2's free-DOF add and its weighted
+ * additions for slave DOFs (TTCC master coefficients) and prescribed DOFs
+ * (TTCC constant terms into SV), spradm.f:818-1002, bit-exact.  MPMCEQ
+ * (nceq+1), MMCEQ, TTCC as SAM holds them; nsv as SPRADM's NSV (0: SM only,
+ * 1: SM and SV, -1: SV only; SV has NEQ entries and is accumulated into).
+ * Returns 0, -2 (|nsv| > 1, the multi-load-case SV, is not supported) or -3. */
+int spr_b200_assemble_ceq(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                          const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
+                          const SPR_INT* mmnpc, const SPR_INT* mpmceq, const SPR_INT* mmceq,
+                          const double* ttcc, SPR_INT nceq, SPR_INT nel, SPR_INT nedof,
+                          const double* em, const double* em_scale, SPR_INT nsv, double* sm,
+                          double* sv);
 /* No counterpart in the reference (SPR never touches device memory).
  * LDL' of one dense symmetric front on the device, in place, for callers that
  * must not allocate device memory (an application allocator owns it all, or
@@ -250,12 +264,38 @@ int spr_b200_dense_ldlt_noalloc(double* d_a, int64_t n, int64_t lda, double tol1
 int spr_b200_elem_open(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                        const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
                        const SPR_INT* mmnpc, SPR_INT nel, SPR_INT nedof, void** handle);
+/* The same with constraint equations (MPMCEQ, MMCEQ as SAM holds them,
+ * nceq = MPAR(7)): the plan also holds SPRAD2's weighted additions and the
+ * SV gather of the prescribed values. */
+int spr_b200_elem_open_ceq(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                           const SPR_INT* meqn, const SPR_INT* madof, const SPR_INT* mpmnpc,
+                           const SPR_INT* mmnpc, const SPR_INT* mpmceq, const SPR_INT* mmceq,
+                           SPR_INT nceq, SPR_INT nel, SPR_INT nedof, void** handle);
 void spr_b200_elem_close(void* handle);
 /* Device SM = 0 then the SPRADM main add of every element: EM_e =
  * d_scale[e]*d_em (one nedof x nedof column-major matrix) or, with d_scale
  * NULL, the e-th matrix of d_em.  Bit-exact with spr_b200_assemble. */
 int spr_b200_elem_assemble(void* handle, double* d_sm, const double* d_em, const double* d_scale,
                            void* stream);
+/* SPRADM with constraint equations on the device (a handle from
+ * spr_b200_elem_open_ceq): device SM = 0 and/or SV = 0 (NEQ), then every
+ * element's additions in SPRADM's order and rounding with the coefficients
+ * of the device array d_ttcc; bit-exact with spr_b200_assemble_ceq.  d_sm or
+ * d_sv NULL skips that part (NSV = -1 or 0).  -2 when d_ttcc is NULL and the
+ * plan has weighted additions. */
+int spr_b200_elem_assemble_ceq(void* handle, double* d_sm, double* d_sv, const double* d_em,
+                               const double* d_scale, const double* d_ttcc, void* stream);
+/* No reference counterpart (SAM ships no element routines): the 24x24
+ * stiffness of every element, an 8-node isoparametric hexahedron with
+ * 2x2x2 Gauss integration, isotropic with Young's modulus d_E[e] and
+ * Poisson's ratio nu, from the node coordinates d_xyz (NANOD x 3, row per
+ * SAM node number - 1; corners in the order (0,0,0) (1,0,0) (1,1,0) (0,1,0)
+ * (0,0,1) (1,0,1) (1,1,1) (0,1,1) of the element's MMNPC).  d_em receives
+ * NEL column-major matrices with node-major DOFs (3a + x/y/z), the layout
+ * spr_b200_elem_assemble reads.  -2 unless every element has 8 nodes of 3
+ * DOFs. */
+int spr_b200_elem_hex8(void* handle, const double* d_xyz, const double* d_E, double nu, double* d_em,
+                       void* stream);
 /* Adjoint element gradient: d_grad[e] = -sum_q lam_q,e^T dK_e u_q,e with
  * dK_e = d_dscale[e]*d_em, or the e-th matrix of d_em when d_dscale is NULL;
  * u, lam: ld x nrhs device arrays in equation order (constrained DOFs are

@@ -96,16 +96,18 @@ class RefSystem:
             raise RuntimeError('%s returned IERR=%d' % (name, v))
 
     # ---------------------------------------------------------------
-    def assemble(self, ke_list):
+    def assemble(self, ke_list, nsv=0):
         """SPRADM once per element; ke_list(iel) -> 24x24 matrix (0-based iel).
 
-        Returns SM = [D(NEQ) | LNZ(NZEROL)] with the assembled matrix in LNZ.
+        Returns SM = [D(NEQ) | LNZ(NZEROL)] with the assembled matrix in LNZ;
+        with nsv = 1 (or -1) returns (SM, SV), SV(NEQ) the right-hand side of
+        the prescribed values of the box's constraint equations (TTCC).
         """
         L = lib()
         box = self.box
         sm = np.zeros(self.neq + self.nzerol, dtype=np.float64)
-        sv = np.zeros(1, dtype=np.float64)
-        ttcc = np.zeros(1, dtype=np.float64)
+        sv = np.zeros(max(self.neq, 1), dtype=np.float64)
+        ttcc = np.ascontiguousarray(getattr(box, 'ttcc', np.zeros(1)), dtype=np.float64)
         iw = np.zeros(int(self.mspar[38]) + 64, dtype=np.int64)
         ierr = C.c_int64(0)
         nedof = 8 * box.nndof
@@ -115,10 +117,10 @@ class RefSystem:
                       _p(self.meqn), _p(box.mpmnpc), _p(box.mmnpc), _p(box.mpmceq),
                       _p(box.mmceq), _p(self.msica), _p(self.mtrees), _p(self.msifa),
                       _p(self.mdofnc), _p(sm), _p(sv), _p(iw), _i(iel + 1), _i(nedof),
-                      _i(-1), _i(0), C.byref(ierr))
+                      _i(-1), _i(nsv), C.byref(ierr))
             if ierr.value < 0:
                 raise RuntimeError('SPRADM(%d) returned IERR=%d' % (iel + 1, ierr.value))
-        return sm
+        return (sm, sv) if nsv else sm
 
     def rhs_to_internal(self, f_dof):
         """Map a per-DOF vector (length NDOF) to SPR equation order via MEQN."""

@@ -34,33 +34,65 @@ def _stream():
 
 
 class ElementOps:
-    """Device element assembly and element gradient of one HexSystem."""
+    """Device element operations of one system: SPRADM assembly (with the
+    box's constraint equations, if it has any), hex8 element stiffness and
+    the adjoint element gradient.  ``hs`` holds the structure (mspar,
+    mtrees, msifa, meqn, neq) and the SAM topology (``hs.box``)."""
 
     def __init__(self, hs):
         lib = load(8)
         vp = C.c_void_p
-        lib.spr_b200_elem_open.argtypes = [vp] * 7 + [C.c_int64, C.c_int64, C.POINTER(vp)]
+        i8 = C.c_int64
+        lib.spr_b200_elem_open.argtypes = [vp] * 7 + [i8, i8, C.POINTER(vp)]
         lib.spr_b200_elem_open.restype = C.c_int
+        lib.spr_b200_elem_open_ceq.argtypes = [vp] * 9 + [i8, i8, i8, C.POINTER(vp)]
+        lib.spr_b200_elem_open_ceq.restype = C.c_int
         lib.spr_b200_elem_close.argtypes = [vp]
         lib.spr_b200_elem_close.restype = None
         lib.spr_b200_elem_assemble.argtypes = [vp, vp, vp, vp, vp]
         lib.spr_b200_elem_assemble.restype = C.c_int
-        lib.spr_b200_elem_grad.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, vp, vp, vp, vp]
+        lib.spr_b200_elem_assemble_ceq.argtypes = [vp] * 7
+        lib.spr_b200_elem_assemble_ceq.restype = C.c_int
+        lib.spr_b200_elem_hex8.argtypes = [vp, vp, vp, C.c_double, vp, vp]
+        lib.spr_b200_elem_hex8.restype = C.c_int
+        lib.spr_b200_elem_grad.argtypes = [vp, vp, vp, i8, i8, vp, vp, vp, vp]
         lib.spr_b200_elem_grad.restype = C.c_int
         self.lib = lib
         self.h = C.c_void_p()
         b = hs.box
-        rc = lib.spr_b200_elem_open(_ptr(hs.mspar), _ptr(hs.mtrees), _ptr(hs.msifa), _ptr(hs.meqn),
-                                    _ptr(b.madof), _ptr(b.mpmnpc), _ptr(b.mmnpc), b.nel, 24, C.byref(self.h))
+        self.nceq = int(getattr(b, 'nceq', 0))
+        if self.nceq > 0:
+            rc = lib.spr_b200_elem_open_ceq(_ptr(hs.mspar), _ptr(hs.mtrees), _ptr(hs.msifa), _ptr(hs.meqn),
+                                            _ptr(b.madof), _ptr(b.mpmnpc), _ptr(b.mmnpc), _ptr(b.mpmceq),
+                                            _ptr(b.mmceq), self.nceq, b.nel, 24, C.byref(self.h))
+        else:
+            rc = lib.spr_b200_elem_open(_ptr(hs.mspar), _ptr(hs.mtrees), _ptr(hs.msifa), _ptr(hs.meqn),
+                                        _ptr(b.madof), _ptr(b.mpmnpc), _ptr(b.mmnpc), b.nel, 24, C.byref(self.h))
         if rc != 0:
             raise RuntimeError('spr_b200_elem_open failed with %d' % rc)
         self.nel = b.nel
         self.neq = hs.neq
 
-    def assemble(self, d_sm, d_em, d_scale=None):
-        rc = self.lib.spr_b200_elem_assemble(self.h, _vp(d_sm), _vp(d_em), _vp(d_scale), _stream())
+    def assemble(self, d_sm, d_em, d_scale=None, d_sv=None, d_ttcc=None):
+        """SM (and SV) = SPRADM over every element; d_ttcc: the constraint
+        coefficients on the device (boxes with constraint equations)."""
+        if self.nceq > 0 or d_sv is not None:
+            rc = self.lib.spr_b200_elem_assemble_ceq(self.h, _vp(d_sm), _vp(d_sv), _vp(d_em), _vp(d_scale),
+                                                     _vp(d_ttcc), _stream())
+        else:
+            rc = self.lib.spr_b200_elem_assemble(self.h, _vp(d_sm), _vp(d_em), _vp(d_scale), _stream())
         if rc != 0:
             raise RuntimeError('spr_b200_elem_assemble failed with %d' % rc)
+
+    def hex8(self, d_xyz, d_E, nu=0.3, out=None):
+        """(NEL, 24, 24) element stiffness matrices from node coordinates
+        (NANOD, 3) and moduli (NEL,), all on the device; out[e] holds K_e
+        column-major (out[e].T is K_e)."""
+        out = torch.empty((self.nel, 24, 24), dtype=torch.float64, device=d_xyz.device) if out is None else out
+        rc = self.lib.spr_b200_elem_hex8(self.h, _vp(d_xyz), _vp(d_E), float(nu), _vp(out), _stream())
+        if rc != 0:
+            raise RuntimeError('spr_b200_elem_hex8 failed with %d' % rc)
+        return out
 
     def grad(self, d_u, d_lam, nrhs, d_em, d_dscale=None, out=None):
         out = torch.empty(self.nel, dtype=torch.float64, device=d_u.device) if out is None else out

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, 'csrc')
 BUILD = os.path.join(HERE, '_build')
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-COMMON = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-O3']
+COMMON = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-O3', '-Xcompiler', '-ffp-contract=off']
 
 ENGINE_SOURCES = ['engine.cu', 'plan.cpp', 'noalloc.cu', 'elements.cu']
 

@@ -569,6 +569,51 @@ Ctx* fc1_locked(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, const I*
 
 }  // namespace
 
+// Element assembly into the packed LNZ of SM (and the right-hand side SV of
+// prescribed values): SPRADM/SPRAD2 (src/SPR/spradm.f:818-1002) for every
+// element in order.  For J = 1..NEDOF and I = 1..J with both DOFs free,
+// SM(NEQ + K) += EM(I,J), K the LNZ position of (max eq, min eq); then,
+// with constraint equations (MPMCEQ/MMCEQ/TTCC, nceq > 0), the weighted
+// additions of the element's slave and prescribed DOFs.  EM of element e is
+// em_scale[e] * em (one reference matrix) when em_scale is given, else the
+// e-th NEDOF x NEDOF column-major matrix of em.  Additions happen in the
+// reference's order and rounding, so SM and SV match SPRADM bit for bit.
+// nsv as SPRADM's NSV: 0 = SM only, 1 = SM and SV, -1 = SV only.
+// Returns 0, -2 (|nsv| > 1: the multi-load-case SV layout is not supported)
+// or -3 when an element's DOF count or pattern does not match.
+template <class T>
+static int assemble_host(const T* mspar, const T* mtrees, const T* msifa, const T* meqn, const T* madof,
+                         const T* mpmnpc, const T* mmnpc, const T* mpmceq, const T* mmceq, const double* ttcc,
+                         int64_t nceq, int64_t nel, int64_t nedof, const double* em, const double* em_scale,
+                         int64_t nsv, double* sm, double* sv) {
+    if (nsv < -1 || nsv > 1 || nedof < 1 || nel < 0 || nceq < 0) return -2;
+    if (nceq > 0 && (!mpmceq || !mmceq || !ttcc)) return -2;
+    const sprb::LnzIndex<T> lx(mspar, mtrees, msifa);
+    const int64_t neq = mspar[7];
+    double* lnz = sm ? sm + neq : nullptr;
+    std::vector<double> ems(em_scale ? (size_t)nedof * nedof : 0);
+    int64_t cur = -1;
+    const double* E = nullptr;
+    return sprb::for_each_contribution(
+        lx, meqn, madof, mpmnpc, mmnpc, mpmceq, mmceq, nceq, nel, nedof, nsv >= 0 && sm, nsv != 0 && sv,
+        [&](bool to_sv, int64_t target, int64_t e, int64_t idx, int kind, int64_t jp, int64_t ip) {
+            if (e != cur) {
+                cur = e;
+                if (em_scale) {
+                    const double sc = em_scale[e];
+                    for (int64_t k = 0; k < nedof * nedof; ++k) ems[k] = sc * em[k];
+                    E = ems.data();
+                } else {
+                    E = em + e * nedof * nedof;
+                }
+            }
+            double v;
+            if (!sprb::contrib_value(kind, E[idx], ttcc, jp, ip, &v)) return;
+            double& dst = to_sv ? sv[target] : lnz[target];
+            dst = dst + v;
+        });
+}
+
 extern "C" {
 
 // SPRFC1 (src/SPR/sprfc1.f:5): LDL' factorisation of SM in place.
@@ -1101,76 +1146,28 @@ int SPR_API(spr_b200_schedule_check)(const I* mspar, const I* mtrees, const I* m
     return 0;
 }
 
-// Element assembly into the packed LNZ of SM: the SPRADM/SPRAD2 main add
-// (src/SPR/spradm.f:818-859) for systems without constraint equations.
-// For every element in order, for J = 1..NEDOF and I = 1..J with both DOFs
-// free, SM(NEQ + K) += EM(I,J), K the LNZ position of (max eq, min eq).
-// EM of element e is em_scale[e] * em (one reference matrix) when em_scale is
-// given, else the e-th NEDOF x NEDOF column-major matrix of em.  Additions
-// happen in the reference's order, so SM matches SPRADM bit for bit.
-// Returns 0, or -3 when an element's DOF count differs from NEDOF.
+// Host SPRADM restatements; see assemble_host.
 int SPR_API(spr_b200_assemble)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
                                const I* mpmnpc, const I* mmnpc, I nel, I nedof, const double* em,
                                const double* em_scale, double* sm) {
-    const int64_t neq = mspar[7], nsuper = mspar[10];
-    const I* xsuper = mtrees + (mspar[44] - 1);
-    const I* xlindx = mtrees + (mspar[45] - 1);
-    const I* lindx = msifa + (mspar[46] - 1);
-    const I* xlnz = msifa + (mspar[47] - 1);
-    std::vector<int32_t> colsn(neq);
-    for (int64_t js = 0; js < nsuper; ++js)
-        for (int64_t c = xsuper[js]; c < xsuper[js + 1]; ++c) colsn[c - 1] = (int32_t)js;
-    double* lnz = sm + neq;
-    std::vector<int64_t> eq(nedof);
-    std::vector<double> ems(em_scale ? (size_t)nedof * nedof : 0);
-    for (int64_t e = 0; e < nel; ++e) {
-        int64_t nd = 0;
-        for (int64_t p = mpmnpc[e]; p < mpmnpc[e + 1]; ++p) {
-            const int64_t node = mmnpc[p - 1];
-            for (int64_t d = madof[node - 1]; d < madof[node]; ++d) {
-                if (nd >= nedof) return -3;
-                eq[nd++] = meqn[d - 1];
-            }
-        }
-        if (nd != nedof) return -3;
-        const double* E;
-        if (em_scale) {
-            const double sc = em_scale[e];
-            for (int64_t k = 0; k < nedof * nedof; ++k) ems[k] = sc * em[k];
-            E = ems.data();
-        } else {
-            E = em + e * nedof * nedof;
-        }
-        for (int64_t J = 0; J < nedof; ++J) {
-            const int64_t jeq = eq[J];
-            if (jeq < 1) continue;
-            for (int64_t Iq = 0; Iq <= J; ++Iq) {
-                const int64_t ieq = eq[Iq];
-                if (ieq < 1) continue;
-                const int64_t col = std::min(ieq, jeq), row = std::max(ieq, jeq);
-                const int64_t js = colsn[col - 1];
-                const int64_t F = xlindx[js + 1] - xlindx[js];
-                const I* rows = lindx + (xlindx[js] - 1);
-                int64_t lo = col - xsuper[js], hi = F - 1;      // the row is at or below the column
-                while (lo < hi) {
-                    const int64_t mid = (lo + hi) >> 1;
-                    if ((int64_t)rows[mid] < row) lo = mid + 1;
-                    else hi = mid;
-                }
-                const int64_t jc = col - xsuper[js];
-                const int64_t k = (xlnz[js] - 1) + jc * F - (jc * (jc - 1)) / 2 + (lo - jc);
-                lnz[k] = lnz[k] + E[Iq + J * nedof];
-            }
-        }
-    }
-    return 0;
+    return assemble_host<I>(mspar, mtrees, msifa, meqn, madof, mpmnpc, mmnpc, nullptr, nullptr, nullptr, 0, nel,
+                            nedof, em, em_scale, 0, sm, nullptr);
 }
 
-// Element-level device operations (assembly gather, adjoint element gradient)
-// on one structure and one SAM element topology.
-int SPR_API(spr_b200_elem_open)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
-                                const I* mpmnpc, const I* mmnpc, I nel, I nedof, void** handle) {
-    if (nel < 0) return -2;
+int SPR_API(spr_b200_assemble_ceq)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn,
+                                   const I* madof, const I* mpmnpc, const I* mmnpc, const I* mpmceq,
+                                   const I* mmceq, const double* ttcc, I nceq, I nel, I nedof, const double* em,
+                                   const double* em_scale, I nsv, double* sm, double* sv) {
+    return assemble_host<I>(mspar, mtrees, msifa, meqn, madof, mpmnpc, mmnpc, mpmceq, mmceq, ttcc, nceq, nel,
+                            nedof, em, em_scale, nsv, sm, sv);
+}
+
+// Element-level device operations (assembly gather, hex8 stiffness, adjoint
+// element gradient) on one structure and one SAM element topology.
+static int elem_open(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
+                     const I* mpmnpc, const I* mmnpc, const I* mpmceq, const I* mmceq, I nceq, I nel, I nedof,
+                     void** handle) {
+    if (nel < 0 || nceq < 0) return -2;
     std::vector<int64_t> ms(60, 0);
     for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
     std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
@@ -1178,13 +1175,29 @@ int SPR_API(spr_b200_elem_open)(const I* mspar, const I* mtrees, const I* msifa,
     std::vector<int64_t> mn = widen(mmnpc, pn[nel] - 1);
     int64_t nnod = 0;
     for (int64_t v : mn) nnod = std::max(nnod, v);
+    std::vector<int64_t> pc = nceq > 0 ? widen(mpmceq, nceq + 1) : std::vector<int64_t>();
+    std::vector<int64_t> mc = nceq > 0 ? widen(mmceq, pc[nceq] - 1) : std::vector<int64_t>();
     std::vector<int64_t> ad = widen(madof, nnod + 1);
-    std::vector<int64_t> eq = widen(meqn, nnod > 0 ? ad[nnod] - 1 : 0);
+    int64_t ndof = nnod > 0 ? ad[nnod] - 1 : 0;
+    for (int64_t v : mc) ndof = std::max(ndof, v);      // MMCEQ holds DOF numbers
+    std::vector<int64_t> eq = widen(meqn, ndof);
     std::unique_ptr<sprb::Elements> e(new sprb::Elements());
-    const int rc = e->open(ms.data(), mt.data(), mf.data(), eq.data(), ad.data(), pn.data(), mn.data(), nel, nedof);
+    const int rc = e->open(ms.data(), mt.data(), mf.data(), eq.data(), ad.data(), pn.data(), mn.data(), nel, nedof,
+                           nceq > 0 ? pc.data() : nullptr, nceq > 0 ? mc.data() : nullptr, nceq);
     if (rc != 0) return rc;
     *handle = e.release();
     return 0;
+}
+
+int SPR_API(spr_b200_elem_open)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
+                                const I* mpmnpc, const I* mmnpc, I nel, I nedof, void** handle) {
+    return elem_open(mspar, mtrees, msifa, meqn, madof, mpmnpc, mmnpc, nullptr, nullptr, 0, nel, nedof, handle);
+}
+
+int SPR_API(spr_b200_elem_open_ceq)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn,
+                                    const I* madof, const I* mpmnpc, const I* mmnpc, const I* mpmceq,
+                                    const I* mmceq, I nceq, I nel, I nedof, void** handle) {
+    return elem_open(mspar, mtrees, msifa, meqn, madof, mpmnpc, mmnpc, mpmceq, mmceq, nceq, nel, nedof, handle);
 }
 
 void SPR_API(spr_b200_elem_close)(void* handle) { delete static_cast<sprb::Elements*>(handle); }
@@ -1192,6 +1205,16 @@ void SPR_API(spr_b200_elem_close)(void* handle) { delete static_cast<sprb::Eleme
 int SPR_API(spr_b200_elem_assemble)(void* handle, double* d_sm, const double* d_em, const double* d_scale,
                                     void* stream) {
     return static_cast<sprb::Elements*>(handle)->assemble(d_sm, d_em, d_scale, (cudaStream_t)stream);
+}
+
+int SPR_API(spr_b200_elem_assemble_ceq)(void* handle, double* d_sm, double* d_sv, const double* d_em,
+                                        const double* d_scale, const double* d_ttcc, void* stream) {
+    return static_cast<sprb::Elements*>(handle)->assemble(d_sm, d_em, d_scale, (cudaStream_t)stream, d_sv, d_ttcc);
+}
+
+int SPR_API(spr_b200_elem_hex8)(void* handle, const double* d_xyz, const double* d_E, double nu, double* d_em,
+                                void* stream) {
+    return static_cast<sprb::Elements*>(handle)->hex8(d_xyz, d_E, nu, d_em, (cudaStream_t)stream);
 }
 
 int SPR_API(spr_b200_elem_grad)(void* handle, const double* d_u, const double* d_lam, int64_t ld, int64_t nrhs,
