@@ -209,12 +209,13 @@ int spr_b200_set_profile(void* handle, int on);
  * the mixed mode's launch lists. */
 int spr_b200_plan_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                         double* out);
-/* Host-only race check of the factorisation's two-stream launch schedule (no GPU
- * needed): happens-before of panels, panel-chain, far and K = S updates and the
- * write-back.  out (4 doubles): [0] ordering violations of the FP64 schedule
- * [1] of the schedule with tensor-core far and K = S updates [2] of the FP64
- * schedule without its side-stream joins (a self-test; > 0 when [3] > 0)
- * [3] far launches. */
+/* Host-only race check of the factorisation's three-stream launch schedule (no
+ * GPU needed): happens-before of panels, panel-chain, look-ahead, far and K = S
+ * updates and the write-back.  out (6 doubles): [0] ordering violations of the
+ * FP64 schedule [1] of the schedule with tensor-core far and K = S updates
+ * [2] of the FP64 schedule without its side-stream joins (a self-test; > 0
+ * when [3] > 0) [3] far launches [4] of the FP64 schedule without its
+ * look-ahead joins (> 0 when [5] > 0) [5] look-ahead launches. */
 int spr_b200_schedule_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                             double* out);
 /* Host element assembly into LNZ, the SPRADM/SPRAD2 main add

@@ -1127,22 +1127,27 @@ int SPR_API(spr_b200_plan_check)(const I* mspar, const I* mtrees, const I* msifa
 // Host-only race check of the factorisation's stream schedule (no GPU needed):
 // out[0] = ordering violations of the FP64 schedule, out[1] = of the schedule
 // with tensor-core far and K = S updates, out[2] = of the FP64 schedule without
-// its side-stream joins (a self-test of the check), out[3] = far launches.
+// its side-stream joins (a self-test of the check), out[3] = far launches,
+// out[4] = violations without the look-ahead joins, out[5] = look-ahead launches.
 int SPR_API(spr_b200_schedule_check)(const I* mspar, const I* mtrees, const I* msifa, double* out) {
     std::vector<int64_t> ms(60, 0);
     for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
     std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
     sprb::Plan p;
     const int rc = sprb::build_plan(ms.data(), mt.data(), mf.data(), p);
-    for (int i = 0; i < 4; ++i) out[i] = 0.0;
+    for (int i = 0; i < 6; ++i) out[i] = 0.0;
     if (rc != 0) return rc;
-    out[0] = (double)sprb::check_schedule(p, false, false);
-    out[1] = (double)sprb::check_schedule(p, true, false);
-    out[2] = (double)sprb::check_schedule(p, false, true);
-    int64_t nfar = 0;
-    for (const auto& lp : p.levels)
+    out[0] = (double)sprb::check_schedule(p, false, 0);
+    out[1] = (double)sprb::check_schedule(p, true, 0);
+    out[2] = (double)sprb::check_schedule(p, false, 1);
+    out[4] = (double)sprb::check_schedule(p, false, 2);
+    int64_t nfar = 0, nahead = 0;
+    for (const auto& lp : p.levels) {
         for (const auto& v : lp.far) nfar += (int64_t)v.size();
+        for (const auto& v : lp.ahead) nahead += (int64_t)v.size();
+    }
     out[3] = (double)nfar;
+    out[5] = (double)nahead;
     return 0;
 }
 

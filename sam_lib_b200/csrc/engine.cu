@@ -163,6 +163,7 @@ struct Engine::Dev {
     float* slab_far = nullptr;                   // slabs of the side-stream launches
     alignas(64) CUtensorMap slab_map_far;
     cudaStream_t side = nullptr;                 // side stream: trailing updates beyond the next super-panel
+    cudaStream_t ahead = nullptr;                // look-ahead stream: in-super-panel columns after the next panel
     std::vector<cudaEvent_t> evpool;             // fork/join events of one factorisation
 };
 
@@ -2448,6 +2449,7 @@ Engine::~Engine() {
     for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : d_->evpool) cudaEventDestroy(e);
     if (d_->side) cudaStreamDestroy(d_->side);
+    if (d_->ahead) cudaStreamDestroy(d_->ahead);
     if (d_->slab) cudaFree(d_->slab);
     if (d_->slab_far) cudaFree(d_->slab_far);
     if (csr_.rowptr) cudaFree(csr_.rowptr);
@@ -2476,13 +2478,16 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
     {
-        // side stream and the fork/join events of one factorisation (two per
-        // step that forks a far update)
+        // side and look-ahead streams and the fork/join events of one
+        // factorisation (two per step that forks a far or look-ahead update)
         size_t nev = 0;
         for (const LevelPlan& lp : P_.levels)
-            for (size_t st = 0; st < lp.far.size(); ++st)
+            for (size_t st = 0; st < lp.far.size(); ++st) {
                 if (!lp.far[st].empty() || !lp.far_tc[st].empty()) nev += 2;
+                if (!lp.ahead[st].empty()) nev += 2;
+            }
         CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&D.ahead, cudaStreamNonBlocking));
         D.evpool.resize(nev);
         for (cudaEvent_t& e : D.evpool) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
@@ -2779,15 +2784,23 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
     auto mark = [&](int phase) {
         if (profile_) marks_.emplace_back(phase, record_event(s));
     };
-    // side stream for the trailing-update columns beyond the next super-panel
+    // side stream for the trailing-update columns beyond the next super-panel,
+    // look-ahead stream for the in-super-panel columns after the next panel
     // (profile mode keeps everything on one stream so the events time it)
     cudaStream_t u = (profile_ || !D.side) ? s : D.side;
+    cudaStream_t la = (profile_ || !D.ahead) ? s : D.ahead;
     size_t evi = 0;
-    cudaEvent_t far_done = nullptr;
+    cudaEvent_t far_done = nullptr, ahead_done = nullptr;
     auto join_far = [&]() {
         if (far_done) {
             cudaStreamWaitEvent(s, far_done, 0);
             far_done = nullptr;
+        }
+    };
+    auto join_ahead = [&]() {
+        if (ahead_done) {
+            cudaStreamWaitEvent(s, ahead_done, 0);
+            ahead_done = nullptr;
         }
     };
     mark(0);
@@ -2864,11 +2877,28 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             // a trailing update's next-super-panel columns were also updated by
             // the previous super-panel's far launch: wait for it first
             if ((st + 1) % (kSuperPanel / kNB) == 0) join_far();
-            // the updates inside the panel chain (K = 64 in-super-panel columns,
-            // the next super-panel's K = 256 columns) are small and on the
-            // critical path: the FP64 kernel's 64x64 tiles start sooner than
-            // the split + tensor-core pair, so they stay FP64 in both modes
+            // the previous step's look-ahead update also wrote the columns
+            // that this step's chain update is about to update
+            join_ahead();
+            cudaEvent_t fork_ahead = nullptr;
+            if (!lp.ahead[st].empty() && la != s) {
+                fork_ahead = D.evpool[evi++];
+                cudaEventRecord(fork_ahead, s);
+            }
+            // the updates inside the panel chain (K = 64: the next panel's
+            // columns; K = 256: the next super-panel's columns) are small and
+            // on the critical path: the FP64 kernel's 64x64 tiles start sooner
+            // than the split + tensor-core pair, so they stay FP64 in both
+            // modes.  They are issued first, the look-ahead columns after them.
             for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            if (!lp.ahead[st].empty()) {
+                if (fork_ahead) cudaStreamWaitEvent(la, fork_ahead, 0);
+                for (const Launch& al : lp.ahead[st]) launch_gemm(al, la, pv, gev);
+                if (la != s) {
+                    ahead_done = D.evpool[evi++];
+                    cudaEventRecord(ahead_done, la);
+                }
+            }
             if (has_far) {
                 if (far_tc)
                     for (const TcLaunch& t : lp.far_tc[st]) launch_tc(t, u, pv, gev, true);
@@ -2880,6 +2910,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 }
             }
         }
+        join_ahead();
         join_far();
         mark(6);
         if (mixed_ == 1 && lp.outer_flops >= tc_min_flops_)

@@ -361,6 +361,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             out.push_back(t);
         };
         lp.far.assign(nsteps, std::vector<Launch>());
+        lp.ahead.assign(nsteps, std::vector<Launch>());
         lp.far_tc.assign(nsteps, std::vector<TcLaunch>());
         lp.far_flops.assign(nsteps, 0.0);
         for (int32_t st = 0; st < nsteps; ++st) {
@@ -374,7 +375,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 add_job(lp.panel[st], Job{js, k0 + nb, k0 + nb, f, k0, k0 + nb, 0}, nrb, true);
             }
             close_launch(lp.panel[st]);
-            std::vector<Job> jl, jfar;
+            std::vector<Job> jl, jahead, jfar;
             for (int32_t js : elim) {
                 const int32_t s = P.S[js], f = P.F[js];
                 if (k0 >= s) continue;
@@ -383,7 +384,11 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 const int32_t sp0 = (k0 / kSuperPanel) * kSuperPanel;
                 const int32_t sp1 = std::min(sp0 + kSuperPanel, s);
                 if (c0 < sp1) {                                     // inside the super-panel
-                    jl.push_back(Job{js, c0, sp1, f, k0, c0, 0});
+                    // the next panel's columns on the panel chain; the ones
+                    // after it beside the next diagonal block and TRSM
+                    const int32_t c1 = std::min(c0 + kNB, sp1);
+                    jl.push_back(Job{js, c0, c1, f, k0, c0, 0});
+                    if (c1 < sp1) jahead.push_back(Job{js, c1, sp1, f, k0, c0, 0});
                     P.gemm_flops += update_flops(c0, sp1, f, nb);
                 }
                 if (c0 == sp1 && sp1 < s) {                          // trailing, K = 256
@@ -401,6 +406,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 }
             }
             emit_updates(jl, lp.update[st]);
+            emit_updates(jahead, lp.ahead[st]);
             emit_updates(jfar, lp.far[st]);
             emit_tc(jfar, lp.far_tc[st], P.slab_rows_far);
             open_launch(lp.fsolve[st]);
@@ -513,6 +519,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         build_map(lp.rect_rows);
         for (Launch& l : lp.panel) build_map(l);
         for (auto& v : lp.update)
+            for (Launch& l : v) build_map(l);
+        for (auto& v : lp.ahead)
             for (Launch& l : v) build_map(l);
         for (Launch& l : lp.outer) build_map(l);
         for (auto& v : lp.far)
@@ -645,6 +653,8 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
         for (const LevelPlan& lp : P.levels) {
             for (const auto& v : lp.update)
                 for (const Launch& l : v) add(l);
+            for (const auto& v : lp.ahead)
+                for (const Launch& l : v) add(l);
             if (which == 0) {
                 for (const auto& v : lp.far)
                     for (const Launch& l : v) add(l);
@@ -688,11 +698,13 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
 //
 // Replays the launch order of the factorisation of every level: per panel
 // step the diagonal block + TRSM and the panel-chain updates on the main
-// stream; at the end of a super-panel the far columns' update on the side
-// stream, forked by an event after the step's TRSM and joined before the
-// next trailing update (every kSuperPanel / kNB steps) and before the K = S
-// update.  Vector clocks give the happens-before order of the two streams.
-// Per large front it counts
+// stream; inside a super-panel the update of the columns after the next
+// panel on the look-ahead stream, forked by an event after the step's TRSM
+// and joined before the next step's chain update; at the end of a
+// super-panel the far columns' update on the side stream, forked by an event
+// after the step's TRSM and joined before the next trailing update (every
+// kSuperPanel / kNB steps) and before the K = S update.  Vector clocks give
+// the happens-before order of the three streams.  Per large front it counts
 //   * a panel whose columns have not received exactly the K ranges [0, k0)
 //     from updates ordered before it, or that an unordered update writes;
 //   * an update whose K panel columns are not final (diagonal block + TRSM
@@ -700,13 +712,15 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc) {
 //   * two updates on different streams that write a common element unordered;
 //   * an update of the S columns not ordered before the write-back.
 // tc: the far and K = S updates take the tensor-core path (split + product on
-// the same stream as the FP64 launch they replace).  skip_join drops the
-// joins, which must make the check fail wherever far launches exist.
+// the same stream as the FP64 launch they replace).  skip_join drops joins
+// (bit 0: the far updates', bit 1: the look-ahead updates'), which must make
+// the check fail wherever such launches exist.
 // ---------------------------------------------------------------------------
 namespace {
+constexpr int kStreams = 3;          // 0 main, 1 side (far columns), 2 look-ahead
 struct SchedOp {
-    int stream;                      // 0 main, 1 side
-    int64_t vc[2];                   // vector clock after the op
+    int stream;
+    int64_t vc[kStreams];            // vector clock after the op
     int32_t c0, c_end, r0, r_end;    // written block (columns, rows)
     int32_t k_lo, k_hi;              // K range applied (updates)
     int kind;                        // 0 panel, 1 update, 2 write-back
@@ -714,20 +728,19 @@ struct SchedOp {
 bool hb(const SchedOp& a, const SchedOp& b) { return a.vc[a.stream] <= b.vc[a.stream]; }
 }  // namespace
 
-int64_t check_schedule(const Plan& P, bool tc, bool skip_join) {
+int64_t check_schedule(const Plan& P, bool tc, int skip_join) {
     int64_t bad = 0;
     for (const LevelPlan& lp : P.levels) {
         if (lp.elim_nodes.empty()) continue;
         std::map<int32_t, std::vector<SchedOp>> ops;     // per front, in issue order
-        int64_t vc_main[2] = {0, 0}, vc_side[2] = {0, 0};
-        int64_t far_done[2] = {-1, -1};
+        int64_t vc[kStreams][kStreams] = {};            // per stream: its vector clock
+        int64_t far_done[kStreams], ahead_done[kStreams];
+        bool far_open = false, ahead_open = false;
         auto issue = [&](int stream, const Job& j, int kind) {
-            int64_t* vc = stream == 0 ? vc_main : vc_side;
-            ++vc[stream];
+            ++vc[stream][stream];
             SchedOp o;
             o.stream = stream;
-            o.vc[0] = vc[0];
-            o.vc[1] = vc[1];
+            for (int q = 0; q < kStreams; ++q) o.vc[q] = vc[stream][q];
             o.kind = kind;
             o.k_lo = j.k_lo;
             o.k_hi = j.k_hi;
@@ -752,29 +765,45 @@ int64_t check_schedule(const Plan& P, bool tc, bool skip_join) {
         auto issue_launch = [&](int stream, const Launch& l, int kind) {
             for (int64_t k = 0; k < l.job_count; ++k) issue(stream, P.jobs[l.job_begin + k], kind);
         };
-        auto wait = [&](int64_t* dst, const int64_t* ev) {
-            dst[0] = std::max(dst[0], ev[0]);
-            dst[1] = std::max(dst[1], ev[1]);
+        auto wait = [&](int dst, const int64_t* ev) {       // dst waits for an event
+            for (int q = 0; q < kStreams; ++q) vc[dst][q] = std::max(vc[dst][q], ev[q]);
+        };
+        auto record = [&](int src, int64_t* ev) {
+            for (int q = 0; q < kStreams; ++q) ev[q] = vc[src][q];
         };
         auto join = [&]() {
-            if (far_done[0] >= 0 && !skip_join) wait(vc_main, far_done);
-            far_done[0] = far_done[1] = -1;
+            if (far_open && !(skip_join & 1)) wait(0, far_done);
+            far_open = false;
+        };
+        auto join_ahead = [&]() {
+            if (ahead_open && !(skip_join & 2)) wait(0, ahead_done);
+            ahead_open = false;
         };
         for (size_t st = 0; st < lp.panel.size(); ++st) {
             issue_launch(0, lp.panel[st], 0);
             const bool has_far = tc ? !lp.far_tc[st].empty() : !lp.far[st].empty();
-            if (has_far) wait(vc_side, vc_main);         // fork after the step's TRSM
+            if (has_far) wait(1, vc[0]);                 // fork after the step's TRSM
             if ((st + 1) % (kSuperPanel / kNB) == 0) join();
+            join_ahead();
+            int64_t fork[kStreams];
+            record(0, fork);
             for (const Launch& ul : lp.update[st]) issue_launch(0, ul, 1);
+            if (!lp.ahead[st].empty()) {
+                wait(2, fork);
+                for (const Launch& al : lp.ahead[st]) issue_launch(2, al, 1);
+                record(2, ahead_done);
+                ahead_open = true;
+            }
             if (has_far) {
                 if (tc)
                     for (const TcLaunch& t : lp.far_tc[st]) issue_launch(1, t.gemm, 1);
                 else
                     for (const Launch& fl : lp.far[st]) issue_launch(1, fl, 1);
-                far_done[0] = vc_side[0];
-                far_done[1] = vc_side[1];
+                record(1, far_done);
+                far_open = true;
             }
         }
+        join_ahead();
         join();
         if (tc)
             for (const TcLaunch& t : lp.outer_tc) issue_launch(0, t.gemm, 1);

@@ -79,6 +79,9 @@ struct LevelPlan {
     Launch assemble;                          // large fronts: extend-add into dense fronts
     std::vector<Launch> panel;                // per panel step: diagonal block + TRSM
     std::vector<std::vector<Launch>> update;  // per panel step: Schur updates (one launch per tile size)
+    // per panel step inside a super-panel: the update of the columns after the
+    // next panel (look-ahead stream, beside the next diagonal block and TRSM)
+    std::vector<std::vector<Launch>> ahead;
     std::vector<Launch> outer;                // update block, K = S (one launch per tile size)
     Launch writeback;                         // S columns -> LNZ
     std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
@@ -195,6 +198,6 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc);
 // of ordering violations, 0 for a race-free schedule.  tc: the far and K = S
 // updates on the tensor-core path; skip_join: the schedule without its
 // side-stream joins (a self-test: must report violations where far launches exist).
-int64_t check_schedule(const Plan& P, bool tc, bool skip_join);
+int64_t check_schedule(const Plan& P, bool tc, int skip_join);
 
 }  // namespace sprb

@@ -145,12 +145,14 @@ def test_length_checks_match_reference_without_a_gpu():
 
 @pytest.mark.parametrize('which', ['box12', 'gold24', 'gold48', 'retained8'])
 def test_factor_stream_schedule_is_race_free(which):
-    """Happens-before replay of the factorisation's two-stream schedule (the
-    far trailing updates on a side stream, forked and joined by events): no
-    panel starts before its columns have all their earlier updates, no update
-    reads a panel that is not final, no two unordered launches write a common
-    element, in the FP64 and the tensor-core form.  Without the joins the same
-    check must fail wherever far launches exist (a self-test of the check)."""
+    """Happens-before replay of the factorisation's three-stream schedule (the
+    far trailing updates on a side stream, the in-super-panel columns after
+    the next panel on a look-ahead stream, both forked and joined by events):
+    no panel starts before its columns have all their earlier updates, no
+    update reads a panel that is not final, no two unordered launches write a
+    common element, in the FP64 and the tensor-core form.  Without either
+    stream's joins the same check must fail wherever that stream has launches
+    (a self-test of the check)."""
     from sam_lib_b200.system import load_structure
     if which == 'box12':
         rs, _ = ref_system(12)
@@ -162,11 +164,13 @@ def test_factor_stream_schedule_is_race_free(which):
     else:
         st = load_structure(int(which[4:]))
         ms, mt, mf = st['mspar'], st['mtrees'], st['msifa']
-    out = np.zeros(4)
+    out = np.zeros(6)
     rc = spr.load(8).spr_b200_schedule_check(spr._ptr(ms), spr._ptr(mt), spr._ptr(mf), spr._ptr(out))
     assert rc == 0
     assert out[0] == 0 and out[1] == 0, 'ordering violations in the factor schedule'
     if out[3] > 0:
-        assert out[2] > 0, 'the check does not see the missing joins'
+        assert out[2] > 0, 'the check does not see the missing far joins'
+    if out[5] > 0:
+        assert out[4] > 0, 'the check does not see the missing look-ahead joins'
     if which.startswith('gold'):
-        assert out[3] > 0
+        assert out[3] > 0 and out[5] > 0
