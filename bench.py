@@ -297,7 +297,8 @@ def form_mixed_ir(torch, spr, n, emod, reps=2):
                                             'TMA, TMEM accumulators)',
                'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
                'flops': 'TF32 tensor flops = 3 products x the algorithmic flops of the tensor-core updates '
-                        '(far trailing columns + K = S updates: %.4g of %.4g)' % (tc_flops, inf['gemm_flops']),
+                        '(far trailing columns, next super-panels and K = S updates above the autotuned '
+                        'threshold: %.4g of %.4g)' % (tc_flops, inf['gemm_flops']),
                'peak_source': src, 'time_s': tc_ms / 1e3}
     rel = float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64))
     del ds

@@ -1072,12 +1072,13 @@ int SPR_API(spr_b200_autotune)(void* handle, const double* d_sm_assembled, doubl
     return static_cast<Engine*>(handle)->autotune(d_sm_assembled, out);
 }
 
-// Mixed mode: out[0] = algorithmic flops of the updates that run on tensor
-// cores (far trailing columns and K = S updates), out[1] = their split +
-// tensor-core time in the last profiled factorisation (ms).
+// Mixed mode: out[0] = algorithmic flops of the updates that ran on tensor
+// cores in the last profiled factorisation (far trailing columns, the next
+// super-panels' K = 256 columns and K = S updates above the tensor-core
+// threshold), out[1] = their split + tensor-core time (ms).
 int SPR_API(spr_b200_tc_stats)(void* handle, double* out) {
     const Engine* e = static_cast<Engine*>(handle);
-    out[0] = e->plan().tc_flops;
+    out[0] = e->timing.tc_flops;
     out[1] = e->timing.tc_ms;
     return 0;
 }

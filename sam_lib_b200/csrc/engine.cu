@@ -2781,6 +2781,7 @@ struct ExchangeHooks : LevelHooks {
 void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_t>& gev) {
     Dev& D = *d_;
     timing.launches = 0;
+    timing.tc_flops = 0.0;
     auto mark = [&](int phase) {
         if (profile_) marks_.emplace_back(phase, record_event(s));
     };
@@ -2886,11 +2887,18 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 cudaEventRecord(fork_ahead, s);
             }
             // the updates inside the panel chain (K = 64: the next panel's
-            // columns; K = 256: the next super-panel's columns) are small and
-            // on the critical path: the FP64 kernel's 64x64 tiles start sooner
-            // than the split + tensor-core pair, so they stay FP64 in both
-            // modes.  They are issued first, the look-ahead columns after them.
-            for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            // columns; K = 256: the next super-panel's columns) are on the
+            // critical path.  The K = 64 ones are small: the FP64 kernel's
+            // 64x64 tiles start sooner than a split + tensor-core pair, so they
+            // stay FP64 in both modes; in mixed mode the K = 256 one takes the
+            // tensor cores when large enough.  They are issued first, the
+            // look-ahead columns after them.
+            if (mixed_ == 1 && !lp.next_tc[st].empty() && lp.next_flops[st] >= tc_min_flops_) {
+                for (const TcLaunch& t : lp.next_tc[st]) launch_tc(t, s, pv, gev);
+                timing.tc_flops += lp.next_flops[st];
+            } else {
+                for (const Launch& ul : lp.update[st]) launch_gemm(ul, s, pv, gev);
+            }
             if (!lp.ahead[st].empty()) {
                 if (fork_ahead) cudaStreamWaitEvent(la, fork_ahead, 0);
                 for (const Launch& al : lp.ahead[st]) launch_gemm(al, la, pv, gev);
@@ -2900,10 +2908,13 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 }
             }
             if (has_far) {
-                if (far_tc)
+                if (far_tc) {
                     for (const TcLaunch& t : lp.far_tc[st]) launch_tc(t, u, pv, gev, true);
-                else
+                    timing.tc_flops += lp.far_flops[st];
+                }
+                else {
                     for (const Launch& fl : lp.far[st]) launch_gemm(fl, u, pv, gev);
+                }
                 if (u != s) {
                     far_done = D.evpool[evi++];
                     cudaEventRecord(far_done, u);
@@ -2913,9 +2924,10 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         join_ahead();
         join_far();
         mark(6);
-        if (mixed_ == 1 && lp.outer_flops >= tc_min_flops_)
+        if (mixed_ == 1 && lp.outer_flops >= tc_min_flops_) {
             for (const TcLaunch& t : lp.outer_tc) launch_tc(t, s, pv, gev);
-        else
+            timing.tc_flops += lp.outer_flops;
+        } else
             for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
         {
             mark(7);

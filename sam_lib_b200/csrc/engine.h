@@ -26,6 +26,7 @@ struct Timing {              // CUDA-event times of the last calls (ms)
     float factor_ms = 0.f, solve_ms = 0.f;
     float gemm_ms = 0.f;     // Schur-update kernels only (sum over launches)
     float tc_ms = 0.f;       // of those, the split + tensor-core launch pairs
+    double tc_flops = 0.0;   // algorithmic flops of the tensor-core launches enqueued by the last factorisation
     int64_t gemm_launches = 0, launches = 0, solve_launches = 0;
     // profile mode: factor time by phase (CUDA events between launch groups):
     // 0 pre-pass, 1 small fronts, 2 extend-add, 3 diagonal blocks, 4 panel

@@ -362,6 +362,8 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         };
         lp.far.assign(nsteps, std::vector<Launch>());
         lp.ahead.assign(nsteps, std::vector<Launch>());
+        lp.next_tc.assign(nsteps, std::vector<TcLaunch>());
+        lp.next_flops.assign(nsteps, 0.0);
         lp.far_tc.assign(nsteps, std::vector<TcLaunch>());
         lp.far_flops.assign(nsteps, 0.0);
         for (int32_t st = 0; st < nsteps; ++st) {
@@ -397,6 +399,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                     const int32_t sp2 = std::min(sp1 + kSuperPanel, s);
                     jl.push_back(Job{js, sp1, sp2, f, sp0, sp1, 0});
                     P.gemm_flops += update_flops(sp1, sp2, f, sp1 - sp0);
+                    lp.next_flops[st] += update_flops(sp1, sp2, f, sp1 - sp0);
                     if (sp2 < s) {
                         jfar.push_back(Job{js, sp2, s, f, sp0, sp1, 0});
                         P.gemm_flops += update_flops(sp2, s, f, sp1 - sp0);
@@ -406,6 +409,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 }
             }
             emit_updates(jl, lp.update[st]);
+            if (lp.next_flops[st] > 0.0) emit_tc(jl, lp.next_tc[st], P.slab_rows);
             emit_updates(jahead, lp.ahead[st]);
             emit_updates(jfar, lp.far[st]);
             emit_tc(jfar, lp.far_tc[st], P.slab_rows_far);
@@ -526,6 +530,11 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (auto& v : lp.far)
             for (Launch& l : v) build_map(l);
         for (auto& v : lp.far_tc)
+            for (TcLaunch& t : v) {
+                build_map(t.split);
+                build_map(t.gemm);
+            }
+        for (auto& v : lp.next_tc)
             for (TcLaunch& t : v) {
                 build_map(t.split);
                 build_map(t.gemm);

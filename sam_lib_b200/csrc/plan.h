@@ -82,6 +82,11 @@ struct LevelPlan {
     // per panel step inside a super-panel: the update of the columns after the
     // next panel (look-ahead stream, beside the next diagonal block and TRSM)
     std::vector<std::vector<Launch>> ahead;
+    // mixed precision: a super-panel's K = 256 update of the next super-panel's
+    // columns (the update[st] jobs of a step that ends a super-panel) as a
+    // split + tensor-core pair, and its algorithmic flops
+    std::vector<std::vector<TcLaunch>> next_tc;
+    std::vector<double> next_flops;
     std::vector<Launch> outer;                // update block, K = S (one launch per tile size)
     Launch writeback;                         // S columns -> LNZ
     std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
