@@ -210,6 +210,7 @@ private:
     bool chol_ = false;                      // factor with SPRF27's pivot rule
     double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
     int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
+    int diag_alg_ = 1;            // k_diag elimination: 1 row pairs in shared memory, 0 register-resident
     std::vector<std::pair<int, cudaEvent_t>> marks_;
     std::vector<size_t> tc_pairs_;        // profile mode: event pairs of the tensor-core launches
     int sm_count_ = 148;
@@ -227,6 +228,7 @@ private:
     double* rbuf_ = nullptr;
     int64_t rbuf_cap_ = 0;
     void launch_gemm(const Launch& l, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
+    void launch_diag(const Launch& pl, cudaStream_t s, const struct PV& pv);
     void upload_plan();
     void ensure_vectors(int64_t nrhs);
     Plan P_;
