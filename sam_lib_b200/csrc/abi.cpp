@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
@@ -313,6 +314,25 @@ bool reduced_rows_retained(Ctx* c, const I* msifa, int64_t ldb, bool peri2e) {
 // True when the host array lies in page-locked memory (cudaMallocHost,
 // cudaHostRegister or a pinned torch tensor): copies from and to it are
 // asynchronous DMA, so they can overlap the factorisation.
+// SPR_B200_TRACE=1: wall-clock milestones of the Fortran entry points on
+// stderr (ms since the entry point was called), for locating host time.
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPR_B200_TRACE");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+std::chrono::steady_clock::time_point g_t0;
+void trace_start() {
+    if (trace_on()) g_t0 = std::chrono::steady_clock::now();
+}
+void trace(const char* what) {
+    if (!trace_on()) return;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_t0).count();
+    fprintf(stderr, "[spr_b200 trace] %9.3f ms  %s\n", ms, what);
+}
+
 bool is_pinned(const void* p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -359,9 +379,11 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     }
     FactorResult r;
     if (streamed) c->streamed_pending = true;
+    trace(streamed ? "factorisation (streamed copies) starts" : "factorisation starts");
     const int frc = streamed ? c->eng.factor_streamed(sm, c->d_sm, tol[0], r, c->copy)
                     : chol   ? c->eng.factor_chol(c->d_sm, tol[0], r, fc4 ? &fc3 : nullptr)
                              : c->eng.factor(c->d_sm, tol[0], r, dcor ? &fc3 : nullptr);
+    trace("factorisation returned");
     if (frc != 0) {
         finish_copies(c);
         msg(lpu, who, "CUDA failure in the factorisation");
@@ -371,6 +393,7 @@ I do_factor(Ctx* c, I* mspar, double* sm, double* tol, I lpu, double* dcor = nul
     if (chol_ok && c->eng.chol_convert(c->d_sm, true) != 0) return -4;
     uint64_t fp = 0;                                  // hash of exactly what the host receives
     if (c->eng.hash(c->d_sm, nsm, fp) != 0) return -4;
+    trace("factor hashed");
     if (streamed) {
         if (!defer && finish_copies(c) != 0) return -4;
     } else if (cudaMemcpyAsync(sm, c->d_sm, nsm * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
@@ -556,6 +579,7 @@ Ctx* fc1_locked(I* mspar, I* mtrees, I* msifa, double* sm, double* tol, const I*
     }
     int err = 0;
     Ctx* c = get_ctx(mspar, mtrees, msifa, err);
+    trace("context found");
     if (!c) {
         mspar[0] = -5;
         *ierr = (err == -2) ? -2 : -4;
@@ -857,9 +881,12 @@ void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, d
     const I op = *iop;
     const bool bwd = op >= 3 && op != 5;
     std::unique_lock<std::mutex> lk(g_mu);
+    trace_start();
+    trace("SPRSOL entered");
     // IOP = 3: the factorisation's last downloads (pinned SM) overlap the solves
     Ctx* fc = nullptr;
     if (op <= 3) fc = fc1_locked(mspar, mtrees, msifa, sm, tol, lpu, ierr, nullptr, nullptr, op == 3);
+    trace("SPRFC1 part done");
     const bool fwd = op >= 2 && op <= 5 && *ierr >= 0;
     if (fwd && bwd) {
         struct Finish {                                  // at every return below
@@ -883,7 +910,10 @@ void SPR_API(sprsol_)(const I* iop, I* mspar, I* mtrees, I* msifa, double* sm, d
         int err = 0;
         Ctx* c = get_ctx(mspar, mtrees, msifa, err);
         const int rc = c ? do_solve(c, mspar, msifa, sm, b, *ldb, *nrhs, 3, false, op <= 3) : -4;
-        if (rc != 0 || finish_copies(fc) != 0) {
+        trace("solves done");
+        const int frc = finish_copies(fc);
+        trace("copies finished");
+        if (rc != 0 || frc != 0) {
             mspar[0] = -7;
             *ierr = -4;
             solve_msg(*lpu, "SPRSOL", rc, "GPU SOLVE FAILED");

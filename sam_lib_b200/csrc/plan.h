@@ -113,8 +113,8 @@ struct LevelPlan {
 constexpr int kBwdCols = 8;                   // columns per CTA in the back-solve update
 constexpr int kSolveBlock = 256;              // width of a solve step (4 diagonal blocks of kNB)
 constexpr int kSolveRows = 128;               // rows per CTA in the forward update (x 2 column halves)
-constexpr int kRectCols = 256;                // columns per CTA in the back-solve rectangle
-constexpr int kRectRows = 256;                // rows per CTA in the back-solve rectangle
+constexpr int kRectCols = 64;                 // columns per CTA of the solves' rectangle launches
+constexpr int kRectRows = 256;                // rows per CTA of the solves' rectangle launches
 
 struct Plan {
     // sizes

@@ -80,10 +80,10 @@ def test_device_hex8_system_factor_and_solve_match_reference(n):
                                        _p(host))
     assert rc == 0 and np.array_equal(sm, host)
     b = np.asfortranarray(np.random.default_rng(7).uniform(-1, 1, size=(rs.neq, 2)))
-    ref_sm, ref_b = sm.copy(), b.copy()
+    ref_sm, ref_b = sm.copy(), b.copy(order='F')
     ierr, tol_r, nneg = rs.sprsol(3, ref_sm, ref_b)
     assert ierr == 0
-    g_sm, g_b = sm.copy(), b.copy()
+    g_sm, g_b = sm.copy(), b.copy(order='F')
     tol = np.array([1e-12, 0.0, 0.0])
     ms = rs.mspar.copy()
     assert spr.sprsol(3, ms, rs.mtrees, rs.msifa, g_sm, g_b, rs.neq, 2, tol) == 0
