@@ -314,24 +314,8 @@ bool reduced_rows_retained(Ctx* c, const I* msifa, int64_t ldb, bool peri2e) {
 // True when the host array lies in page-locked memory (cudaMallocHost,
 // cudaHostRegister or a pinned torch tensor): copies from and to it are
 // asynchronous DMA, so they can overlap the factorisation.
-// SPR_B200_TRACE=1: wall-clock milestones of the Fortran entry points on
-// stderr (ms since the entry point was called), for locating host time.
-bool trace_on() {
-    static const bool on = [] {
-        const char* e = std::getenv("SPR_B200_TRACE");
-        return e && e[0] == '1';
-    }();
-    return on;
-}
-std::chrono::steady_clock::time_point g_t0;
-void trace_start() {
-    if (trace_on()) g_t0 = std::chrono::steady_clock::now();
-}
-void trace(const char* what) {
-    if (!trace_on()) return;
-    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_t0).count();
-    fprintf(stderr, "[spr_b200 trace] %9.3f ms  %s\n", ms, what);
-}
+void trace_start() { sprb::trace_reset(); }
+void trace(const char* what) { sprb::trace_point(what); }
 
 bool is_pinned(const void* p) {
     cudaPointerAttributes a;

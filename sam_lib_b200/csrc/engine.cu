@@ -22,6 +22,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +34,24 @@
 #include "smhash.h"
 
 namespace sprb {
+
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPR_B200_TRACE");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+static std::chrono::steady_clock::time_point g_trace_t0;
+void trace_reset() {
+    if (trace_on()) g_trace_t0 = std::chrono::steady_clock::now();
+}
+void trace_point(const char* what) {
+    if (!trace_on()) return;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_trace_t0).count();
+    fprintf(stderr, "[spr_b200 trace] %9.3f ms  %s\n", ms, what);
+}
+
 
 #define CK(x)                                                                    \
     do {                                                                         \
@@ -636,31 +655,20 @@ __global__ void __launch_bounds__(256) k_assemble(const Job* jobs, int64_t njobs
 // rows i = tx + 16a and columns j = ty + 16b of the block; right-looking with
 // the unscaled column (a_ij -= a_ik * a_jk / d_k), scaled to L at the end.
 // Also forms X = L11^-1 (unit lower) for the panel TRSM and the solves.
-// ALG selects the elimination: 0 keeps the block in registers across all 256
-// threads, 1 keeps it in shared memory with two threads per row (the first
-// 128 threads, a named barrier per column) and is the default.
-template <int PR, int ALG>
+template <int PR>
 __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
-    // ALG 0, register-resident: thread (tx, ty) keeps entries (tx + 16a,
-    // ty + 16b) of the block in v[a][b] through the elimination; each step
-    // publishes one column of the block through shared memory, one barrier per
-    // step.  Entries outside the lower triangle are carried along as
-    // don't-care values (never published nor stored), which keeps the step
-    // free of per-entry tests.
-    // ALG 1, row pairs: threads 2i and 2i+1 own row i of the block in shared
-    // memory.  Step k publishes the unscaled column k, every thread reads the
-    // pivot, row i scales its entry to L and the pair updates its row's
-    // entries k < j <= i (alternate columns each), so a step costs one
-    // 128-thread barrier and at most 32 updates per thread, and the division
-    // no longer waits for a publishing warp.  Both give the same operations in
-    // the same order per entry: a_ij -= (a_ik / d_k) a_jk for k = 0, 1, ...
+    // Register-resident: thread (tx, ty) keeps entries (tx + 16a, ty + 16b) of
+    // the block in v[a][b] through the elimination and of X = L^-1 in x[a][b]
+    // through the inverse; each step publishes one column of the block (or one
+    // row of X) through shared memory, one barrier per step.  Entries outside
+    // the lower triangle are carried along as don't-care values (never
+    // published nor stored), which keeps the step free of per-entry tests.
     __shared__ double A[kNB][kNB + 1];      // L (lower, d on the diagonal)
     __shared__ double vec[2][kNB];          // the published column / row (double buffered)
     __shared__ double rdv[kNB];
     __shared__ double dd[kNB];
     __shared__ double adv[kNB];
     __shared__ double Tb[kNB * kNB / 4];    // T = L21 X11 of the inverse's doubling passes
-    __shared__ int s_failed;
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -669,56 +677,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     double* front = P.arena + P.buf_off[js];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     constexpr int R = kNB / 16;
-    int failed = -1;
-    if (ALG == 1) {
-        for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-            const int i = e % kNB, j = e / kNB;
-            A[i][j] = (i >= j && i < nb && j < nb) ? __ldcg(front + (int64_t)(k0 + i) + (int64_t)(k0 + j) * ld) : 0.0;
-        }
-        if (tid < nb) adv[tid] = __ldcg(P.adiag + fst + k0 + tid);
-        if (tid == 0) s_failed = -1;
-        __syncthreads();
-        if (tid < 2 * kNB) {
-            const int i = tid >> 1, q = tid & 1;
-            for (int k = 0; k < nb; ++k) {
-                double* ck = vec[k & 1];
-                if (q == 0 && i >= k && i < nb) ck[i] = A[i][k];
-                asm volatile("bar.sync 1, 128;\n" ::: "memory");
-                double d = ck[k];
-                if (PR == kPivotReplace) {
-                    const double c0 = d;
-                    d = fc3_pivot(P, c0, adv[k]);
-                    if (tid == 0) fc3_record(P, fst + k0 + k, c0, d);
-                }
-                if (PR == kPivotChol4 && !pivot_fails(PR, d, adv[k], P.tol1))
-                    d = chol4_pivot(P, fst + k0 + k, d, adv[k], tid == 0);
-                if (PR != kPivotReplace && pivot_fails(PR, d, adv[k], P.tol1)) {
-                    if (tid == 0) {
-                        s_failed = k;
-                        record_fail(P, js, k0 + k, d, adv[k]);
-                        if (PR == kPivotChol4) chol4_fail_record(P, fst + k0 + k, d);
-                    }
-                    break;
-                }
-                const double rd = 1.0 / d;
-                if (tid == 0) {
-                    dd[k] = d;
-                    rdv[k] = rd;
-                }
-                if (i > k && i < nb) {
-                    const double w = ck[i] * rd;
-                    if (q == 0) A[i][k] = w;
-                    for (int j = k + 1 + q; j <= i; j += 2) A[i][j] -= w * ck[j];
-                } else if (i == k && q == 0) {
-                    A[k][k] = (PR == kPivotReplace || PR == kPivotChol4) ? d : ck[k];
-                }
-            }
-        }
-        __syncthreads();
-        failed = s_failed;
-    }
     double v[R][R];
-    if (ALG == 0) {
 #pragma unroll
     for (int b = 0; b < R; ++b)
 #pragma unroll
@@ -729,6 +688,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     if (tid < nb) adv[tid] = __ldcg(P.adiag + fst + k0 + tid);
     for (int k = tid; k < 2 * kNB; k += blockDim.x) vec[k / kNB][k % kNB] = 0.0;
     __syncthreads();
+    int failed = -1;
     for (int k = 0; k < nb; ++k) {
         const int buf = k & 1, kb = k >> 4;
         if (ty == (k & 15)) {
@@ -775,7 +735,6 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
                 if (ty + 16 * b > k) v[a][b] -= aik * vj[b];
         }
     }
-    }
     // inertia and TOL(2) of the processed columns (sprfc1.f:1280-1290)
     if (tid < 32) {
         const int kend = failed < 0 ? nb : failed;
@@ -800,7 +759,6 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     }
     if (failed >= 0) return;
     // L below the diagonal (scaled), d on it
-    if (ALG == 0) {
 #pragma unroll
     for (int a = 0; a < R; ++a)
 #pragma unroll
@@ -810,7 +768,6 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
                 A[i][j] = (i > j) ? v[a][b] * rdv[j] : ((PR == kPivotReplace || PR == kPivotChol4) ? dd[j] : v[a][b]);
         }
     __syncthreads();
-    }
     // X = L^-1 by recursive doubling: after the pass of order b, each aligned
     // diagonal block of X of order 2b is final, its lower-left quarter being
     // X21 = -X22 (L21 X11) (X11, X22 from the pass before; unit diagonals).
@@ -2485,9 +2442,6 @@ struct Engine::Transfer {
 Engine::Engine() : d_(new Dev()) {
     const char* e = getenv("SPR_B200_GRAPHS");
     use_graphs_ = !(e && e[0] == '0');
-    // SPR_B200_DIAG=0 selects the register-resident diagonal-block elimination
-    const char* a = getenv("SPR_B200_DIAG");
-    diag_alg_ = (a && a[0] == '0') ? 0 : 1;
 }
 
 cudaGraphExec_t Engine::find_graph(const GraphKey& k) {
@@ -2737,17 +2691,10 @@ static PV make_view(Engine::Dev& D, const Plan& P, double* d_sm, double tol1) {
 void Engine::launch_diag(const Launch& pl, cudaStream_t s, const PV& pv) {
     const Job* jobs = d_->jobs + pl.job_begin;
     const int n = (int)pl.job_count;
-    if (diag_alg_ == 0) {
-        if (pv.fc3 == 2) k_diag<kPivotChol4, 0><<<n, 256, 0, s>>>(jobs, pv);
-        else if (pv.fc3) k_diag<kPivotReplace, 0><<<n, 256, 0, s>>>(jobs, pv);
-        else if (chol_) k_diag<kPivotChol, 0><<<n, 256, 0, s>>>(jobs, pv);
-        else k_diag<kPivotLDL, 0><<<n, 256, 0, s>>>(jobs, pv);
-    } else {
-        if (pv.fc3 == 2) k_diag<kPivotChol4, 1><<<n, 256, 0, s>>>(jobs, pv);
-        else if (pv.fc3) k_diag<kPivotReplace, 1><<<n, 256, 0, s>>>(jobs, pv);
-        else if (chol_) k_diag<kPivotChol, 1><<<n, 256, 0, s>>>(jobs, pv);
-        else k_diag<kPivotLDL, 1><<<n, 256, 0, s>>>(jobs, pv);
-    }
+    if (pv.fc3 == 2) k_diag<kPivotChol4><<<n, 256, 0, s>>>(jobs, pv);
+    else if (pv.fc3) k_diag<kPivotReplace><<<n, 256, 0, s>>>(jobs, pv);
+    else if (chol_) k_diag<kPivotChol><<<n, 256, 0, s>>>(jobs, pv);
+    else k_diag<kPivotLDL><<<n, 256, 0, s>>>(jobs, pv);
 }
 
 void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vector<cudaEvent_t>& gev) {
@@ -2894,6 +2841,7 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         const LevelPlan& lp = P_.levels[L];
         snprintf(lname, sizeof lname, "factor level %zu", L);
         NvtxRange level_range(lname);
+        trace_point(lname);
         if (hooks_) hooks_->before(L, s);
         struct AfterLevel {                      // runs at every exit of this iteration
             const LevelHooks* h;
@@ -3106,11 +3054,13 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     } else {
         enqueue_factor(pv, s, gev);
     }
+    trace_point(graph ? "factor graph launched" : "factor launches enqueued");
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());
     Stats hs;
     CK(cudaMemcpyAsync(&hs, D.st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    trace_point("factor stream synchronised");
     CK(cudaEventElapsedTime(&timing.factor_ms, D.ev0, D.ev1));
     timing.tc_ms = 0.f;
     size_t tp = 0;
@@ -3316,6 +3266,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             });
         for (auto& th : pool) th.join();
     }
+    trace_point("uploads queued, diagonal gathered");
     CK(cudaMemcpyAsync(t.d_diag, t.h_diag, neq * sizeof(double), cudaMemcpyHostToDevice, s));
     StreamHooks hk;
     hk.t = &t;
@@ -3755,7 +3706,7 @@ int dense_factor_with_scratch(double* a, int64_t n, int64_t lda, double tol1, do
     pv.tol1 = tol1;
     for (int64_t stp = 0; stp < nblk; ++stp) {
         const StepJobs& sj = steps[stp];
-        k_diag<kPivotLDL, 1><<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
+        k_diag<kPivotLDL><<<1, 256, 0, s>>>(jobs + sj.panel_begin, pv);
         if (sj.panel_tasks > 0) k_trsm<<<(int)sj.panel_tasks, 128, kTrsmSmem, s>>>(jobs + sj.panel_begin, 1, nullptr, pv);
         if (sj.upd_tasks > 0)
             K_GEMM_SMALL<<<(int)sj.upd_tasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs + sj.upd_begin, sj.upd_jobs, nullptr,

@@ -11,6 +11,13 @@
 
 namespace sprb {
 
+// SPR_B200_TRACE=1: wall-clock milestones on stderr (ms since trace_reset),
+// for locating host time in the entry points.
+bool trace_on();
+void trace_reset();
+void trace_point(const char* what);
+
+
 // Outcome of a factorisation, in the reference's terms (SPRF11/SPRFC1,
 // src/SPR/sprfc1.f:240-283 and :690-708).
 struct FactorResult {
@@ -210,7 +217,6 @@ private:
     bool chol_ = false;                      // factor with SPRF27's pivot rule
     double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
     int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
-    int diag_alg_ = 1;            // k_diag elimination: 1 row pairs in shared memory, 0 register-resident
     std::vector<std::pair<int, cudaEvent_t>> marks_;
     std::vector<size_t> tc_pairs_;        // profile mode: event pairs of the tensor-core launches
     int sm_count_ = 148;
