@@ -175,6 +175,12 @@ struct Engine::Dev {
     int32_t* tri_sync = nullptr;                 // block-ready flags, then one task counter per level
     std::vector<void*> owned;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // page-locked, device-mapped mailbox for the few words the host reads
+    // after each call (the factorisation's Stats, a hash, the solve's
+    // timeout flag): a kernel writes them over the bus, so the read does not
+    // queue on the copy engine behind a streamed factorisation's downloads
+    unsigned long long* mbox = nullptr;         // host address
+    unsigned long long* mbox_dev = nullptr;     // its device address
     unsigned long long* hbuf = nullptr;          // result of k_sm_hash
     // tensor-core (mixed) updates: operand slabs and the TMA map over them
     float* slab = nullptr;
@@ -2469,6 +2475,7 @@ Engine::~Engine() {
     for (cudaEvent_t e : d_->evpool) cudaEventDestroy(e);
     if (d_->side) cudaStreamDestroy(d_->side);
     if (d_->ahead) cudaStreamDestroy(d_->ahead);
+    if (d_->mbox) cudaFreeHost(d_->mbox);
     if (d_->slab) cudaFree(d_->slab);
     if (d_->slab_far) cudaFree(d_->slab_far);
     if (csr_.rowptr) cudaFree(csr_.rowptr);
@@ -2569,6 +2576,8 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
         const char* v = std::getenv("SPR_B200_SOLVE_BLOCKS");
         tri_solve_ = !(v && v[0] == '1');
     }
+    CK(cudaHostAlloc((void**)&D.mbox, 32 * sizeof(unsigned long long), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&D.mbox_dev, D.mbox, 0));
     CK(cudaEventCreate(&D.ev0));
     CK(cudaEventCreate(&D.ev1));
     int smem_max = 0;
@@ -2805,6 +2814,12 @@ struct ExchangeHooks : LevelHooks {
     }
 };
 }  // namespace
+
+// Copies n 8-byte words to the mailbox (one thread per word).
+__global__ void k_mailbox(const unsigned long long* src, int n, unsigned long long* dst) {
+    const int i = threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
 
 void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_t>& gev) {
     Dev& D = *d_;
@@ -3058,8 +3073,12 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());
     Stats hs;
-    CK(cudaMemcpyAsync(&hs, D.st, sizeof(Stats), cudaMemcpyDeviceToHost, s));
+    static_assert(sizeof(Stats) % 8 == 0 && sizeof(Stats) / 8 <= 32, "Stats fits the mailbox");
+    k_mailbox<<<1, 32, 0, s>>>(reinterpret_cast<const unsigned long long*>(D.st), (int)(sizeof(Stats) / 8),
+                               D.mbox_dev);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    std::memcpy(&hs, D.mbox, sizeof(Stats));
     trace_point("factor stream synchronised");
     CK(cudaEventElapsedTime(&timing.factor_ms, D.ev0, D.ev1));
     timing.tc_ms = 0.f;
@@ -3161,8 +3180,10 @@ int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
         k_sm_hash<<<grid, 256, 0, stream_>>>(d_a, n, D.hbuf);
         CK(cudaGetLastError());
     }
-    CK(cudaMemcpyAsync(&hv, D.hbuf, sizeof(hv), cudaMemcpyDeviceToHost, stream_));
+    k_mailbox<<<1, 32, 0, stream_>>>(D.hbuf, 1, D.mbox_dev);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
+    hv = D.mbox[0];
     h = (uint64_t)hv;
     return 0;
 }
@@ -3246,17 +3267,23 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     CK(cudaEventRecord(t.ts, s));
     CK(cudaStreamWaitEvent(cs, t.start, 0));
     // D on the compute stream (the pre-pass writes D of retained supernodes),
-    // LNZ on the copy stream group by group, lowest levels first
-    CK(cudaMemcpyAsync(d_sm, h_sm, neq * sizeof(double), cudaMemcpyHostToDevice, s));
-    for (size_t g = 0; g < t.ranges.size(); ++g) {
+    // LNZ on the copy stream group by group, lowest levels first.  Copies in
+    // one direction share the copy engine in the order they are queued, so
+    // the compute stream's two small uploads (D and the gathered diagonal)
+    // are queued right behind group 0, ahead of the upper groups' gigabytes:
+    // the factorisation then starts as soon as group 0 is up.
+    auto upload_group = [&](size_t g) -> int {
         for (const auto& r : t.ranges[g])
             CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double), cudaMemcpyHostToDevice,
                                cs));
         CK(cudaEventRecord(t.up[g], cs));
         if (g == 0) CK(cudaEventRecord(t.tu, cs));
-    }
+        return 0;
+    };
+    if (upload_group(0) != 0) return -4;
+    CK(cudaMemcpyAsync(d_sm, h_sm, neq * sizeof(double), cudaMemcpyHostToDevice, s));
     // the pre-pass needs every original diagonal before anything is factored
-    // (the zero test of sprfc1.f:465-488): gather them here while LNZ uploads
+    // (the zero test of sprfc1.f:465-488): gather them while group 0 uploads
     {
         const int nt = (int)std::min<int64_t>(8, std::max<int64_t>(1, neq / 65536));
         std::vector<std::thread> pool;
@@ -3266,8 +3293,10 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             });
         for (auto& th : pool) th.join();
     }
-    trace_point("uploads queued, diagonal gathered");
     CK(cudaMemcpyAsync(t.d_diag, t.h_diag, neq * sizeof(double), cudaMemcpyHostToDevice, s));
+    for (size_t g = 1; g < t.ranges.size(); ++g)
+        if (upload_group(g) != 0) return -4;
+    trace_point("uploads queued, diagonal gathered");
     StreamHooks hk;
     hk.t = &t;
     hk.nlev = P_.levels.size();
@@ -3296,8 +3325,10 @@ int Engine::streamed_times(double* out) {
     out[0] = out[1] = out[2] = 0.0;
     if (!xfer_) return 0;
     float a = 0.f, c = 0.f;
-    if (cudaEventElapsedTime(&a, xfer_->ts, xfer_->tu) != cudaSuccess ||
-        cudaEventElapsedTime(&c, xfer_->tf, xfer_->te) != cudaSuccess)
+    // from the call's first copy to the factorisation's first launch, and from
+    // its last launch to the end of the last download
+    if (cudaEventElapsedTime(&a, xfer_->ts, d_->ev0) != cudaSuccess ||
+        cudaEventElapsedTime(&c, d_->ev1, xfer_->te) != cudaSuccess)
         return -4;
     out[0] = a;
     out[1] = timing.factor_ms;
@@ -3565,9 +3596,13 @@ int Engine::solve(const double* d_sm, double* d_b, int64_t ldb, int64_t nrhs, in
     }
     CK(cudaEventRecord(D.ev1, s));
     CK(cudaGetLastError());
-    int tri_timeout = 0;
-    CK(cudaMemcpyAsync(&tri_timeout, &D.st->solve_timeout, sizeof(int), cudaMemcpyDeviceToHost, s));
+    k_mailbox<<<1, 32, 0, s>>>(reinterpret_cast<const unsigned long long*>(D.st), (int)(sizeof(Stats) / 8),
+                               D.mbox_dev);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    Stats hs;
+    std::memcpy(&hs, D.mbox, sizeof(Stats));
+    const int tri_timeout = hs.solve_timeout;
     CK(cudaEventElapsedTime(&timing.solve_ms, D.ev0, D.ev1));
     timing.solve_launches = nl;
     if (tri_timeout) {
