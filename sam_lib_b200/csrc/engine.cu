@@ -2425,12 +2425,17 @@ struct Engine::Transfer {
     int L1 = 0;
     std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges;   // per group: (LNZ offset, doubles)
     std::vector<cudaEvent_t> up, done;                             // per group
+    // the uploads have their own stream: the caller's copy stream then holds
+    // only the downloads, and queueing a group's downloads never waits for
+    // the uploads queued ahead of them to drain
+    cudaStream_t ups = nullptr;
     cudaEvent_t start = nullptr, fin = nullptr;
     cudaEvent_t ts = nullptr, tu = nullptr, tf = nullptr, te = nullptr;   // timing: start, group 0 up, factor end, last download
     std::vector<int64_t> diag_pos;                                 // LNZ offset of each equation's diagonal
     double* h_diag = nullptr;                                      // pinned
     double* d_diag = nullptr;
     ~Transfer() {
+        if (ups) cudaStreamDestroy(ups);
         for (cudaEvent_t e : up) cudaEventDestroy(e);
         for (cudaEvent_t e : done) cudaEventDestroy(e);
         if (start) cudaEventDestroy(start);
@@ -3245,6 +3250,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             CK(cudaEventCreateWithFlags(&t->up[g], cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&t->done[g], cudaEventDisableTiming));
         }
+        CK(cudaStreamCreateWithFlags(&t->ups, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&t->start, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&t->fin, cudaEventDisableTiming));
         CK(cudaEventCreate(&t->ts));
@@ -3262,10 +3268,11 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     cudaStream_t s = stream_;
     double* h_lnz = h_sm + neq;
     double* d_lnz = d_sm + neq;
-    // the copy stream starts after the compute stream's earlier work
+    // the copy streams start after the compute stream's earlier work
     CK(cudaEventRecord(t.start, s));
     CK(cudaEventRecord(t.ts, s));
     CK(cudaStreamWaitEvent(cs, t.start, 0));
+    CK(cudaStreamWaitEvent(t.ups, t.start, 0));
     // D on the compute stream (the pre-pass writes D of retained supernodes),
     // LNZ on the copy stream group by group, lowest levels first.  Copies in
     // one direction share the copy engine in the order they are queued, so
@@ -3275,9 +3282,9 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     auto upload_group = [&](size_t g) -> int {
         for (const auto& r : t.ranges[g])
             CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double), cudaMemcpyHostToDevice,
-                               cs));
-        CK(cudaEventRecord(t.up[g], cs));
-        if (g == 0) CK(cudaEventRecord(t.tu, cs));
+                               t.ups));
+        CK(cudaEventRecord(t.up[g], t.ups));
+        if (g == 0) CK(cudaEventRecord(t.tu, t.ups));
         return 0;
     };
     if (upload_group(0) != 0) return -4;
@@ -3309,6 +3316,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     hooks_ = nullptr;
     streamed_diag_ = nullptr;
     if (rc != 0) {
+        cudaStreamSynchronize(t.ups);
         cudaStreamSynchronize(cs);
         return rc;
     }
