@@ -2431,6 +2431,12 @@ struct Engine::Transfer {
     cudaStream_t ups = nullptr;
     cudaEvent_t start = nullptr, fin = nullptr;
     cudaEvent_t ts = nullptr, tu = nullptr, tf = nullptr, te = nullptr;   // timing: start, group 0 up, factor end, last download
+    // the same ranges cut into chunks of at most kChunk doubles, for the copy
+    // kernel: per group [cbeg[g], cbeg[g + 1]) of (LNZ offset, doubles)
+    static constexpr int64_t kChunk = int64_t(1) << 17;
+    std::vector<int64_t> cbeg;
+    int64_t* d_coff = nullptr;
+    int32_t* d_clen = nullptr;
     std::vector<int64_t> diag_pos;                                 // LNZ offset of each equation's diagonal
     double* h_diag = nullptr;                                      // pinned
     double* d_diag = nullptr;
@@ -2446,6 +2452,8 @@ struct Engine::Transfer {
         if (tf) cudaEventDestroy(tf);
         if (h_diag) cudaFreeHost(h_diag);
         if (d_diag) cudaFree(d_diag);
+        if (d_coff) cudaFree(d_coff);
+        if (d_clen) cudaFree(d_clen);
     }
     int group(int32_t level) const { return level < L1 ? 0 : level - L1 + 1; }
 };
@@ -3193,6 +3201,32 @@ int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
     return 0;
 }
 
+// Copies the chunks [c0, c1) of a level group between host and device
+// memory: dst[o .. o + n) = src[o .. o + n) for each chunk (o, n).  One of
+// the two is page-locked host memory seen through its device address, so
+// the copy crosses the bus as the SMs' loads or stores.  A copy kernel takes
+// a whole group's scattered ranges in one launch: hundreds of queued copy
+// operations make the next kernel launch on any stream wait until they drain.
+__global__ void __launch_bounds__(256) k_copy_chunks(const int64_t* coff, const int32_t* clen, int64_t c0, int64_t c1,
+                                                     const double* __restrict__ src, double* __restrict__ dst) {
+    for (int64_t c = c0 + blockIdx.x; c < c1; c += gridDim.x) {
+        const int64_t o = coff[c];
+        const int n = clen[c];
+        const double* a = src + o;
+        double* b = dst + o;
+        int i = threadIdx.x;
+        for (; i + 3 * 256 < n; i += 4 * 256) {
+            const double v0 = a[i], v1 = a[i + 256], v2 = a[i + 512], v3 = a[i + 768];
+            b[i] = v0;
+            b[i + 256] = v1;
+            b[i + 512] = v2;
+            b[i + 768] = v3;
+        }
+        for (; i < n; i += 256) b[i] = a[i];
+    }
+}
+constexpr int kCopyCtas = 48;
+
 namespace {
 // Waits for each group's upload before its first level; after a group's last
 // level, queues the download of its finished LNZ ranges on the copy stream.
@@ -3201,6 +3235,7 @@ struct StreamHooks : LevelHooks {
     size_t nlev = 0;
     cudaStream_t cs = nullptr;
     double* h_lnz = nullptr;
+    double* h_lnz_dev = nullptr;          // device address of h_lnz (null: copy operations instead of a kernel)
     const double* d_lnz = nullptr;
     void before(size_t L, cudaStream_t s) const override {
         const int g = t->group((int32_t)L);
@@ -3212,6 +3247,13 @@ struct StreamHooks : LevelHooks {
         if (!last_of_group) return;
         cudaEventRecord(t->done[g], s);
         cudaStreamWaitEvent(cs, t->done[g], 0);
+        if (h_lnz_dev) {
+            const int64_t c0 = t->cbeg[g], c1 = t->cbeg[g + 1];
+            if (c1 > c0)
+                k_copy_chunks<<<(int)std::min<int64_t>(kCopyCtas, c1 - c0), 256, 0, cs>>>(t->d_coff, t->d_clen, c0, c1,
+                                                                                       d_lnz, h_lnz_dev);
+            return;
+        }
         for (const auto& r : t->ranges[g])
             cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double), cudaMemcpyDeviceToHost, cs);
     }
@@ -3244,6 +3286,22 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             else
                 rg.emplace_back(off, len);
         }
+        // chunks of at most kChunk doubles, group by group, for the copy kernel
+        t->cbeg.assign(1, 0);
+        std::vector<int64_t> coff;
+        std::vector<int32_t> clen;
+        for (int g = 0; g < ng; ++g) {
+            for (const auto& r : t->ranges[g])
+                for (int64_t o = 0; o < r.second; o += Transfer::kChunk) {
+                    coff.push_back(r.first + o);
+                    clen.push_back((int32_t)std::min<int64_t>(Transfer::kChunk, r.second - o));
+                }
+            t->cbeg.push_back((int64_t)coff.size());
+        }
+        CK(cudaMalloc((void**)&t->d_coff, std::max<size_t>(coff.size(), 1) * sizeof(int64_t)));
+        CK(cudaMalloc((void**)&t->d_clen, std::max<size_t>(clen.size(), 1) * sizeof(int32_t)));
+        CK(cudaMemcpy(t->d_coff, coff.data(), coff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(t->d_clen, clen.data(), clen.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
         t->up.resize(ng);
         t->done.resize(ng);
         for (int g = 0; g < ng; ++g) {
@@ -3268,6 +3326,17 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     cudaStream_t s = stream_;
     double* h_lnz = h_sm + neq;
     double* d_lnz = d_sm + neq;
+    // the device address of the page-locked host SM, if it is mapped (any
+    // page-locked allocation is, with unified addressing): then the copy
+    // kernel moves each level group's ranges in one launch
+    double* h_lnz_dev = nullptr;
+    {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, h_sm) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer)
+            h_lnz_dev = static_cast<double*>(a.devicePointer) + neq;
+        else
+            cudaGetLastError();
+    }
     // the copy streams start after the compute stream's earlier work
     CK(cudaEventRecord(t.start, s));
     CK(cudaEventRecord(t.ts, s));
@@ -3280,9 +3349,17 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     // are queued right behind group 0, ahead of the upper groups' gigabytes:
     // the factorisation then starts as soon as group 0 is up.
     auto upload_group = [&](size_t g) -> int {
-        for (const auto& r : t.ranges[g])
-            CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double), cudaMemcpyHostToDevice,
-                               t.ups));
+        if (h_lnz_dev) {
+            const int64_t c0 = t.cbeg[g], c1 = t.cbeg[g + 1];
+            if (c1 > c0)
+                k_copy_chunks<<<(int)std::min<int64_t>(kCopyCtas, c1 - c0), 256, 0, t.ups>>>(t.d_coff, t.d_clen, c0,
+                                                                                          c1, h_lnz_dev, d_lnz);
+            CK(cudaGetLastError());
+        } else {
+            for (const auto& r : t.ranges[g])
+                CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double),
+                                   cudaMemcpyHostToDevice, t.ups));
+        }
         CK(cudaEventRecord(t.up[g], t.ups));
         if (g == 0) CK(cudaEventRecord(t.tu, t.ups));
         return 0;
@@ -3309,6 +3386,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     hk.nlev = P_.levels.size();
     hk.cs = cs;
     hk.h_lnz = h_lnz;
+    hk.h_lnz_dev = h_lnz_dev;
     hk.d_lnz = d_lnz;
     hooks_ = &hk;
     streamed_diag_ = t.d_diag;
