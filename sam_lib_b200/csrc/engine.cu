@@ -28,6 +28,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 
 #include "engine.h"
@@ -428,6 +430,7 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
     const int npk = F * (F + 1) / 2;
     double* A = sh;
     double* wcol = sh + npk;
+    double* rdk = wcol + F;                   // 1 / d_k of the S pivots
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     // fully-summed columns: the packed trapezoid of LNZ is the front's first SUPSZE entries
     const int supsze = F * S - (S * (S - 1)) / 2;
@@ -484,14 +487,17 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
         if (tid == 0 && near_zero_pivot(P, d, ad)) atomicAdd(&P.st->near_piv, 1ull);
         tmax = fmax(tmax, ad / d);
         const double rd = 1.0 / d;
+        if (tid == 0) rdk[k] = rd;
+        // rows below the S columns stay unscaled until the trailing update
         for (int i = k + 1 + tid; i < F; i += blockDim.x) {
             const double a = A[pk(i, k, F)];
             wcol[i] = a;
-            A[pk(i, k, F)] = a * rd;
+            if (i < S) A[pk(i, k, F)] = a * rd;
         }
         __syncthreads();
         if ((PR == kPivotReplace || PR == kPivotChol4) && tid == 0) A[pk(k, k, F)] = d;   // every thread has read the old pivot
-        for (int j = k + 1 + warp; j < F; j += nwarp) {
+        // rank-1 update of the remaining fully-summed columns (all their rows)
+        for (int j = k + 1 + warp; j < S; j += nwarp) {
             const double ljk = A[pk(j, k, F)];
             double* cj = A + pk(j, j, F) - j;
             // loads of four rows ahead of their stores (shared-memory latency overlaps)
@@ -514,6 +520,56 @@ __global__ void __launch_bounds__(256) k_small_front(const int32_t* nodes, PV P)
             atomicAdd(&P.st->numneg, (unsigned long long)neg);
         }
         return;
+    }
+    if (!ret && S > 0 && S < F) {
+        // The trailing (F-S)^2 block: each thread keeps 4x4 tiles in registers
+        // and applies c -= w_ik (w_jk / d_k) for k = 0 .. S-1 in order, the
+        // same operations in the same order as S rank-1 steps, with one
+        // shared-memory read-modify-write per entry instead of S.
+        const int q = F - S, nt = (q + 3) >> 2;
+        const int ntiles = nt * (nt + 1) / 2;
+        for (int t = tid; t < ntiles; t += blockDim.x) {
+            int bi = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+            while (bi * (bi + 1) / 2 > t) --bi;
+            while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+            const int bj = t - bi * (bi + 1) / 2;
+            const int i0 = S + 4 * bi, j0 = S + 4 * bj;
+            double c[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int i = i0 + a, j = j0 + b;
+                    c[a][b] = (i < F && j <= i) ? A[pk(i, j, F)] : 0.0;
+                }
+            for (int k = 0; k < S; ++k) {
+                const double r = rdk[k];
+                const int base = pk(0, k, F);            // A[base + i] = entry (i, k), i >= k
+                double w[4], l[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) w[a] = (i0 + a < F) ? A[base + i0 + a] : 0.0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) l[b] = ((j0 + b < F) ? A[base + j0 + b] : 0.0) * r;
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) c[a][b] -= w[a] * l[b];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int i = i0 + a, j = j0 + b;
+                    if (i < F && j <= i) A[pk(i, j, F)] = c[a][b];
+                }
+        }
+        __syncthreads();
+        // and now the rows below the S columns to L
+        for (int e = tid; e < S * q; e += blockDim.x) {
+            const int k = e / q, i = S + e % q;
+            A[pk(i, k, F)] *= rdk[k];
+        }
+        __syncthreads();
     }
     // write back the S columns (LNZ layout == packed layout) and the pivots
     double* lnzw = P.lnz + P.lnz_off[js];
@@ -1323,6 +1379,10 @@ __global__ void k_writeback(const Job* jobs, int64_t njobs, const int32_t* tmap,
 // vector are its update vector for the parent.
 // ---------------------------------------------------------------------------
 constexpr int kSolveThreads = 256;
+// threads of a one-CTA-per-front launch (factor or solve) of a size class:
+// the smallest fronts take 128, so that twice as many fronts are in flight
+// per SM (their shared memory allows it)
+inline int small_threads(int maxF) { return maxF <= 64 ? 128 : 256; }
 
 // Small fronts (F <= kSmallMaxF): the front vector and one 32-column block of
 // L live in shared memory; per block, one warp solves the 32x32 triangle and
@@ -2425,18 +2485,10 @@ struct Engine::Transfer {
     int L1 = 0;
     std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges;   // per group: (LNZ offset, doubles)
     std::vector<cudaEvent_t> up, done;                             // per group
-    // the uploads have their own stream: the caller's copy stream then holds
-    // only the downloads, and queueing a group's downloads never waits for
-    // the uploads queued ahead of them to drain
-    cudaStream_t ups = nullptr;
+    cudaStream_t ups = nullptr;                                    // uploads (the caller's copy stream: downloads)
     cudaEvent_t start = nullptr, fin = nullptr;
     cudaEvent_t ts = nullptr, tu = nullptr, tf = nullptr, te = nullptr;   // timing: start, group 0 up, factor end, last download
-    // the same ranges cut into chunks of at most kChunk doubles, for the copy
-    // kernel: per group [cbeg[g], cbeg[g + 1]) of (LNZ offset, doubles)
-    static constexpr int64_t kChunk = int64_t(1) << 17;
-    std::vector<int64_t> cbeg;
-    int64_t* d_coff = nullptr;
-    int32_t* d_clen = nullptr;
+    cudaEvent_t tf0 = nullptr;                                            // timing: factorisation start
     std::vector<int64_t> diag_pos;                                 // LNZ offset of each equation's diagonal
     double* h_diag = nullptr;                                      // pinned
     double* d_diag = nullptr;
@@ -2450,10 +2502,9 @@ struct Engine::Transfer {
         if (tu) cudaEventDestroy(tu);
         if (te) cudaEventDestroy(te);
         if (tf) cudaEventDestroy(tf);
+        if (tf0) cudaEventDestroy(tf0);
         if (h_diag) cudaFreeHost(h_diag);
         if (d_diag) cudaFree(d_diag);
-        if (d_coff) cudaFree(d_coff);
-        if (d_clen) cudaFree(d_clen);
     }
     int group(int32_t level) const { return level < L1 ? 0 : level - L1 + 1; }
 };
@@ -2595,7 +2646,7 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaEventCreate(&D.ev1));
     int smem_max = 0;
     CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + kSmallMaxF) * sizeof(double);
+    const size_t need = ((size_t)kSmallMaxF * (kSmallMaxF + 1) / 2 + 2 * kSmallMaxF) * sizeof(double);
     if ((size_t)smem_max < need) return -4;
     CK(cudaFuncSetAttribute(k_small_front<kPivotLDL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     CK(cudaFuncSetAttribute(k_small_front<kPivotReplace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
@@ -2883,16 +2934,17 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             mark(1);
             for (const LevelPlan::SmallClass& c : lp.small_classes) {
                 const int F = c.maxF;
-                const size_t smem = ((size_t)F * (F + 1) / 2 + F) * sizeof(double);
+                const size_t smem = ((size_t)F * (F + 1) / 2 + 2 * F) * sizeof(double);
+                const int thr = small_threads(F);
                 const int32_t* nodes = D.level_nodes + D.small_begin[L] + c.begin;
                 if (pv.fc3 == 2)
-                    k_small_front<kPivotChol4><<<c.count, 256, smem, s>>>(nodes, pv);
+                    k_small_front<kPivotChol4><<<c.count, thr, smem, s>>>(nodes, pv);
                 else if (pv.fc3)
-                    k_small_front<kPivotReplace><<<c.count, 256, smem, s>>>(nodes, pv);
+                    k_small_front<kPivotReplace><<<c.count, thr, smem, s>>>(nodes, pv);
                 else if (chol_)
-                    k_small_front<kPivotChol><<<c.count, 256, smem, s>>>(nodes, pv);
+                    k_small_front<kPivotChol><<<c.count, thr, smem, s>>>(nodes, pv);
                 else
-                    k_small_front<kPivotLDL><<<c.count, 256, smem, s>>>(nodes, pv);
+                    k_small_front<kPivotLDL><<<c.count, thr, smem, s>>>(nodes, pv);
                 ++timing.launches;
             }
         }
@@ -3201,61 +3253,60 @@ int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
     return 0;
 }
 
-// Copies the chunks [c0, c1) of a level group between host and device
-// memory: dst[o .. o + n) = src[o .. o + n) for each chunk (o, n).  One of
-// the two is page-locked host memory seen through its device address, so
-// the copy crosses the bus as the SMs' loads or stores.  A copy kernel takes
-// a whole group's scattered ranges in one launch: hundreds of queued copy
-// operations make the next kernel launch on any stream wait until they drain.
-__global__ void __launch_bounds__(256) k_copy_chunks(const int64_t* coff, const int32_t* clen, int64_t c0, int64_t c1,
-                                                     const double* __restrict__ src, double* __restrict__ dst) {
-    for (int64_t c = c0 + blockIdx.x; c < c1; c += gridDim.x) {
-        const int64_t o = coff[c];
-        const int n = clen[c];
-        const double* a = src + o;
-        double* b = dst + o;
-        int i = threadIdx.x;
-        for (; i + 3 * 256 < n; i += 4 * 256) {
-            const double v0 = a[i], v1 = a[i + 256], v2 = a[i + 512], v3 = a[i + 768];
-            b[i] = v0;
-            b[i + 256] = v1;
-            b[i + 512] = v2;
-            b[i + 768] = v3;
-        }
-        for (; i < n; i += 256) b[i] = a[i];
-    }
-}
-constexpr int kCopyCtas = 48;
-
 namespace {
-// Waits for each group's upload before its first level; after a group's last
-// level, queues the download of its finished LNZ ranges on the copy stream.
+// Host-side pacing of the streamed copies.  Hundreds of queued copy
+// operations make the next kernel launch wait until they drain, and copies
+// in one direction share the copy engine whatever their stream, so neither
+// all uploads nor all downloads are queued at once: one thread queues a
+// group's uploads once the group two below it is up, another queues a
+// group's downloads once its last level has finished on the device.  The
+// enqueueing thread waits, before a level's first launch, until that level's
+// upload event has been recorded, and marks each group's end event as
+// recorded after its last level.
+struct CopyScheduler {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<char> up_recorded, done_recorded;
+    bool abort = false;
+    int status = 0;
+    void mark(std::vector<char>& v, size_t g) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            v[g] = 1;
+        }
+        cv.notify_all();
+    }
+    bool wait(std::vector<char>& v, size_t g) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return v[g] != 0 || abort; });
+        return v[g] != 0;
+    }
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            abort = true;
+        }
+        cv.notify_all();
+    }
+};
+
 struct StreamHooks : LevelHooks {
     const Engine::Transfer* t = nullptr;
+    CopyScheduler* cs_sched = nullptr;
     size_t nlev = 0;
-    cudaStream_t cs = nullptr;
-    double* h_lnz = nullptr;
-    double* h_lnz_dev = nullptr;          // device address of h_lnz (null: copy operations instead of a kernel)
-    const double* d_lnz = nullptr;
     void before(size_t L, cudaStream_t s) const override {
         const int g = t->group((int32_t)L);
-        if (L == 0 || (g > 0)) cudaStreamWaitEvent(s, t->up[g], 0);
+        if (L == 0 || (g > 0)) {
+            if (!cs_sched->wait(cs_sched->up_recorded, (size_t)g)) return;
+            cudaStreamWaitEvent(s, t->up[g], 0);
+        }
     }
     void after(size_t L, cudaStream_t s) const override {
         const int g = t->group((int32_t)L);
         const bool last_of_group = (L + 1 == nlev) || t->group((int32_t)(L + 1)) != g;
         if (!last_of_group) return;
         cudaEventRecord(t->done[g], s);
-        cudaStreamWaitEvent(cs, t->done[g], 0);
-        if (h_lnz_dev) {
-            const int64_t c0 = t->cbeg[g], c1 = t->cbeg[g + 1];
-            if (c1 > c0)
-                k_copy_chunks<<<(int)std::min<int64_t>(kCopyCtas, c1 - c0), 256, 0, cs>>>(t->d_coff, t->d_clen, c0, c1,
-                                                                                       d_lnz, h_lnz_dev);
-            return;
-        }
-        for (const auto& r : t->ranges[g])
-            cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double), cudaMemcpyDeviceToHost, cs);
+        cs_sched->mark(cs_sched->done_recorded, (size_t)g);
     }
 };
 }  // namespace
@@ -3286,22 +3337,6 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             else
                 rg.emplace_back(off, len);
         }
-        // chunks of at most kChunk doubles, group by group, for the copy kernel
-        t->cbeg.assign(1, 0);
-        std::vector<int64_t> coff;
-        std::vector<int32_t> clen;
-        for (int g = 0; g < ng; ++g) {
-            for (const auto& r : t->ranges[g])
-                for (int64_t o = 0; o < r.second; o += Transfer::kChunk) {
-                    coff.push_back(r.first + o);
-                    clen.push_back((int32_t)std::min<int64_t>(Transfer::kChunk, r.second - o));
-                }
-            t->cbeg.push_back((int64_t)coff.size());
-        }
-        CK(cudaMalloc((void**)&t->d_coff, std::max<size_t>(coff.size(), 1) * sizeof(int64_t)));
-        CK(cudaMalloc((void**)&t->d_clen, std::max<size_t>(clen.size(), 1) * sizeof(int32_t)));
-        CK(cudaMemcpy(t->d_coff, coff.data(), coff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(t->d_clen, clen.data(), clen.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
         t->up.resize(ng);
         t->done.resize(ng);
         for (int g = 0; g < ng; ++g) {
@@ -3315,6 +3350,7 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
         CK(cudaEventCreate(&t->tu));
         CK(cudaEventCreate(&t->te));
         CK(cudaEventCreate(&t->tf));
+        CK(cudaEventCreate(&t->tf0));
         t->diag_pos.resize(neq);
         for (int64_t js = 0; js < P_.nsuper; ++js)
             for (int64_t j = 0; j < P_.S[js]; ++j) t->diag_pos[P_.fst[js] + j] = P_.lnz_off[js] + lnz_col(j, P_.F[js]);
@@ -3323,51 +3359,13 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
         xfer_ = std::move(t);
     }
     Transfer& t = *xfer_;
+    const size_t ng = t.ranges.size();
     cudaStream_t s = stream_;
     double* h_lnz = h_sm + neq;
     double* d_lnz = d_sm + neq;
-    // the device address of the page-locked host SM, if it is mapped (any
-    // page-locked allocation is, with unified addressing): then the copy
-    // kernel moves each level group's ranges in one launch
-    double* h_lnz_dev = nullptr;
-    {
-        cudaPointerAttributes a;
-        if (cudaPointerGetAttributes(&a, h_sm) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer)
-            h_lnz_dev = static_cast<double*>(a.devicePointer) + neq;
-        else
-            cudaGetLastError();
-    }
-    // the copy streams start after the compute stream's earlier work
-    CK(cudaEventRecord(t.start, s));
-    CK(cudaEventRecord(t.ts, s));
-    CK(cudaStreamWaitEvent(cs, t.start, 0));
-    CK(cudaStreamWaitEvent(t.ups, t.start, 0));
-    // D on the compute stream (the pre-pass writes D of retained supernodes),
-    // LNZ on the copy stream group by group, lowest levels first.  Copies in
-    // one direction share the copy engine in the order they are queued, so
-    // the compute stream's two small uploads (D and the gathered diagonal)
-    // are queued right behind group 0, ahead of the upper groups' gigabytes:
-    // the factorisation then starts as soon as group 0 is up.
-    auto upload_group = [&](size_t g) -> int {
-        if (h_lnz_dev) {
-            const int64_t c0 = t.cbeg[g], c1 = t.cbeg[g + 1];
-            if (c1 > c0)
-                k_copy_chunks<<<(int)std::min<int64_t>(kCopyCtas, c1 - c0), 256, 0, t.ups>>>(t.d_coff, t.d_clen, c0,
-                                                                                          c1, h_lnz_dev, d_lnz);
-            CK(cudaGetLastError());
-        } else {
-            for (const auto& r : t.ranges[g])
-                CK(cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double),
-                                   cudaMemcpyHostToDevice, t.ups));
-        }
-        CK(cudaEventRecord(t.up[g], t.ups));
-        if (g == 0) CK(cudaEventRecord(t.tu, t.ups));
-        return 0;
-    };
-    if (upload_group(0) != 0) return -4;
-    CK(cudaMemcpyAsync(d_sm, h_sm, neq * sizeof(double), cudaMemcpyHostToDevice, s));
     // the pre-pass needs every original diagonal before anything is factored
-    // (the zero test of sprfc1.f:465-488): gather them while group 0 uploads
+    // (the zero test of sprfc1.f:465-488): gathered first, so that D and the
+    // diagonals are the first uploads in the copy engine's queue
     {
         const int nt = (int)std::min<int64_t>(8, std::max<int64_t>(1, neq / 65536));
         std::vector<std::thread> pool;
@@ -3377,26 +3375,64 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             });
         for (auto& th : pool) th.join();
     }
+    CK(cudaEventRecord(t.ts, s));
+    // D on the compute stream (the pre-pass writes D of retained supernodes)
+    CK(cudaMemcpyAsync(d_sm, h_sm, neq * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(t.d_diag, t.h_diag, neq * sizeof(double), cudaMemcpyHostToDevice, s));
-    for (size_t g = 1; g < t.ranges.size(); ++g)
-        if (upload_group(g) != 0) return -4;
-    trace_point("uploads queued, diagonal gathered");
+    // the copy streams start after the compute stream's earlier work
+    CK(cudaEventRecord(t.start, s));
+    CK(cudaStreamWaitEvent(cs, t.start, 0));
+    CK(cudaStreamWaitEvent(t.ups, t.start, 0));
+    CopyScheduler sched;
+    sched.up_recorded.assign(ng, 0);
+    sched.done_recorded.assign(ng, 0);
+    std::thread uploader([&]() {
+        for (size_t g = 0; g < ng; ++g) {
+            if (g >= 2 && cudaEventSynchronize(t.up[g - 2]) != cudaSuccess) sched.status = -4;
+            for (const auto& r : t.ranges[g])
+                if (cudaMemcpyAsync(d_lnz + r.first, h_lnz + r.first, r.second * sizeof(double),
+                                    cudaMemcpyHostToDevice, t.ups) != cudaSuccess)
+                    sched.status = -4;
+            if (cudaEventRecord(t.up[g], t.ups) != cudaSuccess) sched.status = -4;
+            if (g == 0) cudaEventRecord(t.tu, t.ups);
+            sched.mark(sched.up_recorded, g);
+        }
+    });
+    std::thread downloader([&]() {
+        for (size_t g = 0; g < ng; ++g) {
+            if (!sched.wait(sched.done_recorded, g)) return;
+            if (cudaEventSynchronize(t.done[g]) != cudaSuccess) sched.status = -4;
+            for (const auto& r : t.ranges[g])
+                if (cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double),
+                                    cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+                    sched.status = -4;
+        }
+    });
+    if (trace_on()) {
+        size_t nu = 0;
+        for (const auto& u : t.ranges) nu += u.size();
+        char b[96];
+        snprintf(b, sizeof b, "diagonal gathered, copy threads started (%zu ranges each way)", nu);
+        trace_point(b);
+    }
     StreamHooks hk;
     hk.t = &t;
+    hk.cs_sched = &sched;
     hk.nlev = P_.levels.size();
-    hk.cs = cs;
-    hk.h_lnz = h_lnz;
-    hk.h_lnz_dev = h_lnz_dev;
-    hk.d_lnz = d_lnz;
     hooks_ = &hk;
     streamed_diag_ = t.d_diag;
+    cudaEventRecord(t.tf0, s);
     const int rc = factor(d_sm, tol1, res, nullptr);
     hooks_ = nullptr;
     streamed_diag_ = nullptr;
-    if (rc != 0) {
+    if (rc != 0) sched.stop();                  // a level that was never enqueued records no end event
+    uploader.join();
+    downloader.join();
+    trace_point("copy threads joined");
+    if (rc != 0 || sched.status != 0) {
         cudaStreamSynchronize(t.ups);
         cudaStreamSynchronize(cs);
-        return rc;
+        return rc != 0 ? rc : -4;
     }
     // D is final only now (and on a zero diagonal it holds the original diagonal)
     CK(cudaEventRecord(t.fin, s));
@@ -3412,9 +3448,9 @@ int Engine::streamed_times(double* out) {
     if (!xfer_) return 0;
     float a = 0.f, c = 0.f;
     // from the call's first copy to the factorisation's first launch, and from
-    // its last launch to the end of the last download
-    if (cudaEventElapsedTime(&a, xfer_->ts, d_->ev0) != cudaSuccess ||
-        cudaEventElapsedTime(&c, d_->ev1, xfer_->te) != cudaSuccess)
+    // its end to the end of the last download
+    if (cudaEventElapsedTime(&a, xfer_->ts, xfer_->tf0) != cudaSuccess ||
+        cudaEventElapsedTime(&c, xfer_->tf, xfer_->te) != cudaSuccess)
         return -4;
     out[0] = a;
     out[1] = timing.factor_ms;
@@ -3508,7 +3544,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 if (!lp.small_nodes.empty()) {
                     mark(0);
                     for (const LevelPlan::SmallClass& c : lp.small_classes) {
-                        k_forward<<<c.count, kSolveThreads, small_solve_smem(c.maxF, nr), s>>>(
+                        k_forward<<<c.count, small_threads(c.maxF), small_solve_smem(c.maxF, nr), s>>>(
                             D.level_nodes + D.small_begin[L] + c.begin, pv, D.vbuf, b, ldb, nr);
                         ++nl;
                     }
@@ -3573,7 +3609,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                 if (!lp.small_nodes.empty()) {
                     mark(5);
                     for (const LevelPlan::SmallClass& c : lp.small_classes) {
-                        k_backward<<<c.count, kSolveThreads, small_solve_smem(c.maxF, nr), s>>>(
+                        k_backward<<<c.count, small_threads(c.maxF), small_solve_smem(c.maxF, nr), s>>>(
                             D.level_nodes + D.small_begin[L] + c.begin, pv, D.vbuf, b, ldb, nr);
                         ++nl;
                     }
