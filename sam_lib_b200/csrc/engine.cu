@@ -1424,14 +1424,15 @@ k_forward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int 
             Ls[i * (kSmallBlk + 1) + c] = (i > c) ? Lb[lnz_col(j0 + c, F) - (j0 + c) + (j0 + i)] : 0.0;
         }
         __syncthreads();
-        if (tid < 32) {                       // triangle of the block (SPRFS5 :600-608)
+        // triangle of the block (SPRFS5 :600-608): a warp per right-hand side,
+        // lane i holding y_i; y_c reaches the lanes below it by a shuffle
+        for (int r = tid >> 5; r < nrhs; r += (int)(blockDim.x >> 5)) {
+            double yi = lane < nb ? wsm[(j0 + lane) * nrhs + r] : 0.0;
             for (int c = 0; c < nb - 1; ++c) {
-                for (int e = lane; e < (nb - c - 1) * nrhs; e += 32) {
-                    const int i = c + 1 + e % (nb - c - 1), r = e / (nb - c - 1);
-                    wsm[(j0 + i) * nrhs + r] -= wsm[(j0 + c) * nrhs + r] * Ls[i * (kSmallBlk + 1) + c];
-                }
-                __syncwarp();
+                const double yc = __shfl_sync(0xffffffffu, yi, c);
+                if (lane > c && lane < nb) yi -= yc * Ls[lane * (kSmallBlk + 1) + c];
             }
+            if (lane < nb) wsm[(j0 + lane) * nrhs + r] = yi;
         }
         __syncthreads();
         for (int e = tid; e < (m - nb) * nrhs; e += blockDim.x) {   // rectangle (SPRFS6)
@@ -1483,15 +1484,15 @@ k_backward(const int32_t* nodes, PV P, double* vbuf, double* b, int64_t ldb, int
             wsm[(j0 + c) * nrhs + r] -= v;
         }
         __syncthreads();
-        if (tid < 32) {                       // triangle of the block, bottom-up
-            for (int c = nb - 2; c >= 0; --c) {
-                if (lane < nrhs) {
-                    double v = 0.0;
-                    for (int i = c + 1; i < nb; ++i) v += Ls[i * (kSmallBlk + 1) + c] * wsm[(j0 + i) * nrhs + lane];
-                    wsm[(j0 + c) * nrhs + lane] -= v;
-                }
-                __syncwarp();
+        // triangle of the block, bottom-up: a warp per right-hand side, lane c
+        // holding x_c; each finished x_i is shuffled to the lanes above it
+        for (int r = tid >> 5; r < nrhs; r += (int)(blockDim.x >> 5)) {
+            double xc = lane < nb ? wsm[(j0 + lane) * nrhs + r] : 0.0;
+            for (int i = nb - 1; i > 0; --i) {
+                const double xi = __shfl_sync(0xffffffffu, xc, i);
+                if (lane < i) xc -= Ls[i * (kSmallBlk + 1) + lane] * xi;
             }
+            if (lane < nb) wsm[(j0 + lane) * nrhs + r] = xc;
         }
     }
     __syncthreads();
