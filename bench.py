@@ -361,7 +361,7 @@ def form_batched(torch, reps=3, cpu_procs=0):
     ds.set_stream(st.cuda_stream)
     ds.build_residual(bs.sm0)
     x = torch.empty_like(bs.b0)
-    out = {}
+    out = {'tile_autotune': ds.autotune_tiles(bs.sm0)}
     ts = []
     for r in range(reps + 1):
         with torch.cuda.stream(st):

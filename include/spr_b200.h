@@ -192,6 +192,13 @@ int spr_b200_phase_ms(void* handle, double* out);
  * quarters of the SMs, out[2] = its factor ms, out[3] = the default's,
  * out[4] = candidates tried. */
 int spr_b200_autotune(void* handle, const double* d_sm_assembled, double* out);
+/* No reference counterpart.  Tile autotuner of the small FP64 Schur updates
+ * (those with fewer than 256 rows): factors a copy of d_sm_assembled with
+ * 64x64 and with 32x32 update tiles and keeps the faster.  out (3 doubles):
+ * the tile chosen, factor ms with 64, factor ms with 32. */
+int spr_b200_autotune_tiles(void* handle, const double* d_sm_assembled, double* out);
+/* Sets that tile explicitly (64 or 32). */
+int spr_b200_set_small_tile(void* handle, int tile);
 /* Mixed mode: out[0] = algorithmic flops of the Schur updates that run on the
  * tensor cores (trailing columns beyond the next super-panel, K = S updates),
  * out[1] = their split + tensor-core time in the last profiled factor (ms). */

@@ -66,6 +66,10 @@ def load(int_kind=8):
         lib.spr_b200_set_exchange.restype = C.c_int
         lib.spr_b200_autotune.argtypes = [vp, vp, vp]
         lib.spr_b200_autotune.restype = C.c_int
+        lib.spr_b200_autotune_tiles.argtypes = [vp, vp, vp]
+        lib.spr_b200_autotune_tiles.restype = C.c_int
+        lib.spr_b200_set_small_tile.argtypes = [vp, C.c_int]
+        lib.spr_b200_set_small_tile.restype = C.c_int
         lib.spr_b200_tc_stats.argtypes = [vp, vp]
         lib.spr_b200_tc_stats.restype = C.c_int
         lib.spr_b200_phase_ms.argtypes = [vp, vp]
@@ -362,6 +366,18 @@ class DeviceSolver:
             raise RuntimeError('spr_b200_autotune failed with %d' % rc)
         return dict(tc_min_flops=out[0], far_sm_quarters=int(out[1]), factor_ms=out[2], default_ms=out[3],
                     candidates=int(out[4]))
+
+    def autotune_tiles(self, d_sm_assembled):
+        """Times the small Schur updates with 64x64 and 32x32 tiles on a copy
+        of the assembled SM and keeps the faster; returns the choice."""
+        out = np.zeros(3)
+        rc = self.lib.spr_b200_autotune_tiles(self.h, C.c_void_p(self._dev(d_sm_assembled)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError('spr_b200_autotune_tiles failed with %d' % rc)
+        return {'small_tile': int(out[0]), 'factor_ms_64': out[1], 'factor_ms_32': out[2]}
+
+    def set_small_tile(self, tile):
+        self.lib.spr_b200_set_small_tile(self.h, int(tile))
 
     def tc_stats(self):
         """Mixed mode: (tensor-core update flops, their time in the last profiled factor, ms)."""

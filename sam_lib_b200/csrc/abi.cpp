@@ -1086,6 +1086,18 @@ int SPR_API(spr_b200_autotune)(void* handle, const double* d_sm_assembled, doubl
     return static_cast<Engine*>(handle)->autotune(d_sm_assembled, out);
 }
 
+// Tile autotuner of the small FP64 Schur updates (see Engine::autotune_tiles):
+// out[0] = tile chosen (64 or 32), out[1] / out[2] = factor ms with each.
+int SPR_API(spr_b200_autotune_tiles)(void* handle, const double* d_sm_assembled, double* out) {
+    return static_cast<Engine*>(handle)->autotune_tiles(d_sm_assembled, out);
+}
+
+// Sets the tile of the small FP64 Schur updates (64 or 32).
+int SPR_API(spr_b200_set_small_tile)(void* handle, int tile) {
+    static_cast<Engine*>(handle)->set_small_tile(tile);
+    return 0;
+}
+
 // Mixed mode: out[0] = algorithmic flops of the updates that ran on tensor
 // cores in the last profiled factorisation (far trailing columns, the next
 // super-panels' K = 256 columns and K = S updates above the tensor-core

@@ -1170,8 +1170,10 @@ k_gemm(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P) {
 #endif
 using GemmBig = gemm::Cfg<kTileBig, SPR_GEMM_BIG_WM, SPR_GEMM_BIG_WN, SPR_GEMM_STAGES>;
 using GemmSmall = gemm::Cfg<kTile, 32, 32, SPR_GEMM_STAGES>;
+using GemmTiny = gemm::Cfg<kTileTiny, 16, 16, SPR_GEMM_STAGES>;
 #define K_GEMM_BIG k_gemm<kTileBig, SPR_GEMM_BIG_WM, SPR_GEMM_BIG_WN, SPR_GEMM_STAGES>
 #define K_GEMM_SMALL k_gemm<kTile, 32, 32, SPR_GEMM_STAGES>
+#define K_GEMM_TINY k_gemm<kTileTiny, 16, 16, SPR_GEMM_STAGES>
 
 // Mixed-precision Schur update: C -= L D L' with 3xTF32 split products on
 // the tensor cores (mma.sync m16n8k8 tf32, FP32 accumulation inside each
@@ -2661,6 +2663,7 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
     CK(cudaFuncSetAttribute(k_inv_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
     CK(cudaFuncSetAttribute(K_GEMM_BIG, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmBig::smem));
     CK(cudaFuncSetAttribute(K_GEMM_SMALL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
+    CK(cudaFuncSetAttribute(K_GEMM_TINY, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmTiny::smem));
     CK(cudaFuncSetAttribute(k_gemm_x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmall::smem));
     CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kSmem));
     return 0;
@@ -2775,12 +2778,17 @@ void Engine::launch_gemm(const Launch& l, cudaStream_t s, const PV& pv, std::vec
     if (l.ntasks <= 0) return;
     if (profile_) gev.push_back(record_event(s));
     const Job* jobs = d_->jobs + l.job_begin;
-    if (mixed_ == 2)
+    if (mixed_ == 2) {
         k_gemm_x3<<<(int)l.ntasks, 128, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
-    else if (l.tile == kTileBig)
+    } else if (l.tile == kTileBig) {
         K_GEMM_BIG<<<(int)l.ntasks, GemmBig::NT, GemmBig::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
-    else
+    } else if (small_tile_ == kTileTiny && l.alt >= 0) {
+        const Launch& a = P_.alt[l.alt];
+        K_GEMM_TINY<<<(int)a.ntasks, GemmTiny::NT, GemmTiny::smem, s>>>(d_->jobs + a.job_begin, a.job_count,
+                                                                       TMAP(a), pv);
+    } else {
         K_GEMM_SMALL<<<(int)l.ntasks, GemmSmall::NT, GemmSmall::smem, s>>>(jobs, l.job_count, TMAP(l), pv);
+    }
     if (profile_) gev.push_back(record_event(s));
     ++timing.launches;
     ++timing.gemm_launches;
@@ -3116,7 +3124,8 @@ int Engine::factor(double* d_sm, double tol1, FactorResult& res, const Singular*
     } restore{&hooks_, saved_hooks};
     const bool graph = use_graphs_ && !profile_ && s != nullptr && !tc_drop_ && wait_ns_ == 2000000000ull && !hooks_;
     if (graph) {
-        const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_, mixed_ | (chol_ ? 16 : 0),
+        const GraphKey key{(const void*)d_sm, nullptr, tol1, far_cap_q_,
+                           mixed_ | (chol_ ? 16 : 0) | (small_tile_ == kTileTiny ? 32 : 0),
                            (int64_t)std::min(tc_min_flops_, 9.0e18), (const void*)pv.dcor, pv.tol4,
                            pv.near_tol};
         cudaGraphExec_t exec = find_graph(key);
@@ -3948,6 +3957,45 @@ int Engine::autotune(const double* d_sm_assembled, double* out) {
     out[2] = best;
     out[3] = def_ms;
     out[4] = tried;
+    return 0;
+}
+
+// Tile shape of the small Schur updates (those with fewer than 4 x 64 rows):
+// each candidate (64 x 64 tiles, 32 x 32 tiles) factors a copy of the
+// assembled SM twice and the faster one is kept.  out[0] = the tile chosen,
+// out[1] / out[2] = factor ms with 64 / 32.
+int Engine::autotune_tiles(const double* d_sm_assembled, double* out) {
+    const int64_t n = P_.neq + P_.nzerol;
+    double* work = nullptr;
+    CK(cudaMalloc((void**)&work, n * sizeof(double)));
+    const int t0 = small_tile_;
+    const int cand[2] = {kTile, kTileTiny};
+    double ms[2] = {0.0, 0.0};
+    int rc = 0;
+    for (int c = 0; c < 2 && rc == 0; ++c) {
+        small_tile_ = cand[c];
+        float best = 1e30f;
+        for (int rep = 0; rep < 2 && rc == 0; ++rep) {
+            if (cudaMemcpyAsync(work, d_sm_assembled, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_) !=
+                cudaSuccess) {
+                rc = -4;
+                break;
+            }
+            FactorResult r;
+            rc = factor(work, 1.0e-12, r);
+            best = std::min(best, timing.factor_ms);
+        }
+        ms[c] = best;
+    }
+    cudaFree(work);
+    if (rc != 0) {
+        small_tile_ = t0;
+        return rc;
+    }
+    small_tile_ = ms[1] < ms[0] ? kTileTiny : kTile;
+    out[0] = small_tile_;
+    out[1] = ms[0];
+    out[2] = ms[1];
     return 0;
 }
 

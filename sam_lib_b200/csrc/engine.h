@@ -112,6 +112,11 @@ public:
     // Mixed mode autotuner (see engine.cu): times candidate engine choices on a
     // copy of the assembled SM and keeps the fastest.  out: 5 doubles.
     int autotune(const double* d_sm_assembled, double* out);
+    // Tile autotuner of the small FP64 Schur updates (64x64 or 32x32 tiles),
+    // timed on a copy of the assembled SM; out: tile, ms with 64, ms with 32.
+    int autotune_tiles(const double* d_sm_assembled, double* out);
+    void set_small_tile(int t) { small_tile_ = (t == kTileTiny) ? kTileTiny : kTile; }
+    int small_tile() const { return small_tile_; }
     // Content hash (smhash.h) of n doubles of device memory, on the engine's stream.
     int hash(const double* d_a, int64_t n, uint64_t& h);
     // Per-supernode negative-pivot counts and failing column of the last factor().
@@ -217,6 +222,7 @@ private:
     bool chol_ = false;                      // factor with SPRF27's pivot rule
     double tc_min_flops_ = 0.0;   // mixed mode: launches below this stay on the FP64 kernel
     int far_cap_q_ = 3;           // side-stream tensor-core launches: quarters of the SMs
+    int small_tile_ = kTile;      // tile of the small FP64 Schur updates (kTile or kTileTiny)
     std::vector<std::pair<int, cudaEvent_t>> marks_;
     std::vector<size_t> tc_pairs_;        // profile mode: event pairs of the tensor-core launches
     int sm_count_ = 148;

@@ -263,6 +263,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         }
     // ---- batched launches of the large path
     P.jobs.clear();
+    P.alt.clear();
     P.rect_off.assign(ns, 0);
     P.rect_entries = 0;
     P.fwd_off.assign(ns, 0);
@@ -331,7 +332,19 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                 }
                 close_launch(l);
                 l.tile = tile;
-                if (l.ntasks > 0) out.push_back(l);
+                if (l.ntasks <= 0) continue;
+                if (pass == 1) {
+                    // the same jobs in kTileTiny tiles, for the tile autotuner
+                    Launch a;
+                    open_launch(a);
+                    for (const Job& j : jl)
+                        if ((j.r_end - j.c0) < 4 * kTileBig) add_job(a, j, tiles_t(j.c0, j.c_end, j.r_end, kTileTiny));
+                    close_launch(a);
+                    a.tile = kTileTiny;
+                    l.alt = (int32_t)P.alt.size();
+                    P.alt.push_back(a);
+                }
+                out.push_back(l);
             }
         };
         // the far and K = S updates for the tensor-core path: slabs of W = L D
@@ -516,6 +529,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
             for (int64_t t = t0; t < t1; ++t) P.task_map.push_back((int32_t)j);
         }
     };
+    for (Launch& l : P.alt) build_map(l);
     for (LevelPlan& lp : P.levels) {
         build_map(lp.assemble);
         build_map(lp.writeback);

@@ -25,6 +25,7 @@ constexpr int kTile = 64;           // Schur-update tile of small updates (rows 
 #define SPR_TILE_BIG 64
 #endif
 constexpr int kTileBig = SPR_TILE_BIG;   // Schur-update tile of large updates
+constexpr int kTileTiny = 32;            // the autotuner's alternative tile for the small updates
 constexpr int kSuperPanel = 256;    // trailing updates are applied per 256 columns (K = 256)
 constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
 
@@ -53,6 +54,7 @@ struct Launch {                      // a contiguous range of Plan::jobs
     int64_t job_begin = 0, job_count = 0, ntasks = 0;
     int32_t tile = kTile;            // Schur-update launches: tile size of the decode
     int64_t map_begin = -1;          // task -> job map of this launch in Plan::task_map
+    int32_t alt = -1;                // a kTile update launch: the same jobs in kTileTiny tiles (Plan::alt)
 };
 
 // A tensor-core Schur-update launch: the split of the panel into FP32 hi/lo
@@ -169,6 +171,7 @@ struct Plan {
     // for every launch: the job (relative to Launch::job_begin) of each task,
     // so a CTA finds its job with one load instead of a binary search
     std::vector<int32_t> task_map;
+    std::vector<Launch> alt;                 // kTileTiny versions of the small-tile update launches
     // statistics (the reference's own counters are recomputed for reporting)
     double factor_flops = 0.0;               // = RINFO(3) formula, src/SPR/sprtrs.f:1961-1969
     double solve_flops = 0.0;                // = RINFO(4) formula, src/SPR/sprtrs.f:1976-1980
