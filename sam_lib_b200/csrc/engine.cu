@@ -731,6 +731,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     __shared__ double dd[kNB];
     __shared__ double adv[kNB];
     __shared__ double Tb[kNB * kNB / 4];    // T = L21 X11 of the inverse's doubling passes
+    __shared__ int s_fail;
     if (P.st->any_fail) return;
     const Job& jb = jobs[blockIdx.x];
     const int js = jb.node, k0 = jb.k_lo, nb = jb.k_hi - jb.k_lo;
@@ -777,11 +778,14 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
         }
         __syncthreads();
         const double d = vec[buf][k];
-        if (PR != kPivotReplace && pivot_fails(PR, d, adv[k], P.tol1)) {
+        // SPRFC4's rule records replacements while it goes, so it stops at a
+        // failing pivot here; the other rules are tested after the loop (the
+        // steps after a failure only compute values that are thrown away)
+        if (PR == kPivotChol4 && pivot_fails(PR, d, adv[k], P.tol1)) {
             failed = k;
             if (tid == 0) {
                 record_fail(P, js, k0 + k, d, adv[k]);
-                if (PR == kPivotChol4) chol4_fail_record(P, fst + k0 + k, d);
+                chol4_fail_record(P, fst + k0 + k, d);
             }
             break;
         }
@@ -796,6 +800,22 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
             for (int b = 0; b < R; ++b)
                 if (ty + 16 * b > k) v[a][b] -= aik * vj[b];
         }
+    }
+    // the first failing pivot (sprfc1.f:1274-1279), for the rules tested here
+    if (PR == kPivotLDL || PR == kPivotChol) {
+        __syncthreads();
+        if (tid < 32) {
+            int f = nb;
+            for (int k = tid; k < nb; k += 32)
+                if (pivot_fails(PR, dd[k], adv[k], P.tol1)) f = min(f, k);
+            for (int o = 16; o > 0; o >>= 1) f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
+            if (tid == 0) {
+                if (f < nb) record_fail(P, js, k0 + f, dd[f], adv[f]);
+                s_fail = f;
+            }
+        }
+        __syncthreads();
+        failed = s_fail < nb ? s_fail : -1;
     }
     // inertia and TOL(2) of the processed columns (sprfc1.f:1280-1290)
     if (tid < 32) {
@@ -835,26 +855,46 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     // X21 = -X22 (L21 X11) (X11, X22 from the pass before; unit diagonals).
     // X is kept transposed in the free upper triangle of A (X[i][j] at A[j][i]),
     // T = L21 X11 in Tb; 12 barriers instead of one per column.
+    // Each thread takes up to kInvQ elements of a pass and runs their sums side
+    // by side (independent chains), each in the same order as one at a time.
+    constexpr int kInvQ = kNB * kNB / 4 / 256;
     for (int b = 1; b < kNB; b <<= 1) {
         const int bb = b * b, tot = (kNB / (2 * b)) * bb;
-        for (int e = tid; e < tot; e += blockDim.x) {
-            const int k = e / bb, r = e - k * bb, i = r / b, j = r - i * b;
-            const int base = 2 * k * b, gi = base + b + i, gj = base + j;
-            double t = 0.0;
-            if (gi < nb) {
-                t = A[gi][gj];                                   // X11[j][j] = 1
-                for (int m = j + 1; m < b; ++m) t += A[gi][base + m] * A[gj][base + m];   // L21[i][m] X11[m][j]
-            }
-            Tb[e] = t;
+        int e_[kInvQ], gi_[kInvQ], gj_[kInvQ], bs_[kInvQ], i_[kInvQ], j_[kInvQ];
+        bool on[kInvQ];
+        double t[kInvQ];
+#pragma unroll
+        for (int q = 0; q < kInvQ; ++q) {
+            const int e = tid + q * (int)blockDim.x;
+            const int kq = e / bb, r = e - kq * bb;
+            e_[q] = e;
+            i_[q] = r / b;
+            j_[q] = r - i_[q] * b;
+            bs_[q] = 2 * kq * b;
+            gi_[q] = bs_[q] + b + i_[q];
+            gj_[q] = bs_[q] + j_[q];
+            on[q] = e < tot && gi_[q] < nb;
+            t[q] = on[q] ? A[gi_[q]][gj_[q]] : 0.0;                // X11[j][j] = 1
         }
+        for (int m = 1; m < b; ++m)
+#pragma unroll
+            for (int q = 0; q < kInvQ; ++q)                            // L21[i][m] X11[m][j], m > j
+                if (on[q] && m > j_[q]) t[q] += A[gi_[q]][bs_[q] + m] * A[gj_[q]][bs_[q] + m];
+#pragma unroll
+        for (int q = 0; q < kInvQ; ++q)
+            if (e_[q] < tot) Tb[e_[q]] = t[q];
         __syncthreads();
-        for (int e = tid; e < tot; e += blockDim.x) {
-            const int k = e / bb, r = e - k * bb, i = r / b, j = r - i * b;
-            const int base = 2 * k * b, gi = base + b + i;
-            double x = Tb[e];                                    // X22[i][i] = 1
-            for (int m = 0; m < i; ++m) x += A[base + b + m][gi] * Tb[k * bb + m * b + j];   // X22[i][m] T[m][j]
-            A[base + j][gi] = -x;
-        }
+        double x[kInvQ];
+#pragma unroll
+        for (int q = 0; q < kInvQ; ++q) x[q] = e_[q] < tot ? Tb[e_[q]] : 0.0;   // X22[i][i] = 1
+        for (int m = 0; m + 1 < b; ++m)
+#pragma unroll
+            for (int q = 0; q < kInvQ; ++q)                            // X22[i][m] T[m][j], m < i
+                if (e_[q] < tot && m < i_[q])
+                    x[q] += A[bs_[q] + b + m][gi_[q]] * Tb[(e_[q] / bb) * bb + m * b + j_[q]];
+#pragma unroll
+        for (int q = 0; q < kInvQ; ++q)
+            if (e_[q] < tot) A[bs_[q] + j_[q]][gi_[q]] = -x[q];
         __syncthreads();
     }
     double* lv = P.linv + P.linv_off[js] + (int64_t)(k0 / kNB) * kNB * kNB;
