@@ -196,6 +196,11 @@ int spr_b200_autotune(void* handle, const double* d_sm_assembled, double* out);
  * (those with fewer than 256 rows): factors a copy of d_sm_assembled with
  * 64x64 and with 32x32 update tiles and keeps the faster.  out (3 doubles):
  * the tile chosen, factor ms with 64, factor ms with 32. */
+/* No reference counterpart.  Self-test of the pivot reciprocal of the
+ * diagonal-block kernels (a hardware approximation refined by two
+ * Newton-Raphson steps): out[2i] = it for x[i], out[2i+1] = the IEEE quotient
+ * 1.0 / x[i], computed on the device (host arrays, n values). */
+int spr_b200_recip_check(const double* x, int64_t n, double* out);
 int spr_b200_autotune_tiles(void* handle, const double* d_sm_assembled, double* out);
 /* Sets that tile explicitly (64 or 32). */
 int spr_b200_set_small_tile(void* handle, int tile);

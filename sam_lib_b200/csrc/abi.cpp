@@ -1086,6 +1086,10 @@ int SPR_API(spr_b200_autotune)(void* handle, const double* d_sm_assembled, doubl
     return static_cast<Engine*>(handle)->autotune(d_sm_assembled, out);
 }
 
+// Self-test of the pivot reciprocal (host arrays): out[2i] = the device's
+// reciprocal of x[i], out[2i+1] = the IEEE quotient 1.0 / x[i].
+int SPR_API(spr_b200_recip_check)(const double* x, int64_t n, double* out) { return sprb::recip_check(x, n, out); }
+
 // Tile autotuner of the small FP64 Schur updates (see Engine::autotune_tiles):
 // out[0] = tile chosen (64 or 32), out[1] / out[2] = factor ms with each.
 int SPR_API(spr_b200_autotune_tiles)(void* handle, const double* d_sm_assembled, double* out) {

@@ -14,6 +14,8 @@ namespace sprb {
 // SPR_B200_TRACE=1: wall-clock milestones on stderr (ms since trace_reset),
 // for locating host time in the entry points.
 bool trace_on();
+// Self-test of the pivot reciprocal: out[2i] = it, out[2i+1] = 1.0 / x[i].
+int recip_check(const double* h_x, int64_t n, double* h_out);
 void trace_reset();
 void trace_point(const char* what);
 
