@@ -776,16 +776,20 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
     for (int k = tid; k < 2 * kNB; k += blockDim.x) vec[k / kNB][k % kNB] = 0.0;
     __syncthreads();
     int failed = -1;
-    for (int k = 0; k < nb; ++k) {
-        const int buf = k & 1, kb = k >> 4;
-        if (ty == (k & 15)) {
+    // columns in groups of 16 (kb static inside a group, so the publishing
+    // threads read their register v[a][kb] directly)
+#pragma unroll
+    for (int kb = 0; kb < R; ++kb) {
+      if (16 * kb >= nb || failed >= 0) break;
+      for (int kk = 0; kk < 16; ++kk) {
+        const int k = 16 * kb + kk;
+        if (k >= nb) break;
+        const int buf = k & 1;
+        if (ty == kk) {
 #pragma unroll
             for (int a = 0; a < R; ++a) {
                 const int i = tx + 16 * a;
-                double c = v[a][0];
-#pragma unroll
-                for (int b = 1; b < R; ++b)
-                    if (b == kb) c = v[a][b];
+                double c = v[a][kb];
                 if (PR == kPivotReplace && i == k) {
                     const double c0 = c;
                     c = fc3_pivot(P, c0, adv[k]);
@@ -824,6 +828,7 @@ __global__ void __launch_bounds__(256) k_diag(const Job* jobs, PV P) {
             for (int b = 0; b < R; ++b)
                 if (ty + 16 * b > k) v[a][b] -= aik * vj[b];
         }
+      }
     }
     // the first failing pivot (sprfc1.f:1274-1279), for the rules tested here
     if (PR == kPivotLDL || PR == kPivotChol) {
