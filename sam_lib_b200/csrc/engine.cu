@@ -29,6 +29,7 @@
 #include <cstring>
 #include <functional>
 #include <condition_variable>
+#include <deque>
 #include <mutex>
 #include <thread>
 
@@ -191,6 +192,7 @@ struct Engine::Dev {
     alignas(64) CUtensorMap slab_map_far;
     cudaStream_t side = nullptr;                 // side stream: trailing updates beyond the next super-panel
     cudaStream_t ahead = nullptr;                // look-ahead stream: in-super-panel columns after the next panel
+    cudaStream_t wbs = nullptr;                  // early writes of final super-panels to LNZ (streamed copies)
     std::vector<cudaEvent_t> evpool;             // fork/join events of one factorisation
 };
 
@@ -2558,6 +2560,20 @@ struct Engine::Transfer {
     std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges;   // per group: (LNZ offset, doubles)
     std::vector<cudaEvent_t> up, done;                             // per group
     cudaStream_t ups = nullptr;                                    // uploads (the caller's copy stream: downloads)
+    // the last level's super-panels come back as they become final: per panel
+    // step, the LNZ ranges of the super-panels ending there and their event
+    int32_t early_level = -1;
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> spranges;
+    std::vector<cudaEvent_t> spev;
+    // per group, the download ranges: the upload ranges without the early
+    // fronts' LNZ
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> dranges;
+    // the early fronts and a device copy of their uploaded LNZ: a front whose
+    // pivot fails later gets its original columns back, in the device LNZ and
+    // on the host, as a factorisation without early writes leaves them
+    std::vector<int32_t> early_nodes;
+    std::vector<std::pair<int64_t, int64_t>> early_ranges;      // LNZ offset, doubles (backup offsets: running sum)
+    double* d_backup = nullptr;
     cudaEvent_t start = nullptr, fin = nullptr;
     cudaEvent_t ts = nullptr, tu = nullptr, tf = nullptr, te = nullptr;   // timing: start, group 0 up, factor end, last download
     cudaEvent_t tf0 = nullptr;                                            // timing: factorisation start
@@ -2566,6 +2582,8 @@ struct Engine::Transfer {
     double* d_diag = nullptr;
     ~Transfer() {
         if (ups) cudaStreamDestroy(ups);
+        for (cudaEvent_t e : spev) cudaEventDestroy(e);
+        if (d_backup) cudaFree(d_backup);
         for (cudaEvent_t e : up) cudaEventDestroy(e);
         for (cudaEvent_t e : done) cudaEventDestroy(e);
         if (start) cudaEventDestroy(start);
@@ -2611,6 +2629,7 @@ Engine::~Engine() {
     for (cudaEvent_t e : d_->evpool) cudaEventDestroy(e);
     if (d_->side) cudaStreamDestroy(d_->side);
     if (d_->ahead) cudaStreamDestroy(d_->ahead);
+    if (d_->wbs) cudaStreamDestroy(d_->wbs);
     if (d_->mbox) cudaFreeHost(d_->mbox);
     if (d_->slab) cudaFree(d_->slab);
     if (d_->slab_far) cudaFree(d_->slab_far);
@@ -2647,9 +2666,17 @@ int Engine::open(const int64_t* mspar, const int64_t* mtrees, const int64_t* msi
             for (size_t st = 0; st < lp.far.size(); ++st) {
                 if (!lp.far[st].empty() || !lp.far_tc[st].empty()) nev += 2;
                 if (!lp.ahead[st].empty()) nev += 2;
+                if (st < lp.wb_sp.size() && lp.wb_sp[st].ntasks > 0) nev += 1;
             }
+        for (const LevelPlan& lp : P_.levels)           // the join after a level's early writes
+            for (const Launch& w : lp.wb_sp)
+                if (w.ntasks > 0) {
+                    nev += 1;
+                    break;
+                }
         CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&D.ahead, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&D.wbs, cudaStreamNonBlocking));
         D.evpool.resize(nev);
         for (cudaEvent_t& e : D.evpool) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
@@ -3028,6 +3055,8 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
         }
         if (lp.large_nodes.empty()) continue;
         const Job* jobs = D.jobs;
+        const bool early = hooks_ && hooks_->early_columns(L);
+        bool wrote_early = false;
         {
             mark(2);
             const Launch& l = lp.assemble;
@@ -3053,6 +3082,19 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 cudaEvent_t e = D.evpool[evi++];
                 cudaEventRecord(e, s);
                 cudaStreamWaitEvent(u, e, 0);
+            }
+            if (early && st < lp.wb_sp.size() && lp.wb_sp[st].ntasks > 0) {
+                // super-panels that end here are final: write them to LNZ beside
+                // the rest of the level, for the caller to copy early
+                const Launch& w = lp.wb_sp[st];
+                cudaEvent_t e = D.evpool[evi++];
+                cudaEventRecord(e, s);
+                cudaStreamWaitEvent(D.wbs, e, 0);
+                k_writeback<<<(int)((w.ntasks * 32 + 255) / 256), 256, 0, D.wbs>>>(jobs + w.job_begin, w.job_count,
+                                                                                 TMAP(w), w.ntasks, pv);
+                ++timing.launches;
+                hooks_->columns_written(L, st, D.wbs);
+                wrote_early = true;
             }
             mark(5);
             // a trailing update's next-super-panel columns were also updated by
@@ -3109,6 +3151,12 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
             timing.tc_flops += lp.outer_flops;
         } else
             for (const Launch& ol : lp.outer) launch_gemm(ol, s, pv, gev);
+        if (wrote_early) {
+            // the level's own write-back rewrites the same values: after the early ones
+            cudaEvent_t e = D.evpool[evi++];
+            cudaEventRecord(e, D.wbs);
+            cudaStreamWaitEvent(s, e, 0);
+        }
         {
             mark(7);
             const Launch& l = lp.writeback;
@@ -3332,6 +3380,12 @@ int Engine::hash(const double* d_a, int64_t n, uint64_t& h) {
     return 0;
 }
 
+// dst[0 .. n) = src[0 .. n) on the device (the early fronts' backup).
+__global__ void k_copy_d(const double* __restrict__ src, double* __restrict__ dst, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 namespace {
 // Host-side pacing of the streamed copies.  Hundreds of queued copy
 // operations make the next kernel launch wait until they drain, and copies
@@ -3343,11 +3397,33 @@ namespace {
 // upload event has been recorded, and marks each group's end event as
 // recorded after its last level.
 struct CopyScheduler {
+    // a download: once ev has completed, copy these LNZ ranges to the host
+    struct Item {
+        cudaEvent_t ev;
+        const std::vector<std::pair<int64_t, int64_t>>* ranges;
+        bool last;
+    };
     std::mutex mu;
     std::condition_variable cv;
-    std::vector<char> up_recorded, done_recorded;
+    std::vector<char> up_recorded;
+    std::deque<Item> downloads;                 // in the order the enqueueing thread recorded them
     bool abort = false;
     int status = 0;
+    void push(const Item& it) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            downloads.push_back(it);
+        }
+        cv.notify_all();
+    }
+    bool pop(Item& it) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return !downloads.empty() || abort; });
+        if (downloads.empty()) return false;
+        it = downloads.front();
+        downloads.pop_front();
+        return true;
+    }
     void mark(std::vector<char>& v, size_t g) {
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -3372,6 +3448,8 @@ struct CopyScheduler {
 struct StreamHooks : LevelHooks {
     const Engine::Transfer* t = nullptr;
     CopyScheduler* cs_sched = nullptr;
+    double* d_lnz = nullptr;
+    int sm_count = 148;
     size_t nlev = 0;
     void before(size_t L, cudaStream_t s) const override {
         const int g = t->group((int32_t)L);
@@ -3379,13 +3457,26 @@ struct StreamHooks : LevelHooks {
             if (!cs_sched->wait(cs_sched->up_recorded, (size_t)g)) return;
             cudaStreamWaitEvent(s, t->up[g], 0);
         }
+        if ((int32_t)L == t->early_level) {
+            // the early fronts' uploaded LNZ, kept in case a pivot of theirs fails
+            int64_t b = 0;
+            for (const auto& r : t->early_ranges) {
+                k_copy_d<<<2 * sm_count, 256, 0, s>>>(d_lnz + r.first, t->d_backup + b, r.second);
+                b += r.second;
+            }
+        }
     }
     void after(size_t L, cudaStream_t s) const override {
         const int g = t->group((int32_t)L);
         const bool last_of_group = (L + 1 == nlev) || t->group((int32_t)(L + 1)) != g;
         if (!last_of_group) return;
         cudaEventRecord(t->done[g], s);
-        cs_sched->mark(cs_sched->done_recorded, (size_t)g);
+        cs_sched->push({t->done[g], &t->dranges[g], (size_t)g + 1 == t->dranges.size()});
+    }
+    bool early_columns(size_t L) const override { return (int32_t)L == t->early_level; }
+    void columns_written(size_t L, size_t st, cudaStream_t ws) const override {
+        cudaEventRecord(t->spev[st], ws);
+        cs_sched->push({t->spev[st], &t->spranges[st], false});
     }
 };
 }  // namespace
@@ -3406,16 +3497,49 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
             t->L1 = L;
         }
         const int ng = 1 + (nlev - t->L1);
+        // the last level's eliminated large fronts: their columns come back
+        // super-panel by super-panel, not with the level's group
+        std::vector<char> early(P_.nsuper, 0);
+        if (nlev > 0) {
+            const LevelPlan& lp = P_.levels[nlev - 1];
+            t->spranges.assign(lp.wb_sp.size(), {});
+            for (size_t st = 0; st < lp.wb_sp.size(); ++st) {
+                const Launch& w = lp.wb_sp[st];
+                for (int64_t j = 0; j < w.job_count; ++j) {
+                    const Job& jb = P_.jobs[w.job_begin + j];
+                    const int64_t f = P_.F[jb.node];
+                    const int64_t a = P_.lnz_off[jb.node] + lnz_col(jb.c0, f);
+                    t->spranges[st].emplace_back(a, lnz_col(jb.c_end, f) - lnz_col(jb.c0, f));
+                    early[jb.node] = 1;
+                    t->early_level = nlev - 1;
+                }
+            }
+            t->spev.resize(lp.wb_sp.size());
+            for (cudaEvent_t& e : t->spev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
         t->ranges.assign(ng, {});
-        for (int64_t js = 0; js < P_.nsuper; ++js) {
-            const int64_t f = P_.F[js], sw = P_.S[js];
-            const int64_t off = P_.lnz_off[js], len = f * sw - sw * (sw - 1) / 2;
-            auto& rg = t->ranges[t->group(P_.level[js])];
+        t->dranges.assign(ng, {});
+        auto append = [](std::vector<std::pair<int64_t, int64_t>>& rg, int64_t off, int64_t len) {
             if (!rg.empty() && rg.back().first + rg.back().second == off)
                 rg.back().second += len;
             else
                 rg.emplace_back(off, len);
+        };
+        int64_t nbackup = 0;
+        for (int64_t js = 0; js < P_.nsuper; ++js) {
+            const int64_t f = P_.F[js], sw = P_.S[js];
+            const int64_t off = P_.lnz_off[js], len = f * sw - sw * (sw - 1) / 2;
+            const int g = t->group(P_.level[js]);
+            append(t->ranges[g], off, len);
+            if (early[js]) {
+                t->early_nodes.push_back((int32_t)js);
+                t->early_ranges.emplace_back(off, len);
+                nbackup += len;
+            } else {
+                append(t->dranges[g], off, len);
+            }
         }
+        if (nbackup > 0) CK(cudaMalloc((void**)&t->d_backup, nbackup * sizeof(double)));
         t->up.resize(ng);
         t->done.resize(ng);
         for (int g = 0; g < ng; ++g) {
@@ -3464,7 +3588,6 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     CK(cudaStreamWaitEvent(t.ups, t.start, 0));
     CopyScheduler sched;
     sched.up_recorded.assign(ng, 0);
-    sched.done_recorded.assign(ng, 0);
     std::thread uploader([&]() {
         for (size_t g = 0; g < ng; ++g) {
             if (g >= 2 && cudaEventSynchronize(t.up[g - 2]) != cudaSuccess) sched.status = -4;
@@ -3478,13 +3601,14 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
         }
     });
     std::thread downloader([&]() {
-        for (size_t g = 0; g < ng; ++g) {
-            if (!sched.wait(sched.done_recorded, g)) return;
-            if (cudaEventSynchronize(t.done[g]) != cudaSuccess) sched.status = -4;
-            for (const auto& r : t.ranges[g])
+        CopyScheduler::Item it;
+        while (sched.pop(it)) {
+            if (cudaEventSynchronize(it.ev) != cudaSuccess) sched.status = -4;
+            for (const auto& r : *it.ranges)
                 if (cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double),
                                     cudaMemcpyDeviceToHost, cs) != cudaSuccess)
                     sched.status = -4;
+            if (it.last) return;
         }
     });
     if (trace_on()) {
@@ -3497,6 +3621,8 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
     StreamHooks hk;
     hk.t = &t;
     hk.cs_sched = &sched;
+    hk.d_lnz = d_lnz;
+    hk.sm_count = std::max(sm_count_, 1);
     hk.nlev = P_.levels.size();
     hooks_ = &hk;
     streamed_diag_ = t.d_diag;
@@ -3512,6 +3638,28 @@ int Engine::factor_streamed(double* h_sm, double* d_sm, double tol1, FactorResul
         cudaStreamSynchronize(t.ups);
         cudaStreamSynchronize(cs);
         return rc != 0 ? rc : -4;
+    }
+    if (res.lierr != 0 && !t.early_nodes.empty()) {
+        // an early front that failed keeps its uploaded columns, on the device
+        // and on the host (its early super-panels are undone)
+        std::vector<int32_t> bad(t.early_nodes.size(), 0);
+        for (size_t i = 0; i < t.early_nodes.size(); ++i)
+            CK(cudaMemcpy(&bad[i], d_->sn_bad + t.early_nodes[i], sizeof(int32_t), cudaMemcpyDeviceToHost));
+        int64_t b = 0;
+        for (size_t i = 0; i < t.early_nodes.size(); ++i) {
+            const auto& r = t.early_ranges[i];
+            if (bad[i]) k_copy_d<<<2 * std::max(sm_count_, 1), 256, 0, s>>>(t.d_backup + b, d_lnz + r.first, r.second);
+            b += r.second;
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(t.fin, s));
+        CK(cudaStreamWaitEvent(cs, t.fin, 0));
+        for (size_t i = 0; i < t.early_nodes.size(); ++i)
+            if (bad[i]) {
+                const auto& r = t.early_ranges[i];
+                CK(cudaMemcpyAsync(h_lnz + r.first, d_lnz + r.first, r.second * sizeof(double),
+                                   cudaMemcpyDeviceToHost, cs));
+            }
     }
     // D is final only now (and on a zero diagonal it holds the original diagonal)
     CK(cudaEventRecord(t.fin, s));

@@ -54,6 +54,10 @@ struct LevelHooks {
     virtual ~LevelHooks() = default;
     virtual void before(size_t level, cudaStream_t s) const = 0;
     virtual void after(size_t level, cudaStream_t s) const = 0;
+    // A level whose super-panels are written to LNZ as soon as they are final
+    // (on a stream of their own); columns_written follows each such write.
+    virtual bool early_columns(size_t level) const { return false; }
+    virtual void columns_written(size_t level, size_t step, cudaStream_t ws) const {}
 };
 
 class Engine {

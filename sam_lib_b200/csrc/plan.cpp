@@ -518,6 +518,20 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
         for (int32_t js : lp.large_nodes)
             add_job(lp.writeback, Job{js, 0, P.S[js], P.F[js], 0, 0, 0}, P.S[js]);
         close_launch(lp.writeback);
+        const int32_t nst = (int32_t)lp.panel.size();
+        lp.wb_sp.assign(nst, Launch());
+        for (int32_t st = 0; st < nst; ++st) {
+            open_launch(lp.wb_sp[st]);
+            for (int32_t js : lp.elim_nodes) {
+                const int32_t s = P.S[js], k0 = st * kNB;
+                if (k0 >= s) continue;
+                const int32_t k1 = std::min(k0 + kNB, s);
+                if (k1 % kSuperPanel != 0 && k1 != s) continue;     // the step does not end a super-panel
+                const int32_t sp0 = (k0 / kSuperPanel) * kSuperPanel;
+                add_job(lp.wb_sp[st], Job{js, sp0, k1, P.F[js], 0, 0, 0}, k1 - sp0);
+            }
+            close_launch(lp.wb_sp[st]);
+        }
     }
     // task -> job maps of every launch
     P.task_map.clear();
@@ -533,6 +547,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
     for (LevelPlan& lp : P.levels) {
         build_map(lp.assemble);
         build_map(lp.writeback);
+        for (Launch& l : lp.wb_sp) build_map(l);
         build_map(lp.rect);
         build_map(lp.rect_rows);
         for (Launch& l : lp.panel) build_map(l);

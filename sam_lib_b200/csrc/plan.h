@@ -91,6 +91,9 @@ struct LevelPlan {
     std::vector<double> next_flops;
     std::vector<Launch> outer;                // update block, K = S (one launch per tile size)
     Launch writeback;                         // S columns -> LNZ
+    // per panel step: the columns of the super-panels that end at that step
+    // (their last panel's TRSM is done), for writing LNZ early
+    std::vector<Launch> wb_sp;
     std::vector<Launch> fsolve;               // forward step: 1 diagonal CTA + row blocks below
     std::vector<Launch> bsolve;               // back step: 1 diagonal CTA + column groups [0, k0)
     // solves in kSolveBlock-wide steps: per step, the diagonal-block launch uses
