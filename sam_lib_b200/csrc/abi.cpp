@@ -1104,7 +1104,7 @@ int SPR_API(spr_b200_set_small_tile)(void* handle, int tile) {
 
 // Mixed mode: out[0] = algorithmic flops of the updates that ran on tensor
 // cores in the last profiled factorisation (far trailing columns, the next
-// super-panels' K = 256 columns and K = S updates above the tensor-core
+// super-panels' columns and K = S updates above the tensor-core
 // threshold), out[1] = their split + tensor-core time (ms).
 int SPR_API(spr_b200_tc_stats)(void* handle, double* out) {
     const Engine* e = static_cast<Engine*>(handle);

@@ -3109,10 +3109,10 @@ void Engine::enqueue_factor(const PV& pv, cudaStream_t s, std::vector<cudaEvent_
                 cudaEventRecord(fork_ahead, s);
             }
             // the updates inside the panel chain (K = 64: the next panel's
-            // columns; K = 256: the next super-panel's columns) are on the
+            // columns; K = kSuperPanel: the next super-panel's columns) are on the
             // critical path.  The K = 64 ones are small: the FP64 kernel's
             // 64x64 tiles start sooner than a split + tensor-core pair, so they
-            // stay FP64 in both modes; in mixed mode the K = 256 one takes the
+            // stay FP64 in both modes; in mixed mode the K = kSuperPanel one takes the
             // tensor cores when large enough.  They are issued first, the
             // look-ahead columns after them.
             if (mixed_ == 1 && !lp.next_tc[st].empty() && lp.next_flops[st] >= tc_min_flops_) {

@@ -406,7 +406,7 @@ int build_plan(const int64_t* mspar, const int64_t* mtrees, const int64_t* msifa
                     if (c1 < sp1) jahead.push_back(Job{js, c1, sp1, f, k0, c0, 0});
                     P.gemm_flops += update_flops(c0, sp1, f, nb);
                 }
-                if (c0 == sp1 && sp1 < s) {                          // trailing, K = 256
+                if (c0 == sp1 && sp1 < s) {                          // trailing, K = kSuperPanel
                     // the next super-panel's columns now; the columns beyond
                     // it on the side stream, overlapping that super-panel
                     const int32_t sp2 = std::min(sp1 + kSuperPanel, s);

@@ -26,7 +26,7 @@ constexpr int kTile = 64;           // Schur-update tile of small updates (rows 
 #endif
 constexpr int kTileBig = SPR_TILE_BIG;   // Schur-update tile of large updates
 constexpr int kTileTiny = 32;            // the autotuner's alternative tile for the small updates
-constexpr int kSuperPanel = 256;    // trailing updates are applied per 256 columns (K = 256)
+constexpr int kSuperPanel = 512;    // trailing updates are applied per 512 columns (K = 512)
 constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front assembly
 
 // A job is one front's share of one batched launch.  Tasks inside a job are
@@ -40,8 +40,9 @@ constexpr int kAsmChunk = 256;      // rows per warp pass in the large-front ass
 //                           over [k_lo, k_hi)
 // Blocked right-looking LDL' of the S fully-summed columns with two levels:
 // 64-wide panels (diagonal block + TRSM) whose updates stay inside their
-// 256-wide super-panel, one K=256 trailing update per super-panel for the
-// remaining fully-summed columns, and one K=S update of the (F-S) block.
+// kSuperPanel-wide super-panel, one K = kSuperPanel trailing update per
+// super-panel for the remaining fully-summed columns, and one K=S update of
+// the (F-S) block.
 struct Job {
     int32_t node;
     int32_t c0, c_end, r_end;
@@ -84,7 +85,7 @@ struct LevelPlan {
     // per panel step inside a super-panel: the update of the columns after the
     // next panel (look-ahead stream, beside the next diagonal block and TRSM)
     std::vector<std::vector<Launch>> ahead;
-    // mixed precision: a super-panel's K = 256 update of the next super-panel's
+    // mixed precision: a super-panel's K = kSuperPanel update of the next super-panel's
     // columns (the update[st] jobs of a step that ends a super-panel) as a
     // split + tensor-core pair, and its algorithmic flops
     std::vector<std::vector<TcLaunch>> next_tc;
