@@ -1971,12 +1971,22 @@ __global__ void k_fwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     const int row = S + (int)(task - jb.task0);
     const int ncc = (S + kRectCols - 1) / kRectCols;
     double* w = vbuf + P.rbase[js] * nrhs;
-    const double* part = pbuf + P.fwd_off[js] * kMaxRHS;
-    for (int r = 0; r < nrhs; ++r) {
-        double v = 0.0;
-        for (int k = 0; k < ncc; ++k) v += part[((int64_t)k * (F - S) + (row - S)) * kMaxRHS + r];
-        w[(int64_t)r * F + row] -= v;
+    const double* part = pbuf + (P.fwd_off[js] + (row - S)) * kMaxRHS;
+    // column tiles in ascending order for every right-hand side; the loads
+    // of several tiles are in flight together
+    double v[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) v[r] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < ncc; ++k) {
+        const double* pk = part + (int64_t)k * (F - S) * kMaxRHS;
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) v[r] += __ldcg(pk + r);
     }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) w[(int64_t)r * F + row] -= v[r];
 }
 
 // back sweep, update rows [S, F): w[c] -= L[S:F, c]' w[S:F].  Phase 1: one
@@ -1986,7 +1996,7 @@ __global__ void k_fwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
 // the partials of each column in a fixed order, so the result is
 // deterministic.
 template <int NR>
-__global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
+__global__ void __launch_bounds__(256, NR <= 4 ? 3 : 2) k_bwd_rect_part(const Job* jobs, int64_t njobs, const int32_t* tmap, PV P,
                                                        const double* vbuf, double* pbuf, int nrhs) {
     __shared__ double ws[kMaxRHS][kRectRows];
     const int64_t task = blockIdx.x;
@@ -2009,8 +2019,9 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
     __syncthreads();
     double* part = pbuf + (P.rect_off[js] + (int64_t)rc * S) * kMaxRHS;
     const int cw = kRectCols / 8;
-    // CG columns at a time per warp (CG x 8 loads in flight per lane)
+    // CG columns at a time per warp (CG x UR loads in flight per lane)
     constexpr int CG = NR <= 4 ? 4 : 2;
+    constexpr int UR = NR <= 4 ? 4 : 2;                // row steps in flight
     for (int a = 0; a < cw; a += CG) {
         const int c0 = cc * kRectCols + warp * cw + a;
         if (c0 >= S) break;
@@ -2027,7 +2038,7 @@ __global__ void __launch_bounds__(256) k_bwd_rect_part(const Job* jobs, int64_t 
         for (int q = 0; q < CG; ++q)
 #pragma unroll
             for (int r = 0; r < NR; ++r) acc[q][r] = 0.0;
-#pragma unroll 2
+#pragma unroll(UR)
         for (int i = lane; i < nr; i += 32) {
             double l[CG];
 #pragma unroll
@@ -2061,12 +2072,21 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     const int c = (int)(task - jb.task0);
     const int nrc = (F - S + kRectRows - 1) / kRectRows;
     double* w = vbuf + P.rbase[js] * nrhs;
-    const double* part = pbuf + P.rect_off[js] * kMaxRHS;
-    for (int r = 0; r < nrhs; ++r) {
-        double v = 0.0;
-        for (int k = 0; k < nrc; ++k) v += part[((int64_t)k * S + c) * kMaxRHS + r];
-        w[(int64_t)r * F + c] -= v;
+    const double* part = pbuf + (P.rect_off[js] + c) * kMaxRHS;
+    // row tiles in ascending order for every right-hand side
+    double v[kMaxRHS];
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r) v[r] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < nrc; ++k) {
+        const double* pk = part + (int64_t)k * S * kMaxRHS;
+#pragma unroll
+        for (int r = 0; r < kMaxRHS; ++r)
+            if (r < nrhs) v[r] += __ldcg(pk + r);
     }
+#pragma unroll
+    for (int r = 0; r < kMaxRHS; ++r)
+        if (r < nrhs) w[(int64_t)r * F + c] -= v[r];
 }
 
 // y_j /= d_j and scatter of the own rows (thread per column)
