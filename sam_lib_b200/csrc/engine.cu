@@ -2060,9 +2060,24 @@ __global__ void __launch_bounds__(256, NR <= 4 ? 3 : 2) k_bwd_rect_part(const Jo
     }
 }
 
+// Each column is summed by a group of kSumLanes lanes: lane g of the group
+// adds the row tiles g, g + kSumLanes, ... in ascending order, and the
+// group's partial sums are added by a fixed butterfly (deterministic), so
+// the few row tiles of a column are loaded together instead of one after
+// another.
+constexpr int kSumLanes = 8;
+__device__ __forceinline__ double group_sum(double v) {
+    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kSumLanes - 1));
+#pragma unroll
+    for (int o = kSumLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, kSumLanes);
+    return v;
+}
+
 __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tmap, int64_t ntasks, PV P, double* vbuf,
                                const double* pbuf, int nrhs) {
-    const int64_t task = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t task = gt / kSumLanes;              // the group's lanes share the task
+    const int g = (int)(gt % kSumLanes);
     if (task >= ntasks) return;
     const Job& jb = job_of(jobs, njobs, tmap, task);
     const int js = jb.node;
@@ -2073,12 +2088,11 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     const int nrc = (F - S + kRectRows - 1) / kRectRows;
     double* w = vbuf + P.rbase[js] * nrhs;
     const double* part = pbuf + (P.rect_off[js] + c) * kMaxRHS;
-    // row tiles in ascending order for every right-hand side
     double v[kMaxRHS];
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r) v[r] = 0.0;
-#pragma unroll 4
-    for (int k = 0; k < nrc; ++k) {
+#pragma unroll 2
+    for (int k = g; k < nrc; k += kSumLanes) {
         const double* pk = part + (int64_t)k * S * kMaxRHS;
 #pragma unroll
         for (int r = 0; r < kMaxRHS; ++r)
@@ -2086,7 +2100,10 @@ __global__ void k_bwd_rect_sum(const Job* jobs, int64_t njobs, const int32_t* tm
     }
 #pragma unroll
     for (int r = 0; r < kMaxRHS; ++r)
-        if (r < nrhs) w[(int64_t)r * F + c] -= v[r];
+        if (r < nrhs) {
+            const double t = group_sum(v[r]);
+            if (g == 0) w[(int64_t)r * F + c] -= t;
+        }
 }
 
 // y_j /= d_j and scatter of the own rows (thread per column)
@@ -3878,7 +3895,7 @@ void Engine::enqueue_solve(const PV& pv, cudaStream_t s, double* d_b, int64_t ld
                         k_bwd_rect_part<kMaxRHS><<<(int)rl.ntasks, 256, 0, s>>>(jobs + rl.job_begin, rl.job_count,
                                                                                 TMAP(rl), pv, D.vbuf, D.pbuf, nr);
                     ++nl;
-                    k_bwd_rect_sum<<<blocks(wb.ntasks), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
+                    k_bwd_rect_sum<<<blocks(wb.ntasks * kSumLanes), 256, 0, s>>>(jobs + wb.job_begin, wb.job_count, TMAP(wb), wb.ntasks, pv,
                                                                       D.vbuf, D.pbuf, nr);
                     ++nl;
                 }
