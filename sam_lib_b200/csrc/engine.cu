@@ -2555,25 +2555,59 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
-// r = b - K x per right-hand side (warp per row); norms[3r..3r+2] = max|r|, max|x|, max|b|
-__global__ void k_residual(const int64_t* rowptr, const int32_t* ci, const double* cv, int64_t neq, const double* b,
-                           const double* x, double* r, int64_t ld, int nrhs, double* norms) {
-    const int lane = threadIdx.x & 31;
-    const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (row >= neq) return;
-    const int64_t p0 = rowptr[row], p1 = rowptr[row + 1];
-    for (int q = 0; q < nrhs; ++q) {
-        const double* xq = x + q * ld;
-        double acc = 0.0;
-        for (int64_t p = p0 + lane; p < p1; p += 32) acc += cv[p] * xq[ci[p]];
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) {
-            const double bi = b[row + q * ld], ri = bi - acc;
-            r[row + q * ld] = ri;
-            atomic_max_nonneg(&norms[3 * q], fabs(ri));
-            atomic_max_nonneg(&norms[3 * q + 1], fabs(xq[row]));
-            atomic_max_nonneg(&norms[3 * q + 2], fabs(bi));
+// r = b - K x for up to NR right-hand sides in one pass over each row (a warp
+// per row, rows taken grid-stride).  Per right-hand side the products of a
+// row are added in the same order as a pass per right-hand side would add
+// them (lane-strided, then the xor tree).  norms[3q..3q+2] = max|r|, max|x|,
+// max|b|: kept per warp in shared memory and reduced per CTA before one
+// atomic each; the maxima compare bit patterns, so a NaN ranks above every
+// number, as in the atomic.
+constexpr int kResThreads = 256;
+__device__ __forceinline__ double max_nonneg(double a, double v) {
+    return __double_as_longlong(v) > __double_as_longlong(a) ? v : a;
+}
+template <int NR>
+__global__ void __launch_bounds__(kResThreads) k_residual(const int64_t* rowptr, const int32_t* ci, const double* cv,
+                                                          int64_t neq, const double* b, const double* x, double* r,
+                                                          int64_t ld, int nrhs, double* norms) {
+    constexpr int kW = kResThreads / 32;
+    __shared__ double red[kW][3 * NR];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int e = 0; e < 3 * NR; ++e) red[warp][e] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * kW;
+    for (int64_t row = (int64_t)blockIdx.x * kW + warp; row < neq; row += stride) {
+        const int64_t p0 = rowptr[row], p1 = rowptr[row + 1];
+        double acc[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) acc[q] = 0.0;
+        for (int64_t p = p0 + lane; p < p1; p += 32) {
+            const double v = cv[p];
+            const int64_t c = ci[p];
+#pragma unroll
+            for (int q = 0; q < NR; ++q)
+                if (q < nrhs) acc[q] += v * x[c + q * ld];
         }
+#pragma unroll
+        for (int q = 0; q < NR; ++q)
+            if (q < nrhs)
+                for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < NR; ++q)
+                if (q < nrhs) {
+                    const double bi = b[row + q * ld], ri = bi - acc[q];
+                    r[row + q * ld] = ri;
+                    red[warp][3 * q] = max_nonneg(red[warp][3 * q], fabs(ri));
+                    red[warp][3 * q + 1] = max_nonneg(red[warp][3 * q + 1], fabs(x[row + q * ld]));
+                    red[warp][3 * q + 2] = max_nonneg(red[warp][3 * q + 2], fabs(bi));
+                }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 * nrhs && threadIdx.x < 3 * NR) {
+        double m = 0.0;
+        for (int w = 0; w < kW; ++w) m = max_nonneg(m, red[w][threadIdx.x]);
+        atomic_max_nonneg(&norms[threadIdx.x], m);
     }
 }
 
@@ -2675,6 +2709,7 @@ Engine::~Engine() {
     if (csr_.cv) cudaFree(csr_.cv);
     if (csr_.rowabs) cudaFree(csr_.rowabs);
     if (rbuf_) cudaFree(rbuf_);
+    if (nbuf_) cudaFree(nbuf_);
     if (guard_copy_) cudaFree(guard_copy_);
     xfer_.reset();
     if (!d_) return;
@@ -4298,16 +4333,33 @@ int Engine::build_residual(const double* d_sm_assembled) {
 int Engine::residual(const double* d_b, const double* d_x, double* d_r, int64_t ld, int64_t nrhs, double* berr) {
     if (!csr_.rowptr) return -2;
     cudaStream_t s = stream_;
-    double* norms = nullptr;
-    CK(cudaMalloc((void**)&norms, 3 * nrhs * sizeof(double)));
+    if (nbuf_cap_ < 3 * nrhs) {
+        if (nbuf_) cudaFree(nbuf_);
+        nbuf_ = nullptr;
+        nbuf_cap_ = 0;
+        CK(cudaMalloc((void**)&nbuf_, 3 * nrhs * sizeof(double)));
+        nbuf_cap_ = 3 * nrhs;
+    }
+    double* norms = nbuf_;
     CK(cudaMemsetAsync(norms, 0, 3 * nrhs * sizeof(double), s));
     const int64_t neq = P_.neq;
-    k_residual<<<(int)((neq * 32 + 255) / 256), 256, 0, s>>>(csr_.rowptr, csr_.ci, csr_.cv, neq, d_b, d_x, d_r, ld,
-                                                            (int)nrhs, norms);
+    constexpr int kW = kResThreads / 32;
+    const int grid =
+        (int)std::max<int64_t>(1, std::min<int64_t>((neq + kW - 1) / kW, 8 * (int64_t)std::max(sm_count_, 1)));
+    for (int64_t q0 = 0; q0 < nrhs; q0 += kMaxRHS) {          // kMaxRHS right-hand sides per pass
+        const int nq = (int)std::min<int64_t>(kMaxRHS, nrhs - q0);
+        const int64_t o = q0 * ld;
+        if (nq <= 4)
+            k_residual<4><<<grid, kResThreads, 0, s>>>(csr_.rowptr, csr_.ci, csr_.cv, neq, d_b + o, d_x + o, d_r + o,
+                                                       ld, nq, norms + 3 * q0);
+        else
+            k_residual<kMaxRHS><<<grid, kResThreads, 0, s>>>(csr_.rowptr, csr_.ci, csr_.cv, neq, d_b + o, d_x + o,
+                                                             d_r + o, ld, nq, norms + 3 * q0);
+    }
+    CK(cudaGetLastError());
     std::vector<double> h(3 * nrhs);
     CK(cudaMemcpyAsync(h.data(), norms, 3 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    cudaFree(norms);
     double worst = 0.0;
     for (int64_t q = 0; q < nrhs; ++q) {
         const double den = csr_.norm_inf * h[3 * q + 1] + h[3 * q + 2];

@@ -245,6 +245,8 @@ private:
     } csr_;
     double* rbuf_ = nullptr;
     int64_t rbuf_cap_ = 0;
+    double* nbuf_ = nullptr;      // the residual's max norms (3 per right-hand side)
+    int64_t nbuf_cap_ = 0;
     void launch_gemm(const Launch& l, cudaStream_t s, const struct PV& pv, std::vector<cudaEvent_t>& gev);
     void launch_diag(const Launch& pl, cudaStream_t s, const struct PV& pv);
     void upload_plan();
