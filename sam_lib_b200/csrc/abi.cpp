@@ -182,7 +182,7 @@ Ctx* get_ctx(I* mspar, I* mtrees, I* msifa, int& err) {
 // routine that computes something else would be ignored silently.  Instead,
 // a non-null routine is run once on a small probe (3x3 / 3x2 operands, the
 // reference's argument conventions) and the call is refused (IERR = -4)
-// unless it reproduces that update.  The verdict is cached per routine.
+// unless it reproduces that update.  The outcome is cached per routine.
 typedef void (*LmvFn)(I*, I*, double*, double*, I*, double*);
 typedef void (*LmmFn)(I*, I*, I*, I*, double*, double*, double*, I*);
 typedef void (*CmvFn)(I*, I*, double*, I*, double*);
