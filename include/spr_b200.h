@@ -230,6 +230,17 @@ int spr_b200_plan_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_I
  * look-ahead joins (> 0 when [5] > 0) [5] look-ahead launches. */
 int spr_b200_schedule_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
                             double* out);
+/* No reference counterpart.  Host-only self-check of the solves' plan (no GPU
+ * needed): each eliminated large front's 64-row triangle blocks are tasks of
+ * its level's dataflow launch, once each and after the block above, with
+ * disjoint ready flags; each front with F > S has one rectangle job and one
+ * forward-rows job of the right sizes, with disjoint partial-sum ranges.
+ * out (5 doubles): [0] rc [1] violations [2] triangle tasks checked [3] and
+ * [4] violations with a planted mistake (two blocks of a front swapped; one
+ * front's forward partials moved onto another's): > 0, or -1 where no front
+ * of the structure admits the mistake. */
+int spr_b200_solve_plan_check(const SPR_INT* mspar, const SPR_INT* mtrees, const SPR_INT* msifa,
+                              double* out);
 /* Host element assembly into LNZ, the SPRADM/SPRAD2 main add
  * (src/SPR/spradm.f:818-859) for systems without constraint equations:
  * SM(NEQ+K) += EM(I,J), J=1..NEDOF, I<=J, elements in order (bit-exact with

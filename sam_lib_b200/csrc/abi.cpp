@@ -1182,6 +1182,28 @@ int SPR_API(spr_b200_schedule_check)(const I* mspar, const I* mtrees, const I* m
     return 0;
 }
 
+// Host-only check of the solves' plan (no GPU needed): out[0] = rc,
+// out[1] = violations of the plan as built, out[2] = triangle tasks checked,
+// out[3] and out[4] = violations reported with a planted mistake (two blocks
+// of a front swapped; one front's forward partials moved onto another's),
+// -1 where the structure has no front the mistake applies to.
+int SPR_API(spr_b200_solve_plan_check)(const I* mspar, const I* mtrees, const I* msifa, double* out) {
+    std::vector<int64_t> ms(60, 0);
+    for (int i = 0; i < 58; ++i) ms[i] = (int64_t)mspar[i];
+    std::vector<int64_t> mt = widen(mtrees, mspar[3]), mf = widen(msifa, mspar[2]);
+    sprb::Plan p;
+    const int rc = sprb::build_plan(ms.data(), mt.data(), mf.data(), p);
+    for (int i = 0; i < 5; ++i) out[i] = 0.0;
+    out[0] = rc;
+    if (rc != 0) return rc;
+    int64_t ntask = 0;
+    out[1] = (double)sprb::check_solve_plan(p, 0, &ntask);
+    out[2] = (double)ntask;
+    out[3] = (double)sprb::check_solve_plan(p, 1);
+    out[4] = (double)sprb::check_solve_plan(p, 2);
+    return 0;
+}
+
 // Host SPRADM restatements; see assemble_host.
 int SPR_API(spr_b200_assemble)(const I* mspar, const I* mtrees, const I* msifa, const I* meqn, const I* madof,
                                const I* mpmnpc, const I* mmnpc, I nel, I nedof, const double* em,

@@ -766,6 +766,146 @@ struct SchedOp {
 bool hb(const SchedOp& a, const SchedOp& b) { return a.vc[a.stream] <= b.vc[a.stream]; }
 }  // namespace
 
+// number of tasks of job j of launch l
+static int64_t job_tasks(const Plan& P, const Launch& l, int64_t j) {
+    const int64_t t0 = P.jobs[l.job_begin + j].task0;
+    const int64_t t1 = (j + 1 < l.job_count) ? P.jobs[l.job_begin + j + 1].task0 : l.ntasks;
+    return t1 - t0;
+}
+
+// disjoint half-open ranges inside [0, cap): the number of ranges that are not
+static int64_t range_faults(std::vector<std::pair<int64_t, int64_t>> iv, int64_t cap) {
+    int64_t bad = 0;
+    for (const auto& r : iv)
+        if (r.first < 0 || r.second > cap) ++bad;
+    std::sort(iv.begin(), iv.end());
+    for (size_t k = 1; k < iv.size(); ++k)
+        if (iv[k].first < iv[k - 1].second) ++bad;
+    return bad;
+}
+
+int64_t check_solve_plan(const Plan& P, int plant, int64_t* tasks) {
+    const int64_t ns = P.nsuper;
+    // the two arrays a planted mistake changes, as copies
+    std::vector<int32_t> tt = P.tri_tasks;
+    std::vector<int64_t> fo = P.fwd_off;
+    if (plant == 1) {                      // swap blocks 0 and 1 of the first front with two blocks
+        bool done = false;
+        for (const LevelPlan& lp : P.levels) {
+            for (int64_t t = lp.tri_begin; t < lp.tri_begin + lp.tri_count && !done; ++t) {
+                if (tt[2 * t + 1] != 0) continue;
+                for (int64_t u = t + 1; u < lp.tri_begin + lp.tri_count; ++u)
+                    if (tt[2 * u] == tt[2 * t] && tt[2 * u + 1] == 1) {
+                        std::swap(tt[2 * t + 1], tt[2 * u + 1]);
+                        done = true;
+                        break;
+                    }
+            }
+            if (done) break;
+        }
+        if (!done) return -1;
+    } else if (plant == 2) {               // one front's forward partials onto another's
+        bool done = false;
+        for (const LevelPlan& lp : P.levels) {
+            int32_t first = -1;
+            for (int32_t js : lp.elim_nodes) {
+                if (P.F[js] <= P.S[js]) continue;
+                if (first < 0) {
+                    first = js;
+                } else {
+                    fo[js] = fo[first];
+                    done = true;
+                    break;
+                }
+            }
+            if (done) break;
+        }
+        if (!done) return -1;
+    } else if (plant != 0) {
+        return -1;
+    }
+    int64_t bad = 0, nt = 0;
+    // ready flags: one per block of each eliminated large front, disjoint
+    {
+        std::vector<std::pair<int64_t, int64_t>> iv;
+        std::vector<uint8_t> elim(ns, 0);
+        for (const LevelPlan& lp : P.levels)
+            for (int32_t js : lp.elim_nodes) elim[js] = 1;
+        for (int64_t js = 0; js < ns; ++js) {
+            if (!elim[js]) continue;
+            if (P.tri_off[js] < 0) {
+                ++bad;
+                continue;
+            }
+            iv.emplace_back(P.tri_off[js], P.tri_off[js] + (P.S[js] + kNB - 1) / kNB);
+        }
+        bad += range_faults(iv, P.tri_flags);
+    }
+    for (const LevelPlan& lp : P.levels) {
+        // triangle tasks: each block once, after the block above it
+        std::vector<int64_t> first(ns, -1);             // first block-position slot of each front
+        std::vector<int64_t> pos;
+        for (int32_t js : lp.elim_nodes) {
+            first[js] = (int64_t)pos.size();
+            pos.resize(pos.size() + (P.S[js] + kNB - 1) / kNB, -1);
+        }
+        if (lp.tri_begin < 0 || 2 * (lp.tri_begin + lp.tri_count) > (int64_t)tt.size()) {
+            ++bad;
+            continue;
+        }
+        for (int64_t t = lp.tri_begin; t < lp.tri_begin + lp.tri_count; ++t) {
+            ++nt;
+            const int32_t js = tt[2 * t], b = tt[2 * t + 1];
+            if (js < 0 || js >= ns || first[js] < 0 || b < 0 || b >= (P.S[js] + kNB - 1) / kNB) {
+                ++bad;
+                continue;
+            }
+            int64_t& at = pos[first[js] + b];
+            if (at >= 0) ++bad;                                          // listed twice
+            at = t;
+            if (b > 0 && pos[first[js] + b - 1] < 0) ++bad;              // before the block above it
+        }
+        for (int64_t v : pos)
+            if (v < 0) ++bad;                                            // a block never listed
+        // rectangles: one job per front with F > S, of the right sizes, with
+        // disjoint partial-sum ranges
+        std::vector<int64_t> nrect(ns, 0), nrows(ns, 0);
+        std::vector<std::pair<int64_t, int64_t>> riv, fiv;
+        for (int64_t j = 0; j < lp.rect.job_count; ++j) {
+            const Job& jb = P.jobs[lp.rect.job_begin + j];
+            const int32_t js = jb.node;
+            if (js < 0 || js >= ns || first[js] < 0) {
+                ++bad;
+                continue;
+            }
+            const int64_t f = P.F[js], s = P.S[js];
+            const int64_t nrc = (f - s + kRectRows - 1) / kRectRows, ncc = (s + kRectCols - 1) / kRectCols;
+            if (f <= s || jb.k_lo != nrc || jb.k_hi != ncc || job_tasks(P, lp.rect, j) != nrc * ncc) ++bad;
+            ++nrect[js];
+            riv.emplace_back(P.rect_off[js], P.rect_off[js] + nrc * s);
+            fiv.emplace_back(fo[js], fo[js] + ncc * (f - s));
+        }
+        for (int64_t j = 0; j < lp.rect_rows.job_count; ++j) {
+            const Job& jb = P.jobs[lp.rect_rows.job_begin + j];
+            const int32_t js = jb.node;
+            if (js < 0 || js >= ns || first[js] < 0) {
+                ++bad;
+                continue;
+            }
+            if (job_tasks(P, lp.rect_rows, j) != (int64_t)P.F[js] - P.S[js]) ++bad;
+            ++nrows[js];
+        }
+        for (int32_t js : lp.elim_nodes) {
+            const int64_t want = P.F[js] > P.S[js] ? 1 : 0;
+            if (nrect[js] != want || nrows[js] != want) ++bad;
+        }
+        bad += range_faults(riv, P.rect_entries);
+        bad += range_faults(fiv, P.fwd_entries);
+    }
+    if (tasks) *tasks = nt;
+    return bad;
+}
+
 int64_t check_schedule(const Plan& P, bool tc, int skip_join) {
     int64_t bad = 0;
     for (const LevelPlan& lp : P.levels) {

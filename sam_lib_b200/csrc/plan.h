@@ -211,5 +211,17 @@ void check_coverage(const Plan& P, int64_t& fp64, int64_t& tc);
 // updates on the tensor-core path; skip_join: the schedule without its
 // side-stream joins (a self-test: must report violations where far launches exist).
 int64_t check_schedule(const Plan& P, bool tc, int skip_join);
+// Self-check of the solves' plan: every eliminated large front of a level has
+// each of its 64-row triangle blocks as one task of that level's dataflow
+// launch, after the task of the block above it (the forward sweep takes them
+// in list order, the back sweep in reverse), with its own ready flag (the
+// fronts' flag ranges disjoint and inside Plan::tri_flags); each front with
+// F > S has one rectangle job and one forward-rows job of the right sizes,
+// and the partial-sum ranges of a level's fronts (rect_off, fwd_off) are
+// disjoint and inside their scratch.  Returns the number of violations.
+// plant: 0 checks P as built; 1 swaps the first two blocks of a front in a
+// copy, 2 moves one front's forward partials onto another's in a copy (a
+// self-test: both must report violations where such fronts exist).
+int64_t check_solve_plan(const Plan& P, int plant, int64_t* tasks = nullptr);
 
 }  // namespace sprb

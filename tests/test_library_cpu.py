@@ -174,3 +174,32 @@ def test_factor_stream_schedule_is_race_free(which):
         assert out[4] > 0, 'the check does not see the missing look-ahead joins'
     if which.startswith('gold'):
         assert out[3] > 0 and out[5] > 0
+
+
+@pytest.mark.parametrize('which', ['box6', 'box12', 'gold24', 'gold48', 'retained8'])
+def test_solve_plan_is_consistent(which):
+    """The solves' plan: every triangle block of every eliminated large front
+    is one task of its level's dataflow launch, listed after the block above
+    it (the forward sweep's dependency order; the back sweep takes the list
+    in reverse), with its own ready flag; rectangle and forward-rows jobs
+    match the fronts, and the partial-sum ranges of a level do not overlap.
+    Two planted mistakes (blocks swapped, partial ranges made to overlap)
+    must be reported (a self-test of the check)."""
+    from sam_lib_b200.system import load_structure
+    if which.startswith('box'):
+        rs, _ = ref_system(int(which[3:]))
+        ms, mt, mf = rs.mspar, rs.mtrees, rs.msifa
+    elif which == 'retained8':
+        rs, _ = ref_system(8, retain=True)
+        ms, mt, mf = rs.mspar.copy(), rs.mtrees, rs.msifa
+        ms[56] = 1
+    else:
+        st = load_structure(int(which[4:]))
+        ms, mt, mf = st['mspar'], st['mtrees'], st['msifa']
+    out = np.zeros(5)
+    rc = spr.load(8).spr_b200_solve_plan_check(spr._ptr(ms), spr._ptr(mt), spr._ptr(mf), spr._ptr(out))
+    assert rc == 0 and out[0] == 0
+    assert out[1] == 0, 'solve plan violations'
+    assert out[3] != 0 and out[4] != 0
+    if which.startswith('gold'):
+        assert out[2] > 0 and out[3] > 0 and out[4] > 0
