@@ -203,3 +203,45 @@ def test_solve_plan_is_consistent(which):
     assert out[3] != 0 and out[4] != 0
     if which.startswith('gold'):
         assert out[2] > 0 and out[3] > 0 and out[4] > 0
+
+
+def test_product_does_not_reach_the_oracle_or_the_tests():
+    """The package imports neither the oracle nor the test tree, and none of
+    its code (docstrings and comments aside) names their files: the checker
+    is never part of the product path."""
+    import ast
+    pkg = os.path.join(ROOT, 'sam_lib_b200')
+    pat = re.compile(r'\boracle\b|refpipe|liboracle|libsprref|\btests?/|conftest')
+    hits = []
+    for d, _, files in os.walk(pkg):
+        if '_build' in d or '__pycache__' in d:
+            continue
+        for f in files:
+            path = os.path.join(d, f)
+            rel = os.path.relpath(path, ROOT)
+            if f.endswith('.py'):
+                tree = ast.parse(open(path, encoding='utf-8').read())
+                docs = set()
+                for node in ast.walk(tree):
+                    if isinstance(node, (ast.Module, ast.FunctionDef, ast.ClassDef, ast.AsyncFunctionDef)):
+                        if node.body and isinstance(node.body[0], ast.Expr) and \
+                                isinstance(node.body[0].value, ast.Constant):
+                            docs.add(id(node.body[0].value))
+                for node in ast.walk(tree):
+                    if isinstance(node, ast.Import):
+                        names = [a.name for a in node.names]
+                    elif isinstance(node, ast.ImportFrom):
+                        names = [node.module or '']
+                    elif isinstance(node, ast.Constant) and isinstance(node.value, str) and id(node) not in docs:
+                        names = [node.value]
+                    else:
+                        continue
+                    for nm in names:
+                        if pat.search(nm) or nm.split('.')[0] in ('oracle', 'tests', 'conftest'):
+                            hits.append('%s:%d: %s' % (rel, node.lineno, nm[:80]))
+            elif f.endswith(('.cu', '.cpp', '.h', '.cuh')):
+                text = re.sub(r'/\*.*?\*/', '', open(path, encoding='utf-8').read(), flags=re.S)
+                for k, line in enumerate(text.splitlines(), 1):
+                    if pat.search(line.split('//')[0]):
+                        hits.append('%s: %s' % (rel, line.strip()))
+    assert not hits, '\n'.join(hits)
